@@ -1,0 +1,114 @@
+"""Orientation conventions of the reference, restated in numpy (host side).
+
+A particle orientation is a *view*: a unit view vector v (the projection
+direction) and an in-plane rotation angle a.  The reference turns it into a
+rotation matrix through a quaternion:
+
+* ``View::quaternion``  bsoft/include/View.h:131-152
+* ``Matrix3(Quaternion)`` bsoft/include/Matrix3.h:30-42 (with ``check``,
+  Matrix3.h:21-29: |d| < 1e-12 -> 0, clamp to [-1, 1])
+* ``View::normalize`` / ``check``  View.h:30-35, 110-116
+* ``angle_set_negPI_to_PI``  bsoft/src/util/utilities.cpp:606-615
+
+The matrix maps the 2-D Fourier pixel (h, k, 0) of a particle image onto the
+3-D frequency R (h, k, 0) of the map (Bimage_reconstruct.cpp:150-158), so its
+third column is the view vector.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+SMALLFLOAT = 1e-30
+TRIGPRECISION = 1e-30
+
+
+def angle_set_negpi_to_pi(angle: float) -> float:
+    if not math.isfinite(angle):
+        return 0.0
+    n = int(angle / math.pi)                       # C++ truncation toward zero
+    rem = int(math.fmod(n, 2))                     # C++ % keeps the sign
+    return angle - (n + rem) * math.pi
+
+
+def normalize_view(view):
+    x, y, z, a = (float(t) for t in view)
+    size = math.sqrt(x * x + y * y + z * z)
+    if size < SMALLFLOAT:
+        x, y, z = 0.0, 0.0, 1.0
+    else:
+        x, y, z = x / size, y / size, z / size
+    x = 0.0 if abs(x) < TRIGPRECISION else x
+    y = 0.0 if abs(y) < TRIGPRECISION else y
+    z = 0.0 if abs(z) < TRIGPRECISION else z
+    a = angle_set_negpi_to_pi(a)
+    if abs(a) < TRIGPRECISION:
+        a = 0.0
+    return x, y, z, a
+
+
+def view_to_quaternion(view):
+    x, y, z, a = normalize_view(view)
+    ang = a / 2.0
+    ca, sa = math.cos(ang), math.sin(ang)
+    z1 = z + 1.0
+    q = [ca, 0.0, 0.0, sa]
+    if z < 1.0 - SMALLFLOAT:
+        if z <= SMALLFLOAT - 1.0:
+            q = [0.0, sa, ca, 0.0]
+        else:
+            f1 = math.sqrt(z1 / 2.0)
+            f2 = math.sqrt(1.0 / (2 * z1))
+            q = [f1 * ca, f2 * (x * sa - y * ca), f2 * (x * ca + y * sa), f1 * sa]
+    return [0.0 if abs(t) < TRIGPRECISION else t for t in q]
+
+
+def quaternion_to_matrix(q) -> np.ndarray:
+    q0, q1, q2, q3 = q
+    d = np.array([
+        [q0*q0 + q1*q1 - q2*q2 - q3*q3, 2*q1*q2 - 2*q0*q3, 2*q1*q3 + 2*q0*q2],
+        [2*q1*q2 + 2*q0*q3, q0*q0 - q1*q1 + q2*q2 - q3*q3, 2*q2*q3 - 2*q0*q1],
+        [2*q1*q3 - 2*q0*q2, 2*q2*q3 + 2*q0*q1, q0*q0 - q1*q1 - q2*q2 + q3*q3],
+    ], dtype=np.float64)
+    d[np.abs(d) < 1e-12] = 0.0
+    return np.clip(d, -1.0, 1.0)
+
+
+def view_to_matrix(view) -> np.ndarray:
+    return quaternion_to_matrix(view_to_quaternion(view))
+
+
+def views_to_matrices(views: np.ndarray) -> np.ndarray:
+    return np.stack([view_to_matrix(v) for v in np.asarray(views, dtype=np.float64)])
+
+
+def random_views(rng: np.random.Generator, n: int) -> np.ndarray:
+    """Views uniform on SO(3): view vector uniform on the sphere and angle
+    uniform on [-pi, pi) (the stabiliser of the view vector is the in-plane
+    rotation, so this is the Haar measure).  Returns (n, 4): x, y, z, angle."""
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    a = rng.uniform(-math.pi, math.pi, size=n)
+    return np.concatenate([v, a[:, None]], axis=1)
+
+
+def matrix_to_view(m: np.ndarray):
+    """Inverse of view_to_matrix for proper rotations: (x, y, z, angle)."""
+    m = np.asarray(m, dtype=np.float64)
+    x, y, z = (float(t) for t in m[:, 2])
+    v = (0.0, 0.0, -1.0) if z <= -1 + 1e-12 else (x, y, z)
+    return (*v, angle_set_negpi_to_pi(_solve_angle(m, v)))
+
+
+def _solve_angle(m, v):
+    r0 = view_to_matrix((*v, 0.0))
+    rz = r0.T @ m
+    return math.atan2(rz[1, 0], rz[0, 0])
+
+
+def angular_distance_deg(ra: np.ndarray, rb: np.ndarray) -> np.ndarray:
+    """Geodesic angle (degrees) between rotation matrices (..., 3, 3)."""
+    t = np.einsum("...ij,...ij->...", ra, rb)
+    c = np.clip((t - 1.0) / 2.0, -1.0, 1.0)
+    return np.degrees(np.arccos(c))

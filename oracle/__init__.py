@@ -1,0 +1,132 @@
+"""ctypes front end of the FP64 CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke``
+and by the CPU-baseline leg of bench.py, and only as the checker.  The
+product path (bsoft_b200) never imports this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+class ReconCfg(C.Structure):
+    _fields_ = [("n", C.c_int), ("ft", C.c_int), ("map", C.c_int), ("map_sampling", C.c_double),
+                ("hi_res", C.c_double), ("interp", C.c_int), ("ctf_action", C.c_int),
+                ("wiener", C.c_double)]
+
+
+class Particle(C.Structure):
+    _fields_ = [("origin", C.c_double * 2), ("bkg_center", C.c_double * 2), ("mat", C.c_double * 9),
+                ("pixel", C.c_double), ("scale", C.c_double), ("weight", C.c_double),
+                ("ctf", C.c_double * 7)]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "restatement"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.orc_insert.argtypes = [C.POINTER(ReconCfg), C.POINTER(C.c_float), C.POINTER(Particle), C.c_long,
+                                 dp, dp, dp, dp]
+        L.orc_insert.restype = C.c_int
+        L.orc_particle_transform.argtypes = [C.POINTER(ReconCfg), C.POINTER(C.c_float), C.POINTER(Particle), dp]
+        L.orc_particle_transform.restype = C.c_int
+        L.orc_finish.argtypes = [C.POINTER(ReconCfg), dp, dp, dp, dp, dp, C.c_int]
+        L.orc_finish.restype = C.c_long
+        L.orc_fsc.argtypes = [C.c_int, dp, dp, C.c_int, dp]
+        L.orc_central_section.argtypes = [C.c_int, dp, dp, C.c_double, dp]
+        L.orc_frc_score.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp]
+        L.orc_frc_score.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def cfg_from_plan(plan) -> ReconCfg:
+    return ReconCfg(plan.n, plan.ft, plan.map, plan.map_sampling, plan.hi_res, plan.interp,
+                    plan.ctf_action, plan.wiener)
+
+
+def particles_from_params(params: np.ndarray):
+    from bsoft_b200.plan import P_ORIGIN, P_BKG, P_MAT, P_PIXEL, P_SCALE, P_WEIGHT, P_CTF
+    arr = (Particle * len(params))()
+    for i, r in enumerate(params):
+        p = arr[i]
+        p.origin[:] = list(r[P_ORIGIN:P_ORIGIN + 2])
+        p.bkg_center[:] = list(r[P_BKG:P_BKG + 2])
+        p.mat[:] = list(r[P_MAT:P_MAT + 9])
+        p.pixel, p.scale, p.weight = r[P_PIXEL], r[P_SCALE], r[P_WEIGHT]
+        p.ctf[:] = list(r[P_CTF:P_CTF + 7])
+    return arr
+
+
+def insert(plan, images: np.ndarray, params: np.ndarray, vol=None, weight=None, power=None, weight2=None,
+           aux=False):
+    N3 = plan.map ** 3
+    if vol is None:
+        vol = np.zeros(2 * N3)
+        weight = np.zeros(N3)
+        if aux:
+            power = np.zeros(N3)
+            weight2 = np.zeros(N3)
+    imgs = np.ascontiguousarray(images, dtype=np.float32)
+    cfg = cfg_from_plan(plan)
+    parts = particles_from_params(params)
+    rc = lib().orc_insert(C.byref(cfg), imgs.ctypes.data_as(C.POINTER(C.c_float)), parts, len(params),
+                          _dp(vol), _dp(weight), _dp(power), _dp(weight2))
+    if rc:
+        raise RuntimeError(f"orc_insert failed: {rc}")
+    return vol, weight, power, weight2
+
+
+def finish(plan, vol, weight, power=None, weight2=None, sinc=None):
+    if sinc is None:
+        sinc = plan.interp == 2
+    out = np.zeros(plan.map ** 3)
+    cfg = cfg_from_plan(plan)
+    cov = lib().orc_finish(C.byref(cfg), _dp(vol), _dp(weight), _dp(power), _dp(weight2), _dp(out), int(sinc))
+    return out.reshape(plan.map, plan.map, plan.map), cov
+
+
+def reconstruct(plan, images: np.ndarray, sel=None):
+    """Full-map FP64 reconstruction of the selected particles (all by default)."""
+    params = plan.params if sel is None else plan.params[sel]
+    imgs = images if sel is None else images[sel]
+    vol, w, _, _ = insert(plan, imgs, params)
+    m, _ = finish(plan, vol, w)
+    return m
+
+
+def particle_transform(plan, image: np.ndarray, params_row: np.ndarray) -> np.ndarray:
+    out = np.zeros(2 * plan.ft * plan.ft)
+    cfg = cfg_from_plan(plan)
+    parts = particles_from_params(params_row[None])
+    img = np.ascontiguousarray(image, dtype=np.float32)
+    rc = lib().orc_particle_transform(C.byref(cfg), img.ctypes.data_as(C.POINTER(C.c_float)), parts, _dp(out))
+    if rc:
+        raise RuntimeError(f"orc_particle_transform failed: {rc}")
+    return out.view(np.complex128).reshape(plan.ft, plan.ft)
+
+
+def ref_binary(name: str) -> str:
+    return os.path.join(REF_DIR, name)

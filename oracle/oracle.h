@@ -1,0 +1,77 @@
+/*
+ * oracle.h - FP64 CPU restatement of the reference's single-particle
+ * reconstruction and projection-matching path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this; it
+ * is the checker that the CUDA path is compared against (tests/, the smoke
+ * check and the CPU-baseline leg of bench.py).  Every function cites the
+ * reference lines it restates.  The restatement itself is pinned against
+ * the reference's own programs compiled from source (oracle/_ref) through
+ * the fixtures under tests/golden/.
+ */
+#ifndef BSOFT_ORACLE_H
+#define BSOFT_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Reconstruction geometry shared by all particles of a run. */
+typedef struct {
+    int    n;            /* particle box edge (images are n x n)            */
+    int    ft;           /* padded transform edge (part_ft_size)            */
+    int    map;          /* map edge N                                      */
+    double map_sampling; /* angstrom / voxel of the map                     */
+    double hi_res;       /* resolution limit after Bimage::check_resolution */
+    int    interp;       /* 0 nearest, 1 weighted nearest, 2 trilinear      */
+    int    ctf_action;   /* 0 none, 1 flip, 2 apply, >=3 Wiener-type        */
+    double wiener;       /* Wiener factor (0 -> plain multiply unless flip)  */
+} orc_recon_cfg;
+
+/* Per-particle parameters (host-prepared, see bsoft_b200/recon.py). */
+typedef struct {
+    double origin[2];     /* particle origin, pixels                         */
+    double bkg_center[2]; /* centre of the background circle (file origin)   */
+    double mat[9];        /* view rotation matrix, row-major                 */
+    double pixel;         /* particle pixel size, angstrom                   */
+    double scale;         /* 1/magnification (1 if none)                     */
+    double weight;        /* particle weight (1, or selection for bootstrap) */
+    double ctf[7];        /* abw00 abw20 abw22 abw2m2 abw40 abw11 abw1m1     */
+} orc_particle;
+
+/* Accumulate particles into FP64 volumes: vol (2*N^3, complex), weight
+ * (N^3); power and weight2 (N^3) may be NULL.  Returns 0 or <0 on error. */
+int orc_insert(const orc_recon_cfg* cfg, const float* images, const orc_particle* parts,
+               long nparts, double* vol, double* weight, double* power, double* weight2);
+
+/* One particle's transform after pad, FFT, origin shift and CTF:
+ * out = ft*ft complex doubles.  Used to check the 2-D stage on its own. */
+int orc_particle_transform(const orc_recon_cfg* cfg, const float* image,
+                           const orc_particle* part, double* out);
+
+/* Weigh, shift to centre, inverse 3-D FFT (1/sqrt(N^3)), real part and, when
+ * sinc != 0, the trilinear sinc compensation.  vol/weight are modified in
+ * place; map_out receives N^3 floats.  Returns coverage (voxels weighed). */
+long orc_finish(const orc_recon_cfg* cfg, double* vol, double* weight, double* power,
+                double* weight2, double* map_out, int sinc);
+
+/* Half-map FSC over radial shells (Bimage::fsc): nshell values. */
+int orc_fsc(int N, const double* vol1, const double* vol2, int nshell, double* fsc);
+
+/* ---- projection matching (match_oracle.c) ---- */
+
+/* Central section of a complex N^3 map (standard FFT layout, origin at 0)
+ * by trilinear interpolation: out = N*N complex doubles. */
+int orc_central_section(int N, const double* vol, const double* mat, double max_rad,
+                        double* out);
+
+/* Shell-weighted Fourier ring correlation score between an image transform
+ * and a reference section with the reference's per-shell normalisation. */
+double orc_frc_score(int N, const double* img, const double* ref, int rmin, int rmax,
+                     const double* ctf2d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
