@@ -1,0 +1,74 @@
+"""ctypes binding of libbsgpu.so (the C ABI in include/bsgpu.h).
+
+The library is built in-tree (bsoft_b200/_build/libbsgpu.so) by
+``bsoft_b200.build.build()``.  There is no CPU fallback: if the library or a
+usable sm_100 device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libbsgpu.so")
+
+BSG_DEVICE_PTR = 1
+BSG_SINC = 2
+PARTICLE_DOUBLES = 32
+
+
+class ReconConfig(C.Structure):
+    _fields_ = [("n", C.c_int), ("ft", C.c_int), ("map", C.c_int), ("map_sampling", C.c_double),
+                ("hi_res", C.c_double), ("interp", C.c_int), ("ctf_action", C.c_int), ("wiener", C.c_double),
+                ("nmaps", C.c_int), ("fom", C.c_int), ("batch", C.c_int), ("device", C.c_int)]
+
+
+class ReconStats(C.Structure):
+    _fields_ = [("launches", C.c_long), ("insert_launches", C.c_long), ("insert_ms", C.c_double),
+                ("fft2d_ms", C.c_double), ("h2d_ms", C.c_double), ("particles", C.c_long)]
+
+
+class BsgError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load():
+    """Load libbsgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise BsgError(f"{LIB_PATH} is missing: run bsoft_b200.build.build() (nvcc, sm_100a)")
+    L = C.CDLL(LIB_PATH)
+    vp, fp, dp = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double)
+    sig = {
+        "bsg_recon_create": ([C.POINTER(ReconConfig), C.POINTER(vp)], C.c_int),
+        "bsg_recon_destroy": ([vp], None),
+        "bsg_recon_insert": ([vp, vp, vp, C.c_long, C.c_int], C.c_int),
+        "bsg_recon_finish": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
+        "bsg_recon_accumulators": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
+        "bsg_recon_fsc": ([vp, C.c_int, dp], C.c_int),
+        "bsg_particle_spectra": ([vp, vp, vp, C.c_long, vp, C.c_int], C.c_int),
+        "bsg_recon_set_timing": ([vp, C.c_int], C.c_int),
+        "bsg_recon_get_stats": ([vp, C.POINTER(ReconStats)], C.c_int),
+        "bsg_recon_reset": ([vp], C.c_int),
+        "bsg_recon_synchronize": ([vp], C.c_int),
+        "bsg_recon_stream": ([vp], vp),
+        "bsg_last_error": ([], C.c_char_p),
+        "bsg_version": ([], C.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().bsg_last_error().decode(errors="replace")
+        raise BsgError(f"{what} failed ({rc}): {msg}")

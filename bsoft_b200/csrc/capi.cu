@@ -1,0 +1,457 @@
+// capi.cu - the extern "C" boundary of libbsgpu.so (declared in
+// include/bsgpu.h): context lifetime, device memory, the batched insertion
+// pipeline (image upload, 2-D stage, gridding) and map finishing.
+#include "context.cuh"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+namespace bsg {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+cudaError_t prepare_fft2d_attributes();
+cudaError_t prepare_finish_attributes();
+cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s);
+cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool sinc, cudaStream_t s);
+
+struct Timed {
+    cudaEvent_t a, b;
+    int kind;   // 0 insert, 1 fft2d, 2 h2d
+};
+
+struct Recon : Context {
+    cudaStream_t copy_stream = nullptr;
+    float* d_imgbuf[2] = {nullptr, nullptr};
+    DevParticle* h_partbuf[2] = {nullptr, nullptr};
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
+    cudaEvent_t compute_done[2] = {nullptr, nullptr};
+    std::vector<Timed> timed;
+    bool broken = false;
+};
+
+static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+
+static int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(BSG_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+static void host_twiddles(int L, std::vector<float2>& out) {
+    out.resize(std::max(1, L / 2));
+    for (int j = 0; j < L / 2; ++j) {
+        double a = -2.0 * M_PI * j / L;
+        out[j] = make_float2((float)cos(a), (float)sin(a));
+    }
+    if (L / 2 == 0) out[0] = make_float2(1.f, 0.f);
+}
+
+// 32-double C-ABI record -> device record (see bsgpu.h for the layout)
+static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
+    const Geometry& g = r.g;
+    memset(&d, 0, sizeof(d));
+    d.shx = q[0] / g.ft * 2.0 * M_PI;                 // Bimage_complex.cpp:510 shift = origin/size*2pi
+    d.shy = q[1] / g.ft * 2.0 * M_PI;
+    d.bx = q[2];
+    d.by = q[3];
+    const double* R = q + 4;
+    const double pixel = q[13], scale = q[14] > 0 ? q[14] : 1.0;
+    d.fs = 1.0 / (g.ft * pixel);                       // mg_ctf.cpp:84 freq_scale = 1/real_size
+    d.c00 = q[16]; d.c20 = q[17]; d.c22 = q[18]; d.c2m2 = q[19]; d.c40 = q[20]; d.c11 = q[21]; d.c1m1 = q[22];
+    const double inv = scale / (g.ft * pixel);         // Bimage_reconstruct.cpp:145 invscale
+    for (int i = 0; i < 3; ++i) {
+        d.ad[i] = R[3 * i + 0] * inv * g.mscale;
+        d.bd[i] = R[3 * i + 1] * inv * g.mscale;
+        d.af[i] = (float)d.ad[i];
+        d.bf[i] = (float)d.bd[i];
+    }
+    double nn = sqrt(R[2] * R[2] + R[5] * R[5] + R[8] * R[8]);
+    if (nn <= 0) nn = 1;
+    d.nrm[0] = R[2] / nn; d.nrm[1] = R[5] / nn; d.nrm[2] = R[8] / nn;
+    d.slab = (float)(fabs(d.nrm[0]) + fabs(d.nrm[1]) + fabs(d.nrm[2]));
+    d.step = (float)(inv * g.mscale);
+    d.inv2 = inv * inv;
+    double pw = q[15];
+    double pad_ratio = (double)g.ft / (double)g.n;     // mg_reconstruct.cpp:192-199
+    if (pad_ratio > 1) { pad_ratio *= pad_ratio * 0.6; pw /= pad_ratio; }
+    d.pw = (float)pw;
+    d.half = (int)q[23];
+}
+
+static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
+    const double hf = r.g.ft / 2.0;
+    for (long i = 0; i < np; ++i) {
+        const double s2max = 2.0 * hf * hf * parts[i].inv2;
+        if (s2max > r.g.maxs2) return true;
+        if ((r.g.maxs2 - s2max) * r.g.mscale < 1.0) return true;
+        if (r.g.mins2 > 0) return true;
+    }
+    return false;
+}
+
+static int alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return fail(BSG_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    return BSG_OK;
+}
+
+static void free_all(Recon* r) {
+    auto F = [](void* p) { if (p) cudaFree(p); };
+    for (int i = 0; i < 2; ++i) {
+        F(r->d_imgbuf[i]); F(r->d_vol[i]); F(r->d_w[i]); F(r->d_pow[i]); F(r->d_w2[i]);
+        F(r->d_half_weighed[i]);
+        if (r->h_partbuf[i]) cudaFreeHost(r->h_partbuf[i]);
+        if (r->copy_done[i]) cudaEventDestroy(r->copy_done[i]);
+        if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
+    }
+    F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc);
+    for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+    r->timed.clear();
+    if (r->stream) cudaStreamDestroy(r->stream);
+    if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
+}
+
+static int run_batch_kernels(Recon* r, const float* d_img, long np, float2* spec_out, bool insert) {
+    cudaStream_t s = r->stream;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
+    CK(launch_background(*r, d_img, (int)np, s));
+    CK(launch_rows(*r, d_img, (int)np, s));
+    CK(launch_cols(*r, (int)np, spec_out, s));
+    r->stats.launches += 3;
+    if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 1}); }
+    if (!insert) return BSG_OK;
+    for (int h = 0; h < r->nhalves; ++h) {
+        if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
+        CK(launch_insert(*r, spec_out, 0, (int)np, r->nhalves == 2 ? h : -1, s));
+        if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 0}); }
+        r->stats.launches += 1;
+        r->stats.insert_launches += 1;
+    }
+    r->stats.particles += np;
+    return BSG_OK;
+}
+
+// Upload one batch's particle records through a pinned staging buffer.
+static int upload_params(Recon* r, int buf, const double* params, long np) {
+    // the staging buffer may still feed an in-flight copy from two batches ago
+    CK(cudaEventSynchronize(r->compute_done[buf]));
+    DevParticle* hp = r->h_partbuf[buf];
+    for (long i = 0; i < np; ++i) make_dev_particle(*r, params + i * BSG_PARTICLE_DOUBLES, hp[i]);
+    r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
+    CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->stream));
+    return BSG_OK;
+}
+
+static int process(Recon* r, const float* images, const double* params, long nparts, int flags,
+                   float* spectra_out) {
+    const size_t img_elems = (size_t)r->g.n * r->g.n;
+    const bool dev = flags & BSG_DEVICE_PTR;
+    for (long off = 0, bi = 0; off < nparts; off += r->batch, ++bi) {
+        const long np = std::min<long>(r->batch, nparts - off);
+        const int buf = (int)(bi & 1);
+        int rc = upload_params(r, buf, params + off * BSG_PARTICLE_DOUBLES, np);
+        if (rc) return rc;
+        const float* d_img;
+        if (dev) {
+            d_img = images + off * img_elems;
+        } else {
+            // the buffer is free once the batch that last used it has finished
+            CK(cudaStreamWaitEvent(r->copy_stream, r->compute_done[buf], 0));
+            cudaEvent_t a = nullptr, b = nullptr;
+            if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, r->copy_stream); }
+            CK(cudaMemcpyAsync(r->d_imgbuf[buf], images + off * img_elems, sizeof(float) * img_elems * np,
+                               cudaMemcpyHostToDevice, r->copy_stream));
+            if (r->timing) { cudaEventRecord(b, r->copy_stream); r->timed.push_back({a, b, 2}); }
+            CK(cudaEventRecord(r->copy_done[buf], r->copy_stream));
+            CK(cudaStreamWaitEvent(r->stream, r->copy_done[buf], 0));
+            d_img = r->d_imgbuf[buf];
+        }
+        rc = run_batch_kernels(r, d_img, np, r->d_spec, spectra_out == nullptr);
+        if (rc) return rc;
+        if (spectra_out) {
+            const size_t bytes = sizeof(float2) * r->spec_elems() * np;
+            float* dst = spectra_out + off * r->spec_elems() * 2;
+            CK(cudaMemcpyAsync(dst, r->d_spec, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                               r->stream));
+        }
+        CK(cudaEventRecord(r->compute_done[buf], r->stream));
+    }
+    return BSG_OK;
+}
+
+static int ensure_finish_buffers(Recon* r) {
+    const size_t N3 = r->vol_elems();
+    if (!r->d_work) { int rc = alloc((void**)&r->d_work, sizeof(float2) * N3); if (rc) return rc; }
+    if (!r->d_map) { int rc = alloc((void**)&r->d_map, sizeof(float) * N3); if (rc) return rc; }
+    if (r->g.fom && !r->d_fom) { int rc = alloc((void**)&r->d_fom, sizeof(float) * N3); if (rc) return rc; }
+    return BSG_OK;
+}
+
+}  // namespace bsg
+
+using namespace bsg;
+
+extern "C" {
+
+const char* bsg_last_error(void) { return g_err; }
+const char* bsg_version(void) { return "bsgpu 0.1.0 (sm_100a)"; }
+
+int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
+    if (!cfg || !out) return fail(BSG_ERR_ARG, "bsg_recon_create: null argument");
+    *out = nullptr;
+    const int n = cfg->n, ft = cfg->ft, N = cfg->map;
+    if (n < 2 || !is_pow2(ft) || ft < 32 || ft > 1024 || ft < n)
+        return fail(BSG_ERR_ARG, "bsg_recon_create: transform size %d must be a power of two in [32, 1024] and >= box %d", ft, n);
+    if (!is_pow2(N) || N < 8 || N > 512 || N > ft)
+        return fail(BSG_ERR_ARG, "bsg_recon_create: map size %d must be a power of two in [8, 512] and <= %d", N, ft);
+    if (cfg->interp < 0 || cfg->interp > 2) return fail(BSG_ERR_ARG, "bsg_recon_create: interp %d", cfg->interp);
+    if (cfg->nmaps < 1 || cfg->nmaps > 3) return fail(BSG_ERR_ARG, "bsg_recon_create: nmaps %d", cfg->nmaps);
+    if (!(cfg->map_sampling > 0) || !(cfg->hi_res > 0)) return fail(BSG_ERR_ARG, "bsg_recon_create: sampling/resolution");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
+        return fail(BSG_ERR_NODEV, "bsg_recon_create: CUDA device %d not available", cfg->device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major < 10)
+        return fail(BSG_ERR_NODEV, "bsg_recon_create: device %d is not sm_100 class", cfg->device);
+    CK(cudaSetDevice(cfg->device));
+
+    Recon* r = new (std::nothrow) Recon();
+    if (!r) return fail(BSG_ERR_NOMEM, "bsg_recon_create: host allocation");
+    r->cfg = *cfg;
+    r->device = cfg->device;
+    Geometry& g = r->g;
+    g.n = n; g.ft = ft; g.map = N; g.logft = ilog2i(ft);
+    g.interp = cfg->interp; g.ctf_action = cfg->ctf_action; g.wiener = cfg->wiener;
+    g.hi_res = cfg->hi_res < 0.5 ? 0.5 : cfg->hi_res;      // Bimage_reconstruct.cpp:136
+    g.maxs2 = 1.0 / (g.hi_res * g.hi_res);
+    g.mins2 = 0.0;
+    g.ctf_shi2 = 1.0 / (cfg->hi_res * cfg->hi_res);        // mg_ctf.cpp:50-58
+    g.mscale = N * cfg->map_sampling;
+    g.fom = cfg->fom ? 1 : 0;
+    g.gate = 1;
+    r->nhalves = cfg->nmaps >= 2 ? 2 : 1;
+    int batch = cfg->batch;
+    if (batch <= 0) {
+        const double per = 8.0 * ft * ft;
+        batch = (int)std::min(4096.0, std::max(32.0, 2.0e9 / per));
+    }
+    r->batch = batch;
+
+    int rc = BSG_OK;
+    auto A = [&](void** p, size_t bytes) { if (!rc) rc = alloc(p, bytes); };
+    if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        free_all(r); delete r;
+        return fail(BSG_ERR_CUDA, "bsg_recon_create: stream creation failed");
+    }
+    const size_t N3 = (size_t)N * N * N;
+    for (int i = 0; i < 2; ++i) {
+        A((void**)&r->d_imgbuf[i], sizeof(float) * (size_t)n * n * batch);
+        if (!rc && cudaMallocHost((void**)&r->h_partbuf[i], sizeof(DevParticle) * batch) != cudaSuccess)
+            rc = fail(BSG_ERR_NOMEM, "bsg_recon_create: pinned host allocation");
+        if (!rc && (cudaEventCreateWithFlags(&r->copy_done[i], cudaEventDisableTiming) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&r->compute_done[i], cudaEventDisableTiming) != cudaSuccess))
+            rc = fail(BSG_ERR_CUDA, "bsg_recon_create: event creation failed");
+    }
+    A((void**)&r->d_part, sizeof(DevParticle) * batch);
+    A((void**)&r->d_bkg, sizeof(double) * batch);
+    A((void**)&r->d_phase, sizeof(float2) * 2 * ft * (size_t)batch);
+    A((void**)&r->d_rows, sizeof(float2) * (size_t)n * (ft / 2 + 1) * batch);
+    A((void**)&r->d_spec, sizeof(float2) * (size_t)ft * ft * batch);
+    A((void**)&r->d_tw, sizeof(float2) * std::max(1, ft / 2));
+    A((void**)&r->d_twmap, sizeof(float2) * std::max(1, N / 2));
+    for (int h = 0; h < r->nhalves; ++h) {
+        A((void**)&r->d_vol[h], sizeof(float2) * N3);
+        A((void**)&r->d_w[h], sizeof(float) * N3);
+        if (g.fom) { A((void**)&r->d_pow[h], sizeof(float) * N3); A((void**)&r->d_w2[h], sizeof(float) * N3); }
+    }
+    if (rc) { free_all(r); delete r; return rc; }
+    std::vector<float2> tw;
+    host_twiddles(ft, tw);
+    cudaError_t e = cudaMemcpy(r->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice);
+    host_twiddles(N, tw);
+    if (e == cudaSuccess) e = cudaMemcpy(r->d_twmap, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = prepare_fft2d_attributes();
+    if (e == cudaSuccess) e = prepare_finish_attributes();
+    if (e != cudaSuccess) { free_all(r); delete r; return fail(BSG_ERR_CUDA, "bsg_recon_create: %s", cudaGetErrorString(e)); }
+    for (int i = 0; i < 2; ++i) {
+        cudaEventRecord(r->compute_done[i], r->stream);
+    }
+    *out = reinterpret_cast<bsg_recon*>(r);
+    return bsg_recon_reset(*out);
+}
+
+void bsg_recon_destroy(bsg_recon* h) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return;
+    cudaSetDevice(r->device);
+    if (r->stream) cudaStreamSynchronize(r->stream);
+    if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
+    free_all(r);
+    delete r;
+}
+
+int bsg_recon_reset(bsg_recon* h) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return fail(BSG_ERR_ARG, "bsg_recon_reset: null context");
+    CK(cudaSetDevice(r->device));
+    const size_t N3 = r->vol_elems();
+    for (int i = 0; i < r->nhalves; ++i) {
+        CK(cudaMemsetAsync(r->d_vol[i], 0, sizeof(float2) * N3, r->stream));
+        CK(cudaMemsetAsync(r->d_w[i], 0, sizeof(float) * N3, r->stream));
+        if (r->g.fom) {
+            CK(cudaMemsetAsync(r->d_pow[i], 0, sizeof(float) * N3, r->stream));
+            CK(cudaMemsetAsync(r->d_w2[i], 0, sizeof(float) * N3, r->stream));
+        }
+    }
+    return BSG_OK;
+}
+
+int bsg_recon_insert(bsg_recon* h, const float* images, const double* params, long nparts, int flags) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !images || !params || nparts < 0) return fail(BSG_ERR_ARG, "bsg_recon_insert: bad argument");
+    if (r->broken) return fail(BSG_ERR_STATE, "bsg_recon_insert: context unusable after an earlier CUDA error");
+    if (nparts == 0) return BSG_OK;
+    for (long i = 0; i < nparts; ++i) {
+        const double* q = params + i * BSG_PARTICLE_DOUBLES;
+        if (!(q[13] > 0)) return fail(BSG_ERR_ARG, "bsg_recon_insert: particle %ld has pixel size %g", i, q[13]);
+        const int half = (int)q[23];
+        if (half < 0 || half > 1) return fail(BSG_ERR_ARG, "bsg_recon_insert: particle %ld half-map index %d", i, half);
+    }
+    CK(cudaSetDevice(r->device));
+    int rc = process(r, images, params, nparts, flags, nullptr);
+    if (rc == BSG_ERR_CUDA) r->broken = true;
+    return rc;
+}
+
+int bsg_particle_spectra(bsg_recon* h, const float* images, const double* params, long nparts, float* out, int flags) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !images || !params || !out || nparts < 0) return fail(BSG_ERR_ARG, "bsg_particle_spectra: bad argument");
+    CK(cudaSetDevice(r->device));
+    int rc = process(r, images, params, nparts, flags, out);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int flags) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !map_out) return fail(BSG_ERR_ARG, "bsg_recon_finish: bad argument");
+    if (imap < 0 || imap > 2 || (imap > 0 && r->nhalves < 2) || (imap == 0 && r->cfg.nmaps == 2 && false))
+        return fail(BSG_ERR_ARG, "bsg_recon_finish: map %d not available (nmaps = %d)", imap, r->cfg.nmaps);
+    if (fom_out && !r->g.fom) return fail(BSG_ERR_ARG, "bsg_recon_finish: FOM requested but fom = 0");
+    CK(cudaSetDevice(r->device));
+    int rc = ensure_finish_buffers(r);
+    if (rc) return rc;
+    const bool sinc = (flags & BSG_SINC) != 0;
+    const bool dev = (flags & BSG_DEVICE_PTR) != 0;
+    float* dst = dev ? map_out : r->d_map;
+    CK(launch_weigh(*r, imap, r->stream));
+    CK(launch_ifft3(*r, r->d_work, dst, sinc, r->stream));
+    r->stats.launches += 4;
+    const size_t N3 = r->vol_elems();
+    if (!dev) CK(cudaMemcpyAsync(map_out, r->d_map, sizeof(float) * N3, cudaMemcpyDeviceToHost, r->stream));
+    if (fom_out) CK(cudaMemcpyAsync(fom_out, r->d_fom, sizeof(float) * N3,
+                                    dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+int bsg_recon_accumulators(bsg_recon* h, int half, float* vol_out, float* weight_out, int flags) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || half < 0 || half >= r->nhalves) return fail(BSG_ERR_ARG, "bsg_recon_accumulators: bad half %d", half);
+    CK(cudaSetDevice(r->device));
+    const size_t N3 = r->vol_elems();
+    const cudaMemcpyKind k = (flags & BSG_DEVICE_PTR) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (vol_out) CK(cudaMemcpyAsync(vol_out, r->d_vol[half], sizeof(float2) * N3, k, r->stream));
+    if (weight_out) CK(cudaMemcpyAsync(weight_out, r->d_w[half], sizeof(float) * N3, k, r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+int bsg_recon_fsc(bsg_recon* h, int nshell, double* fsc_out) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !fsc_out || nshell < 1) return fail(BSG_ERR_ARG, "bsg_recon_fsc: bad argument");
+    if (r->nhalves < 2) return fail(BSG_ERR_STATE, "bsg_recon_fsc: needs half maps (nmaps >= 2)");
+    CK(cudaSetDevice(r->device));
+    const size_t N3 = r->vol_elems();
+    for (int i = 0; i < 2; ++i)
+        if (!r->d_half_weighed[i]) { int rc = alloc((void**)&r->d_half_weighed[i], sizeof(float2) * N3); if (rc) return rc; }
+    if (r->d_fsc) { cudaFree(r->d_fsc); r->d_fsc = nullptr; }
+    int rc = alloc((void**)&r->d_fsc, sizeof(double) * 3 * (size_t)r->g.map * nshell + sizeof(double) * nshell);
+    if (rc) return rc;
+    double* d_out = r->d_fsc + 3 * (size_t)r->g.map * nshell;
+    CK(launch_fsc(*r, nshell, d_out, r->stream));
+    r->stats.launches += 4;
+    CK(cudaMemcpyAsync(fsc_out, d_out, sizeof(double) * nshell, cudaMemcpyDeviceToHost, r->stream));
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+int bsg_recon_set_timing(bsg_recon* h, int enable) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return fail(BSG_ERR_ARG, "bsg_recon_set_timing: null context");
+    r->timing = enable != 0;
+    return BSG_OK;
+}
+
+int bsg_recon_get_stats(bsg_recon* h, bsg_recon_stats* st) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !st) return fail(BSG_ERR_ARG, "bsg_recon_get_stats: bad argument");
+    CK(cudaSetDevice(r->device));
+    CK(cudaStreamSynchronize(r->stream));
+    CK(cudaStreamSynchronize(r->copy_stream));
+    for (auto& t : r->timed) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, t.a, t.b);
+        if (t.kind == 0) r->stats.insert_ms += ms;
+        else if (t.kind == 1) r->stats.fft2d_ms += ms;
+        else r->stats.h2d_ms += ms;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    r->timed.clear();
+    *st = r->stats;
+    return BSG_OK;
+}
+
+int bsg_recon_synchronize(bsg_recon* h) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return fail(BSG_ERR_ARG, "bsg_recon_synchronize: null context");
+    CK(cudaSetDevice(r->device));
+    CK(cudaStreamSynchronize(r->copy_stream));
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+void* bsg_recon_stream(bsg_recon* h) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    return r ? (void*)r->stream : nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,51 @@
+// context.cuh - the state behind an opaque bsg_recon handle.
+#pragma once
+
+#include "common.cuh"
+
+namespace bsg {
+
+struct Context {
+    bsg_recon_config cfg;
+    Geometry g;
+    int device = 0;
+    int batch = 0;
+    int nhalves = 1;
+    cudaStream_t stream = nullptr;
+
+    // per-batch device buffers
+    float* d_img = nullptr;          // batch x n x n
+    DevParticle* d_part = nullptr;   // batch
+    double* d_bkg = nullptr;         // batch
+    float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
+    float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms
+    float2* d_spec = nullptr;        // batch x ft x ft: particle spectra
+    float2* d_tw = nullptr;          // ft/2 twiddles exp(-2 pi i j / ft)
+    float2* d_twmap = nullptr;       // N/2 twiddles exp(-2 pi i j / N)
+
+    // accumulators per half map, reference index order
+    float2* d_vol[2] = {nullptr, nullptr};
+    float* d_w[2] = {nullptr, nullptr};
+    float* d_pow[2] = {nullptr, nullptr};
+    float* d_w2[2] = {nullptr, nullptr};
+
+    // finishing buffers (allocated on first use)
+    float2* d_work = nullptr;        // N^3 complex
+    float* d_map = nullptr;          // N^3 real
+    float* d_fom = nullptr;          // N^3 real
+    float2* d_half_weighed[2] = {nullptr, nullptr};
+    double* d_fsc = nullptr;         // FSC partial sums
+
+    // host staging (pinned)
+    DevParticle* h_part = nullptr;
+    float* h_stage = nullptr;        // batch x n x n pinned image staging
+
+    bool timing = false;
+    bsg_recon_stats stats{};
+    cudaEvent_t ev[8]{};
+
+    size_t spec_elems() const { return (size_t)g.ft * g.ft; }
+    size_t vol_elems() const { return (size_t)g.map * g.map * g.map; }
+};
+
+}  // namespace bsg

@@ -1,0 +1,274 @@
+// finish.cu - from accumulated central sections to the real-space map.
+// Reference steps (bsoft/src):
+//   sum of partial maps + weigh   mg/mg_reconstruct.cpp:306-331,
+//                                 img/Bimage_reconstruct.cpp:486-515
+//   SNR (FOM) map                 img/Bimage_reconstruct.cpp:610-634
+//   phase_shift_to_center         img/Bimage_complex.cpp:545-552 (= (-1)^(h+k+l))
+//   fft_back (1/sqrt(N^3)), real  img/Bimage.h:903-908, Bimage_complex.cpp:170-186
+//   filter_sinc (trilinear)       img/Bimage_filter.cpp:484-509
+//
+// weigh_kernel is one pass over the voxels; the 3-D inverse transform is
+// three passes of warp FFTs (x lines contiguous; y and z lines staged 16 at
+// a time through shared memory so global accesses stay coalesced).  The last
+// pass writes only the real part, scaled and sinc-weighted.
+#include "context.cuh"
+#include "fft_dev.cuh"
+
+#include <math.h>
+
+namespace bsg {
+
+#define SMALLFLOAT_F 1e-30f
+
+struct WeighArgs {
+    const float2* v0; const float* w0; const float* p0; const float* q0;
+    const float2* v1; const float* w1; const float* p1; const float* q1;   // second half or null
+    float2* out;      // weighed, centre-shifted complex volume
+    float* fom;       // optional SNR map
+    int N;
+};
+
+__global__ void weigh_kernel(WeighArgs a) {
+    const size_t N = a.N, N3 = N * N * N;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3; i += (size_t)gridDim.x * blockDim.x) {
+        float2 v = a.v0[i];
+        float w = a.w0[i];
+        float p = a.p0 ? a.p0[i] : 0.f, q = a.q0 ? a.q0[i] : 0.f;
+        if (a.v1) {
+            const float2 v1 = a.v1[i];
+            v.x += v1.x; v.y += v1.y;
+            w += a.w1[i];
+            if (a.p1) { p += a.p1[i]; q += a.q1[i]; }
+        }
+        float2 F = make_float2(0.f, 0.f);
+        if (w > SMALLFLOAT_F) {
+            q = w - q / w;
+            F = make_float2(v.x / w, v.y / w);
+            if (q > 1.f) p /= q;
+            else if (w > 1.f) p /= w;
+            if (p < 0.f) p = 0.f;
+        } else {
+            p = 0.f;
+            w = q = SMALLFLOAT_F;
+        }
+        if (a.fom) {
+            // fspace_reconstruction_snr on the weighed channels
+            const double signal = (double)F.x * F.x + (double)F.y * F.y;
+            double noise = (double)p - signal;
+            if (noise < signal) noise = signal;
+            float f = 0.f;
+            if (w > 1.f && signal > 1e-30 && noise > 1e-30) f = (float)((w * signal - p) / noise);
+            a.fom[i] = (i == 0) ? 1.f : f;
+        }
+        // (-1)^(h+k+l): signed and unsigned indices share parity for even N
+        const size_t x = i % N, y = (i / N) % N, z = i / (N * N);
+        if ((x + y + z) & 1) { F.x = -F.x; F.y = -F.y; }
+        a.out[i] = F;
+    }
+}
+
+// x-lines: one warp per line, 8 lines per CTA
+constexpr int XW = 8;
+__global__ void __launch_bounds__(XW * 32) fft_x_kernel(float2* data, const float2* tw, int N, int logN) {
+    extern __shared__ float2 sm[];
+    float2* stw = sm;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2* buf = sm + N / 2 + warp * N;
+    for (int i = threadIdx.x; i < N / 2; i += blockDim.x) stw[i] = tw[i];
+    __syncthreads();
+    const size_t line = (size_t)blockIdx.x * XW + warp;
+    if (line >= (size_t)N * N) return;
+    float2* p = data + line * N;
+    for (int i = lane; i < N; i += 32) buf[bitrev(i, logN)] = p[i];
+    __syncwarp();
+    warp_fft<true>(buf, N, logN, stw);
+    for (int i = lane; i < N; i += 32) p[i] = buf[i];
+}
+
+// strided lines (y: stride N, z: stride N*N): 16 adjacent x per CTA.
+constexpr int SW = 16;
+struct StridedArgs {
+    float2* data;
+    const float2* tw;
+    int N, logN;
+    int axis;          // 1 = y, 2 = z
+    float* real_out;   // when set: write the real part * scale (* sinc) instead
+    float scale;
+    int sinc;
+};
+
+__global__ void __launch_bounds__(SW * 32) fft_strided_kernel(StridedArgs a) {
+    extern __shared__ float2 sm[];
+    const int N = a.N;
+    float2* stw = sm;
+    float2* tile = sm + N / 2;        // SW x N
+    for (int i = threadIdx.x; i < N / 2; i += blockDim.x) stw[i] = a.tw[i];
+    // blockIdx.x: x-chunk, blockIdx.y: the remaining coordinate (z for axis y, y for axis z)
+    const int x0 = blockIdx.x * SW;
+    const int other = blockIdx.y;
+    const size_t stride = a.axis == 1 ? (size_t)N : (size_t)N * N;
+    const size_t obase = a.axis == 1 ? (size_t)other * N * N : (size_t)other * N;
+    for (int i = threadIdx.x; i < SW * N; i += blockDim.x) {
+        const int c = i % SW, j = i / SW;
+        const int x = x0 + c;
+        float2 v = make_float2(0.f, 0.f);
+        if (x < N) v = a.data[obase + (size_t)j * stride + x];
+        tile[c * N + bitrev(j, a.logN)] = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5;
+    if (x0 + warp < N) warp_fft<true>(tile + warp * N, N, a.logN, stw);
+    __syncthreads();
+    for (int i = threadIdx.x; i < SW * N; i += blockDim.x) {
+        const int c = i % SW, j = i / SW;
+        const int x = x0 + c;
+        if (x >= N) continue;
+        const size_t idx = obase + (size_t)j * stride + x;
+        const float2 v = tile[c * N + j];
+        if (a.real_out) {
+            float r = v.x * a.scale;
+            if (a.sinc) {
+                // filter_sinc: r = pi |d|, d = (index - N/2) / N, weight (r / sin r)^2
+                const int yy = a.axis == 1 ? j : other;
+                const int zz = a.axis == 1 ? other : j;
+                const double o = (double)(N / 2);
+                const double dx = (x - o) / N, dy = (yy - o) / N, dz = (zz - o) / N;
+                const double rr = 3.14159265358979323846 * sqrt(dx * dx + dy * dy + dz * dz);
+                if (rr != 0.0) { const double w = rr / sin(rr); r = (float)(w * w * r); }
+            }
+            a.real_out[idx] = r;
+        } else {
+            a.data[idx] = v;
+        }
+    }
+}
+
+cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s) {
+    WeighArgs a{};
+    const int N = c.g.map;
+    int h0 = 0;
+    bool both = false;
+    if (c.nhalves == 2) {
+        if (imap == 0) both = true;
+        else h0 = imap - 1;
+    }
+    a.v0 = c.d_vol[h0]; a.w0 = c.d_w[h0]; a.p0 = c.d_pow[h0]; a.q0 = c.d_w2[h0];
+    if (both) { a.v1 = c.d_vol[1]; a.w1 = c.d_w[1]; a.p1 = c.d_pow[1]; a.q1 = c.d_w2[1]; }
+    a.out = c.d_work;
+    a.fom = c.g.fom ? c.d_fom : nullptr;
+    a.N = N;
+    weigh_kernel<<<148 * 8, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool sinc, cudaStream_t s) {
+    const int N = c.g.map, logN = ilog2i(N);
+    {
+        const size_t lines = (size_t)N * N;
+        const size_t smem = sizeof(float2) * ((size_t)N / 2 + (size_t)XW * N);
+        fft_x_kernel<<<(unsigned)((lines + XW - 1) / XW), XW * 32, smem, s>>>(vol, c.d_twmap, N, logN);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    const size_t smem = sizeof(float2) * ((size_t)N / 2 + (size_t)SW * N);
+    dim3 grid((N + SW - 1) / SW, N);
+    StridedArgs a{};
+    a.data = vol; a.tw = c.d_twmap; a.N = N; a.logN = logN;
+    a.axis = 1;
+    fft_strided_kernel<<<grid, SW * 32, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    a.axis = 2;
+    a.real_out = real_out;
+    a.scale = (float)(1.0 / sqrt((double)N * N * N));
+    a.sinc = sinc ? 1 : 0;
+    fft_strided_kernel<<<grid, SW * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finish(const Context& c, int imap, float* map_out, float* fom_out, bool sinc, cudaStream_t s) {
+    (void)fom_out;
+    cudaError_t e = launch_weigh(c, imap, s);
+    if (e != cudaSuccess) return e;
+    return launch_ifft3(c, c.d_work, map_out, sinc, s);
+}
+
+// Weighed (not centre-shifted) half map for the FSC: reuse weigh_kernel and
+// undo nothing - the FSC only uses products F1 conj(F2) and |F|^2, which the
+// (-1)^(h+k+l) factor leaves unchanged.
+cudaError_t launch_weigh_into(const Context& c, int imap, float2* out, cudaStream_t s) {
+    WeighArgs a{};
+    const int h0 = imap - 1;
+    a.v0 = c.d_vol[h0]; a.w0 = c.d_w[h0]; a.p0 = nullptr; a.q0 = nullptr;
+    a.out = out; a.fom = nullptr; a.N = c.g.map;
+    weigh_kernel<<<148 * 8, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// FSC partial sums: one CTA per z-plane; thread r accumulates shell r of
+// that plane in a fixed order (rows, then columns), then fsc_reduce sums the
+// planes in order - deterministic, FP64 throughout.
+__global__ void fsc_plane_kernel(const float2* v1, const float2* v2, int N, int nshell, double* part) {
+    const int z = blockIdx.x;
+    const int l = sfreq(z, N);
+    for (int r = threadIdx.x; r < nshell; r += blockDim.x) {
+        double num = 0, d1 = 0, d2 = 0;
+        const double rlo = r - 0.5, rhi = r + 0.5;
+        for (int y = 0; y < N; ++y) {
+            const int k = sfreq(y, N);
+            const double kl = (double)k * k + (double)l * l;
+            if (kl >= rhi * rhi) continue;
+            // |h| range that can land in shell r = round(sqrt(h^2 + kl))
+            const int hlo = rlo * rlo > kl ? (int)floor(sqrt(rlo * rlo - kl)) : 0;
+            const int hhi = min(N / 2, (int)ceil(sqrt(rhi * rhi - kl)));
+            for (int hh = hlo; hh <= hhi; ++hh) {
+                const double r2 = (double)hh * hh + kl;
+                if ((int)floor(sqrt(r2) + 0.5) != r) continue;
+                for (int sgn = 0; sgn < 2; ++sgn) {
+                    if (sgn && (hh == 0 || hh == N / 2)) continue;
+                    const int x = (sgn ? -hh : hh) & (N - 1);
+                    const size_t i = ((size_t)z * N + y) * N + x;
+                    const float2 a = v1[i], b = v2[i];
+                    num += (double)a.x * b.x + (double)a.y * b.y;
+                    d1 += (double)a.x * a.x + (double)a.y * a.y;
+                    d2 += (double)b.x * b.x + (double)b.y * b.y;
+                }
+            }
+        }
+        double* o = part + ((size_t)z * nshell + r) * 3;
+        o[0] = num; o[1] = d1; o[2] = d2;
+    }
+}
+
+__global__ void fsc_reduce_kernel(const double* part, int N, int nshell, double* fsc) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nshell) return;
+    double num = 0, d1 = 0, d2 = 0;
+    for (int z = 0; z < N; ++z) {
+        const double* o = part + ((size_t)z * nshell + r) * 3;
+        num += o[0]; d1 += o[1]; d2 += o[2];
+    }
+    fsc[r] = (d1 > 0 && d2 > 0) ? num / sqrt(d1 * d2) : 0.0;
+}
+
+cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream_t s) {
+    cudaError_t e = launch_weigh_into(c, 1, c.d_half_weighed[0], s);
+    if (e != cudaSuccess) return e;
+    e = launch_weigh_into(c, 2, c.d_half_weighed[1], s);
+    if (e != cudaSuccess) return e;
+    fsc_plane_kernel<<<c.g.map, 128, 0, s>>>(c.d_half_weighed[0], c.d_half_weighed[1], c.g.map, nshell, c.d_fsc);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    fsc_reduce_kernel<<<(nshell + 127) / 128, 128, 0, s>>>(c.d_fsc, c.g.map, nshell, out_dev);
+    return cudaGetLastError();
+}
+
+cudaError_t prepare_finish_attributes() {
+    cudaError_t e = cudaFuncSetAttribute(fft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(sizeof(float2) * (256 + XW * 512)));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(fft_strided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(float2) * (256 + SW * 512)));
+}
+
+}  // namespace bsg

@@ -1,0 +1,133 @@
+/*
+ * bsgpu.h - C ABI of the B200 (sm_100a) single-particle reconstruction and
+ * projection-matching library (libbsgpu.so).
+ *
+ * The reference (Bsoft) has no plugin or FFI layer; its boundary for this
+ * path is the C++ library call surface that `breconstruct` / `brefine`
+ * drive.  Each entry point below names the reference interface it replaces:
+ *
+ *   bsg_recon_create     <- per-map set-up in particle_reconstruct
+ *                           (bsoft/src/mg/mg_reconstruct.cpp:100-125) and the
+ *                           plan created in breconstruct.cpp:268
+ *   bsg_recon_insert     <- particle_reconstruct's per-particle loop
+ *                           (mg_reconstruct.cpp:143-229): pad, fft, origin
+ *                           shift, img_ctf_apply_complex, fspace_pack_2D
+ *                           (bsoft/include/mg_reconstruct.h:16-19,
+ *                            bsoft/include/Bimage.h:934-939)
+ *   bsg_recon_finish     <- img_reconstruction_sum_weigh (mg_reconstruct.h:20,
+ *                           mg_reconstruct.cpp:266-361) + fft_back
+ *                           (Bimage.h:903-908) + filter_sinc
+ *                           (breconstruct.cpp:328-359)
+ *   bsg_recon_fsc        <- Bimage::fsc (bsoft/src/img/Bimage_resolution.cpp:330-406)
+ *   bsg_particle_spectra <- the 2-D half of particle_reconstruct
+ *                           (Bimage::fft + phase_shift_to_origin +
+ *                            img_ctf_apply_complex), exposed on its own
+ *
+ * Conventions: every function returns 0 (BSG_OK) or a negative BSG_ERR_*
+ * code and leaves a message for bsg_last_error() (thread-local), the way the
+ * reference returns NULL / <0 after error_show (bsoft/src/util/utilities.cpp:745).
+ * Host buffers are caller-owned; a context owns its device memory and one
+ * CUDA stream, and is used by one host thread at a time.
+ */
+#ifndef BSGPU_H
+#define BSGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BSG_OK          0
+#define BSG_ERR_ARG    -1   /* invalid argument / unsupported size          */
+#define BSG_ERR_CUDA   -2   /* CUDA runtime error                           */
+#define BSG_ERR_STATE  -3   /* call out of order / context unusable         */
+#define BSG_ERR_NOMEM  -4   /* device or host allocation failed             */
+#define BSG_ERR_NODEV  -5   /* no usable sm_100 device                      */
+
+/* flags */
+#define BSG_DEVICE_PTR  1   /* image / output pointers are device pointers  */
+#define BSG_SINC        2   /* bsg_recon_finish: apply the trilinear sinc   */
+
+/* Per-particle record: 32 doubles, host layout (see bsoft_b200/plan.py):
+ *   [0..1]  origin x, y (pixels)              Bparticle::ori
+ *   [2..3]  background circle centre (pixels) image origin from the file
+ *   [4..12] rotation matrix, row-major        View::matrix (View.h:153-156)
+ *   [13]    particle pixel size (angstrom)
+ *   [14]    frequency scale = 1/magnification (1 if none)
+ *   [15]    particle weight (1, or selection number when bootstrapping)
+ *   [16..22] CTF: abw00 abw20 abw22 abw2m2 abw40 abw11 abw1m1 (ctf.h:321-351)
+ *   [23]    half-map index (0 or 1)
+ */
+#define BSG_PARTICLE_DOUBLES 32
+
+typedef struct {
+    int    n;            /* particle box edge                                 */
+    int    ft;           /* padded transform edge: power of two in [32, 1024] */
+    int    map;          /* map edge N: even, 8 <= N <= 512, N <= ft          */
+    double map_sampling; /* angstrom / voxel                                  */
+    double hi_res;       /* resolution limit (angstrom) after check_resolution */
+    int    interp;       /* 0 nearest, 1 weighted nearest, 2 trilinear        */
+    int    ctf_action;   /* 0 none, 1 flip, 2 apply, >= 3 Wiener-type         */
+    double wiener;       /* Wiener factor                                     */
+    int    nmaps;        /* 1 full map, 2 two half maps, 3 full + half maps   */
+    int    fom;          /* 1: accumulate power and weight^2 as well          */
+    int    batch;        /* particles per device batch, 0 = automatic         */
+    int    device;       /* CUDA device ordinal                               */
+} bsg_recon_config;
+
+typedef struct bsg_recon bsg_recon;
+
+/* Kernel timing collected with CUDA events on the context's stream
+ * (enabled with bsg_recon_set_timing). */
+typedef struct {
+    long   launches;          /* all kernels this library launched          */
+    long   insert_launches;   /* gridding kernel launches                   */
+    double insert_ms;         /* summed device time of the gridding kernel  */
+    double fft2d_ms;          /* background + row + column passes           */
+    double h2d_ms;            /* host-to-device copies of particle images   */
+    long   particles;         /* particles inserted                         */
+} bsg_recon_stats;
+
+int  bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out);
+void bsg_recon_destroy(bsg_recon* r);
+
+/* Insert nparts particles: images (nparts x n x n float32, x fastest) and
+ * params (nparts x BSG_PARTICLE_DOUBLES, host).  Accumulation order is fixed
+ * (particle order, then pixel order), so results are bitwise reproducible. */
+int  bsg_recon_insert(bsg_recon* r, const float* images, const double* params,
+                      long nparts, int flags);
+
+/* Weigh map imap (0 full, 1/2 half maps; see nmaps), shift the origin to the
+ * centre, inverse-transform and (with BSG_SINC) apply the sinc weighting.
+ * map_out: N^3 float32 real-space map; fom_out (optional, needs fom = 1):
+ * N^3 float32 signal-to-noise map (fspace_reconstruction_snr). */
+int  bsg_recon_finish(bsg_recon* r, int imap, float* map_out, float* fom_out, int flags);
+
+/* Raw accumulators of half h (0/1; 0 when nmaps == 1): complex volume
+ * (2*N^3 float32) and weights (N^3 float32), reference index order. */
+int  bsg_recon_accumulators(bsg_recon* r, int half, float* vol_out, float* weight_out, int flags);
+
+/* Fourier shell correlation of the two weighed half maps (nmaps >= 2):
+ * nshell doubles, shell r = round(|frequency|). */
+int  bsg_recon_fsc(bsg_recon* r, int nshell, double* fsc_out);
+
+/* The 2-D stage alone: padded FFT, origin shift and CTF of nparts images;
+ * out = nparts x ft x ft complex64 (interleaved), reference pixel order. */
+int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* params,
+                          long nparts, float* out, int flags);
+
+int  bsg_recon_set_timing(bsg_recon* r, int enable);
+int  bsg_recon_get_stats(bsg_recon* r, bsg_recon_stats* st);
+int  bsg_recon_reset(bsg_recon* r);          /* zero the accumulators        */
+int  bsg_recon_synchronize(bsg_recon* r);
+void* bsg_recon_stream(bsg_recon* r);        /* the context's cudaStream_t  */
+
+const char* bsg_last_error(void);
+const char* bsg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

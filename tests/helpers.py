@@ -1,0 +1,74 @@
+"""Shared test helpers: golden-fixture loading and error metrics."""
+from __future__ import annotations
+
+import os
+import shlex
+
+import numpy as np
+
+from bsoft_b200.io import mrc
+from bsoft_b200.plan import INTERP, ReconOptions, load_images, plan_reconstruction
+from bsoft_b200.project import read_project
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+CASES = ["ctf16_tri_none", "ctf16_tri_flip", "ctf16_near_apply", "ctf16_wtd_correct",
+         "ctf16_tri_flip_res", "ctf16_tri_flip_half", "plain24_tri", "plain24_near"]
+
+
+def rel_l2(a, b) -> float:
+    a = np.asarray(a)
+    b = np.asarray(b)
+    a = a.astype(np.complex128 if np.iscomplexobj(a) else np.float64)
+    b = b.astype(np.complex128 if np.iscomplexobj(b) else np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def materialize_dataset(name: str, directory: str) -> str:
+    """Write a golden dataset's stacks and STAR file into `directory`."""
+    z = np.load(os.path.join(GOLDEN, f"ds_{name}.npz"))
+    for fn in z["stack_names"]:
+        mrc.write_stack(os.path.join(directory, str(fn)), z["stack_" + str(fn)], pixel_size=1.0)
+    # the pixel size that matters is the STAR one; rewrite headers with it
+    path = os.path.join(directory, "particles.star")
+    with open(path, "w") as f:
+        f.write(str(z["star"]))
+    proj = read_project(path)
+    for mg in proj.micrographs:
+        stack = z["stack_" + mg.particle_file]
+        mrc.write_stack(os.path.join(directory, mg.particle_file), stack, pixel_size=float(mg.pixel[0]))
+    return path
+
+
+def options_from_args(args: str) -> ReconOptions:
+    """Map a breconstruct option string onto ReconOptions (the subset the
+    fixtures use; prefix matching as bsoft/src/util/options.cpp does)."""
+    opt = ReconOptions()
+    toks = shlex.split(args)
+    i = 0
+    while i < len(toks):
+        t = toks[i].lstrip("-")
+        val = toks[i + 1] if i + 1 < len(toks) and not toks[i + 1].startswith("-") else None
+        if "interpolation".startswith(t):
+            opt.interp = INTERP[{"n": "nearest", "w": "weighted", "t": "trilinear"}[val[0]]]
+        elif t == "CTF":
+            v = val.lower()
+            opt.ctf_action = 1 if "fli" in v else 2 if "app" in v else 3 if "cor" in v else 4 if "wie" in v else 0
+        elif "resolution".startswith(t):
+            opt.resolution = float(val)
+        elif t == "halfmaps":
+            opt.nmaps = 2
+        elif t == "pad":
+            opt.pad = int(val)
+        i += 2 if val is not None else 1
+    return opt
+
+
+def load_case(name: str, directory: str):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    star = materialize_dataset(str(z["dataset"]), directory)
+    opt = options_from_args(str(z["options"]))
+    plan = plan_reconstruction(read_project(star), opt)
+    images = load_images(plan)
+    refs = {k: z[k] for k in z.files if k.startswith("map")}
+    return plan, images, refs

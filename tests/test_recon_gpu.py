@@ -1,0 +1,140 @@
+"""CUDA reconstruction path against the FP64 oracle and the reference's own
+breconstruct outputs (golden fixtures).  Tolerance for maps: relative L2
+<= 1e-5, FSC >= 0.999."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from bsoft_b200.plan import P_MAP, ReconOptions, load_images, plan_reconstruction
+from bsoft_b200.project import read_project
+from bsoft_b200.recon import Reconstructor
+from bsoft_b200.synth import DatasetSpec, generate, write_dataset
+from tests.helpers import CASES, GOLDEN, load_case, materialize_dataset, rel_l2
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def fsc(a, b):
+    A, B = np.fft.fftn(a), np.fft.fftn(b)
+    N = a.shape[0]
+    f = np.fft.fftfreq(N) * N
+    r = np.rint(np.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + f[None, None, :] ** 2)).astype(int)
+    out = []
+    for s in range(1, N // 2):
+        m = r == s
+        out.append(np.real(np.sum(A[m] * np.conj(B[m]))) / np.sqrt(np.sum(abs(A[m]) ** 2) * np.sum(abs(B[m]) ** 2)))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_gpu_matches_reference_and_oracle(case, tmp_path):
+    plan, images, refs = load_case(case, str(tmp_path))
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        if plan.nmaps == 2:
+            for h, key in ((1, "map_01"), (2, "map_02")):
+                m = rec.finish(h)
+                sel = np.nonzero(plan.params[:, P_MAP] == h - 1)[0]
+                orc = oracle.reconstruct(plan, images, sel)
+                assert rel_l2(m, orc) < TOL, (key, rel_l2(m, orc))
+                assert rel_l2(m, refs[key]) < TOL, (key, rel_l2(m, refs[key]))
+        else:
+            m = rec.finish(0)
+            orc = oracle.reconstruct(plan, images)
+            assert rel_l2(m, orc) < TOL, rel_l2(m, orc)
+            assert rel_l2(m, refs["map"]) < TOL, rel_l2(m, refs["map"])
+            assert fsc(m, refs["map"]).min() > 0.999
+
+
+@pytest.mark.parametrize("probe", ["probe_ctf16_0", "probe_ctf16_37"])
+def test_gpu_particle_spectrum_matches_reference(probe, tmp_path):
+    z = np.load(os.path.join(GOLDEN, probe + ".npz"))
+    star = materialize_dataset(str(z["dataset"]), str(tmp_path))
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=int(z["interp"]),
+                                                                ctf_action=int(z["ctf_action"])))
+    i = int(z["index"])
+    img = load_images(plan, [i])
+    with Reconstructor(plan) as rec:
+        S = rec.spectra(img, plan.params[i:i + 1])[0]
+    ref = z["ctf"][..., 0] + 1j * z["ctf"][..., 1]
+    assert rel_l2(S, ref) < 2e-6
+    F = oracle.particle_transform(plan, img[0], plan.params[i])
+    assert rel_l2(S, F) < 2e-6
+
+
+def _dataset(tmp_path, **kw):
+    spec = DatasetSpec(**kw)
+    ph, imgs, meta = generate(spec)
+    star = write_dataset(str(tmp_path), spec, ph, imgs, meta)
+    return star
+
+
+def test_gpu_c1_scale_against_oracle(tmp_path):
+    # configs[0] geometry (64^2 images -> 64^3, CTF flip, trilinear), 300 particles
+    star = _dataset(tmp_path, box=64, n_particles=300, n_blobs=50, seed=21, snr=0.1)
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        m = rec.finish()
+    orc = oracle.reconstruct(plan, images)
+    assert rel_l2(m, orc) < TOL
+    assert fsc(m, orc).min() > 0.999
+
+
+def test_gpu_bitwise_deterministic_and_batch_invariant(tmp_path):
+    star = _dataset(tmp_path, box=32, n_particles=120, n_blobs=12, seed=22, snr=0.3)
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
+    images = load_images(plan)
+    outs = []
+    for _ in range(2):
+        with Reconstructor(plan) as rec:
+            rec.insert(images, plan.params)
+            outs.append(rec.accumulators(0))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    # different device batch sizes and split insert calls: same sums within rounding
+    with Reconstructor(plan, batch=7) as rec:
+        rec.insert(images[:50], plan.params[:50])
+        rec.insert(images[50:], plan.params[50:])
+        v, w = rec.accumulators(0)
+    assert rel_l2(v, outs[0][0]) < 1e-6 and rel_l2(w, outs[0][1]) < 1e-6
+
+
+def test_gpu_device_pointer_input(tmp_path):
+    torch = pytest.importorskip("torch")
+    star = _dataset(tmp_path, box=32, n_particles=40, n_blobs=8, seed=23)
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        host = rec.finish()
+    dev = torch.from_numpy(images).cuda()
+    with Reconstructor(plan) as rec:
+        rec.insert(dev, plan.params)
+        rec.synchronize()
+        devm = rec.finish()
+    assert np.array_equal(host, devm)
+
+
+def test_gpu_half_maps_fsc(tmp_path):
+    star = _dataset(tmp_path, box=32, n_particles=200, n_blobs=12, seed=24, snr=1.0)
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1, nmaps=3))
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        full = rec.finish(0)
+        f = rec.fsc()
+    assert rel_l2(full, oracle.reconstruct(plan, images)) < TOL
+    assert f.shape == (16,) and f[1] > 0.5 and np.all(f <= 1.0 + 1e-9)
+
+
+def test_gpu_rejects_bad_sizes(tmp_path):
+    from bsoft_b200._lib import BsgError
+    star = _dataset(tmp_path, box=16, n_particles=4, n_blobs=2, seed=25)
+    plan = plan_reconstruction(read_project(star), ReconOptions())
+    plan.ft = 48
+    with pytest.raises(BsgError):
+        Reconstructor(plan)
