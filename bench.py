@@ -1,0 +1,352 @@
+"""Benchmark: batched Fourier-space insertion (particles/s).
+
+Workload (one B200): 50,000 float32 256x256 particle images of a 256^3
+blob phantom (400 blobs), micrographs of Poisson(200) particles, per-particle
+defocus U[0.8, 3.5] um with astigmatism U[0, 0.1] um, SNR 0.05, inserted with
+trilinear interpolation and CTF phase flipping (pad 2 -> 512^2 transforms)
+into a 256^3 complex64 map with float32 weights.
+
+A step = one batch of `--batch` particles through the whole hot path: image
+upload (e2e leg only), background + padded 2-D FFT + origin shift + CTF, and
+gridding into the map.  The timed region is `--steps` steps after
+`--warmup` untimed ones.  Inputs are synthetic (seeded); each step's images
+(524 MB for 2,000 particles) are larger than L2.
+
+Legs reported on one JSON line:
+  value       particles/s with images already resident in HBM (CUDA events
+              on the library stream, barrier + synchronize around the region)
+  e2e         particles/s through the C ABI with pinned HOST images: every
+              step uploads its images; the finished map (weigh, 3-D inverse
+              FFT, sinc) is read back at the end of the region
+  roofline    the gridding kernel against measured HBM bandwidth, with the
+              per-particle algorithmic bytes 22 N^2 (Hermitian-half complex64
+              + float32 weight read and written over 0.75 N^2 voxels, plus the
+              4 n^2 image)
+  cpu_baseline  the reference's own breconstruct (compiled from its sources,
+              oracle/_ref) on a bounded sample of the same workload, all host
+              threads
+
+`--impl reference` times only the reference CPU implementation (rank 0).
+Multi-GPU (`torchrun --nproc-per-node N`): each rank reconstructs its own
+shard of particles (weak scaling) and the partial maps are summed with one
+NCCL all-reduce before finishing, as the reference sums per-thread partial
+maps (mg_reconstruct.cpp:306-324).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PARTICLES = 50000
+BOX = 256
+WORKLOAD = "batched-insertion-256"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    self.samples.append([t.strip() for t in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[0]) for s in self.samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 6 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 6 for i in range(4)
+                          if s[2 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_workload(n_particles, rank=0, world=1):
+    from bsoft_b200.synth import batched_insertion_workload
+    w = batched_insertion_workload(n_particles=n_particles, box=BOX, pool=512)
+    # shard: rank r takes particles r, r+world, ... (weak scaling keeps the
+    # per-rank count fixed by generating world x particles)
+    return w
+
+
+def plan_for(w):
+    from bsoft_b200.plan import ReconPlan
+    return ReconPlan(n=BOX, ft=2 * BOX, map=BOX, map_sampling=w["pixel"], hi_res=w["hi_res"], interp=2,
+                     ctf_action=1, wiener=0.0, params=w["params"], nmaps=1)
+
+
+def reference_sample(w, n_sample: int, threads: int):
+    """Time the reference's breconstruct on `n_sample` particles of the
+    workload written as MRC + STAR (writing is not timed)."""
+    import oracle
+    from bsoft_b200.ctf import CTFParams
+    from bsoft_b200.geometry import matrix_to_view
+    from bsoft_b200.io import mrc
+    from bsoft_b200.plan import P_CTF, P_MAT, P_ORIGIN
+    from bsoft_b200.project import Micrograph, Project, write_project
+    exe = oracle.ref_binary("breconstruct")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/breconstruct not built"
+    d = tempfile.mkdtemp(prefix="bench_ref_")
+    P = w["params"][:n_sample]
+    imgs = w["pool"][np.arange(n_sample) % w["pool"].shape[0]]
+    mrc.write_stack(os.path.join(d, "p.mrcs"), imgs, w["pixel"])
+    views = np.array([matrix_to_view(P[i, P_MAT:P_MAT + 9].reshape(3, 3)) for i in range(n_sample)])
+    # defocus from the CTF coefficient (abw20 = -pi lambda def)
+    from bsoft_b200.ctf import electron_wavelength
+    lam = electron_wavelength(200000.0)
+    defocus = P[:, P_CTF + 1] / (-math.pi * lam)
+    proj = Project(base_dir=d)
+    proj.micrographs.append(Micrograph(
+        id="mg1", particle_file="p.mrcs", box_size=BOX, pixel_size=w["pixel"],
+        ctf=CTFParams.from_amp_contrast(200000.0, 2.7e7, 0.07, float(defocus[0])),
+        part_id=np.arange(1, n_sample + 1), origin=np.concatenate([P[:, P_ORIGIN:P_ORIGIN + 2],
+                                                                   np.zeros((n_sample, 1))], 1),
+        view=views, defocus=defocus, magnification=np.ones(n_sample), select=np.ones(n_sample, dtype=np.int64),
+        pixel=np.full(n_sample, w["pixel"])))
+    write_project(os.path.join(d, "p.star"), proj)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, "-interp", "trilinear", "-CTF", "flip", "-threads", str(threads), "-recon",
+                        os.path.join(d, "ref.mrc"), os.path.join(d, "p.star")], cwd=d, env=env,
+                       capture_output=True, text=True)
+    dt = time.perf_counter() - t0
+    if r.returncode != 0:
+        return None, f"breconstruct failed: {r.stderr[-200:]}"
+    return n_sample / dt, f"{n_sample} particles of the workload ({BOX}^2 -> {BOX}^3, trilinear, CTF flip), wall {dt:.1f} s"
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_threads_for_reference():
+    # each reference thread holds a 20 B/voxel partial map (335 MB at 256^3)
+    return max(1, min(cpu_threads(), 32))
+
+
+def run_reference(args):
+    """The reference processes its particle list in one pass, so the timed
+    steps (one particle per thread each) run inside one breconstruct call;
+    the warm-up is a separate small call."""
+    threads = cpu_threads_for_reference()
+    n = threads * args.steps
+    w = make_workload(max(n, 2 * threads))
+    if args.warmup:
+        v, sample = reference_sample(w, 2 * threads, threads)
+        if v is None:
+            print(json.dumps({"impl": "reference", "unavailable": sample}))
+            return
+    value, sample = reference_sample(w, n, threads)
+    if value is None:
+        print(json.dumps({"impl": "reference", "unavailable": sample}))
+        return
+    print(json.dumps({
+        "impl": "reference", "metric": "particles/s (insertion)", "value": value, "unit": "particles/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": N_PARTICLES, "box": BOX, "map": BOX, "ft": 2 * BOX,
+                   "interp": "trilinear", "ctf": "flip"},
+        "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "vs_baseline": None}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=25)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=2000)
+    ap.add_argument("--impl", default="gpu")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from bsoft_b200.recon import Reconstructor
+
+    B = args.batch
+    per_rank = B * (args.warmup + args.steps)
+    w = make_workload(max(per_rank, 2 * B))
+    plan = plan_for(w)
+    P = w["params"]
+    pool = w["pool"]
+    npool = pool.shape[0]
+
+    # two distinct step buffers (each > L2), alternating between steps
+    def step_images(i):
+        idx = (np.arange(B) + i * B) % npool
+        return np.ascontiguousarray(pool[idx])
+
+    host = [torch.from_numpy(step_images(i)).pin_memory() for i in range(2)]
+    dev = [h.cuda() for h in host]
+    stream_of = lambda rec: torch.cuda.ExternalStream(rec.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    # ---- value: device-resident inputs
+    rec = Reconstructor(plan, batch=B, device=local)
+    s = stream_of(rec)
+    for i in range(args.warmup):
+        rec.insert(dev[i % 2], P[i * B:(i + 1) * B])
+    rec.synchronize()
+    rec.set_timing(True)
+    st0 = rec.stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(s)
+        for i in range(args.steps):
+            j = args.warmup + i
+            rec.insert(dev[j % 2], P[j * B:(j + 1) * B])
+        ev1.record(s)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    st1 = rec.stats()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    particles = B * args.steps * world
+    value = particles / (ms / 1e3)
+    launches = st1["launches"] - st0["launches"]
+    ins_launch = st1["insert_launches"] - st0["insert_launches"]
+    ins_ms = st1["insert_ms"] - st0["insert_ms"]
+    fft_ms = st1["fft2d_ms"] - st0["fft2d_ms"]
+    rec.close()
+
+    # ---- e2e: pinned host images through the C ABI, map read back at the end
+    rec = Reconstructor(plan, batch=B, device=local)
+    for i in range(args.warmup):
+        rec.insert(host[i % 2].numpy(), P[i * B:(i + 1) * B])
+    rec.synchronize()
+    rec.reset()
+    out = np.empty((BOX, BOX, BOX), dtype=np.float32)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        j = args.warmup + i
+        rec.insert(host[j % 2].numpy(), P[j * B:(j + 1) * B])
+    if dist is not None:
+        rec.synchronize()
+    rec.finish(0, out=out)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = particles / e2e_s
+    rec.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # roofline of the gridding kernel
+    peak, peak_kind = peaks()
+    per_particle = 22.0 * BOX * BOX
+    avg_launch_ms = ins_ms / max(1, ins_launch)
+    achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
+    roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+            "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
+            "algorithmic_bytes_per_particle": per_particle,
+            "fft2d_ms_per_step": round(fft_ms / args.steps, 3)}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads_for_reference()
+        v, sample = reference_sample(w, max(2 * threads, threads * 8), threads)
+        if v is not None:
+            cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
+        else:
+            cpu = {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
+
+    line = {
+        "metric": "particles/s (insertion)", "value": round(value, 1), "unit": "particles/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": N_PARTICLES, "particles_timed": particles,
+                   "batch_per_step": B, "box": BOX, "map": BOX, "ft": 2 * BOX, "interp": "trilinear",
+                   "ctf": "flip", "l2": "inputs larger than L2 (524 MB per step)", "parallelism": f"dp{world}"},
+        "e2e": {"value": round(e2e, 1), "unit": "particles/s", "h2d_bytes_per_step": B * BOX * BOX * 4,
+                "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps},
+        "roofline": roof, "cpu_baseline": cpu, "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -2,6 +2,7 @@
 // include/bsgpu.h): context lifetime, device memory, the batched insertion
 // pipeline (image upload, 2-D stage, gridding) and map finishing.
 #include "context.cuh"
+#include "fft_dev.cuh"
 
 #include <math.h>
 #include <stdarg.h>
@@ -227,8 +228,9 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     const int n = cfg->n, ft = cfg->ft, N = cfg->map;
     if (n < 2 || !is_pow2(ft) || ft < 32 || ft > 1024 || ft < n)
         return fail(BSG_ERR_ARG, "bsg_recon_create: transform size %d must be a power of two in [32, 1024] and >= box %d", ft, n);
-    if (!is_pow2(N) || N < 8 || N > 512 || N > ft)
-        return fail(BSG_ERR_ARG, "bsg_recon_create: map size %d must be a power of two in [8, 512] and <= %d", N, ft);
+    int radices[16];
+    if ((N & 1) || N < 8 || N > 512 || N > ft || factor_radices(N, radices) < 0)
+        return fail(BSG_ERR_ARG, "bsg_recon_create: map size %d must be even, in [8, 512], <= %d and a product of 2, 3, 5, 7", N, ft);
     if (cfg->interp < 0 || cfg->interp > 2) return fail(BSG_ERR_ARG, "bsg_recon_create: interp %d", cfg->interp);
     if (cfg->nmaps < 1 || cfg->nmaps > 3) return fail(BSG_ERR_ARG, "bsg_recon_create: nmaps %d", cfg->nmaps);
     if (!(cfg->map_sampling > 0) || !(cfg->hi_res > 0)) return fail(BSG_ERR_ARG, "bsg_recon_create: sampling/resolution");
@@ -284,7 +286,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     A((void**)&r->d_rows, sizeof(float2) * (size_t)n * (ft / 2 + 1) * batch);
     A((void**)&r->d_spec, sizeof(float2) * (size_t)ft * ft * batch);
     A((void**)&r->d_tw, sizeof(float2) * std::max(1, ft / 2));
-    A((void**)&r->d_twmap, sizeof(float2) * std::max(1, N / 2));
+    A((void**)&r->d_twmap, sizeof(float2) * N);
     for (int h = 0; h < r->nhalves; ++h) {
         A((void**)&r->d_vol[h], sizeof(float2) * N3);
         A((void**)&r->d_w[h], sizeof(float) * N3);
@@ -294,8 +296,12 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     std::vector<float2> tw;
     host_twiddles(ft, tw);
     cudaError_t e = cudaMemcpy(r->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice);
-    host_twiddles(N, tw);
-    if (e == cudaSuccess) e = cudaMemcpy(r->d_twmap, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice);
+    tw.resize(N);
+    for (int j = 0; j < N; ++j) {
+        const double ang = -2.0 * M_PI * j / N;
+        tw[j] = make_float2((float)cos(ang), (float)sin(ang));
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(r->d_twmap, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = prepare_fft2d_attributes();
     if (e == cudaSuccess) e = prepare_finish_attributes();
     if (e != cudaSuccess) { free_all(r); delete r; return fail(BSG_ERR_CUDA, "bsg_recon_create: %s", cudaGetErrorString(e)); }

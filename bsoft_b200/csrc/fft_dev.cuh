@@ -80,3 +80,79 @@ __device__ __forceinline__ void warp_fft(float2* x, int L, int logL, const float
 }
 
 }  // namespace bsg
+
+namespace bsg {
+
+// Mixed-radix Stockham autosort transform by one warp, for lengths that are
+// not powers of two (maps such as 24^3 or 384^3).  Stage with radix R and
+// running product Ns (Ns = 1 at the start): element j in [0, N/R) loads R
+// values strided N/R, twiddles them by exp(-+2 pi i r (j mod Ns)/(Ns R)),
+// does an R-point DFT and stores them at (j / Ns) Ns R + (j mod Ns) + r Ns.
+// `roots` holds exp(-2 pi i t / N), t < N.  x and y are ping-pong buffers of
+// N values; the result is left in x.
+constexpr int MAXRADIX = 8;
+
+template <bool INVERSE>
+__device__ __forceinline__ float2 root_at(const float2* roots, int t, int N) {
+    t %= N;
+    float2 w = roots[t];
+    if (INVERSE) w.y = -w.y;
+    return w;
+}
+
+template <bool INVERSE>
+__device__ void warp_fft_mixed(float2* x, float2* y, int N, const int* radix, int nstage, const float2* roots) {
+    const int lane = threadIdx.x & 31;
+    float2* src = x;
+    float2* dst = y;
+    int Ns = 1;
+    for (int st = 0; st < nstage; ++st) {
+        const int R = radix[st];
+        const int NR = N / R;
+        for (int j = lane; j < NR; j += 32) {
+            const int k = j % Ns;
+            float2 v[MAXRADIX];
+            const int tstep = (N / (Ns * R)) * k;       // twiddle exponent per r
+            for (int r = 0; r < R; ++r) {
+                float2 a = src[j + r * NR];
+                if (r && k) a = cmul(a, root_at<INVERSE>(roots, r * tstep, N));
+                v[r] = a;
+            }
+            // R-point DFT: out[q] = sum_r v[r] exp(-+2 pi i r q / R)
+            float2 o[MAXRADIX];
+            const int rs = N / R;                       // root index step for exp(-2 pi i / R)
+            for (int q = 0; q < R; ++q) {
+                float2 acc = v[0];
+                for (int r = 1; r < R; ++r) {
+                    const float2 w = root_at<INVERSE>(roots, ((r * q) % R) * rs, N);
+                    const float2 t = cmul(v[r], w);
+                    acc.x += t.x;
+                    acc.y += t.y;
+                }
+                o[q] = acc;
+            }
+            const int base = (j / Ns) * Ns * R + k;
+            for (int r = 0; r < R; ++r) dst[base + r * Ns] = o[r];
+        }
+        __syncwarp();
+        Ns *= R;
+        float2* t = src; src = dst; dst = t;
+    }
+    if (src != x) {
+        for (int i = lane; i < N; i += 32) x[i] = src[i];
+        __syncwarp();
+    }
+}
+
+// Factor n into radices (4 first, then 2, 3, 5, 7).  Returns the number of
+// stages, or -1 if n has a prime factor above 7.
+__host__ __device__ inline int factor_radices(int n, int* radix) {
+    int ns = 0;
+    while (n % 4 == 0) { radix[ns++] = 4; n /= 4; }
+    const int primes[4] = {2, 3, 5, 7};
+    for (int i = 0; i < 4; ++i)
+        while (n % primes[i] == 0) { radix[ns++] = primes[i]; n /= primes[i]; }
+    return n == 1 ? ns : -1;
+}
+
+}  // namespace bsg

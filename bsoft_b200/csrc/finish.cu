@@ -67,21 +67,36 @@ __global__ void weigh_kernel(WeighArgs a) {
     }
 }
 
+// Radix plan of a map edge: power of two -> in-place radix-2/4 DIT on
+// bit-reversed input; otherwise mixed-radix Stockham (needs N scratch).
+struct Radix {
+    int mixed;
+    int nstage;
+    int r[16];
+};
+
 // x-lines: one warp per line, 8 lines per CTA
 constexpr int XW = 8;
-__global__ void __launch_bounds__(XW * 32) fft_x_kernel(float2* data, const float2* tw, int N, int logN) {
+__global__ void __launch_bounds__(XW * 32) fft_x_kernel(float2* data, const float2* tw, int N, int logN, Radix rp) {
     extern __shared__ float2 sm[];
-    float2* stw = sm;
+    float2* stw = sm;                              // N roots
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float2* buf = sm + N / 2 + warp * N;
-    for (int i = threadIdx.x; i < N / 2; i += blockDim.x) stw[i] = tw[i];
+    const int per = rp.mixed ? 2 * N : N;
+    float2* buf = sm + N + warp * per;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = tw[i];
     __syncthreads();
     const size_t line = (size_t)blockIdx.x * XW + warp;
     if (line >= (size_t)N * N) return;
     float2* p = data + line * N;
-    for (int i = lane; i < N; i += 32) buf[bitrev(i, logN)] = p[i];
-    __syncwarp();
-    warp_fft<true>(buf, N, logN, stw);
+    if (rp.mixed) {
+        for (int i = lane; i < N; i += 32) buf[i] = p[i];
+        __syncwarp();
+        warp_fft_mixed<true>(buf, buf + N, N, rp.r, rp.nstage, stw);
+    } else {
+        for (int i = lane; i < N; i += 32) buf[bitrev(i, logN)] = p[i];
+        __syncwarp();
+        warp_fft<true>(buf, N, logN, stw);
+    }
     for (int i = lane; i < N; i += 32) p[i] = buf[i];
 }
 
@@ -95,14 +110,16 @@ struct StridedArgs {
     float* real_out;   // when set: write the real part * scale (* sinc) instead
     float scale;
     int sinc;
+    Radix rp;
 };
 
 __global__ void __launch_bounds__(SW * 32) fft_strided_kernel(StridedArgs a) {
     extern __shared__ float2 sm[];
     const int N = a.N;
-    float2* stw = sm;
-    float2* tile = sm + N / 2;        // SW x N
-    for (int i = threadIdx.x; i < N / 2; i += blockDim.x) stw[i] = a.tw[i];
+    const int per = a.rp.mixed ? 2 * N : N;
+    float2* stw = sm;                 // N roots
+    float2* tile = sm + N;            // SW lines of `per`
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = a.tw[i];
     // blockIdx.x: x-chunk, blockIdx.y: the remaining coordinate (z for axis y, y for axis z)
     const int x0 = blockIdx.x * SW;
     const int other = blockIdx.y;
@@ -113,18 +130,21 @@ __global__ void __launch_bounds__(SW * 32) fft_strided_kernel(StridedArgs a) {
         const int x = x0 + c;
         float2 v = make_float2(0.f, 0.f);
         if (x < N) v = a.data[obase + (size_t)j * stride + x];
-        tile[c * N + bitrev(j, a.logN)] = v;
+        tile[c * per + (a.rp.mixed ? j : (int)bitrev(j, a.logN))] = v;
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5;
-    if (x0 + warp < N) warp_fft<true>(tile + warp * N, N, a.logN, stw);
+    if (x0 + warp < N) {
+        if (a.rp.mixed) warp_fft_mixed<true>(tile + warp * per, tile + warp * per + N, N, a.rp.r, a.rp.nstage, stw);
+        else warp_fft<true>(tile + warp * N, N, a.logN, stw);
+    }
     __syncthreads();
     for (int i = threadIdx.x; i < SW * N; i += blockDim.x) {
         const int c = i % SW, j = i / SW;
         const int x = x0 + c;
         if (x >= N) continue;
         const size_t idx = obase + (size_t)j * stride + x;
-        const float2 v = tile[c * N + j];
+        const float2 v = tile[c * per + j];
         if (a.real_out) {
             float r = v.x * a.scale;
             if (a.sinc) {
@@ -161,19 +181,28 @@ cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+static Radix radix_plan(int N) {
+    Radix rp{};
+    rp.mixed = (N & (N - 1)) != 0;
+    if (rp.mixed) rp.nstage = factor_radices(N, rp.r);
+    return rp;
+}
+
 cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool sinc, cudaStream_t s) {
     const int N = c.g.map, logN = ilog2i(N);
+    const Radix rp = radix_plan(N);
+    const size_t per = rp.mixed ? 2 * (size_t)N : (size_t)N;
     {
         const size_t lines = (size_t)N * N;
-        const size_t smem = sizeof(float2) * ((size_t)N / 2 + (size_t)XW * N);
-        fft_x_kernel<<<(unsigned)((lines + XW - 1) / XW), XW * 32, smem, s>>>(vol, c.d_twmap, N, logN);
+        const size_t smem = sizeof(float2) * ((size_t)N + XW * per);
+        fft_x_kernel<<<(unsigned)((lines + XW - 1) / XW), XW * 32, smem, s>>>(vol, c.d_twmap, N, logN, rp);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    const size_t smem = sizeof(float2) * ((size_t)N / 2 + (size_t)SW * N);
+    const size_t smem = sizeof(float2) * ((size_t)N + SW * per);
     dim3 grid((N + SW - 1) / SW, N);
     StridedArgs a{};
-    a.data = vol; a.tw = c.d_twmap; a.N = N; a.logN = logN;
+    a.data = vol; a.tw = c.d_twmap; a.N = N; a.logN = logN; a.rp = rp;
     a.axis = 1;
     fft_strided_kernel<<<grid, SW * 32, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();
@@ -226,7 +255,7 @@ __global__ void fsc_plane_kernel(const float2* v1, const float2* v2, int N, int 
                 if ((int)floor(sqrt(r2) + 0.5) != r) continue;
                 for (int sgn = 0; sgn < 2; ++sgn) {
                     if (sgn && (hh == 0 || hh == N / 2)) continue;
-                    const int x = (sgn ? -hh : hh) & (N - 1);
+                    const int x = sgn ? (N - hh) % N : hh;
                     const size_t i = ((size_t)z * N + y) * N + x;
                     const float2 a = v1[i], b = v2[i];
                     num += (double)a.x * b.x + (double)a.y * b.y;
@@ -265,10 +294,10 @@ cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream
 
 cudaError_t prepare_finish_attributes() {
     cudaError_t e = cudaFuncSetAttribute(fft_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(sizeof(float2) * (256 + XW * 512)));
+                                         (int)(sizeof(float2) * (512 + XW * 1024)));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(fft_strided_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(float2) * (256 + SW * 512)));
+                                (int)(sizeof(float2) * (512 + SW * 1024)));
 }
 
 }  // namespace bsg

@@ -184,3 +184,54 @@ def write_dataset(outdir: str, spec: DatasetSpec, ph: Phantom, imgs: np.ndarray,
     path = os.path.join(outdir, star_name)
     write_project(path, proj)
     return path
+
+
+def batched_insertion_workload(n_particles: int = 50000, box: int = 256, n_blobs: int = 400, pool: int = 512,
+                               pixel: float = 1.5, snr: float = 0.05, mean_per_micrograph: float = 200.0,
+                               defocus_range=(8000.0, 35000.0), astig_range=(0.0, 1000.0),
+                               volt: float = 200000.0, cs: float = 2.7e7, amp_contrast: float = 0.07,
+                               seed: int = 2):
+    """Synthetic stand-in for a large insertion job: per-particle parameter
+    records (C-ABI layout, see plan.py) for `n_particles` particles grouped
+    into micrographs of Poisson(mean) particles with per-particle defocus and
+    astigmatism, and a pool of `pool` distinct CTF-modulated noisy
+    projections of one blob phantom.  Particle i uses pool image i % pool;
+    the images carry the value distribution of the workload, the records its
+    geometry."""
+    from .plan import (P_BKG, P_CTF, P_MAP, P_MAT, P_ORIGIN, P_PIXEL, P_SCALE, P_WEIGHT, PARTICLE_DOUBLES,
+                       check_resolution)
+    rng = np.random.default_rng(seed)
+    ph = random_phantom(rng, box, n_blobs)
+    views = random_views(rng, n_particles)
+    mats = views_to_matrices(views)
+    origins = box // 2 + rng.uniform(-2.0, 2.0, size=(n_particles, 2))
+    defocus = rng.uniform(*defocus_range, size=n_particles)
+    dev = rng.uniform(*astig_range, size=n_particles)
+    ast = rng.uniform(-math.pi, math.pi, size=n_particles)
+    counts = []
+    left = n_particles
+    while left > 0:
+        c = int(max(1, min(left, rng.poisson(mean_per_micrograph))))
+        counts.append(c)
+        left -= c
+    P = np.zeros((n_particles, PARTICLE_DOUBLES))
+    P[:, P_ORIGIN:P_ORIGIN + 2] = origins
+    P[:, P_BKG:P_BKG + 2] = 0.0
+    P[:, P_MAT:P_MAT + 9] = mats.reshape(n_particles, 9)
+    P[:, P_PIXEL] = pixel
+    P[:, P_SCALE] = 1.0
+    P[:, P_WEIGHT] = 1.0
+    for i in range(n_particles):
+        P[i, P_CTF:P_CTF + 7] = CTFParams.from_amp_contrast(volt, cs, amp_contrast, defocus[i], dev[i],
+                                                            ast[i]).coefficients()
+    P[:, P_MAP] = np.arange(n_particles) % 2
+    pool = min(pool, n_particles)
+    imgs = np.empty((pool, box, box), dtype=np.float32)
+    chunk = 64
+    for s in range(0, pool, chunk):
+        e = min(pool, s + chunk)
+        p = project_blobs(ph, mats[s:e], np.concatenate([origins[s:e], np.zeros((e - s, 1))], 1), box)
+        p = apply_ctf(p, P[s:e, P_CTF:P_CTF + 7], pixel)
+        imgs[s:e] = add_noise(rng, p, snr).astype(np.float32)
+    hi_res = check_resolution(pixel, box, pixel)
+    return dict(params=P, pool=imgs, counts=counts, phantom=ph, hi_res=hi_res, pixel=pixel, box=box)

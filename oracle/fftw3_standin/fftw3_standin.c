@@ -113,27 +113,45 @@ void fftwf_execute_dft(const fftwf_plan p, fftwf_complex* in, fftwf_complex* out
     double* x = (double*)malloc(sizeof(double) * 2 * total);
     if (!x) return;
     for (long i = 0; i < total; ++i) { x[2*i] = in[i][0]; x[2*i+1] = in[i][1]; }
-    /* transform along each axis with the pre-planned 1-D sub-plans */
+    /* transform along each axis with the pre-planned 1-D sub-plans; strided
+     * axes are gathered 16 lines at a time for cache locality, and large
+     * transforms spread their lines over OpenMP threads (FFTW's threaded
+     * planner does the equivalent; nested calls from the reference's own
+     * parallel regions stay single-threaded) */
     for (int d = 0; d < p->rank; ++d) {
         long n = p->n[d];
         if (n < 2) continue;
         long stride = 1;
         for (int e = d + 1; e < p->rank; ++e) stride *= p->n[e];
         long outer = total / (n * stride);
-        double* line = (double*)malloc(sizeof(double) * 2 * n);
-        double* work = (double*)malloc(sizeof(double) * (fft64_work_size(p->sub[d]) + 2));
-        for (long o = 0; o < outer; ++o)
-            for (long s = 0; s < stride; ++s) {
-                double* base = x + 2 * (o * n * stride + s);
-                if (stride == 1) {
-                    fft64_exec_1d(p->sub[d], base, work);
-                    continue;
-                }
-                for (long k = 0; k < n; ++k) { line[2*k] = base[2*k*stride]; line[2*k+1] = base[2*k*stride+1]; }
-                fft64_exec_1d(p->sub[d], line, work);
-                for (long k = 0; k < n; ++k) { base[2*k*stride] = line[2*k]; base[2*k*stride+1] = line[2*k+1]; }
+        const long G = 16;
+        long ngroups = outer * ((stride + G - 1) / G);
+        const fft64_1d* sub = p->sub[d];
+        #pragma omp parallel for schedule(dynamic, 4) if (total >= 65536)
+        for (long gi = 0; gi < ngroups; ++gi) {
+            long o = gi / ((stride + G - 1) / G);
+            long s0 = (gi % ((stride + G - 1) / G)) * G;
+            long cnt = stride - s0 < G ? stride - s0 : G;
+            double* buf = (double*)malloc(sizeof(double) * 2 * n * G);
+            double* work = (double*)malloc(sizeof(double) * (fft64_work_size(sub) + 2));
+            double* base = x + 2 * (o * n * stride + s0);
+            if (stride == 1) {
+                fft64_exec_1d(sub, base, work);
+            } else {
+                for (long k = 0; k < n; ++k)
+                    for (long c = 0; c < cnt; ++c) {
+                        buf[2*(c*n + k)] = base[2*(k*stride + c)];
+                        buf[2*(c*n + k)+1] = base[2*(k*stride + c)+1];
+                    }
+                for (long c = 0; c < cnt; ++c) fft64_exec_1d(sub, buf + 2*c*n, work);
+                for (long k = 0; k < n; ++k)
+                    for (long c = 0; c < cnt; ++c) {
+                        base[2*(k*stride + c)] = buf[2*(c*n + k)];
+                        base[2*(k*stride + c)+1] = buf[2*(c*n + k)+1];
+                    }
             }
-        free(line); free(work);
+            free(buf); free(work);
+        }
     }
     for (long i = 0; i < total; ++i) { out[i][0] = (float)x[2*i]; out[i][1] = (float)x[2*i+1]; }
     free(x);
