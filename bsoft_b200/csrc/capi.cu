@@ -288,9 +288,9 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     A((void**)&r->d_tw, sizeof(float2) * std::max(1, ft / 2));
     A((void**)&r->d_twmap, sizeof(float2) * N);
     for (int h = 0; h < r->nhalves; ++h) {
-        A((void**)&r->d_vol[h], sizeof(float2) * N3);
-        A((void**)&r->d_w[h], sizeof(float) * N3);
-        if (g.fom) { A((void**)&r->d_pow[h], sizeof(float) * N3); A((void**)&r->d_w2[h], sizeof(float) * N3); }
+        A((void**)&r->d_vol[h], sizeof(double2) * N3);
+        A((void**)&r->d_w[h], sizeof(double) * N3);
+        if (g.fom) { A((void**)&r->d_pow[h], sizeof(double) * N3); A((void**)&r->d_w2[h], sizeof(double) * N3); }
     }
     if (rc) { free_all(r); delete r; return rc; }
     std::vector<float2> tw;
@@ -328,11 +328,11 @@ int bsg_recon_reset(bsg_recon* h) {
     CK(cudaSetDevice(r->device));
     const size_t N3 = r->vol_elems();
     for (int i = 0; i < r->nhalves; ++i) {
-        CK(cudaMemsetAsync(r->d_vol[i], 0, sizeof(float2) * N3, r->stream));
-        CK(cudaMemsetAsync(r->d_w[i], 0, sizeof(float) * N3, r->stream));
+        CK(cudaMemsetAsync(r->d_vol[i], 0, sizeof(double2) * N3, r->stream));
+        CK(cudaMemsetAsync(r->d_w[i], 0, sizeof(double) * N3, r->stream));
         if (r->g.fom) {
-            CK(cudaMemsetAsync(r->d_pow[i], 0, sizeof(float) * N3, r->stream));
-            CK(cudaMemsetAsync(r->d_w2[i], 0, sizeof(float) * N3, r->stream));
+            CK(cudaMemsetAsync(r->d_pow[i], 0, sizeof(double) * N3, r->stream));
+            CK(cudaMemsetAsync(r->d_w2[i], 0, sizeof(double) * N3, r->stream));
         }
     }
     return BSG_OK;
@@ -388,14 +388,14 @@ int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int
     return BSG_OK;
 }
 
-int bsg_recon_accumulators(bsg_recon* h, int half, float* vol_out, float* weight_out, int flags) {
+int bsg_recon_accumulators(bsg_recon* h, int half, double* vol_out, double* weight_out, int flags) {
     Recon* r = reinterpret_cast<Recon*>(h);
     if (!r || half < 0 || half >= r->nhalves) return fail(BSG_ERR_ARG, "bsg_recon_accumulators: bad half %d", half);
     CK(cudaSetDevice(r->device));
     const size_t N3 = r->vol_elems();
     const cudaMemcpyKind k = (flags & BSG_DEVICE_PTR) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-    if (vol_out) CK(cudaMemcpyAsync(vol_out, r->d_vol[half], sizeof(float2) * N3, k, r->stream));
-    if (weight_out) CK(cudaMemcpyAsync(weight_out, r->d_w[half], sizeof(float) * N3, k, r->stream));
+    if (vol_out) CK(cudaMemcpyAsync(vol_out, r->d_vol[half], sizeof(double2) * N3, k, r->stream));
+    if (weight_out) CK(cudaMemcpyAsync(weight_out, r->d_w[half], sizeof(double) * N3, k, r->stream));
     CK(cudaStreamSynchronize(r->stream));
     return BSG_OK;
 }

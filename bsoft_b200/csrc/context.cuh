@@ -23,11 +23,13 @@ struct Context {
     float2* d_tw = nullptr;          // ft/2 twiddles exp(-2 pi i j / ft)
     float2* d_twmap = nullptr;       // N/2 twiddles exp(-2 pi i j / N)
 
-    // accumulators per half map, reference index order
-    float2* d_vol[2] = {nullptr, nullptr};
-    float* d_w[2] = {nullptr, nullptr};
-    float* d_pow[2] = {nullptr, nullptr};
-    float* d_w2[2] = {nullptr, nullptr};
+    // accumulators per half map, reference index order, FP64 (each batch's
+    // per-voxel sums are folded in once, so the long reduction over the
+    // whole particle set is carried in double precision)
+    double2* d_vol[2] = {nullptr, nullptr};
+    double* d_w[2] = {nullptr, nullptr};
+    double* d_pow[2] = {nullptr, nullptr};
+    double* d_w2[2] = {nullptr, nullptr};
 
     // finishing buffers (allocated on first use)
     float2* d_work = nullptr;        // N^3 complex

@@ -21,8 +21,8 @@ namespace bsg {
 #define SMALLFLOAT_F 1e-30f
 
 struct WeighArgs {
-    const float2* v0; const float* w0; const float* p0; const float* q0;
-    const float2* v1; const float* w1; const float* p1; const float* q1;   // second half or null
+    const double2* v0; const double* w0; const double* p0; const double* q0;
+    const double2* v1; const double* w1; const double* p1; const double* q1;   // second half or null
     float2* out;      // weighed, centre-shifted complex volume
     float* fom;       // optional SNR map
     int N;
@@ -31,33 +31,33 @@ struct WeighArgs {
 __global__ void weigh_kernel(WeighArgs a) {
     const size_t N = a.N, N3 = N * N * N;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3; i += (size_t)gridDim.x * blockDim.x) {
-        float2 v = a.v0[i];
-        float w = a.w0[i];
-        float p = a.p0 ? a.p0[i] : 0.f, q = a.q0 ? a.q0[i] : 0.f;
+        double2 v = a.v0[i];
+        double w = a.w0[i];
+        double p = a.p0 ? a.p0[i] : 0.0, q = a.q0 ? a.q0[i] : 0.0;
         if (a.v1) {
-            const float2 v1 = a.v1[i];
+            const double2 v1 = a.v1[i];
             v.x += v1.x; v.y += v1.y;
             w += a.w1[i];
             if (a.p1) { p += a.p1[i]; q += a.q1[i]; }
         }
         float2 F = make_float2(0.f, 0.f);
-        if (w > SMALLFLOAT_F) {
+        if (w > 1e-30) {
             q = w - q / w;
-            F = make_float2(v.x / w, v.y / w);
-            if (q > 1.f) p /= q;
-            else if (w > 1.f) p /= w;
-            if (p < 0.f) p = 0.f;
+            F = make_float2((float)(v.x / w), (float)(v.y / w));
+            if (q > 1.0) p /= q;
+            else if (w > 1.0) p /= w;
+            if (p < 0.0) p = 0.0;
         } else {
-            p = 0.f;
-            w = q = SMALLFLOAT_F;
+            p = 0.0;
+            w = q = 1e-30;
         }
         if (a.fom) {
             // fspace_reconstruction_snr on the weighed channels
             const double signal = (double)F.x * F.x + (double)F.y * F.y;
-            double noise = (double)p - signal;
+            double noise = p - signal;
             if (noise < signal) noise = signal;
             float f = 0.f;
-            if (w > 1.f && signal > 1e-30 && noise > 1e-30) f = (float)((w * signal - p) / noise);
+            if (w > 1.0 && signal > 1e-30 && noise > 1e-30) f = (float)((w * signal - p) / noise);
             a.fom[i] = (i == 0) ? 1.f : f;
         }
         // (-1)^(h+k+l): signed and unsigned indices share parity for even N

@@ -41,10 +41,10 @@ struct InsertArgs {
     int interp;
     int gate;                  // 1: test the s^2 window / taper per pixel
     double maxs2, mins2, mscale;
-    float2* vol;
-    float* w;
-    float* pow;
-    float* w2;
+    double2* vol;
+    double* w;
+    double* pow;
+    double* w2;
 };
 
 // Does particle P's plane come within reach of the brick for alias combination
@@ -71,12 +71,28 @@ __device__ __forceinline__ unsigned brick_mask(const DevParticle& P, int x0, int
     return mask;
 }
 
+// Per (voxel, particle) partial sums in float (a handful of terms each)...
 struct Acc {
     float2 v, m;      // voxel and mirror complex sums
     float w, wm;      // weights
     float p, pm;      // power (fom)
     float q, qm;      // weight^2 (fom)
 };
+
+// ... folded into the per-voxel running sums over the batch in double.
+struct AccD {
+    double vx, vy, mx, my, w, wm, p, pm, q, qm;
+};
+
+template <bool FOM>
+__device__ __forceinline__ void fold(AccD& d, const Acc& a, bool mirror) {
+    d.vx += a.v.x; d.vy += a.v.y; d.w += a.w;
+    if (FOM) { d.p += a.p; d.q += a.q; }
+    if (mirror) {
+        d.mx += a.m.x; d.my += a.m.y; d.wm += a.wm;
+        if (FOM) { d.pm += a.pm; d.qm += a.qm; }
+    }
+}
 
 __device__ __forceinline__ float pixel_weight_gate(const InsertArgs& a, const DevParticle& P, int h, int k,
                                                    bool& keep) {
@@ -218,7 +234,7 @@ __device__ __forceinline__ void gather_nearest(const InsertArgs& a, const DevPar
 }
 
 template <bool FOM, bool GATE>
-__global__ void __launch_bounds__(BT) insert_kernel(InsertArgs a) {
+__global__ void __launch_bounds__(BT, 2) insert_kernel(InsertArgs a) {
     const int N = a.N;
     const int tx = threadIdx.x % BX, ty = (threadIdx.x / BX) % BY, tz = threadIdx.x / (BX * BY);
     const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * BZ;
@@ -228,7 +244,7 @@ __global__ void __launch_bounds__(BT) insert_kernel(InsertArgs a) {
 
     __shared__ unsigned s_list[BT];
     __shared__ int s_warp[BT / 32 + 1];
-    Acc acc = {};
+    AccD acc = {};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     for (int base = 0; base < a.np; base += BT) {
@@ -259,27 +275,29 @@ __global__ void __launch_bounds__(BT) insert_kernel(InsertArgs a) {
             if (!valid) continue;
             const DevParticle& P = a.part[pi];
             const float2* S = a.spec + (size_t)pi * a.ft * a.ft;
+            Acc part = {};
             for (int al = 0; al < 8; ++al) {
                 if (!(am & (1u << al))) continue;
                 const float cx = (float)(x - ((al & 1) ? N : 0));
                 const float cy = (float)(y - ((al & 2) ? N : 0));
                 const float cz = (float)(z - ((al & 4) ? N : 0));
-                if (a.interp == 2) gather_trilinear<FOM, GATE>(a, P, S, cx, cy, cz, mirror, acc);
-                else gather_nearest<FOM, GATE>(a, P, S, cx, cy, cz, mirror, a.interp == 1, acc);
+                if (a.interp == 2) gather_trilinear<FOM, GATE>(a, P, S, cx, cy, cz, mirror, part);
+                else gather_nearest<FOM, GATE>(a, P, S, cx, cy, cz, mirror, a.interp == 1, part);
             }
+            fold<FOM>(acc, part, mirror);
         }
         __syncthreads();
     }
     if (!valid) return;
     const size_t idx = ((size_t)z * N + y) * N + x;
-    float2 o = a.vol[idx];
-    a.vol[idx] = make_float2(o.x + acc.v.x, o.y + acc.v.y);
+    double2 o = a.vol[idx];
+    a.vol[idx] = make_double2(o.x + acc.vx, o.y + acc.vy);
     a.w[idx] += acc.w;
     if (FOM) { a.pow[idx] += acc.p; a.w2[idx] += acc.q; }
     if (mirror) {
         const size_t midx = ((size_t)((N - z) % N) * N + (N - y) % N) * N + (N - x) % N;
-        float2 om = a.vol[midx];
-        a.vol[midx] = make_float2(om.x + acc.m.x, om.y + acc.m.y);
+        double2 om = a.vol[midx];
+        a.vol[midx] = make_double2(om.x + acc.mx, om.y + acc.my);
         a.w[midx] += acc.wm;
         if (FOM) { a.pow[midx] += acc.pm; a.w2[midx] += acc.qm; }
     }

@@ -109,8 +109,8 @@ class Reconstructor:
 
     def accumulators(self, half: int = 0):
         N = self.N
-        vol = np.empty((N, N, N, 2), dtype=np.float32)
-        w = np.empty((N, N, N), dtype=np.float32)
+        vol = np.empty((N, N, N, 2), dtype=np.float64)
+        w = np.empty((N, N, N), dtype=np.float64)
         _lib.check(_lib.load().bsg_recon_accumulators(self._h, half, C.c_void_p(vol.ctypes.data),
                                                       C.c_void_p(w.ctypes.data), 0), "bsg_recon_accumulators")
         return vol[..., 0] + 1j * vol[..., 1], w

@@ -105,8 +105,9 @@ int  bsg_recon_insert(bsg_recon* r, const float* images, const double* params,
 int  bsg_recon_finish(bsg_recon* r, int imap, float* map_out, float* fom_out, int flags);
 
 /* Raw accumulators of half h (0/1; 0 when nmaps == 1): complex volume
- * (2*N^3 float32) and weights (N^3 float32), reference index order. */
-int  bsg_recon_accumulators(bsg_recon* r, int half, float* vol_out, float* weight_out, int flags);
+ * (2*N^3 doubles) and weights (N^3 doubles), reference index order (the
+ * accumulators are kept in FP64 on the device). */
+int  bsg_recon_accumulators(bsg_recon* r, int half, double* vol_out, double* weight_out, int flags);
 
 /* Fourier shell correlation of the two weighed half maps (nmaps >= 2):
  * nshell doubles, shell r = round(|frequency|). */

@@ -101,6 +101,9 @@ def test_gpu_bitwise_deterministic_and_batch_invariant(tmp_path):
         rec.insert(images[50:], plan.params[50:])
         v, w = rec.accumulators(0)
     assert rel_l2(v, outs[0][0]) < 1e-6 and rel_l2(w, outs[0][1]) < 1e-6
+    # and the FP64 oracle's accumulators
+    ov, ow, _, _ = oracle.insert(plan, images, plan.params)
+    assert rel_l2(v.reshape(-1), ov.view(np.complex128)) < 1e-6 and rel_l2(w.reshape(-1), ow) < 1e-6
 
 
 def test_gpu_device_pointer_input(tmp_path):
