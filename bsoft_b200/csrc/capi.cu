@@ -4,6 +4,8 @@
 #include "context.cuh"
 #include "fft_dev.cuh"
 
+#include <cudaTypedefs.h>
+
 #include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
@@ -28,6 +30,8 @@ cudaError_t prepare_fft2d_attributes();
 cudaError_t prepare_finish_attributes();
 cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s);
 cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool sinc, cudaStream_t s);
+int tile_edge_for_step(double step);
+cudaError_t prepare_insert_attributes();
 
 struct Timed {
     cudaEvent_t a, b;
@@ -113,6 +117,40 @@ static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
     return false;
 }
 
+// TMA descriptors over the centred spectra buffer: 3-D
+// (h + ft/2 innermost, k + ft/2, particle), 8-byte elements (one complex64),
+// square boxes of 32 and 64 pixels, zero fill outside.
+static int make_spec_maps(Recon* r) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+        q != cudaDriverEntryPointSuccess)
+        return fail(BSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    const int ft = r->g.ft;
+    const cuuint64_t dims[3] = {(cuuint64_t)ft + 2, (cuuint64_t)ft + 1, (cuuint64_t)r->batch};
+    const cuuint64_t strides[2] = {(cuuint64_t)(ft + 2) * 8, (cuuint64_t)(ft + 2) * (ft + 1) * 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const int edges[2] = {32, 64};
+    for (int i = 0; i < 2; ++i) {
+        const cuuint32_t box[3] = {(cuuint32_t)edges[i], (cuuint32_t)edges[i], 1};
+        CUresult e = encode(&r->spec_map[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, r->d_spec, dims, strides, box,
+                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (e != CUDA_SUCCESS) return fail(BSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
+    }
+    return BSG_OK;
+}
+
+// Failures the kernels report through the mapped status word (bounded waits).
+static int check_status(Recon* r) {
+    if (r->h_status && *(volatile int*)r->h_status) {
+        r->broken = true;
+        return fail(BSG_ERR_CUDA, "a gridding kernel gave up waiting for a shared-memory tile; results are invalid");
+    }
+    return BSG_OK;
+}
+
 static int alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) return fail(BSG_ERR_NOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
@@ -130,6 +168,7 @@ static void free_all(Recon* r) {
     }
     F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
     F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc);
+    if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();
     if (r->stream) cudaStreamDestroy(r->stream);
@@ -164,6 +203,12 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
     DevParticle* hp = r->h_partbuf[buf];
     for (long i = 0; i < np; ++i) make_dev_particle(*r, params + i * BSG_PARTICLE_DOUBLES, hp[i]);
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
+    int edge = 32;
+    for (long i = 0; i < np; ++i) {
+        const int e = tile_edge_for_step(hp[i].step);
+        if (e == 0 || e > edge) edge = 64;
+    }
+    r->tile_edge = edge;
     CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->stream));
     return BSG_OK;
 }
@@ -195,10 +240,22 @@ static int process(Recon* r, const float* images, const double* params, long npa
         rc = run_batch_kernels(r, d_img, np, r->d_spec, spectra_out == nullptr);
         if (rc) return rc;
         if (spectra_out) {
-            const size_t bytes = sizeof(float2) * r->spec_elems() * np;
-            float* dst = spectra_out + off * r->spec_elems() * 2;
-            CK(cudaMemcpyAsync(dst, r->d_spec, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                               r->stream));
+            // centred device layout -> the reference's pixel order (the four
+            // quadrants swap places)
+            const int ft = r->g.ft, hf = ft / 2;
+            const size_t sp = sizeof(float2) * r->spec_pitch(), dp = sizeof(float2) * ft;
+            const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+            for (long i = 0; i < np; ++i) {
+                const float2* src = r->d_spec + (size_t)i * r->spec_elems();
+                float2* dst = reinterpret_cast<float2*>(spectra_out) + (size_t)(off + i) * ft * ft;
+                for (int qy = 0; qy < 2; ++qy)
+                    for (int qx = 0; qx < 2; ++qx) {
+                        // reference rows [qy*hf, qy*hf+hf) hold k = qy ? rows - ft : rows
+                        const float2* s0 = src + (size_t)(qy ? 0 : hf) * r->spec_pitch() + (qx ? 0 : hf);
+                        float2* d0 = dst + (size_t)qy * hf * ft + qx * hf;
+                        CK(cudaMemcpy2DAsync(d0, dp, s0, sp, sizeof(float2) * hf, hf, kind, r->stream));
+                    }
+            }
         }
         CK(cudaEventRecord(r->compute_done[buf], r->stream));
     }
@@ -284,7 +341,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     A((void**)&r->d_bkg, sizeof(double) * batch);
     A((void**)&r->d_phase, sizeof(float2) * 2 * ft * (size_t)batch);
     A((void**)&r->d_rows, sizeof(float2) * (size_t)n * (ft / 2 + 1) * batch);
-    A((void**)&r->d_spec, sizeof(float2) * (size_t)ft * ft * batch);
+    A((void**)&r->d_spec, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch);
     A((void**)&r->d_tw, sizeof(float2) * std::max(1, ft / 2));
     A((void**)&r->d_twmap, sizeof(float2) * N);
     for (int h = 0; h < r->nhalves; ++h) {
@@ -292,6 +349,14 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
         A((void**)&r->d_w[h], sizeof(double) * N3);
         if (g.fom) { A((void**)&r->d_pow[h], sizeof(double) * N3); A((void**)&r->d_w2[h], sizeof(double) * N3); }
     }
+    if (!rc && cudaHostAlloc((void**)&r->h_status, sizeof(int), cudaHostAllocMapped) != cudaSuccess)
+        rc = fail(BSG_ERR_NOMEM, "bsg_recon_create: mapped status word");
+    if (!rc && cudaHostGetDevicePointer((void**)&r->d_status, r->h_status, 0) != cudaSuccess)
+        rc = fail(BSG_ERR_CUDA, "bsg_recon_create: status word mapping");
+    if (!rc) *r->h_status = 0;
+    if (!rc && cudaMemset(r->d_spec, 0, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch) != cudaSuccess)
+        rc = fail(BSG_ERR_CUDA, "bsg_recon_create: clearing the spectra buffer");
+    if (!rc) rc = make_spec_maps(r);
     if (rc) { free_all(r); delete r; return rc; }
     std::vector<float2> tw;
     host_twiddles(ft, tw);
@@ -304,6 +369,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     if (e == cudaSuccess) e = cudaMemcpy(r->d_twmap, tw.data(), sizeof(float2) * N, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = prepare_fft2d_attributes();
     if (e == cudaSuccess) e = prepare_finish_attributes();
+    if (e == cudaSuccess) e = prepare_insert_attributes();
     if (e != cudaSuccess) { free_all(r); delete r; return fail(BSG_ERR_CUDA, "bsg_recon_create: %s", cudaGetErrorString(e)); }
     for (int i = 0; i < 2; ++i) {
         cudaEventRecord(r->compute_done[i], r->stream);
@@ -385,7 +451,7 @@ int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int
     if (fom_out) CK(cudaMemcpyAsync(fom_out, r->d_fom, sizeof(float) * N3,
                                     dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, r->stream));
     CK(cudaStreamSynchronize(r->stream));
-    return BSG_OK;
+    return check_status(r);
 }
 
 int bsg_recon_accumulators(bsg_recon* h, int half, double* vol_out, double* weight_out, int flags) {
@@ -443,7 +509,7 @@ int bsg_recon_get_stats(bsg_recon* h, bsg_recon_stats* st) {
     }
     r->timed.clear();
     *st = r->stats;
-    return BSG_OK;
+    return check_status(r);
 }
 
 int bsg_recon_synchronize(bsg_recon* h) {
@@ -452,7 +518,7 @@ int bsg_recon_synchronize(bsg_recon* h) {
     CK(cudaSetDevice(r->device));
     CK(cudaStreamSynchronize(r->copy_stream));
     CK(cudaStreamSynchronize(r->stream));
-    return BSG_OK;
+    return check_status(r);
 }
 
 void* bsg_recon_stream(bsg_recon* h) {

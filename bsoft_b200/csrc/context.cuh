@@ -3,6 +3,8 @@
 
 #include "common.cuh"
 
+#include <cuda.h>
+
 namespace bsg {
 
 struct Context {
@@ -19,7 +21,7 @@ struct Context {
     double* d_bkg = nullptr;         // batch
     float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
     float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms
-    float2* d_spec = nullptr;        // batch x ft x ft: particle spectra
+    float2* d_spec = nullptr;        // batch x (ft+1) x (ft+2): centred, padded particle spectra
     float2* d_tw = nullptr;          // ft/2 twiddles exp(-2 pi i j / ft)
     float2* d_twmap = nullptr;       // N/2 twiddles exp(-2 pi i j / N)
 
@@ -38,6 +40,12 @@ struct Context {
     float2* d_half_weighed[2] = {nullptr, nullptr};
     double* d_fsc = nullptr;         // FSC partial sums
 
+    // TMA descriptors over d_spec for the 32 x 32 and 64 x 64 pixel tiles
+    CUtensorMap spec_map[2];
+    int tile_edge = 32;
+    int* d_status = nullptr;         // device view of h_status (mapped)
+    int* h_status = nullptr;         // kernel-reported failures (bounded waits)
+
     // host staging (pinned)
     DevParticle* h_part = nullptr;
     float* h_stage = nullptr;        // batch x n x n pinned image staging
@@ -46,7 +54,8 @@ struct Context {
     bsg_recon_stats stats{};
     cudaEvent_t ev[8]{};
 
-    size_t spec_elems() const { return (size_t)g.ft * g.ft; }
+    size_t spec_elems() const { return (size_t)(g.ft + 1) * (g.ft + 2); }
+    int spec_pitch() const { return g.ft + 2; }
     size_t vol_elems() const { return (size_t)g.map * g.map * g.map; }
 };
 

@@ -21,7 +21,10 @@
 //                      then the fused epilogue 1/ft * shift * CTF, written for
 //                      the stored column h and its mirror -h (conjugate
 //                      symmetry of a real image's transform), i.e. the full
-//                      ft x ft spectrum in the reference's pixel order.
+//                      ft x ft spectrum, stored centred and padded as
+//                      [k + ft/2][h + ft/2] with row pitch ft + 2 and ft + 1
+//                      rows (the extra row/columns stay zero) so that the
+//                      gridding kernel can fetch pixel tiles with TMA.
 #include "context.cuh"
 #include "fft_dev.cuh"
 
@@ -186,7 +189,9 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
     const DevParticle& P = a.part[b];
     const float2* ex = a.phase + (size_t)b * 2 * ft;
     const float2* ey = ex + ft;
-    float2* out = a.spec + (size_t)b * ft * ft;
+    // centred, padded layout: [k + ft/2][h + ft/2], row pitch ft + 2
+    const int pitch = ft + 2, hf = ft / 2;
+    float2* out = a.spec + (size_t)b * (ft + 1) * pitch;
     const int fm = ft - 1;
     for (int i = threadIdx.x; i < COL_W * ft; i += blockDim.x) {
         const int c = i % COL_W, kk = i / COL_W;
@@ -195,12 +200,13 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
         const int k = sfreq(kk, ft);
         const int h = sfreq(hidx, ft);            // hidx == ft/2 -> -ft/2
         float2 g = cols[c * ft + kk];
-        out[(size_t)kk * ft + hidx] = cmul(g, pixel_factor(a, P, ex, ey, h, k));
+        float2* row = out + (size_t)(k + hf) * pitch + hf;
+        row[h] = cmul(g, pixel_factor(a, P, ex, ey, h, k));
         if (hidx >= 1 && hidx < ft / 2) {
             // F(-h, k) = conj(G(h, -k)) * factor(-h, k)
             float2 gm = cols[c * ft + ((-kk) & fm)];
             gm.y = -gm.y;
-            out[(size_t)kk * ft + (ft - hidx)] = cmul(gm, pixel_factor(a, P, ex, ey, -h, k));
+            row[-h] = cmul(gm, pixel_factor(a, P, ex, ey, -h, k));
         }
     }
 }
