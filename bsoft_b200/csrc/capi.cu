@@ -99,6 +99,9 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
     d.slab = (float)(fabs(d.nrm[0]) + fabs(d.nrm[1]) + fabs(d.nrm[2]));
     d.step = (float)(inv * g.mscale);
     d.inv2 = inv * inv;
+    d.inv_st2 = 1.0 / ((double)d.step * (double)d.step);
+    d.inv_step = 1.0f / d.step;
+    for (int i = 0; i < 3; ++i) d.ib[i] = fabsf(d.bf[i]) > 1e-6f ? 1.0f / d.bf[i] : 0.0f;
     double pw = q[15];
     double pad_ratio = (double)g.ft / (double)g.n;     // mg_reconstruct.cpp:192-199
     if (pad_ratio > 1) { pad_ratio *= pad_ratio * 0.6; pw /= pad_ratio; }

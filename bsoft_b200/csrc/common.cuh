@@ -32,6 +32,9 @@ struct alignas(16) DevParticle {
     double ad[3], bd[3];    // map frequency per unit pixel step: R[:,0]*inv*mscale, R[:,1]*inv*mscale
     double nrm[3];          // unit plane normal R[:,2]
     double inv2;            // (scale/(ft*pixel))^2: s2 per unit pixel^2
+    double inv_st2;         // 1 / step^2: pixel coordinate per unit of ad.c
+    float  ib[3];           // 1 / bf[i] (0 when |bf[i]| <= 1e-6)
+    float  inv_step;        // 1 / step
     float  af[3], bf[3];    // float copies of ad / bd
     float  pw;              // particle weight / (pad_ratio^2 * 0.6)
     float  slab;            // sum |nrm_i|: plane reaches a voxel cube iff |n.c| < slab

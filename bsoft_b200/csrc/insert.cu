@@ -21,15 +21,21 @@
 // separately, which keeps the reference's non-Hermitian edge exact.
 // Planes z = 0 and z = N/2 are their own mirrors and are computed directly.
 //
+// Work decomposition: a thread block owns a 16 x 16 x 4 voxel tile and each
+// thread one z-column of 4 voxels, so the slab of a particle's plane cuts
+// the columns of a warp alike and the lanes stay busy.  Particles whose
+// plane reaches the tile are found by the whole block (256 per round) and
+// compacted in order.
+//
 // Data movement: spectra live in HBM in a centred, padded layout
 // [particle][k + ft/2][h + ft/2] of (ft + 1) x (ft + 2) complex64 values.
-// A thread block owns an 8 x 8 x 4 voxel brick.  Particles whose plane
-// reaches the brick are found by the whole block (256 per round) and
-// compacted in order; for each of them one thread issues a TMA tile load
-// (cp.async.bulk.tensor.3d, no multicast) of the brick's pixel footprint
-// into shared memory, double-buffered on two mbarriers, and all threads
-// gather from shared memory.  Footprints too large for the tile (only for
-// unusual sampling) fall back to direct loads.
+// For each listed particle one thread copies the particle record to shared
+// memory and issues a TMA tile load (cp.async.bulk.tensor.3d, no multicast)
+// of the tile's pixel footprint; a 3-stage ring of full/empty mbarriers
+// lets every warp run ahead independently (no block-wide barrier per
+// particle).  Footprints too large for the tile (only for unusual
+// sampling) fall back to direct loads.  All waits are bounded; a wait that
+// runs out sets a status word the host checks.
 #include "context.cuh"
 
 #include <cuda.h>
@@ -37,10 +43,12 @@
 
 namespace bsg {
 
-constexpr int BX = 8, BY = 8, BZ = 4;
-constexpr int BT = BX * BY * BZ;
+constexpr int BX = 16, BY = 16, BZ = 4;  // voxel tile of one thread block
+constexpr int BT = BX * BY;               // one thread per z-column
+constexpr int NWARPS = BT / 32;
+constexpr int STAGES = 3;                 // TMA ring depth
 constexpr int MAX_ITEMS = 512;            // (particle, alias) work items per round
-constexpr long WAIT_LIMIT = 1L << 26;     // bounded mbarrier waits
+constexpr long WAIT_LIMIT = 1L << 24;     // bounded mbarrier waits (about a second)
 
 struct InsertArgs {
     const float2* spec;        // batch x (ft+1) x (ft+2), centred
@@ -226,14 +234,12 @@ __device__ __forceinline__ void accumulate(const Src& S, int h, int k, float wt,
 
 template <bool FOM, bool GATE>
 __device__ __forceinline__ void gather_trilinear(const InsertArgs& a, const DevParticle& P, const Src& S,
-                                                 float cx, float cy, float cz, bool mirror, Acc& acc) {
+                                                 double cxd, double cyd, double czd, double t, bool mirror,
+                                                 Acc& acc) {
     const int hf = a.ft / 2;
-    const double cxd = cx, cyd = cy, czd = cz;
-    const double t = P.nrm[0] * cxd + P.nrm[1] * cyd + P.nrm[2] * czd;
-    if (fabs(t) >= (double)P.slab) return;
-    const double st2 = (double)P.step * (double)P.step;
-    const double u = (P.ad[0] * cxd + P.ad[1] * cyd + P.ad[2] * czd) / st2;
-    const double v = (P.bd[0] * cxd + P.bd[1] * cyd + P.bd[2] * czd) / st2;
+    // plane coordinates (pixels) of the voxel's projection
+    const double u = (P.ad[0] * cxd + P.ad[1] * cyd + P.ad[2] * czd) * P.inv_st2;
+    const double v = (P.bd[0] * cxd + P.bd[1] * cyd + P.bd[2] * czd) * P.inv_st2;
     const int h0 = (int)rint(u), k0 = (int)rint(v);
     // offsets of pixel (h0, k0) from the voxel in double, then float steps
     const float d0x = (float)(h0 * P.ad[0] + k0 * P.bd[0] - cxd);
@@ -241,14 +247,11 @@ __device__ __forceinline__ void gather_trilinear(const InsertArgs& a, const DevP
     const float d0z = (float)(h0 * P.ad[2] + k0 * P.bd[2] - czd);
     const float ax = P.af[0], ay = P.af[1], az = P.af[2];
     const float bx = P.bf[0], by = P.bf[1], bz = P.bf[2];
-    const float rad = sqrtf(fmaxf(0.f, 3.f - (float)(t * t))) / P.step;
+    const float ibx = P.ib[0], iby = P.ib[1], ibz = P.ib[2];
+    const float rad = sqrtf(fmaxf(0.f, 3.f - (float)(t * t))) * P.inv_step;
     const float uu = (float)(u - h0);
-    int dh0 = (int)ceilf(uu - rad), dh1 = (int)floorf(uu + rad);
-    dh0 = max(dh0, -hf - h0);
-    dh1 = min(dh1, hf - h0);
-    const float ibx = fabsf(bx) > 1e-6f ? 1.f / bx : 0.f;
-    const float iby = fabsf(by) > 1e-6f ? 1.f / by : 0.f;
-    const float ibz = fabsf(bz) > 1e-6f ? 1.f / bz : 0.f;
+    const int dh0 = max((int)ceilf(uu - rad), -hf - h0);
+    const int dh1 = min((int)floorf(uu + rad), hf - h0);
     for (int dh = dh0; dh <= dh1; ++dh) {
         const float ex = fmaf((float)dh, ax, d0x);
         const float ey = fmaf((float)dh, ay, d0y);
@@ -285,15 +288,12 @@ __device__ __forceinline__ void gather_trilinear(const InsertArgs& a, const DevP
 // double m in fspace_2D_interpolate); decisions in double.
 template <bool FOM, bool GATE>
 __device__ __forceinline__ void gather_nearest(const InsertArgs& a, const DevParticle& P, const Src& S,
-                                               double cx, double cy, double cz, bool mirror, bool weighted,
-                                               Acc& acc) {
+                                               double cx, double cy, double cz, double t, bool mirror,
+                                               bool weighted, Acc& acc) {
     const int hf = a.ft / 2;
-    const double t = P.nrm[0] * cx + P.nrm[1] * cy + P.nrm[2] * cz;
-    if (fabs(t) > 0.5 * P.slab + 1e-9) return;
-    const double st2 = (double)P.step * (double)P.step;
-    const double u = (P.ad[0] * cx + P.ad[1] * cy + P.ad[2] * cz) / st2;
-    const double v = (P.bd[0] * cx + P.bd[1] * cy + P.bd[2] * cz) / st2;
-    const double rad = sqrt(fmax(0.0, 0.75 - t * t)) / P.step + 1e-9;
+    const double u = (P.ad[0] * cx + P.ad[1] * cy + P.ad[2] * cz) * P.inv_st2;
+    const double v = (P.bd[0] * cx + P.bd[1] * cy + P.bd[2] * cz) * P.inv_st2;
+    const double rad = sqrt(fmax(0.0, 0.75 - t * t)) * P.inv_step + 1e-9;
     const int hlo = max((int)ceil(u - rad), -hf), hhi = min((int)floor(u + rad), hf);
     const int klo = max((int)ceil(v - rad), -hf), khi = min((int)floor(v + rad), hf);
     for (int h = hlo; h <= hhi; ++h) {
@@ -321,49 +321,89 @@ __device__ __forceinline__ void gather_nearest(const InsertArgs& a, const DevPar
     }
 }
 
+// One particle (alias `al`) against this thread's column of BZ voxels.
 template <bool FOM, bool GATE>
-__device__ __forceinline__ void gather(const InsertArgs& a, const DevParticle& P, const Src& S, int x, int y,
-                                       int z, int al, bool mirror, AccD& acc) {
+__device__ __forceinline__ void gather_column(const InsertArgs& a, const DevParticle& P, const Src& S, int x,
+                                              int y, int z0, int al, AccD* acc) {
     const int N = a.N;
-    const float cx = (float)(x - ((al & 1) ? N : 0));
-    const float cy = (float)(y - ((al & 2) ? N : 0));
-    const float cz = (float)(z - ((al & 4) ? N : 0));
-    Acc part = {};
-    if (a.interp == 2) gather_trilinear<FOM, GATE>(a, P, S, cx, cy, cz, mirror, part);
-    else gather_nearest<FOM, GATE>(a, P, S, cx, cy, cz, mirror, a.interp == 1, part);
-    fold<FOM>(acc, part, mirror);
+    if (x >= N || y >= N) return;
+    const double cx = (double)(x - ((al & 1) ? N : 0));
+    const double cy = (double)(y - ((al & 2) ? N : 0));
+    const double czb = (double)(z0 - ((al & 4) ? N : 0));
+    const double tb = P.nrm[0] * cx + P.nrm[1] * cy + P.nrm[2] * czb;
+    const double reach = a.interp == 2 ? (double)P.slab : 0.5 * P.slab + 1e-9;
+#pragma unroll
+    for (int iz = 0; iz < BZ; ++iz) {
+        const int z = z0 + iz;
+        const double t = tb + P.nrm[2] * iz;
+        if (z > N / 2 || !(fabs(t) < reach || (a.interp != 2 && fabs(t) <= reach))) continue;
+        const bool mirror = z > 0 && z < N / 2;
+        Acc part = {};
+        if (a.interp == 2) gather_trilinear<FOM, GATE>(a, P, S, cx, cy, czb + iz, t, mirror, part);
+        else gather_nearest<FOM, GATE>(a, P, S, cx, cy, czb + iz, t, mirror, a.interp == 1, part);
+        fold<FOM>(acc[iz], part, mirror);
+    }
 }
 
 template <bool FOM, bool GATE, int TW>
-__global__ void __launch_bounds__(BT, 2) insert_kernel(InsertArgs a, const __grid_constant__ CUtensorMap tmap) {
+__global__ void __launch_bounds__(BT, FOM ? 1 : 2) insert_kernel(InsertArgs a, const __grid_constant__ CUtensorMap tmap) {
     const int N = a.N, hf = a.ft / 2;
-    const int tx = threadIdx.x % BX, ty = (threadIdx.x / BX) % BY, tz = threadIdx.x / (BX * BY);
+    const int cxl = threadIdx.x % BX, cyl = threadIdx.x / BX;
     const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * BZ;
-    const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
-    const bool valid = x < N && y < N && z <= N / 2;
-    const bool mirror = valid && z > 0 && z < N / 2;
+    const int x = x0 + cxl, y = y0 + cyl;
     const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
 
-    extern __shared__ __align__(128) float2 s_dyn[];      // 2 x TW x TW pixel tiles
-    float2* const s_tile[2] = {s_dyn, s_dyn + TW * TW};
-    __shared__ __align__(8) uint64_t s_bar[2];
+    extern __shared__ __align__(128) float2 s_dyn[];      // STAGES x TW x TW pixel tiles
+    __shared__ __align__(16) DevParticle s_part[STAGES];
+    __shared__ int s_meta[STAGES][4];                     // c0, r0, fits, particle index
+    __shared__ __align__(8) uint64_t s_full[STAGES];
+    __shared__ __align__(8) uint64_t s_empty[STAGES];
     __shared__ unsigned s_list[BT];
-    __shared__ unsigned short s_item[MAX_ITEMS];     // (list entry << 3) | alias
-    __shared__ int s_warp[BT / 32 + 1];
+    __shared__ unsigned short s_item[MAX_ITEMS];          // (list entry << 3) | alias
+    __shared__ int s_warp[NWARPS + 1];
     __shared__ int s_nitems;
-    __shared__ int s_org[2][3];                      // tile c0, r0, fits
 
     if (threadIdx.x == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int s = 0; s < STAGES; ++s) { mbar_init(&s_full[s], 1); mbar_init(&s_empty[s], NWARPS); }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    uint32_t parity0 = 0u, parity1 = 0u;
-    bool wait_failed = false;
-
-    AccD acc = {};
+    bool failed = false;
+    AccD acc[BZ];
+#pragma unroll
+    for (int i = 0; i < BZ; ++i) acc[i] = AccD{};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    long g = 0;                                           // items started before this round
+
+    // producer step (thread 0): item `it` of this round, global number gi
+    auto produce = [&](int it, long gi, int base) {
+        const int st = (int)(gi % STAGES);
+        const long use = gi / STAGES;
+        if (use >= 1 && !failed && !mbar_wait(&s_empty[st], (uint32_t)((use - 1) & 1))) failed = true;
+        const unsigned item = s_item[it];
+        const int pi = base + (int)(s_list[item >> 3] & 0xffffu);
+        const int al = item & 7;
+        const DevParticle& P = a.part[pi];
+        s_part[st] = P;
+        int hl, hh, kl, kh;
+        brick_footprint(P, x0 - ((al & 1) ? N : 0), y0 - ((al & 2) ? N : 0), z0 - ((al & 4) ? N : 0), hf,
+                        hl, hh, kl, kh);
+        const int c0 = (hl + hf) & ~1;                    // 16-byte aligned x coordinate
+        const int r0 = kl + hf;
+        const bool fits = (hh + hf - c0 < TW) && (kh + hf - r0 < TW);
+        s_meta[st][0] = c0;
+        s_meta[st][1] = r0;
+        s_meta[st][2] = fits ? 1 : 0;
+        s_meta[st][3] = pi;
+        if (fits && !failed) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&s_full[st], (uint32_t)(TW * TW * sizeof(float2)));
+            tma_load_3d(s_dyn + (size_t)st * TW * TW, &tmap, c0, r0, a.p_base + pi, &s_full[st]);
+        } else {
+            if (!fits) s_meta[st][2] = 0;
+            mbar_arrive(&s_full[st]);
+        }
+    };
 
     for (int base = 0; base < a.np; base += BT) {
         const int p = base + threadIdx.x;
@@ -379,15 +419,15 @@ __global__ void __launch_bounds__(BT, 2) insert_kernel(InsertArgs a, const __gri
         __syncthreads();
         if (threadIdx.x == 0) {
             int run = 0;
-            for (int w = 0; w < BT / 32; ++w) { const int c = s_warp[w]; s_warp[w] = run; run += c; }
-            s_warp[BT / 32] = run;
+            for (int w = 0; w < NWARPS; ++w) { const int c = s_warp[w]; s_warp[w] = run; run += c; }
+            s_warp[NWARPS] = run;
         }
         __syncthreads();
         if (mask) s_list[s_warp[warp] + before] = (unsigned)threadIdx.x | (mask << 16);
         __syncthreads();
         if (threadIdx.x == 0) {
             int n = 0;
-            const int cnt = s_warp[BT / 32];
+            const int cnt = s_warp[NWARPS];
             for (int e = 0; e < cnt; ++e) {
                 const unsigned am = s_list[e] >> 16;
                 for (int al = 0; al < 8; ++al)
@@ -403,85 +443,72 @@ __global__ void __launch_bounds__(BT, 2) insert_kernel(InsertArgs a, const __gri
         if (nitems > MAX_ITEMS) {
             // more items than the list holds (not reached for supported
             // sizes): a direct-load pass over this round's entries
-            const int cnt = s_warp[BT / 32];
-            for (int e = 0; e < cnt && valid; ++e) {
+            const int cnt = s_warp[NWARPS];
+            for (int e = 0; e < cnt; ++e) {
                 const unsigned ent = s_list[e];
                 const int pi = base + (int)(ent & 0xffffu);
                 const Src S{nullptr, 0, 0, TW, a.spec + (size_t)(a.p_base + pi) * spec_stride, a.pitch, hf};
                 for (int al = 0; al < 8; ++al)
-                    if ((ent >> (16 + al)) & 1u) gather<FOM, GATE>(a, a.part[pi], S, x, y, z, al, mirror, acc);
+                    if ((ent >> (16 + al)) & 1u) gather_column<FOM, GATE>(a, a.part[pi], S, x, y, z0, al, acc);
             }
             __syncthreads();
             continue;
         }
-        // pipeline over items: tile of item it+1 loads while item it is gathered
-        for (int it = -1; it < nitems; ++it) {
-            const int nb = (it + 1) & 1;
-            if (threadIdx.x == 0 && it + 1 < nitems) {
-                // thread 0 starts the tile load of item it+1 into buffer nb
-                const unsigned item = s_item[it + 1];
-                const int pi = base + (int)(s_list[item >> 3] & 0xffffu);
-                const int al = item & 7;
-                const DevParticle& P = a.part[pi];
-                int hl, hh, kl, kh;
-                brick_footprint(P, x0 - ((al & 1) ? N : 0), y0 - ((al & 2) ? N : 0), z0 - ((al & 4) ? N : 0),
-                                hf, hl, hh, kl, kh);
-                const int c0 = (hl + hf) & ~1;            // 16-byte aligned x coordinate
-                const int r0 = kl + hf;
-                const bool fits = (hh + hf - c0 < TW) && (kh + hf - r0 < TW);
-                s_org[nb][0] = c0;
-                s_org[nb][1] = r0;
-                s_org[nb][2] = fits ? 1 : 0;
-                if (fits) {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    mbar_expect_tx(&s_bar[nb], (uint32_t)(TW * TW * sizeof(float2)));
-                    tma_load_3d(s_tile[nb], &tmap, c0, r0, a.p_base + pi, &s_bar[nb]);
-                } else {
-                    mbar_arrive(&s_bar[nb]);
-                }
+        if (threadIdx.x == 0)
+            for (int j = 0; j < STAGES - 1 && j < nitems; ++j) produce(j, g + j, base);
+        for (int it = 0; it < nitems; ++it) {
+            if (threadIdx.x == 0 && it + STAGES - 1 < nitems) produce(it + STAGES - 1, g + it + STAGES - 1, base);
+            const long gi = g + it;
+            const int st = (int)(gi % STAGES);
+            if (!failed && !mbar_wait(&s_full[st], (uint32_t)((gi / STAGES) & 1))) failed = true;
+            if (!failed) {
+                const DevParticle& P = s_part[st];
+                const int pi = s_meta[st][3];
+                const Src S{s_meta[st][2] ? s_dyn + (size_t)st * TW * TW : nullptr, s_meta[st][0], s_meta[st][1],
+                            TW, a.spec + (size_t)(a.p_base + pi) * spec_stride, a.pitch, hf};
+                gather_column<FOM, GATE>(a, P, S, x, y, z0, s_item[it] & 7, acc);
             }
-            if (it < 0) continue;
-            const int b = it & 1;
-            const uint32_t par = b ? parity1 : parity0;
-            if (!wait_failed && !mbar_wait(&s_bar[b], par)) wait_failed = true;
-            if (b) parity1 ^= 1u; else parity0 ^= 1u;
-            if (valid && !wait_failed) {
-                const unsigned item = s_item[it];
-                const int pi = base + (int)(s_list[item >> 3] & 0xffffu);
-                const Src S{s_org[b][2] ? s_tile[b] : nullptr, s_org[b][0], s_org[b][1], TW,
-                            a.spec + (size_t)(a.p_base + pi) * spec_stride, a.pitch, hf};
-                gather<FOM, GATE>(a, a.part[pi], S, x, y, z, item & 7, mirror, acc);
-            }
-            __syncthreads();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s_empty[st]);
         }
+        g += nitems;
+        __syncthreads();
     }
-    if (wait_failed) {
-        // a tile never arrived: report it, and give any copy still in flight
-        // a bounded chance to land before the block's shared memory is released
+    if (failed) {
+        // a tile never arrived: report it and give copies still in flight a
+        // bounded chance to land before the block's shared memory is released
         if (threadIdx.x == 0) atomicExch(a.status, 1);
-        mbar_wait(&s_bar[0], parity0);
-        mbar_wait(&s_bar[1], parity1);
+        for (int s = 0; s < STAGES; ++s) {
+            const long last = g - 1 - ((g - 1 - s) % STAGES + STAGES) % STAGES;   // last item on stage s
+            if (g > 0 && last >= 0) mbar_wait(&s_full[s], (uint32_t)((last / STAGES) & 1));
+        }
         return;
     }
-    if (!valid) return;
-    const size_t idx = ((size_t)z * N + y) * N + x;
-    double2 o = a.vol[idx];
-    a.vol[idx] = make_double2(o.x + acc.vx, o.y + acc.vy);
-    a.w[idx] += acc.w;
-    if (FOM) { a.pow[idx] += acc.p; a.w2[idx] += acc.q; }
-    if (mirror) {
-        const size_t midx = ((size_t)((N - z) % N) * N + (N - y) % N) * N + (N - x) % N;
-        double2 om = a.vol[midx];
-        a.vol[midx] = make_double2(om.x + acc.mx, om.y + acc.my);
-        a.w[midx] += acc.wm;
-        if (FOM) { a.pow[midx] += acc.pm; a.w2[midx] += acc.qm; }
+    if (x >= N || y >= N) return;
+#pragma unroll
+    for (int iz = 0; iz < BZ; ++iz) {
+        const int z = z0 + iz;
+        if (z > N / 2) break;
+        const AccD& c = acc[iz];
+        const size_t idx = ((size_t)z * N + y) * N + x;
+        double2 o = a.vol[idx];
+        a.vol[idx] = make_double2(o.x + c.vx, o.y + c.vy);
+        a.w[idx] += c.w;
+        if (FOM) { a.pow[idx] += c.p; a.w2[idx] += c.q; }
+        if (z > 0 && z < N / 2) {
+            const size_t midx = ((size_t)((N - z) % N) * N + (N - y) % N) * N + (N - x) % N;
+            double2 om = a.vol[midx];
+            a.vol[midx] = make_double2(om.x + c.mx, om.y + c.my);
+            a.w[midx] += c.wm;
+            if (FOM) { a.pow[midx] += c.pm; a.w2[midx] += c.qm; }
+        }
     }
 }
 
 template <int TW>
 static cudaError_t launch_tw(const InsertArgs& a, const CUtensorMap& map, bool fom, bool gate, dim3 grid,
                              cudaStream_t s) {
-    const size_t smem = 2 * sizeof(float2) * TW * TW;
+    const size_t smem = STAGES * sizeof(float2) * TW * TW;
     if (fom) {
         if (gate) insert_kernel<true, true, TW><<<grid, BT, smem, s>>>(a, map);
         else insert_kernel<true, false, TW><<<grid, BT, smem, s>>>(a, map);
@@ -494,7 +521,7 @@ static cudaError_t launch_tw(const InsertArgs& a, const CUtensorMap& map, bool f
 
 template <int TW>
 static cudaError_t set_smem_tw() {
-    const int smem = (int)(2 * sizeof(float2) * TW * TW);
+    const int smem = (int)(STAGES * sizeof(float2) * TW * TW);
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(insert_kernel<true, true, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(insert_kernel<true, false, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
@@ -508,8 +535,8 @@ cudaError_t prepare_insert_attributes() {
     return set_smem_tw<64>();
 }
 
-// Edge of the square pixel tile that always holds a brick's footprint at
-// this voxels-per-pixel step (brick_footprint with the widest orientation).
+// Edge of the square pixel tile that always holds a voxel tile's footprint
+// at this voxels-per-pixel step (brick_footprint, widest orientation).
 int tile_edge_for_step(double step) {
     const double E = sqrt(pow(0.5 * (BX - 1) + 1.0, 2) + pow(0.5 * (BY - 1) + 1.0, 2) + pow(0.5 * (BZ - 1) + 1.0, 2));
     const int need = (int)ceil(2.0 * E / step) + 4;      // +2 rounding, +1 alignment, +1 inclusive
