@@ -4,7 +4,6 @@
 #include "context.cuh"
 #include "fft_dev.cuh"
 
-#include <cudaTypedefs.h>
 
 #include <math.h>
 #include <stdarg.h>
@@ -120,31 +119,6 @@ static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
     return false;
 }
 
-// TMA descriptors over the centred spectra buffer: 3-D
-// (h + ft/2 innermost, k + ft/2, particle), 8-byte elements (one complex64),
-// square boxes of 32 and 64 pixels, zero fill outside.
-static int make_spec_maps(Recon* r) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
-        q != cudaDriverEntryPointSuccess)
-        return fail(BSG_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-    auto encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-    const int ft = r->g.ft;
-    const cuuint64_t dims[3] = {(cuuint64_t)ft + 2, (cuuint64_t)ft + 1, (cuuint64_t)r->batch};
-    const cuuint64_t strides[2] = {(cuuint64_t)(ft + 2) * 8, (cuuint64_t)(ft + 2) * (ft + 1) * 8};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const int edges[2] = {32, 64};
-    for (int i = 0; i < 2; ++i) {
-        const cuuint32_t box[3] = {(cuuint32_t)edges[i], (cuuint32_t)edges[i], 1};
-        CUresult e = encode(&r->spec_map[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, r->d_spec, dims, strides, box,
-                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (e != CUDA_SUCCESS) return fail(BSG_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
-    }
-    return BSG_OK;
-}
-
 // Failures the kernels report through the mapped status word (bounded waits).
 static int check_status(Recon* r) {
     if (r->h_status && *(volatile int*)r->h_status) {
@@ -170,7 +144,7 @@ static void free_all(Recon* r) {
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
     F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
-    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();
@@ -182,6 +156,7 @@ static int run_batch_kernels(Recon* r, const float* d_img, long np, float2* spec
     cudaStream_t s = r->stream;
     cudaEvent_t a = nullptr, b = nullptr;
     if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
+    CK(cudaMemsetAsync(r->d_fmax, 0, sizeof(unsigned), s));
     CK(launch_background(*r, d_img, (int)np, s));
     CK(launch_rows(*r, d_img, (int)np, s));
     CK(launch_cols(*r, (int)np, spec_out, s));
@@ -206,12 +181,15 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
     DevParticle* hp = r->h_partbuf[buf];
     for (long i = 0; i < np; ++i) make_dev_particle(*r, params + i * BSG_PARTICLE_DOUBLES, hp[i]);
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
-    int edge = 32;
-    for (long i = 0; i < np; ++i) {
-        const int e = tile_edge_for_step(hp[i].step);
-        if (e == 0 || e > edge) edge = 64;
-    }
-    r->tile_edge = edge;
+    // fixed-point range of the gridding sums: the largest particle weight
+    // and the most contributions one voxel can take from one batch (at most
+    // (2/step + 1)^2 pixels per plane crossing, up to 4 wrap-around aliases)
+    float pwm = 0.f, smin = 1e30f;
+    for (long i = 0; i < np; ++i) { pwm = std::max(pwm, hp[i].pw); smin = std::min(smin, hp[i].step); }
+    r->pw_max = pwm;
+    const double per = 4.0 * pow(2.0 / std::max(1e-3f, smin) + 1.0, 2.0);
+    const int need = (int)ceil(log2((double)np * per + 1.0));
+    r->fix_bits = std::max(20, std::min(44, 62 - need));
     CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->stream));
     return BSG_OK;
 }
@@ -359,7 +337,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     if (!rc) *r->h_status = 0;
     if (!rc && cudaMemset(r->d_spec, 0, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch) != cudaSuccess)
         rc = fail(BSG_ERR_CUDA, "bsg_recon_create: clearing the spectra buffer");
-    if (!rc) rc = make_spec_maps(r);
+    if (!rc) rc = alloc((void**)&r->d_fmax, sizeof(unsigned));
     if (rc) { free_all(r); delete r; return rc; }
     std::vector<float2> tw;
     host_twiddles(ft, tw);

@@ -40,9 +40,10 @@ struct Context {
     float2* d_half_weighed[2] = {nullptr, nullptr};
     double* d_fsc = nullptr;         // FSC partial sums
 
-    // TMA descriptors over d_spec for the 32 x 32 and 64 x 64 pixel tiles
-    CUtensorMap spec_map[2];
-    int tile_edge = 32;
+    // batch statistics for the fixed-point gridding sums
+    unsigned* d_fmax = nullptr;      // max |Re F|, |Im F| of the batch (float bits)
+    float pw_max = 0.f;              // max particle weight of the batch
+    int fix_bits = 44;               // largest |F w| maps below 2^fix_bits
     int* d_status = nullptr;         // device view of h_status (mapped)
     int* h_status = nullptr;         // kernel-reported failures (bounded waits)
 
