@@ -7,31 +7,36 @@
 // (trilinear) voxels around m, with index wrap-around, on a full complex
 // N^3 map, plus w to the weight map (and w |F|^2, w^2 to the FOM channels).
 //
-// Here a thread block owns a 16 x 16 x 4 tile of the map and keeps its sums
-// in shared memory for the whole batch.  Particles whose plane (or one of
-// its wrap-around aliases) reaches the tile are found by the block, 256 at a
-// time, and compacted in order; the warps then walk those particles' pixel
-// footprints row by row (lanes along h, so spectrum reads are coalesced) and
-// add each pixel's contributions to the tile.
+// Decomposition: one warp owns one 8 x 8 x 8 tile of the map and keeps its
+// sums in shared memory (float), folding them into the FP64 accumulators
+// in HBM every FOLD particles.  Nothing else writes the tile, so there are
+// no atomics and no block-wide barriers.  The warp tests 32 particles at a
+// time against its tile (plane slab and reach, per wrap-around alias) and
+// walks the pixels of each particle that reaches it, in particle order.
 //
-// Determinism: the shared sums are 64-bit fixed point.  Each contribution
-// is the float product F * w exactly as computed, scaled by a power of two
-// chosen per batch so that the largest possible |F * w| is below 2^44, and
-// added with an integer atomic.  Integer addition is associative, so every
-// schedule gives bitwise the same sums; the quantum (2^-44 of the batch's
-// largest term) is far below float resolution.  At the end of the batch the
-// tile is converted to double and added to the FP64 accumulators in HBM
-// (each voxel belongs to exactly one block).
+// Conflict-free lanes: the pixels of a particle's footprint are visited on
+// a lattice of spacing L = ceil(sqrt(3)/step) pixels (step = voxels per
+// pixel), L^2 phases one after another.  Two lattice points are at least
+// sqrt(3) voxels apart in the map, so their base voxels floor(m) differ in
+// some axis, and for any one corner offset the lanes of a warp touch
+// distinct voxels: a plain read-modify-write of shared memory is exact.
+// The order of every voxel's sum (particle, alias, phase, lattice point,
+// corner) is fixed, so results are bitwise reproducible.
+//
+// Each phase's lattice points are enumerated exactly: lane j computes the
+// h-interval of lattice row j from the three slab constraints of the tile
+// box, a warp scan turns the row counts into offsets, and lanes take points
+// in order.
 #include "context.cuh"
 
 #include <math.h>
 
 namespace bsg {
 
-constexpr int TX = 16, TY = 16, TZ = 4;   // map tile of one thread block
-constexpr int TV = TX * TY * TZ;          // voxels per tile
-constexpr int NT = 256;                   // threads per block
-constexpr int NWARPS = NT / 32;
+constexpr int T = 8;                      // tile edge (voxels)
+constexpr int TV = T * T * T;             // voxels per tile
+constexpr int WARPS = 4;                  // warps (tiles) per block
+constexpr int FOLD = 128;                 // particles between folds into FP64
 
 struct InsertArgs {
     const float2* spec;        // batch x (ft+1) x (ft+2), centred
@@ -40,11 +45,9 @@ struct InsertArgs {
     int np;
     int half;                  // only particles of this half map (-1: all)
     int N, ft, pitch;
+    int ntx;                   // tiles per axis
     int interp;
     double maxs2, mins2, mscale;
-    const unsigned* fmax_bits; // batch max of |Re F|, |Im F| (float bits)
-    float pw_max;              // batch max particle weight
-    int fix_bits;              // largest |F w| maps below 2^fix_bits
     double2* vol;
     double* w;
     double* pow;
@@ -55,19 +58,19 @@ struct InsertArgs {
 // combination a (bit i set: axis i shifted by -N)?  Bitmask over the 8.
 __device__ __forceinline__ unsigned tile_mask(const DevParticle& P, int x0, int y0, int z0, int N, int ft) {
     unsigned mask = 0;
-    const float ex = 0.5f * (TX - 1), ey = 0.5f * (TY - 1), ez = 0.5f * (TZ - 1);
+    const float e = 0.5f * (T - 1);
     const float hf = 0.5f * ft;
     const float rx = hf * (fabsf(P.af[0]) + fabsf(P.bf[0])) + 1.0f;
     const float ry = hf * (fabsf(P.af[1]) + fabsf(P.bf[1])) + 1.0f;
     const float rz = hf * (fabsf(P.af[2]) + fabsf(P.bf[2])) + 1.0f;
     const float n0 = (float)P.nrm[0], n1 = (float)P.nrm[1], n2 = (float)P.nrm[2];
-    const float slack = P.slab + fabsf(n0) * ex + fabsf(n1) * ey + fabsf(n2) * ez + 1e-3f;
+    const float slack = P.slab + (fabsf(n0) + fabsf(n1) + fabsf(n2)) * e + 1e-3f;
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
-        const float cx = x0 - ((a & 1) ? N : 0) + ex;
-        const float cy = y0 - ((a & 2) ? N : 0) + ey;
-        const float cz = z0 - ((a & 4) ? N : 0) + ez;
-        if (fabsf(cx) - ex > rx || fabsf(cy) - ey > ry || fabsf(cz) - ez > rz) continue;
+        const float cx = x0 - ((a & 1) ? N : 0) + e;
+        const float cy = y0 - ((a & 2) ? N : 0) + e;
+        const float cz = z0 - ((a & 4) ? N : 0) + e;
+        if (fabsf(cx) - e > rx || fabsf(cy) - e > ry || fabsf(cz) - e > rz) continue;
         if (fabsf(n0 * cx + n1 * cy + n2 * cz) > slack) continue;
         mask |= 1u << a;
     }
@@ -85,38 +88,92 @@ __device__ __forceinline__ float pixel_weight_gate(const InsertArgs& a, const De
     return d < 1.0 ? (float)sqrt(d > 0 ? d : 0.0) : 1.0f;
 }
 
-struct Tile {
-    unsigned long long* re;
-    unsigned long long* im;
-    unsigned long long* w;
-    unsigned long long* p;
-    unsigned long long* q;
-    float sF, sW, sP, sQ;      // fixed-point scales (powers of two)
+struct TileAcc {
+    float* re;
+    float* im;
+    float* w;
+    float* p;
+    float* q;
 };
 
 template <bool FOM>
-__device__ __forceinline__ void add_voxel(const Tile& T, int idx, float2 f, float w) {
-    atomicAdd(T.re + idx, (unsigned long long)__float2ll_rn(f.x * w * T.sF));
-    atomicAdd(T.im + idx, (unsigned long long)__float2ll_rn(f.y * w * T.sF));
-    atomicAdd(T.w + idx, (unsigned long long)__float2ll_rn(w * T.sW));
+__device__ __forceinline__ void add_voxel(const TileAcc& A, int i, float2 f, float w) {
+    A.re[i] = fmaf(f.x, w, A.re[i]);
+    A.im[i] = fmaf(f.y, w, A.im[i]);
+    A.w[i] += w;
     if (FOM) {
-        atomicAdd(T.p + idx, (unsigned long long)__float2ll_rn(w * (f.x * f.x + f.y * f.y) * T.sP));
-        atomicAdd(T.q + idx, (unsigned long long)__float2ll_rn(w * w * T.sQ));
+        A.p[i] = fmaf(w, f.x * f.x + f.y * f.y, A.p[i]);
+        A.q[i] = fmaf(w, w, A.q[i]);
     }
 }
 
-// Walk the pixels of one particle whose contributions reach the tile (alias
-// origin ox, oy, oz): warp `warp` takes pixel rows k = k_lo + warp,
-// + NWARPS, ...; lanes step along h.
+// One pixel (h, k) of particle P against the tile at alias origin o.  All
+// lanes of the warp call this together (`act` false for idle lanes); the
+// __syncwarp after each corner orders the shared-memory updates of
+// different corner offsets, which may touch the same voxel from different
+// lanes.
+template <bool FOM, bool GATE>
+__device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P, const float2* S, const TileAcc& A,
+                                      double ox, double oy, double oz, int h, int k, bool act) {
+    const int hf = a.ft / 2;
+    float wt = P.pw;
+    if (GATE && act) {
+        bool keep;
+        const float tw = pixel_weight_gate(a, P, h, k, keep);
+        if (!keep) act = false;
+        wt *= tw;
+    }
+    // map frequency relative to the tile origin, in double as the reference
+    // forms it
+    const double mx = h * P.ad[0] + k * P.bd[0] - ox;
+    const double my = h * P.ad[1] + k * P.bd[1] - oy;
+    const double mz = h * P.ad[2] + k * P.bd[2] - oz;
+    const float2 f = act ? __ldg(S + (size_t)(k + hf) * a.pitch + (h + hf)) : make_float2(0.f, 0.f);
+    if (a.interp != 2) {
+        const double fx = floor(mx + 0.5), fy = floor(my + 0.5), fz = floor(mz + 0.5);
+        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+        float w = wt;
+        if (a.interp == 1) {
+            const double dx = mx - fx, dy = my - fy, dz = mz - fz;
+            w = (float)((double)wt * (1.0 - sqrt(dx * dx + dy * dy + dz * dz)));
+        }
+        if (act && (unsigned)ix < T && (unsigned)iy < T && (unsigned)iz < T && w > 0.f)
+            add_voxel<FOM>(A, (iz * T + iy) * T + ix, f, w);
+        __syncwarp();
+        return;
+    }
+    const double flx = floor(mx), fly = floor(my), flz = floor(mz);
+    const int ix = (int)flx, iy = (int)fly, iz = (int)flz;
+    const float rx = (float)(mx - flx), ry = (float)(my - fly), rz = (float)(mz - flz);
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz) {
+        const int z = iz + dz;
+        const float wz = dz ? rz : 1.f - rz;
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+            const int y = iy + dy;
+            const float wyz = (dy ? ry : 1.f - ry) * wz * wt;
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = ix + dx;
+                if (act && (unsigned)x < T && (unsigned)y < T && (unsigned)z < T)
+                    add_voxel<FOM>(A, (z * T + y) * T + x, f, (dx ? rx : 1.f - rx) * wyz);
+                __syncwarp();
+            }
+        }
+    }
+}
+
+// Walk the pixels of particle P (alias origin o) whose contributions can
+// reach the tile, phase by phase of the lattice.
 template <bool FOM, bool GATE>
 __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevParticle& P, const float2* S,
-                                                 const Tile& T, double ox, double oy, double oz, int warp,
-                                                 int lane) {
+                                                 const TileAcc& A, double ox, double oy, double oz, int lane,
+                                                 int* s_row) {
     const int hf = a.ft / 2;
-    // open box of map frequencies that touch the tile (tent support 1 voxel)
+    // open box of map frequencies whose tent touches the tile
     const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
-    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
-    // pixel bounding box: the box projected on the plane's two axes
+    const double hi[3] = {ox + T, oy + T, oz + T};
     double vc = 0, hv = 0, uc = 0, hu = 0;
     for (int i = 0; i < 3; ++i) {
         const double c = 0.5 * (lo[i] + hi[i]), e = 0.5 * (hi[i] - lo[i]);
@@ -125,176 +182,149 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     }
     vc *= P.inv_st2; hv *= P.inv_st2; uc *= P.inv_st2; hu *= P.inv_st2;
     const int k_lo = max((int)ceil(vc - hv), -hf), k_hi = min((int)floor(vc + hv), hf - 1);
-    const int hb_lo = max((int)ceil(uc - hu), -hf), hb_hi = min((int)floor(uc + hu), hf - 1);
-    const bool nearest = a.interp != 2;
-    for (int k = k_lo + warp; k <= k_hi; k += NWARPS) {
-        // h interval of row k: lo_i < h ad_i + k bd_i < hi_i on every axis
-        double hl = hb_lo, hh = hb_hi;
-        bool empty = false;
-        for (int i = 0; i < 3; ++i) {
-            const double base = k * P.bd[i];
-            if (fabs(P.ad[i]) > 1e-12) {
-                double p0 = (lo[i] - base) / P.ad[i], p1 = (hi[i] - base) / P.ad[i];
-                if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
-                hl = fmax(hl, ceil(p0));
-                hh = fmin(hh, floor(p1));
-            } else if (!(base > lo[i] && base < hi[i])) {
-                empty = true;
-            }
-        }
-        if (empty || hl > hh) continue;
-        const int h_lo = (int)hl, h_hi = (int)hh;
-        const float2* row = S + (size_t)(k + hf) * a.pitch + hf;
-        for (int h = h_lo + lane; h <= h_hi; h += 32) {
-            float wt = P.pw;
-            if (GATE) {
-                bool keep;
-                const float tw = pixel_weight_gate(a, P, h, k, keep);
-                if (!keep) continue;
-                wt *= tw;
-            }
-            const float2 f = __ldg(row + h);
-            // map frequency relative to the tile origin, in double as the
-            // reference forms it
-            const double mx = h * P.ad[0] + k * P.bd[0] - ox;
-            const double my = h * P.ad[1] + k * P.bd[1] - oy;
-            const double mz = h * P.ad[2] + k * P.bd[2] - oz;
-            if (nearest) {
-                const double fx = floor(mx + 0.5), fy = floor(my + 0.5), fz = floor(mz + 0.5);
-                const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
-                if (ix < 0 || ix >= TX || iy < 0 || iy >= TY || iz < 0 || iz >= TZ) continue;
-                float w = wt;
-                if (a.interp == 1) {
-                    const double dx = mx - fx, dy = my - fy, dz = mz - fz;
-                    w = (float)((double)wt * (1.0 - sqrt(dx * dx + dy * dy + dz * dz)));
-                }
-                if (!(w > 0.f)) continue;
-                add_voxel<FOM>(T, (iz * TY + iy) * TX + ix, f, w);
-                continue;
-            }
-            const double flx = floor(mx), fly = floor(my), flz = floor(mz);
-            const int ix = (int)flx, iy = (int)fly, iz = (int)flz;
-            const float rx = (float)(mx - flx), ry = (float)(my - fly), rz = (float)(mz - flz);
-            const float wx[2] = {1.f - rx, rx}, wy[2] = {1.f - ry, ry}, wz[2] = {1.f - rz, rz};
-#pragma unroll
-            for (int dz = 0; dz < 2; ++dz) {
-                const int z = iz + dz;
-                if (z < 0 || z >= TZ) continue;
-#pragma unroll
-                for (int dy = 0; dy < 2; ++dy) {
-                    const int y = iy + dy;
-                    if (y < 0 || y >= TY) continue;
-                    const float wyz = wy[dy] * wz[dz] * wt;
-#pragma unroll
-                    for (int dx = 0; dx < 2; ++dx) {
-                        const int x = ix + dx;
-                        if (x < 0 || x >= TX) continue;
-                        add_voxel<FOM>(T, (z * TY + y) * TX + x, f, wx[dx] * wyz);
+    const int h_lo = max((int)ceil(uc - hu), -hf), h_hi = min((int)floor(uc + hu), hf - 1);
+    if (k_lo > k_hi || h_lo > h_hi) return;
+    // lattice spacing: points L apart are >= sqrt(3) voxels apart
+    const int L = max(1, (int)ceilf(1.7320508f * P.inv_step));
+    // per-axis 1 / ad (0 when the axis does not vary along h)
+    double ia[3];
+    for (int i = 0; i < 3; ++i) ia[i] = fabs(P.ad[i]) > 1e-12 ? 1.0 / P.ad[i] : 0.0;
+    for (int pk = 0; pk < L; ++pk) {
+        const int k0 = k_lo + pk;
+        if (k0 > k_hi) break;
+        const int nrows = (k_hi - k0) / L + 1;
+        for (int ph = 0; ph < L; ++ph) {
+            const int h0 = h_lo + ph;
+            if (h0 > h_hi) break;
+            for (int jb = 0; jb < nrows; jb += 32) {
+                // lane j: exact lattice range of row k = k0 + L (jb + j)
+                const int j = jb + lane;
+                int istart = 0, cnt = 0, k = 0;
+                if (j < nrows) {
+                    k = k0 + L * j;
+                    double hl = h0, hh = h_hi;
+                    bool empty = false;
+                    for (int i = 0; i < 3; ++i) {
+                        const double base = k * P.bd[i];
+                        if (ia[i] != 0.0) {
+                            double p0 = (lo[i] - base) * ia[i], p1 = (hi[i] - base) * ia[i];
+                            if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
+                            hl = fmax(hl, p0);
+                            hh = fmin(hh, p1);
+                        } else if (!(base > lo[i] && base < hi[i])) {
+                            empty = true;
+                        }
+                    }
+                    if (!empty && hl <= hh) {
+                        // lattice h = h0 + L i inside [hl, hh]
+                        const int i0 = (int)ceil((hl - h0) / L), i1 = (int)floor((hh - h0) / L);
+                        if (i1 >= i0) { istart = i0; cnt = i1 - i0 + 1; }
                     }
                 }
+                // exclusive scan of the row counts
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                s_row[lane] = incl;                        // inclusive end of row j
+                s_row[32 + lane] = istart;
+                s_row[64 + lane] = k;
+                __syncwarp();
+                for (int t0 = 0; t0 < total; t0 += 32) {
+                    const int t = t0 + lane;
+                    const bool act = t < total;
+                    int r = 0;                              // row holding point t
+#pragma unroll
+                    for (int sft = 16; sft > 0; sft >>= 1)
+                        if (s_row[r + sft - 1] <= t) r += sft;
+                    r = min(r, 31);
+                    const int before = r ? s_row[r - 1] : 0;
+                    const int h = h0 + L * (s_row[32 + r] + (t - before));
+                    pixel<FOM, GATE>(a, P, S, A, ox, oy, oz, h, s_row[64 + r], act);
+                }
+                __syncwarp();
             }
         }
     }
 }
 
-__device__ __forceinline__ float pow2_scale(float maxval, int bits) {
-    if (!(maxval > 0.f)) return 1.f;
-    int e;
-    frexpf(maxval, &e);                   // maxval < 2^e
-    return ldexpf(1.f, bits - e);
+template <bool FOM>
+__device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A, int x0, int y0, int z0, int lane) {
+    const int N = a.N;
+    for (int i = lane; i < TV; i += 32) {
+        const int lx = i % T, ly = (i / T) % T, lz = i / (T * T);
+        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+        if (x < N && y < N && z < N) {
+            const size_t idx = ((size_t)z * N + y) * N + x;
+            double2 o = a.vol[idx];
+            o.x += A.re[i];
+            o.y += A.im[i];
+            a.vol[idx] = o;
+            a.w[idx] += A.w[i];
+            if (FOM) { a.pow[idx] += A.p[i]; a.w2[idx] += A.q[i]; }
+        }
+        A.re[i] = 0.f; A.im[i] = 0.f; A.w[i] = 0.f;
+        if (FOM) { A.p[i] = 0.f; A.q[i] = 0.f; }
+    }
+    __syncwarp();
 }
 
 template <bool FOM, bool GATE>
-__global__ void __launch_bounds__(NT) insert_kernel(InsertArgs a) {
+__global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
+    constexpr int NCH = FOM ? 5 : 3;
+    __shared__ float s_acc[WARPS][NCH * TV];
+    __shared__ int s_rows[WARPS][96];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tile = blockIdx.x * WARPS + warp;
+    const int ntx = a.ntx;
+    if (tile >= ntx * ntx * ntx) return;
+    const int x0 = (tile % ntx) * T, y0 = ((tile / ntx) % ntx) * T, z0 = (tile / (ntx * ntx)) * T;
     const int N = a.N;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
     const int hf = a.ft / 2;
     const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
+    TileAcc A;
+    A.re = s_acc[warp]; A.im = A.re + TV; A.w = A.im + TV;
+    A.p = FOM ? A.w + TV : nullptr; A.q = FOM ? A.p + TV : nullptr;
+    for (int i = lane; i < NCH * TV; i += 32) s_acc[warp][i] = 0.f;
+    __syncwarp();
 
-    extern __shared__ __align__(16) unsigned long long s_acc[];   // 3 or 5 channels x TV
-    __shared__ unsigned s_list[NT];
-    __shared__ int s_warp[NWARPS + 1];
-
-    const int nch = FOM ? 5 : 3;
-    for (int i = threadIdx.x; i < nch * TV; i += NT) s_acc[i] = 0ull;
-
-    // fixed-point scales for this batch (identical in every block)
-    const float fmax = __uint_as_float(*a.fmax_bits);
-    Tile T;
-    T.re = s_acc; T.im = s_acc + TV; T.w = s_acc + 2 * TV;
-    T.p = FOM ? s_acc + 3 * TV : nullptr; T.q = FOM ? s_acc + 4 * TV : nullptr;
-    T.sF = pow2_scale(fmax * a.pw_max, a.fix_bits);
-    T.sW = pow2_scale(a.pw_max, a.fix_bits);
-    T.sP = pow2_scale(fmax * fmax * 2.f * a.pw_max, a.fix_bits);
-    T.sQ = pow2_scale(a.pw_max * a.pw_max, a.fix_bits);
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int base = 0; base < a.np; base += NT) {
-        const int p = base + threadIdx.x;
+    int since_fold = 0;
+    for (int base = 0; base < a.np; base += 32) {
+        const int p = base + lane;
         unsigned mask = 0;
         if (p < a.np) {
             const DevParticle& P = a.part[p];
             if (P.half == a.half || a.half < 0) mask = tile_mask(P, x0, y0, z0, N, a.ft);
         }
-        // ordered compaction of (particle, alias mask)
-        const unsigned ball = __ballot_sync(0xffffffffu, mask != 0);
-        const int before = __popc(ball & ((1u << lane) - 1));
-        if (lane == 0) s_warp[warp] = __popc(ball);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int run = 0;
-            for (int w = 0; w < NWARPS; ++w) { const int c = s_warp[w]; s_warp[w] = run; run += c; }
-            s_warp[NWARPS] = run;
-        }
-        __syncthreads();
-        if (mask) s_list[s_warp[warp] + before] = (unsigned)threadIdx.x | (mask << 16);
-        __syncthreads();
-        const int cnt = s_warp[NWARPS];
-        // every warp walks every listed particle (its own rows of each); the
-        // integer sums make the order irrelevant, so warps never wait
-        for (int e = 0; e < cnt; ++e) {
-            const unsigned ent = s_list[e];
-            const int pi = base + (int)(ent & 0xffffu);
+        unsigned todo = __ballot_sync(0xffffffffu, mask != 0);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const unsigned am = __shfl_sync(0xffffffffu, mask, src);
+            const int pi = base + src;
             const DevParticle& P = a.part[pi];
             const float2* S = a.spec + (size_t)(a.p_base + pi) * spec_stride;
-            for (int al = 0; al < 8; ++al) {
-                if (!((ent >> (16 + al)) & 1u)) continue;
-                scatter_particle<FOM, GATE>(a, P, S, T, (double)(x0 - ((al & 1) ? N : 0)),
-                                            (double)(y0 - ((al & 2) ? N : 0)), (double)(z0 - ((al & 4) ? N : 0)),
-                                            warp, lane);
-            }
+            for (int al = 0; al < 8; ++al)
+                if ((am >> al) & 1u)
+                    scatter_particle<FOM, GATE>(a, P, S, A, (double)(x0 - ((al & 1) ? N : 0)),
+                                                (double)(y0 - ((al & 2) ? N : 0)),
+                                                (double)(z0 - ((al & 4) ? N : 0)), lane, s_rows[warp]);
         }
-        __syncthreads();
-    }
-    // fixed point -> double, added to the map accumulators
-    const double iF = 1.0 / T.sF, iW = 1.0 / T.sW, iP = 1.0 / T.sP, iQ = 1.0 / T.sQ;
-    for (int i = threadIdx.x; i < TV; i += NT) {
-        const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        if (x >= N || y >= N || z >= N) continue;
-        const size_t idx = ((size_t)z * N + y) * N + x;
-        double2 o = a.vol[idx];
-        o.x += (double)(long long)T.re[i] * iF;
-        o.y += (double)(long long)T.im[i] * iF;
-        a.vol[idx] = o;
-        a.w[idx] += (double)(long long)T.w[i] * iW;
-        if (FOM) {
-            a.pow[idx] += (double)(long long)T.p[i] * iP;
-            a.w2[idx] += (double)(long long)T.q[i] * iQ;
+        since_fold += 32;
+        if (since_fold >= FOLD) {
+            fold_tile<FOM>(a, A, x0, y0, z0, lane);
+            since_fold = 0;
         }
     }
+    fold_tile<FOM>(a, A, x0, y0, z0, lane);
 }
 
 int tile_edge_for_step(double) { return 32; }
 
-cudaError_t prepare_insert_attributes() {
-    cudaError_t e = cudaFuncSetAttribute(insert_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(5 * TV * sizeof(unsigned long long)));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(insert_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(5 * TV * sizeof(unsigned long long)));
-}
+cudaError_t prepare_insert_attributes() { return cudaSuccess; }
 
 cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int np, int half, cudaStream_t s) {
     InsertArgs a;
@@ -306,27 +336,24 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.N = c.g.map;
     a.ft = c.g.ft;
     a.pitch = c.g.ft + 2;
+    a.ntx = (c.g.map + T - 1) / T;
     a.interp = c.g.interp;
     a.maxs2 = c.g.maxs2;
     a.mins2 = c.g.mins2;
     a.mscale = c.g.mscale;
-    a.fmax_bits = c.d_fmax;
-    a.pw_max = c.pw_max;
-    a.fix_bits = c.fix_bits;
     const int h = half < 0 ? 0 : half;
     a.vol = c.d_vol[h];
     a.w = c.d_w[h];
     a.pow = c.d_pow[h];
     a.w2 = c.d_w2[h];
-    const int N = c.g.map;
-    dim3 grid((N + TX - 1) / TX, (N + TY - 1) / TY, (N + TZ - 1) / TZ);
-    const size_t smem = (c.g.fom ? 5 : 3) * TV * sizeof(unsigned long long);
+    const int ntiles = a.ntx * a.ntx * a.ntx;
+    const unsigned blocks = (unsigned)((ntiles + WARPS - 1) / WARPS);
     if (c.g.fom) {
-        if (c.g.gate) insert_kernel<true, true><<<grid, NT, smem, s>>>(a);
-        else insert_kernel<true, false><<<grid, NT, smem, s>>>(a);
+        if (c.g.gate) insert_kernel<true, true><<<blocks, WARPS * 32, 0, s>>>(a);
+        else insert_kernel<true, false><<<blocks, WARPS * 32, 0, s>>>(a);
     } else {
-        if (c.g.gate) insert_kernel<false, true><<<grid, NT, smem, s>>>(a);
-        else insert_kernel<false, false><<<grid, NT, smem, s>>>(a);
+        if (c.g.gate) insert_kernel<false, true><<<blocks, WARPS * 32, 0, s>>>(a);
+        else insert_kernel<false, false><<<blocks, WARPS * 32, 0, s>>>(a);
     }
     return cudaGetLastError();
 }
