@@ -8,8 +8,9 @@
 // N^3 map, plus w to the weight map (and w |F|^2, w^2 to the FOM channels).
 //
 // Decomposition: one warp owns one 8 x 8 x 8 tile of the map and keeps its
-// sums in shared memory (float), folding them into the FP64 accumulators
-// in HBM every FOLD particles.  Nothing else writes the tile, so there are
+// sums in shared memory in FP64 (each contribution is the float product
+// F * w, as the reference forms it), adding them to the FP64 accumulators in
+// HBM at the end of the batch.  Nothing else writes the tile, so there are
 // no atomics and no block-wide barriers.  The warp tests 32 particles at a
 // time against its tile (plane slab and reach, per wrap-around alias) and
 // walks the pixels of each particle that reaches it, in particle order.
@@ -36,7 +37,6 @@ namespace bsg {
 constexpr int T = 8;                      // tile edge (voxels)
 constexpr int TV = T * T * T;             // voxels per tile
 constexpr int WARPS = 4;                  // warps (tiles) per block
-constexpr int FOLD = 128;                 // particles between folds into FP64
 
 struct InsertArgs {
     const float2* spec;        // batch x (ft+1) x (ft+2), centred
@@ -89,21 +89,21 @@ __device__ __forceinline__ float pixel_weight_gate(const InsertArgs& a, const De
 }
 
 struct TileAcc {
-    float* re;
-    float* im;
-    float* w;
-    float* p;
-    float* q;
+    double* re;
+    double* im;
+    double* w;
+    double* p;
+    double* q;
 };
 
 template <bool FOM>
 __device__ __forceinline__ void add_voxel(const TileAcc& A, int i, float2 f, float w) {
-    A.re[i] = fmaf(f.x, w, A.re[i]);
-    A.im[i] = fmaf(f.y, w, A.im[i]);
-    A.w[i] += w;
+    A.re[i] += (double)(f.x * w);
+    A.im[i] += (double)(f.y * w);
+    A.w[i] += (double)w;
     if (FOM) {
-        A.p[i] = fmaf(w, f.x * f.x + f.y * f.y, A.p[i]);
-        A.q[i] = fmaf(w, w, A.q[i]);
+        A.p[i] += (double)(w * (f.x * f.x + f.y * f.y));
+        A.q[i] += (double)(w * w);
     }
 }
 
@@ -266,8 +266,8 @@ __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A,
             a.w[idx] += A.w[i];
             if (FOM) { a.pow[idx] += A.p[i]; a.w2[idx] += A.q[i]; }
         }
-        A.re[i] = 0.f; A.im[i] = 0.f; A.w[i] = 0.f;
-        if (FOM) { A.p[i] = 0.f; A.q[i] = 0.f; }
+        A.re[i] = 0.0; A.im[i] = 0.0; A.w[i] = 0.0;
+        if (FOM) { A.p[i] = 0.0; A.q[i] = 0.0; }
     }
     __syncwarp();
 }
@@ -275,7 +275,8 @@ __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A,
 template <bool FOM, bool GATE>
 __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     constexpr int NCH = FOM ? 5 : 3;
-    __shared__ float s_acc[WARPS][NCH * TV];
+    extern __shared__ double s_dacc[];                 // WARPS x NCH x TV
+    double* const my_acc = s_dacc + (size_t)(threadIdx.x >> 5) * NCH * TV;
     __shared__ int s_rows[WARPS][96];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int tile = blockIdx.x * WARPS + warp;
@@ -286,12 +287,11 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     const int hf = a.ft / 2;
     const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
     TileAcc A;
-    A.re = s_acc[warp]; A.im = A.re + TV; A.w = A.im + TV;
+    A.re = my_acc; A.im = A.re + TV; A.w = A.im + TV;
     A.p = FOM ? A.w + TV : nullptr; A.q = FOM ? A.p + TV : nullptr;
-    for (int i = lane; i < NCH * TV; i += 32) s_acc[warp][i] = 0.f;
+    for (int i = lane; i < NCH * TV; i += 32) my_acc[i] = 0.0;
     __syncwarp();
 
-    int since_fold = 0;
     for (int base = 0; base < a.np; base += 32) {
         const int p = base + lane;
         unsigned mask = 0;
@@ -313,18 +313,18 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
                                                 (double)(y0 - ((al & 2) ? N : 0)),
                                                 (double)(z0 - ((al & 4) ? N : 0)), lane, s_rows[warp]);
         }
-        since_fold += 32;
-        if (since_fold >= FOLD) {
-            fold_tile<FOM>(a, A, x0, y0, z0, lane);
-            since_fold = 0;
-        }
     }
     fold_tile<FOM>(a, A, x0, y0, z0, lane);
 }
 
 int tile_edge_for_step(double) { return 32; }
 
-cudaError_t prepare_insert_attributes() { return cudaSuccess; }
+cudaError_t prepare_insert_attributes() {
+    const int smem = (int)(WARPS * 5 * TV * sizeof(double));
+    cudaError_t e = cudaFuncSetAttribute(insert_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(insert_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
 
 cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int np, int half, cudaStream_t s) {
     InsertArgs a;
@@ -348,12 +348,13 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.w2 = c.d_w2[h];
     const int ntiles = a.ntx * a.ntx * a.ntx;
     const unsigned blocks = (unsigned)((ntiles + WARPS - 1) / WARPS);
+    const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TV * sizeof(double);
     if (c.g.fom) {
-        if (c.g.gate) insert_kernel<true, true><<<blocks, WARPS * 32, 0, s>>>(a);
-        else insert_kernel<true, false><<<blocks, WARPS * 32, 0, s>>>(a);
+        if (c.g.gate) insert_kernel<true, true><<<blocks, WARPS * 32, smem, s>>>(a);
+        else insert_kernel<true, false><<<blocks, WARPS * 32, smem, s>>>(a);
     } else {
-        if (c.g.gate) insert_kernel<false, true><<<blocks, WARPS * 32, 0, s>>>(a);
-        else insert_kernel<false, false><<<blocks, WARPS * 32, 0, s>>>(a);
+        if (c.g.gate) insert_kernel<false, true><<<blocks, WARPS * 32, smem, s>>>(a);
+        else insert_kernel<false, false><<<blocks, WARPS * 32, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
