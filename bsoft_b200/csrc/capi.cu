@@ -29,7 +29,8 @@ cudaError_t prepare_fft2d_attributes();
 cudaError_t prepare_finish_attributes();
 cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s);
 cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool sinc, cudaStream_t s);
-int tile_edge_for_step(double step);
+int insert_num_shapes();
+void insert_shape(int i, int* tx, int* ty, int* tz);
 cudaError_t prepare_insert_attributes();
 
 struct Timed {
@@ -119,6 +120,31 @@ static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
     return false;
 }
 
+// Tile visiting order for the current shape: nearest to the Fourier origin
+// (counting wrap-around) first, since every particle's plane passes there.
+static int set_shape(Recon* r, int shape) {
+    if (shape < 0 || shape >= insert_num_shapes()) return fail(BSG_ERR_ARG, "tile shape %d out of range", shape);
+    int tx, ty, tz;
+    insert_shape(shape, &tx, &ty, &tz);
+    const int N = r->g.map;
+    const int nx = (N + tx - 1) / tx, ny = (N + ty - 1) / ty, nz = (N + tz - 1) / tz;
+    std::vector<std::pair<double, int>> d((size_t)nx * ny * nz);
+    for (int z = 0; z < nz; ++z)
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x) {
+                auto dist = [N](double c) { return std::min(fabs(c), fabs(c - N)); };
+                const double cx = dist((x + 0.5) * tx), cy = dist((y + 0.5) * ty), cz = dist((z + 0.5) * tz);
+                const int i = (z * ny + y) * nx + x;
+                d[i] = {cx * cx + cy * cy + cz * cz, i};
+            }
+    std::stable_sort(d.begin(), d.end());
+    std::vector<int> order(d.size());
+    for (size_t i = 0; i < d.size(); ++i) order[i] = d[i].second;
+    CK(cudaMemcpy(r->d_tile_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
+    r->shape = shape;
+    return BSG_OK;
+}
+
 // Failures the kernels report through the mapped status word (bounded waits).
 static int check_status(Recon* r) {
     if (r->h_status && *(volatile int*)r->h_status) {
@@ -144,7 +170,7 @@ static void free_all(Recon* r) {
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
     F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
-    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax); F(r->d_tile_order);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();
@@ -338,6 +364,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     if (!rc && cudaMemset(r->d_spec, 0, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch) != cudaSuccess)
         rc = fail(BSG_ERR_CUDA, "bsg_recon_create: clearing the spectra buffer");
     if (!rc) rc = alloc((void**)&r->d_fmax, sizeof(unsigned));
+    if (!rc) rc = alloc((void**)&r->d_tile_order, sizeof(int) * (size_t)((N + 7) / 8) * ((N + 7) / 8) * ((N + 7) / 8));
     if (rc) { free_all(r); delete r; return rc; }
     std::vector<float2> tw;
     host_twiddles(ft, tw);
@@ -354,6 +381,10 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     if (e != cudaSuccess) { free_all(r); delete r; return fail(BSG_ERR_CUDA, "bsg_recon_create: %s", cudaGetErrorString(e)); }
     for (int i = 0; i < 2; ++i) {
         cudaEventRecord(r->compute_done[i], r->stream);
+    }
+    {
+        const int rc2 = set_shape(r, 1);
+        if (rc2) { free_all(r); delete r; return rc2; }
     }
     *out = reinterpret_cast<bsg_recon*>(r);
     return bsg_recon_reset(*out);
@@ -464,6 +495,54 @@ int bsg_recon_fsc(bsg_recon* h, int nshell, double* fsc_out) {
     CK(cudaMemcpyAsync(fsc_out, d_out, sizeof(double) * nshell, cudaMemcpyDeviceToHost, r->stream));
     CK(cudaStreamSynchronize(r->stream));
     return BSG_OK;
+}
+
+int bsg_recon_set_tile_shape(bsg_recon* h, int shape) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return fail(BSG_ERR_ARG, "bsg_recon_set_tile_shape: null context");
+    CK(cudaSetDevice(r->device));
+    return set_shape(r, shape);
+}
+
+int bsg_recon_autotune(bsg_recon* h, const float* images, const double* params, long nparts, int flags,
+                       double* ms_out, int* best_out) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !images || !params || nparts < 1) return fail(BSG_ERR_ARG, "bsg_recon_autotune: bad argument");
+    CK(cudaSetDevice(r->device));
+    const bool was_timing = r->timing;
+    const bsg_recon_stats saved = r->stats;
+    int best = r->shape;
+    double best_ms = 1e300;
+    for (int sh = 0; sh < insert_num_shapes(); ++sh) {
+        if (sh == 3 && r->g.fom) { if (ms_out) ms_out[sh] = -1; continue; }
+        int rc = set_shape(r, sh);
+        if (rc) return rc;
+        rc = bsg_recon_reset(h);
+        if (rc) return rc;
+        r->timing = true;
+        for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
+        r->timed.clear();
+        rc = process(r, images, params, nparts, flags, nullptr);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(r->stream));
+        double ms = 0;
+        for (auto& t : r->timed) {
+            float e = 0.f;
+            cudaEventElapsedTime(&e, t.a, t.b);
+            if (t.kind == 0) ms += e;
+            cudaEventDestroy(t.a);
+            cudaEventDestroy(t.b);
+        }
+        r->timed.clear();
+        if (ms_out) ms_out[sh] = ms;
+        if (ms < best_ms) { best_ms = ms; best = sh; }
+    }
+    r->timing = was_timing;
+    r->stats = saved;
+    int rc = set_shape(r, best);
+    if (rc) return rc;
+    if (best_out) *best_out = best;
+    return bsg_recon_reset(h);
 }
 
 int bsg_recon_set_timing(bsg_recon* h, int enable) {

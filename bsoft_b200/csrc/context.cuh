@@ -44,6 +44,8 @@ struct Context {
     unsigned* d_fmax = nullptr;      // max |Re F|, |Im F| of the batch (float bits)
     float pw_max = 0.f;              // max particle weight of the batch
     int fix_bits = 44;               // largest |F w| maps below 2^fix_bits
+    int shape = 1;                   // gridding tile shape (insert.cu kShapes)
+    int* d_tile_order = nullptr;     // tile visiting order for `shape`
     int* d_status = nullptr;         // device view of h_status (mapped)
     int* h_status = nullptr;         // kernel-reported failures (bounded waits)
 

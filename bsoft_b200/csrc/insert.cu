@@ -7,7 +7,8 @@
 // (trilinear) voxels around m, with index wrap-around, on a full complex
 // N^3 map, plus w to the weight map (and w |F|^2, w^2 to the FOM channels).
 //
-// Decomposition: one warp owns one 8 x 8 x 8 tile of the map and keeps its
+// Decomposition: one warp owns one tile of the map (8 x 8 x 8, 16 x 16 x 4,
+// 16 x 8 x 8 or 16 x 16 x 8 voxels; the autotuner picks the shape) and keeps its
 // sums in shared memory in FP64 (each contribution is the float product
 // F * w, as the reference forms it), adding them to the FP64 accumulators in
 // HBM at the end of the batch.  Nothing else writes the tile, so there are
@@ -22,7 +23,9 @@
 // some axis, and for any one corner offset the lanes of a warp touch
 // distinct voxels: a plain read-modify-write of shared memory is exact.
 // The order of every voxel's sum (particle, alias, phase, lattice point,
-// corner) is fixed, so results are bitwise reproducible.
+// corner) is fixed, so results are bitwise reproducible.  Tiles are visited
+// heaviest first (nearest to the Fourier origin, where every particle's
+// plane passes) so the long ones do not trail the launch.
 //
 // Each phase's lattice points are enumerated exactly: lane j computes the
 // h-interval of lattice row j from the three slab constraints of the tile
@@ -34,8 +37,6 @@
 
 namespace bsg {
 
-constexpr int T = 8;                      // tile edge (voxels)
-constexpr int TV = T * T * T;             // voxels per tile
 constexpr int WARPS = 4;                  // warps (tiles) per block
 
 struct InsertArgs {
@@ -45,7 +46,8 @@ struct InsertArgs {
     int np;
     int half;                  // only particles of this half map (-1: all)
     int N, ft, pitch;
-    int ntx;                   // tiles per axis
+    int ntx, nty, ntz;         // tiles per axis
+    const int* order;          // tile visiting order (heaviest first)
     int interp;
     double maxs2, mins2, mscale;
     double2* vol;
@@ -56,21 +58,22 @@ struct InsertArgs {
 
 // Does particle P's plane come within reach of the tile for alias
 // combination a (bit i set: axis i shifted by -N)?  Bitmask over the 8.
+template <int TX, int TY, int TZ>
 __device__ __forceinline__ unsigned tile_mask(const DevParticle& P, int x0, int y0, int z0, int N, int ft) {
     unsigned mask = 0;
-    const float e = 0.5f * (T - 1);
+    const float ex = 0.5f * (TX - 1), ey = 0.5f * (TY - 1), ez = 0.5f * (TZ - 1);
     const float hf = 0.5f * ft;
     const float rx = hf * (fabsf(P.af[0]) + fabsf(P.bf[0])) + 1.0f;
     const float ry = hf * (fabsf(P.af[1]) + fabsf(P.bf[1])) + 1.0f;
     const float rz = hf * (fabsf(P.af[2]) + fabsf(P.bf[2])) + 1.0f;
     const float n0 = (float)P.nrm[0], n1 = (float)P.nrm[1], n2 = (float)P.nrm[2];
-    const float slack = P.slab + (fabsf(n0) + fabsf(n1) + fabsf(n2)) * e + 1e-3f;
+    const float slack = P.slab + fabsf(n0) * ex + fabsf(n1) * ey + fabsf(n2) * ez + 1e-3f;
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
-        const float cx = x0 - ((a & 1) ? N : 0) + e;
-        const float cy = y0 - ((a & 2) ? N : 0) + e;
-        const float cz = z0 - ((a & 4) ? N : 0) + e;
-        if (fabsf(cx) - e > rx || fabsf(cy) - e > ry || fabsf(cz) - e > rz) continue;
+        const float cx = x0 - ((a & 1) ? N : 0) + ex;
+        const float cy = y0 - ((a & 2) ? N : 0) + ey;
+        const float cz = z0 - ((a & 4) ? N : 0) + ez;
+        if (fabsf(cx) - ex > rx || fabsf(cy) - ey > ry || fabsf(cz) - ez > rz) continue;
         if (fabsf(n0 * cx + n1 * cy + n2 * cz) > slack) continue;
         mask |= 1u << a;
     }
@@ -112,7 +115,7 @@ __device__ __forceinline__ void add_voxel(const TileAcc& A, int i, float2 f, flo
 // __syncwarp after each corner orders the shared-memory updates of
 // different corner offsets, which may touch the same voxel from different
 // lanes.
-template <bool FOM, bool GATE>
+template <bool FOM, bool GATE, int TX, int TY, int TZ>
 __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P, const float2* S, const TileAcc& A,
                                       double ox, double oy, double oz, int h, int k, bool act) {
     const int hf = a.ft / 2;
@@ -137,8 +140,8 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
             const double dx = mx - fx, dy = my - fy, dz = mz - fz;
             w = (float)((double)wt * (1.0 - sqrt(dx * dx + dy * dy + dz * dz)));
         }
-        if (act && (unsigned)ix < T && (unsigned)iy < T && (unsigned)iz < T && w > 0.f)
-            add_voxel<FOM>(A, (iz * T + iy) * T + ix, f, w);
+        if (act && (unsigned)ix < TX && (unsigned)iy < TY && (unsigned)iz < TZ && w > 0.f)
+            add_voxel<FOM>(A, (iz * TY + iy) * TX + ix, f, w);
         __syncwarp();
         return;
     }
@@ -156,8 +159,8 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
 #pragma unroll
             for (int dx = 0; dx < 2; ++dx) {
                 const int x = ix + dx;
-                if (act && (unsigned)x < T && (unsigned)y < T && (unsigned)z < T)
-                    add_voxel<FOM>(A, (z * T + y) * T + x, f, (dx ? rx : 1.f - rx) * wyz);
+                if (act && (unsigned)x < TX && (unsigned)y < TY && (unsigned)z < TZ)
+                    add_voxel<FOM>(A, (z * TY + y) * TX + x, f, (dx ? rx : 1.f - rx) * wyz);
                 __syncwarp();
             }
         }
@@ -166,14 +169,14 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
 
 // Walk the pixels of particle P (alias origin o) whose contributions can
 // reach the tile, phase by phase of the lattice.
-template <bool FOM, bool GATE>
+template <bool FOM, bool GATE, int TX, int TY, int TZ>
 __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevParticle& P, const float2* S,
                                                  const TileAcc& A, double ox, double oy, double oz, int lane,
                                                  int* s_row) {
     const int hf = a.ft / 2;
     // open box of map frequencies whose tent touches the tile
     const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
-    const double hi[3] = {ox + T, oy + T, oz + T};
+    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
     double vc = 0, hv = 0, uc = 0, hu = 0;
     for (int i = 0; i < 3; ++i) {
         const double c = 0.5 * (lo[i] + hi[i]), e = 0.5 * (hi[i] - lo[i]);
@@ -243,7 +246,7 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                     r = min(r, 31);
                     const int before = r ? s_row[r - 1] : 0;
                     const int h = h0 + L * (s_row[32 + r] + (t - before));
-                    pixel<FOM, GATE>(a, P, S, A, ox, oy, oz, h, s_row[64 + r], act);
+                    pixel<FOM, GATE, TX, TY, TZ>(a, P, S, A, ox, oy, oz, h, s_row[64 + r], act);
                 }
                 __syncwarp();
             }
@@ -251,11 +254,12 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     }
 }
 
-template <bool FOM>
+template <bool FOM, int TX, int TY, int TZ>
 __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A, int x0, int y0, int z0, int lane) {
     const int N = a.N;
+    constexpr int TV = TX * TY * TZ;
     for (int i = lane; i < TV; i += 32) {
-        const int lx = i % T, ly = (i / T) % T, lz = i / (T * T);
+        const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
         const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
         if (x < N && y < N && z < N) {
             const size_t idx = ((size_t)z * N + y) * N + x;
@@ -272,17 +276,18 @@ __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A,
     __syncwarp();
 }
 
-template <bool FOM, bool GATE>
+template <bool FOM, bool GATE, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     constexpr int NCH = FOM ? 5 : 3;
+    constexpr int TV = TX * TY * TZ;
     extern __shared__ double s_dacc[];                 // WARPS x NCH x TV
     double* const my_acc = s_dacc + (size_t)(threadIdx.x >> 5) * NCH * TV;
     __shared__ int s_rows[WARPS][96];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tile = blockIdx.x * WARPS + warp;
-    const int ntx = a.ntx;
-    if (tile >= ntx * ntx * ntx) return;
-    const int x0 = (tile % ntx) * T, y0 = ((tile / ntx) % ntx) * T, z0 = (tile / (ntx * ntx)) * T;
+    const int slot = blockIdx.x * WARPS + warp;
+    if (slot >= a.ntx * a.nty * a.ntz) return;
+    const int tile = a.order[slot];
+    const int x0 = (tile % a.ntx) * TX, y0 = ((tile / a.ntx) % a.nty) * TY, z0 = (tile / (a.ntx * a.nty)) * TZ;
     const int N = a.N;
     const int hf = a.ft / 2;
     const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
@@ -297,7 +302,7 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
         unsigned mask = 0;
         if (p < a.np) {
             const DevParticle& P = a.part[p];
-            if (P.half == a.half || a.half < 0) mask = tile_mask(P, x0, y0, z0, N, a.ft);
+            if (P.half == a.half || a.half < 0) mask = tile_mask<TX, TY, TZ>(P, x0, y0, z0, N, a.ft);
         }
         unsigned todo = __ballot_sync(0xffffffffu, mask != 0);
         while (todo) {
@@ -309,23 +314,62 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
             const float2* S = a.spec + (size_t)(a.p_base + pi) * spec_stride;
             for (int al = 0; al < 8; ++al)
                 if ((am >> al) & 1u)
-                    scatter_particle<FOM, GATE>(a, P, S, A, (double)(x0 - ((al & 1) ? N : 0)),
+                    scatter_particle<FOM, GATE, TX, TY, TZ>(a, P, S, A, (double)(x0 - ((al & 1) ? N : 0)),
                                                 (double)(y0 - ((al & 2) ? N : 0)),
                                                 (double)(z0 - ((al & 4) ? N : 0)), lane, s_rows[warp]);
         }
     }
-    fold_tile<FOM>(a, A, x0, y0, z0, lane);
+    fold_tile<FOM, TX, TY, TZ>(a, A, x0, y0, z0, lane);
 }
 
-int tile_edge_for_step(double) { return 32; }
+// Tile shapes the autotuner chooses from (map voxels per warp).
+struct Shape { int tx, ty, tz; };
+static const Shape kShapes[] = {{8, 8, 8}, {16, 16, 4}, {16, 8, 8}, {16, 16, 8}};
+constexpr int kNumShapes = 4;
+
+int insert_num_shapes() { return kNumShapes; }
+void insert_shape(int i, int* tx, int* ty, int* tz) { *tx = kShapes[i].tx; *ty = kShapes[i].ty; *tz = kShapes[i].tz; }
+
+template <int TX, int TY, int TZ>
+static cudaError_t set_smem_shape() {
+    const int smem = (int)(WARPS * 5 * TX * TY * TZ * sizeof(double));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(insert_kernel<true, true, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(insert_kernel<true, false, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(insert_kernel<false, true, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(insert_kernel<false, false, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
 
 cudaError_t prepare_insert_attributes() {
-    const int smem = (int)(WARPS * 5 * TV * sizeof(double));
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(insert_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(insert_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    if ((e = cudaFuncSetAttribute(insert_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(insert_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = set_smem_shape<8, 8, 8>()) != cudaSuccess) return e;
+    if ((e = set_smem_shape<16, 16, 4>()) != cudaSuccess) return e;
+    if ((e = set_smem_shape<16, 8, 8>()) != cudaSuccess) return e;
+    // 16 x 16 x 8 in FP64 needs 5 x 2048 x 8 B per warp with FOM: beyond one
+    // SM's shared memory for 4 warps, so only the non-FOM variants exist
+    const int smem = (int)(WARPS * 3 * 16 * 16 * 8 * sizeof(double));
+    if ((e = cudaFuncSetAttribute(insert_kernel<false, true, 16, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(insert_kernel<false, false, 16, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+template <int TX, int TY, int TZ>
+static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStream_t s) {
+    InsertArgs a = a0;
+    const int N = c.g.map;
+    a.ntx = (N + TX - 1) / TX;
+    a.nty = (N + TY - 1) / TY;
+    a.ntz = (N + TZ - 1) / TZ;
+    const int ntiles = a.ntx * a.nty * a.ntz;
+    const unsigned blocks = (unsigned)((ntiles + WARPS - 1) / WARPS);
+    const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TX * TY * TZ * sizeof(double);
+    if (c.g.fom) {
+        if (c.g.gate) insert_kernel<true, true, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
+        else insert_kernel<true, false, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
+    } else {
+        if (c.g.gate) insert_kernel<false, true, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
+        else insert_kernel<false, false, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int np, int half, cudaStream_t s) {
@@ -338,7 +382,6 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.N = c.g.map;
     a.ft = c.g.ft;
     a.pitch = c.g.ft + 2;
-    a.ntx = (c.g.map + T - 1) / T;
     a.interp = c.g.interp;
     a.maxs2 = c.g.maxs2;
     a.mins2 = c.g.mins2;
@@ -348,17 +391,13 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.w = c.d_w[h];
     a.pow = c.d_pow[h];
     a.w2 = c.d_w2[h];
-    const int ntiles = a.ntx * a.ntx * a.ntx;
-    const unsigned blocks = (unsigned)((ntiles + WARPS - 1) / WARPS);
-    const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TV * sizeof(double);
-    if (c.g.fom) {
-        if (c.g.gate) insert_kernel<true, true><<<blocks, WARPS * 32, smem, s>>>(a);
-        else insert_kernel<true, false><<<blocks, WARPS * 32, smem, s>>>(a);
-    } else {
-        if (c.g.gate) insert_kernel<false, true><<<blocks, WARPS * 32, smem, s>>>(a);
-        else insert_kernel<false, false><<<blocks, WARPS * 32, smem, s>>>(a);
+    a.order = c.d_tile_order;
+    switch (c.shape) {
+        case 0: return launch_shape<8, 8, 8>(a, c, s);
+        case 2: return launch_shape<16, 8, 8>(a, c, s);
+        case 3: if (!c.g.fom) return launch_shape<16, 16, 8>(a, c, s); return launch_shape<16, 16, 4>(a, c, s);
+        default: return launch_shape<16, 16, 4>(a, c, s);
     }
-    return cudaGetLastError();
 }
 
 }  // namespace bsg

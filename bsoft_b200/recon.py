@@ -132,6 +132,24 @@ class Reconstructor:
                                                     C.c_void_p(out.ctypes.data), 0), "bsg_particle_spectra")
         return out[..., 0] + 1j * out[..., 1]
 
+    def autotune(self, images, params: np.ndarray):
+        """Time every gridding tile shape on these particles, keep the
+        fastest, then clear the accumulators (call before inserting)."""
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        ptr, dev = _ptr(images if hasattr(images, "data_ptr") else np.ascontiguousarray(images, np.float32))
+        keep = images
+        ms = np.zeros(8)
+        best = C.c_int(0)
+        _lib.check(_lib.load().bsg_recon_autotune(self._h, ptr, C.c_void_p(params.ctypes.data), params.shape[0],
+                                                  _lib.BSG_DEVICE_PTR if dev else 0,
+                                                  ms.ctypes.data_as(C.POINTER(C.c_double)), C.byref(best)),
+                   "bsg_recon_autotune")
+        del keep
+        return best.value, ms[:4]
+
+    def set_tile_shape(self, shape: int):
+        _lib.check(_lib.load().bsg_recon_set_tile_shape(self._h, shape), "bsg_recon_set_tile_shape")
+
     def reset(self):
         _lib.check(_lib.load().bsg_recon_reset(self._h), "bsg_recon_reset")
 

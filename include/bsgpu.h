@@ -118,6 +118,16 @@ int  bsg_recon_fsc(bsg_recon* r, int nshell, double* fsc_out);
 int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* params,
                           long nparts, float* out, int flags);
 
+/* Gridding tile shape (0: 8x8x8, 1: 16x16x4 (default), 2: 16x8x8,
+ * 3: 16x16x8 without FOM).  bsg_recon_autotune times every shape on the
+ * given particles, keeps the fastest and then clears the accumulators: call
+ * it before inserting.  ms_out (optional) receives one time per shape
+ * (-1 where the shape does not apply); best_out the chosen shape.  The
+ * reference has no counterpart (it has no tunable tiling). */
+int  bsg_recon_set_tile_shape(bsg_recon* r, int shape);
+int  bsg_recon_autotune(bsg_recon* r, const float* images, const double* params, long nparts,
+                        int flags, double* ms_out, int* best_out);
+
 int  bsg_recon_set_timing(bsg_recon* r, int enable);
 int  bsg_recon_get_stats(bsg_recon* r, bsg_recon_stats* st);
 int  bsg_recon_reset(bsg_recon* r);          /* zero the accumulators        */
