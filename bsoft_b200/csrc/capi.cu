@@ -142,6 +142,18 @@ static int set_shape(Recon* r, int shape) {
     for (size_t i = 0; i < d.size(); ++i) order[i] = d[i].second;
     CK(cudaMemcpy(r->d_tile_order, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice));
     r->shape = shape;
+    // replicas: enough warps to fill the GPU several times over and to split
+    // the tiles near the origin, which every particle reaches
+    const long ntiles = (long)nx * ny * nz;
+    int R = (int)std::min<long>(16, std::max<long>(4, (131072 + ntiles - 1) / ntiles));
+    const size_t need = (size_t)R * (r->g.fom ? 5 : 3) * r->vol_elems() * sizeof(double);
+    if (r->d_part_sums) { cudaFree(r->d_part_sums); r->d_part_sums = nullptr; }
+    if (cudaMalloc((void**)&r->d_part_sums, need) != cudaSuccess) {
+        // not enough memory for replicas: run each tile in one warp
+        r->d_part_sums = nullptr;
+        R = 1;
+    }
+    r->replicas = R;
     return BSG_OK;
 }
 
@@ -170,7 +182,7 @@ static void free_all(Recon* r) {
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
     F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
-    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax); F(r->d_tile_order);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax); F(r->d_tile_order); F(r->d_part_sums);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();

@@ -46,6 +46,8 @@ struct Context {
     int fix_bits = 44;               // largest |F w| maps below 2^fix_bits
     int shape = 1;                   // gridding tile shape (insert.cu kShapes)
     int* d_tile_order = nullptr;     // tile visiting order for `shape`
+    int replicas = 1;                // warps per tile, each on a slice of the particles
+    double* d_part_sums = nullptr;   // replica partial sums (replicas > 1)
     int* d_status = nullptr;         // device view of h_status (mapped)
     int* h_status = nullptr;         // kernel-reported failures (bounded waits)
 

@@ -25,7 +25,9 @@
 // The order of every voxel's sum (particle, alias, phase, lattice point,
 // corner) is fixed, so results are bitwise reproducible.  Tiles are visited
 // heaviest first (nearest to the Fourier origin, where every particle's
-// plane passes) so the long ones do not trail the launch.
+// plane passes) so the long ones do not trail the launch, and each tile has
+// R replica warps that take consecutive slices of the particle list into
+// private partial sums; a combine pass adds the replicas in order.
 //
 // Each phase's lattice points are enumerated exactly: lane j computes the
 // h-interval of lattice row j from the three slab constraints of the tile
@@ -48,6 +50,8 @@ struct InsertArgs {
     int N, ft, pitch;
     int ntx, nty, ntz;         // tiles per axis
     const int* order;          // tile visiting order (heaviest first)
+    int R;                     // replicas per tile (each takes a slice of the particles)
+    double* part;              // R > 1: replica partial sums, R x channels x N^3
     int interp;
     double maxs2, mins2, mscale;
     double2* vol;
@@ -254,21 +258,34 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     }
 }
 
+// Tile sums -> HBM: added to the map accumulators (one replica), or stored
+// into this replica's partial buffer (combined later in replica order).
 template <bool FOM, int TX, int TY, int TZ>
-__device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A, int x0, int y0, int z0, int lane) {
+__device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A, int x0, int y0, int z0, int r,
+                                          int lane) {
     const int N = a.N;
     constexpr int TV = TX * TY * TZ;
+    const size_t N3 = (size_t)N * N * N;
+    const int nch = FOM ? 5 : 3;
     for (int i = lane; i < TV; i += 32) {
         const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
         const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
         if (x < N && y < N && z < N) {
             const size_t idx = ((size_t)z * N + y) * N + x;
-            double2 o = a.vol[idx];
-            o.x += A.re[i];
-            o.y += A.im[i];
-            a.vol[idx] = o;
-            a.w[idx] += A.w[i];
-            if (FOM) { a.pow[idx] += A.p[i]; a.w2[idx] += A.q[i]; }
+            if (a.R > 1) {
+                double* pb = a.part + (size_t)r * nch * N3 + idx;
+                pb[0] = A.re[i];
+                pb[N3] = A.im[i];
+                pb[2 * N3] = A.w[i];
+                if (FOM) { pb[3 * N3] = A.p[i]; pb[4 * N3] = A.q[i]; }
+            } else {
+                double2 o = a.vol[idx];
+                o.x += A.re[i];
+                o.y += A.im[i];
+                a.vol[idx] = o;
+                a.w[idx] += A.w[i];
+                if (FOM) { a.pow[idx] += A.p[i]; a.w2[idx] += A.q[i]; }
+            }
         }
         A.re[i] = 0.0; A.im[i] = 0.0; A.w[i] = 0.0;
         if (FOM) { A.p[i] = 0.0; A.q[i] = 0.0; }
@@ -284,9 +301,12 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     double* const my_acc = s_dacc + (size_t)(threadIdx.x >> 5) * NCH * TV;
     __shared__ int s_rows[WARPS][96];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int slot = blockIdx.x * WARPS + warp;
+    const int gw = blockIdx.x * WARPS + warp;
+    const int slot = gw / a.R, rep = gw % a.R;       // replicas of a tile are adjacent
     if (slot >= a.ntx * a.nty * a.ntz) return;
     const int tile = a.order[slot];
+    // this replica's slice of the particles
+    const int p_lo = (int)((long)a.np * rep / a.R), p_hi = (int)((long)a.np * (rep + 1) / a.R);
     const int x0 = (tile % a.ntx) * TX, y0 = ((tile / a.ntx) % a.nty) * TY, z0 = (tile / (a.ntx * a.nty)) * TZ;
     const int N = a.N;
     const int hf = a.ft / 2;
@@ -297,10 +317,10 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     for (int i = lane; i < NCH * TV; i += 32) my_acc[i] = 0.0;
     __syncwarp();
 
-    for (int base = 0; base < a.np; base += 32) {
+    for (int base = p_lo; base < p_hi; base += 32) {
         const int p = base + lane;
         unsigned mask = 0;
-        if (p < a.np) {
+        if (p < p_hi) {
             const DevParticle& P = a.part[p];
             if (P.half == a.half || a.half < 0) mask = tile_mask<TX, TY, TZ>(P, x0, y0, z0, N, a.ft);
         }
@@ -319,7 +339,27 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
                                                 (double)(z0 - ((al & 4) ? N : 0)), lane, s_rows[warp]);
         }
     }
-    fold_tile<FOM, TX, TY, TZ>(a, A, x0, y0, z0, lane);
+    fold_tile<FOM, TX, TY, TZ>(a, A, x0, y0, z0, rep, lane);
+}
+
+// vol += sum over replicas, in replica order.
+template <bool FOM>
+__global__ void combine_kernel(InsertArgs a) {
+    const size_t N3 = (size_t)a.N * a.N * a.N;
+    const int nch = FOM ? 5 : 3;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3; i += (size_t)gridDim.x * blockDim.x) {
+        double re = 0, im = 0, w = 0, p = 0, q = 0;
+        for (int r = 0; r < a.R; ++r) {
+            const double* pb = a.part + (size_t)r * nch * N3 + i;
+            re += pb[0]; im += pb[N3]; w += pb[2 * N3];
+            if (FOM) { p += pb[3 * N3]; q += pb[4 * N3]; }
+        }
+        double2 o = a.vol[i];
+        o.x += re; o.y += im;
+        a.vol[i] = o;
+        a.w[i] += w;
+        if (FOM) { a.pow[i] += p; a.w2[i] += q; }
+    }
 }
 
 // Tile shapes the autotuner chooses from (map voxels per warp).
@@ -360,7 +400,7 @@ static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStre
     a.nty = (N + TY - 1) / TY;
     a.ntz = (N + TZ - 1) / TZ;
     const int ntiles = a.ntx * a.nty * a.ntz;
-    const unsigned blocks = (unsigned)((ntiles + WARPS - 1) / WARPS);
+    const unsigned blocks = (unsigned)(((long)ntiles * a.R + WARPS - 1) / WARPS);
     const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TX * TY * TZ * sizeof(double);
     if (c.g.fom) {
         if (c.g.gate) insert_kernel<true, true, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
@@ -369,6 +409,10 @@ static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStre
         if (c.g.gate) insert_kernel<false, true, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
         else insert_kernel<false, false, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
     }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || a.R == 1) return e;
+    if (c.g.fom) combine_kernel<true><<<148 * 8, 256, 0, s>>>(a);
+    else combine_kernel<false><<<148 * 8, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -392,6 +436,8 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.pow = c.d_pow[h];
     a.w2 = c.d_w2[h];
     a.order = c.d_tile_order;
+    a.R = c.replicas;
+    a.part = c.d_part_sums;
     switch (c.shape) {
         case 0: return launch_shape<8, 8, 8>(a, c, s);
         case 2: return launch_shape<16, 8, 8>(a, c, s);
