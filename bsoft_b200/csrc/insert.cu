@@ -51,7 +51,7 @@ struct InsertArgs {
     int ntx, nty, ntz;         // tiles per axis
     const int* order;          // tile visiting order (heaviest first)
     int R;                     // replicas per tile (each takes a slice of the particles)
-    double* part;              // R > 1: replica partial sums, R x channels x N^3
+    double* psum;              // R > 1: replica partial sums, R x channels x N^3
     int interp;
     double maxs2, mins2, mscale;
     double2* vol;
@@ -273,7 +273,7 @@ __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A,
         if (x < N && y < N && z < N) {
             const size_t idx = ((size_t)z * N + y) * N + x;
             if (a.R > 1) {
-                double* pb = a.part + (size_t)r * nch * N3 + idx;
+                double* pb = a.psum + (size_t)r * nch * N3 + idx;
                 pb[0] = A.re[i];
                 pb[N3] = A.im[i];
                 pb[2 * N3] = A.w[i];
@@ -350,7 +350,7 @@ __global__ void combine_kernel(InsertArgs a) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3; i += (size_t)gridDim.x * blockDim.x) {
         double re = 0, im = 0, w = 0, p = 0, q = 0;
         for (int r = 0; r < a.R; ++r) {
-            const double* pb = a.part + (size_t)r * nch * N3 + i;
+            const double* pb = a.psum + (size_t)r * nch * N3 + i;
             re += pb[0]; im += pb[N3]; w += pb[2 * N3];
             if (FOM) { p += pb[3 * N3]; q += pb[4 * N3]; }
         }
@@ -437,7 +437,7 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int n
     a.w2 = c.d_w2[h];
     a.order = c.d_tile_order;
     a.R = c.replicas;
-    a.part = c.d_part_sums;
+    a.psum = c.d_part_sums;
     switch (c.shape) {
         case 0: return launch_shape<8, 8, 8>(a, c, s);
         case 2: return launch_shape<16, 8, 8>(a, c, s);
