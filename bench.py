@@ -250,8 +250,14 @@ def main():
         if dist is not None:
             dist.barrier()
 
+    # ---- tile shape from the project's autotuner (untimed, on warm-up data)
+    rec = Reconstructor(plan, batch=B, device=local)
+    shape, shape_ms = rec.autotune(dev[0][: min(B, 512)], P[: min(B, 512)])
+    rec.close()
+
     # ---- value: device-resident inputs
     rec = Reconstructor(plan, batch=B, device=local)
+    rec.set_tile_shape(shape)
     s = stream_of(rec)
     for i in range(args.warmup):
         rec.insert(dev[i % 2], P[i * B:(i + 1) * B])
@@ -284,6 +290,7 @@ def main():
 
     # ---- e2e: pinned host images through the C ABI, map read back at the end
     rec = Reconstructor(plan, batch=B, device=local)
+    rec.set_tile_shape(shape)
     for i in range(args.warmup):
         rec.insert(host[i % 2].numpy(), P[i * B:(i + 1) * B])
     rec.synchronize()
@@ -320,7 +327,8 @@ def main():
             "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
             "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
             "algorithmic_bytes_per_particle": per_particle,
-            "fft2d_ms_per_step": round(fft_ms / args.steps, 3)}
+            "fft2d_ms_per_step": round(fft_ms / args.steps, 3), "tile_shape": int(shape),
+            "autotune_ms_per_shape": [round(float(x), 2) for x in shape_ms]}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:

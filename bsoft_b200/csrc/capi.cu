@@ -395,7 +395,7 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
         cudaEventRecord(r->compute_done[i], r->stream);
     }
     {
-        const int rc2 = set_shape(r, 1);
+        const int rc2 = set_shape(r, 0);
         if (rc2) { free_all(r); delete r; return rc2; }
     }
     *out = reinterpret_cast<bsg_recon*>(r);

@@ -44,7 +44,7 @@ struct Context {
     unsigned* d_fmax = nullptr;      // max |Re F|, |Im F| of the batch (float bits)
     float pw_max = 0.f;              // max particle weight of the batch
     int fix_bits = 44;               // largest |F w| maps below 2^fix_bits
-    int shape = 1;                   // gridding tile shape (insert.cu kShapes)
+    int shape = 0;                   // gridding tile shape (insert.cu kShapes)
     int* d_tile_order = nullptr;     // tile visiting order for `shape`
     int replicas = 1;                // warps per tile, each on a slice of the particles
     double* d_part_sums = nullptr;   // replica partial sums (replicas > 1)

@@ -118,7 +118,7 @@ int  bsg_recon_fsc(bsg_recon* r, int nshell, double* fsc_out);
 int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* params,
                           long nparts, float* out, int flags);
 
-/* Gridding tile shape (0: 8x8x8, 1: 16x16x4 (default), 2: 16x8x8,
+/* Gridding tile shape (0: 8x8x8 (default), 1: 16x16x4, 2: 16x8x8,
  * 3: 16x16x8 without FOM).  bsg_recon_autotune times every shape on the
  * given particles, keeps the fastest and then clears the accumulators: call
  * it before inserting.  ms_out (optional) receives one time per shape
