@@ -134,6 +134,25 @@ int  bsg_recon_reset(bsg_recon* r);          /* zero the accumulators        */
 int  bsg_recon_synchronize(bsg_recon* r);
 void* bsg_recon_stream(bsg_recon* r);        /* the context's cudaStream_t  */
 
+/* The 2-D stage without any device allocation by the library, for callers
+ * that manage all device memory themselves (a pipeline that reserves its
+ * memory up front, or a host that forbids device allocations after start-up).
+ * No counterpart in the reference: it never runs on a GPU.
+ *
+ * d_images (nparts x n x n float32) and d_out (nparts x ft x ft complex64,
+ * the same order as bsg_particle_spectra) are device pointers owned by the
+ * caller; params is the host record array.  Work goes to `stream` (a
+ * cudaStream_t, NULL for the default stream).  The intermediate data use a
+ * fixed scratch area of BSG_NOALLOC_SCRATCH_BYTES inside the library, held
+ * on every GPU that loads it until exit; a call needing more (too many or
+ * too large particles) fails with BSG_ERR_ARG and says how many fit.  The
+ * first call on a device looks up that area's address: make it before any
+ * stream capture.  Calls share the area, so calls whose work overlaps on
+ * the GPU race: serialise them. */
+#define BSG_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int  bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const float* d_images, const double* params,
+                                  long nparts, float* d_out, void* stream);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 
