@@ -173,10 +173,11 @@ def cpu_threads_for_reference():
 
 def run_reference(args):
     """The reference processes its particle list in one pass, so the timed
-    steps (one particle per thread each) run inside one breconstruct call;
-    the warm-up is a separate small call."""
+    steps run inside one breconstruct call (one particle per thread per step,
+    at least 8 per thread so the map set-up and final transform do not
+    dominate); the warm-up is a separate small call."""
     threads = cpu_threads_for_reference()
-    n = threads * args.steps
+    n = threads * max(args.steps, 8)
     w = make_workload(max(n, 2 * threads))
     if args.warmup:
         v, sample = reference_sample(w, 2 * threads, threads)

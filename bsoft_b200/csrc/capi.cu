@@ -205,7 +205,7 @@ static int run_batch_kernels(Recon* r, const float* d_img, long np, float2* spec
         if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
         CK(launch_insert(*r, spec_out, 0, (int)np, r->nhalves == 2 ? h : -1, s));
         if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 0}); }
-        r->stats.launches += 1;
+        r->stats.launches += r->replicas > 1 ? 2 : 1;     // gridding (+ replica combine)
         r->stats.insert_launches += 1;
     }
     r->stats.particles += np;
