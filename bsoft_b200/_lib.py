@@ -28,6 +28,24 @@ class ReconStats(C.Structure):
                 ("fft2d_ms", C.c_double), ("h2d_ms", C.c_double), ("particles", C.c_long)]
 
 
+class MatchConfig(C.Structure):
+    _fields_ = [("n", C.c_int), ("map", C.c_int), ("map_sampling", C.c_double), ("pixel", C.c_double),
+                ("hi_res", C.c_double), ("lo_res", C.c_double), ("kernel_width", C.c_int),
+                ("kernel_power", C.c_int), ("batch", C.c_int), ("device", C.c_int)]
+
+
+class MatchInfo(C.Structure):
+    _fields_ = [("diam", C.c_int), ("npix", C.c_int), ("nshell", C.c_int), ("hi_res", C.c_double),
+                ("max_rad", C.c_double), ("section_res", C.c_double), ("map_sampling_cut", C.c_double),
+                ("pixel_cut", C.c_double)]
+
+
+MATCH_APPLY_CTF = 1
+MATCH_INVERT = 2
+MATCH_CTF_DOUBLES = 8
+MATCH_HYP_DOUBLES = 12
+
+
 class BsgError(RuntimeError):
     pass
 
@@ -59,6 +77,15 @@ def load():
         "bsg_recon_reset": ([vp], C.c_int),
         "bsg_recon_synchronize": ([vp], C.c_int),
         "bsg_recon_stream": ([vp], vp),
+        "bsg_match_create": ([C.POINTER(MatchConfig), C.POINTER(vp)], C.c_int),
+        "bsg_match_destroy": ([vp], None),
+        "bsg_match_info": ([vp, C.POINTER(MatchInfo)], C.c_int),
+        "bsg_match_set_reference": ([vp, vp, dp, C.c_int], C.c_int),
+        "bsg_match_reference_transform": ([vp, vp, C.c_int], C.c_int),
+        "bsg_match_sections": ([vp, dp, C.c_long, vp, C.c_int], C.c_int),
+        "bsg_match_set_images": ([vp, vp, C.c_long, dp, C.c_double, C.c_double, C.c_int], C.c_int),
+        "bsg_match_prepared": ([vp, C.c_long, C.c_long, vp, C.c_int], C.c_int),
+        "bsg_match_score": ([vp, dp, C.c_long, dp, dp, C.c_int], C.c_int),
         "bsg_last_error": ([], C.c_char_p),
         "bsg_version": ([], C.c_char_p),
     }

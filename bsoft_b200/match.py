@@ -1,0 +1,136 @@
+"""Host-side mirror of the reference's projection-matching operators on the
+GPU (brefine's scoring path, bsoft/src/mg/mg_refine.cpp).
+
+``Matcher`` holds one prepared reference map and a set of prepared particle
+images on the device and scores (image, view, origin) hypotheses with the
+reference's FRC figure of merit:
+
+    m = Matcher(n=128, map=128, map_sampling=1.5, pixel=1.5, hi_res=3.75)
+    m.set_reference(volume, origin=(64, 64, 64))      # project_refine_orientations
+    m.set_images(images, ctf_records)                 # part_refine_orientation
+    fom, cv = m.score(hypotheses)                     # img_recip_space_fom
+
+Hypotheses are rows of 12 doubles: image index, the view matrix (row-major,
+as View::matrix) and the origin (x, y) in pixels of the particle image.
+CTF records are rows of 8 doubles: volt, abw00, abw20, abw22, abw2m2, abw40,
+flags (MATCH_APPLY_CTF | MATCH_INVERT), 0.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import MATCH_APPLY_CTF, MATCH_INVERT, MATCH_CTF_DOUBLES, MATCH_HYP_DOUBLES  # noqa: F401
+
+
+def _ptr(a):
+    if hasattr(a, "data_ptr") and getattr(a, "is_cuda", False):
+        return C.c_void_p(a.data_ptr()), True
+    return C.c_void_p(a.ctypes.data), False
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Matcher:
+    def __init__(self, n: int, map: int, map_sampling: float, pixel: float, hi_res: float, lo_res: float = 0.0,
+                 kernel_width: int = 8, kernel_power: int = 2, batch: int = 0, device: int = 0):
+        L = _lib.load()
+        cfg = _lib.MatchConfig(n, map, map_sampling, pixel, hi_res, lo_res, kernel_width, kernel_power, batch, device)
+        h = C.c_void_p()
+        _lib.check(L.bsg_match_create(C.byref(cfg), C.byref(h)), "bsg_match_create")
+        self._h = h
+        info = _lib.MatchInfo()
+        _lib.check(L.bsg_match_info(h, C.byref(info)), "bsg_match_info")
+        self.info = info
+        self.diam = info.diam
+        self.n = n
+        self.N = map
+        self.nimg = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().bsg_match_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_reference(self, volume, origin=None) -> None:
+        if origin is None:
+            origin = (self.N // 2,) * 3
+        o = np.ascontiguousarray(origin, dtype=np.float64)
+        if not (hasattr(volume, "data_ptr") and getattr(volume, "is_cuda", False)):
+            volume = np.ascontiguousarray(volume, dtype=np.float32)
+        p, dev = _ptr(volume)
+        _lib.check(_lib.load().bsg_match_set_reference(self._h, p, _dp(o), _lib.BSG_DEVICE_PTR if dev else 0),
+                   "bsg_match_set_reference")
+
+    def reference_transform(self) -> np.ndarray:
+        D = self.diam
+        out = np.empty((D, D, D), dtype=np.complex64)
+        _lib.check(_lib.load().bsg_match_reference_transform(self._h, C.c_void_p(out.ctypes.data), 0),
+                   "bsg_match_reference_transform")
+        return out
+
+    def sections(self, mats) -> np.ndarray:
+        m = np.ascontiguousarray(mats, dtype=np.float64).reshape(-1, 9)
+        D = self.diam
+        out = np.empty((len(m), D, D), dtype=np.complex64)
+        _lib.check(_lib.load().bsg_match_sections(self._h, _dp(m), len(m), C.c_void_p(out.ctypes.data), 0),
+                   "bsg_match_sections")
+        return out
+
+    def set_images(self, images, ctf, file_avg: float = 0.0, file_std: float = 0.0) -> None:
+        """Prepare particle images (nimg, n, n) with their CTF records
+        (nimg, 8).  file_std > 0: normalise by the stack file's statistics,
+        as the reference does for particles read from a stack."""
+        c = np.ascontiguousarray(ctf, dtype=np.float64).reshape(-1, MATCH_CTF_DOUBLES)
+        if not (hasattr(images, "data_ptr") and getattr(images, "is_cuda", False)):
+            images = np.ascontiguousarray(images, dtype=np.float32)
+        nimg = images.shape[0]
+        if len(c) != nimg:
+            raise ValueError("one CTF record per image")
+        p, dev = _ptr(images)
+        _lib.check(_lib.load().bsg_match_set_images(self._h, p, nimg, _dp(c), float(file_avg), float(file_std),
+                                                    _lib.BSG_DEVICE_PTR if dev else 0), "bsg_match_set_images")
+        self.nimg = nimg
+
+    def prepared(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        count = self.nimg - first if count is None else count
+        D = self.diam
+        out = np.empty((count, D, D), dtype=np.complex64)
+        _lib.check(_lib.load().bsg_match_prepared(self._h, first, count, C.c_void_p(out.ctypes.data), 0),
+                   "bsg_match_prepared")
+        return out
+
+    def score(self, hyps):
+        h = np.ascontiguousarray(hyps, dtype=np.float64).reshape(-1, MATCH_HYP_DOUBLES)
+        fom = np.empty(len(h))
+        cv = np.empty(len(h))
+        _lib.check(_lib.load().bsg_match_score(self._h, _dp(h), len(h), _dp(fom), _dp(cv), 0), "bsg_match_score")
+        return fom, cv
+
+
+def ctf_record(volt: float, coefs, apply: bool = True, invert: bool = False) -> np.ndarray:
+    """CTF record from the aberration weights [abw00, abw20, abw22, abw2m2, abw40, ...]."""
+    c = np.asarray(coefs, dtype=np.float64)
+    flags = (MATCH_APPLY_CTF if apply else 0) | (MATCH_INVERT if invert else 0)
+    return np.array([volt, c[0], c[1], c[2], c[3], c[4], flags, 0.0])
+
+
+def hypothesis(img: int, mat, origin) -> np.ndarray:
+    m = np.asarray(mat, dtype=np.float64).reshape(9)
+    return np.array([img, *m, origin[0], origin[1]], dtype=np.float64)

@@ -153,6 +153,84 @@ void* bsg_recon_stream(bsg_recon* r);        /* the context's cudaStream_t  */
 int  bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const float* d_images, const double* params,
                                   long nparts, float* d_out, void* stream);
 
+/* ---- projection matching (brefine's scoring path) -------------------------
+ *
+ *   bsg_match_create        <- project_refine_orientations' set-up
+ *                              (bsoft/src/mg/mg_refine.cpp:279-316): resolution
+ *                              checks, transform cut edge, FSI_Kernel
+ *                              (bsoft/include/FSI_Kernel.h:28-68)
+ *   bsg_match_set_reference <- pref->fft(), change_transform_size, clearing the
+ *                              zero-frequency term, phase_shift_to_origin
+ *                              (mg_refine.cpp:279-365)
+ *   bsg_match_sections      <- Bimage::central_section (Bimage.h:995,
+ *                              bsoft/src/img/Bimage_project.cpp:288-338) at the
+ *                              resolution img_fit_in_recip_space_grid uses
+ *                              (hi_res / 1.11, mg_refine.cpp:885)
+ *   bsg_match_set_images    <- part_refine_orientation's particle preparation
+ *                              (mg_refine.cpp:509-563)
+ *   bsg_match_score         <- one hypothesis of img_fit_in_recip_space_grid:
+ *                              origin, phase_shift_to_origin, central_section,
+ *                              img_recip_space_fom (mg_refine.cpp:660-781,
+ *                              external linkage, no header in the reference)
+ */
+#define BSG_MATCH_APPLY_CTF  1   /* CTF record flag: multiply the reference by the CTF (APPLY_CTF) */
+#define BSG_MATCH_INVERT     2   /* CTF record flag: contrast inversion (INVERT)                 */
+
+/* Per-image CTF record, 8 doubles: volt, abw00, abw20, abw22, abw2m2, abw40,
+ * flags (BSG_MATCH_*), 0.  As in img_recip_space_fom the CTF is applied only
+ * when the defocus abw20 / (-pi lambda) is at least 1 angstrom. */
+#define BSG_MATCH_CTF_DOUBLES 8
+/* Hypothesis record, 12 doubles: image index, view matrix (row-major, as
+ * View::matrix), origin x, y in pixels of the particle image. */
+#define BSG_MATCH_HYP_DOUBLES 12
+
+typedef struct {
+    int    n;             /* particle box edge: power of two, 32..512           */
+    int    map;           /* reference map edge N: power of two, 8..512         */
+    double map_sampling;  /* angstrom / voxel of the reference map              */
+    double pixel;         /* angstrom / pixel of the particle images            */
+    double hi_res;        /* high resolution limit (angstrom)                   */
+    double lo_res;        /* low resolution limit (angstrom), 0 = none          */
+    int    kernel_width;  /* FSI kernel width (reference default 8, max 8)      */
+    int    kernel_power;  /* FSI kernel power (reference default 2)             */
+    int    batch;         /* images per device chunk, 0 = automatic             */
+    int    device;        /* CUDA device ordinal                                */
+} bsg_match_config;
+
+typedef struct {
+    int    diam;             /* edge of the cut transforms                      */
+    int    npix;             /* pixels entering a figure of merit               */
+    int    nshell;           /* shells kept                                     */
+    double hi_res;           /* resolution after the reference's checks         */
+    double max_rad;          /* FRC radius (pixels of the cut transform)        */
+    double section_res;      /* central-section limit (hi_res / 1.11)           */
+    double map_sampling_cut; /* sampling of the cut reference transform         */
+    double pixel_cut;        /* sampling of the cut particle transforms         */
+} bsg_match_info_t;
+
+typedef struct bsg_match bsg_match;
+
+int  bsg_match_create(const bsg_match_config* cfg, bsg_match** out);
+void bsg_match_destroy(bsg_match* m);
+int  bsg_match_info(const bsg_match* m, bsg_match_info_t* info);
+
+/* Reference map (N^3 float32, x fastest) and its origin in voxels. */
+int  bsg_match_set_reference(bsg_match* m, const float* map, const double* origin, int flags);
+/* The prepared reference transform: diam^3 complex64, reference order. */
+int  bsg_match_reference_transform(bsg_match* m, float* out, int flags);
+/* Central sections for nviews row-major matrices: nviews x diam^2 complex64. */
+int  bsg_match_sections(bsg_match* m, const double* mats, long nviews, float* out, int flags);
+/* Particle images (nimg x n x n float32) with their CTF records; file_avg /
+ * file_std are the statistics rescale_to_avg_std divides by (for a stack
+ * read by the reference: the file header's), file_std <= 0 uses each
+ * image's own.  Replaces the images held before. */
+int  bsg_match_set_images(bsg_match* m, const float* images, long nimg, const double* ctf,
+                          double file_avg, double file_std, int flags);
+/* Prepared particle transforms [first, first+count): diam^2 complex64 each. */
+int  bsg_match_prepared(bsg_match* m, long first, long count, float* out, int flags);
+/* FRC figure of merit (and cross-validation figure) of nhyp hypotheses. */
+int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, double* cv, int flags);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 

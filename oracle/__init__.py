@@ -51,9 +51,22 @@ def lib():
         L.orc_finish.argtypes = [C.POINTER(ReconCfg), dp, dp, dp, dp, dp, C.c_int]
         L.orc_finish.restype = C.c_long
         L.orc_fsc.argtypes = [C.c_int, dp, dp, C.c_int, dp]
-        L.orc_central_section.argtypes = [C.c_int, dp, dp, C.c_double, dp]
-        L.orc_frc_score.argtypes = [C.c_int, dp, dp, C.c_int, C.c_int, dp]
-        L.orc_frc_score.restype = C.c_double
+        L.orc_fsi_kernel.argtypes = [C.c_int, C.c_int, dp]
+        L.orc_fsi_kernel.restype = C.c_int
+        L.orc_match_diam.argtypes = [C.c_int, C.c_double, C.c_double]
+        L.orc_match_diam.restype = C.c_int
+        L.orc_match_map.argtypes = [C.c_int, C.POINTER(C.c_float), dp, C.c_double, C.c_double, dp,
+                                    C.POINTER(C.c_int)]
+        L.orc_match_map.restype = C.c_int
+        L.orc_central_section.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, dp, C.c_int, dp]
+        L.orc_central_section.restype = C.c_int
+        L.orc_match_particle.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int, C.c_double, C.c_double, dp]
+        L.orc_match_particle.restype = C.c_int
+        L.orc_phase_shift_2d.argtypes = [C.c_int, dp, dp]
+        L.orc_phase_shift_2d.restype = None
+        L.orc_recip_space_fom.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                          C.c_double, C.c_int, dp, C.c_int, dp]
+        L.orc_recip_space_fom.restype = C.c_double
         _lib = L
     return _lib
 
@@ -130,3 +143,80 @@ def particle_transform(plan, image: np.ndarray, params_row: np.ndarray) -> np.nd
 
 def ref_binary(name: str) -> str:
     return os.path.join(REF_DIR, name)
+
+
+# ---- projection matching -------------------------------------------------
+
+def fsi_kernel(width: int = 8, power: int = 2) -> np.ndarray:
+    """FSI_Kernel table, shape (513, width)."""
+    w = 1 if power < 0 else width
+    t = np.zeros(513 * w)
+    lib().orc_fsi_kernel(width, power, _dp(t))
+    return t.reshape(513, w)
+
+
+def match_diam(N: int, sampling: float, hi_res: float) -> int:
+    return int(lib().orc_match_diam(N, sampling, hi_res))
+
+
+def match_map(vol: np.ndarray, origin, sampling: float, hi_res: float) -> np.ndarray:
+    """Prepared reference transform (diam, diam, diam) complex128."""
+    N = vol.shape[0]
+    v = np.ascontiguousarray(vol, dtype=np.float32)
+    spec = np.zeros(2 * N ** 3)
+    d = C.c_int(0)
+    o = np.asarray(origin, dtype=np.float64)
+    rc = lib().orc_match_map(N, v.ctypes.data_as(C.POINTER(C.c_float)), _dp(o), sampling, hi_res, _dp(spec),
+                             C.byref(d))
+    if rc:
+        raise RuntimeError(f"orc_match_map failed: {rc}")
+    D = d.value
+    return spec[:2 * D ** 3].view(np.complex128).reshape(D, D, D)
+
+
+def central_section(spec: np.ndarray, mat: np.ndarray, real_size: float, resolution: float,
+                    kernel: np.ndarray) -> np.ndarray:
+    D = spec.shape[0]
+    s = np.ascontiguousarray(spec, dtype=np.complex128)
+    m = np.ascontiguousarray(mat, dtype=np.float64).reshape(9)
+    k = np.ascontiguousarray(kernel, dtype=np.float64)
+    out = np.zeros(2 * D * D)
+    rc = lib().orc_central_section(D, _dp(s.view(np.float64)), _dp(m), real_size, resolution, _dp(k),
+                                   k.shape[1], _dp(out))
+    if rc:
+        raise RuntimeError(f"orc_central_section failed: {rc}")
+    return out.view(np.complex128).reshape(D, D)
+
+
+def match_particle(image: np.ndarray, diam: int, file_avg: float = 0.0, file_std: float = 0.0) -> np.ndarray:
+    """Prepared particle transform; file_avg/file_std are the stack's header
+    statistics (file_std 0: the image's own)."""
+    n = image.shape[0]
+    img = np.ascontiguousarray(image, dtype=np.float32)
+    out = np.zeros(2 * diam * diam)
+    rc = lib().orc_match_particle(n, img.ctypes.data_as(C.POINTER(C.c_float)), diam, file_avg, file_std,
+                                  _dp(out))
+    if rc:
+        raise RuntimeError(f"orc_match_particle failed: {rc}")
+    return out.view(np.complex128).reshape(diam, diam)
+
+
+def phase_shift_2d(spec: np.ndarray, origin) -> np.ndarray:
+    s = np.ascontiguousarray(spec, dtype=np.complex128).copy()
+    o = np.asarray(origin, dtype=np.float64)
+    lib().orc_phase_shift_2d(s.shape[0], _dp(s.view(np.float64)), _dp(o))
+    return s
+
+
+def recip_space_fom(img: np.ndarray, ref: np.ndarray, img_real_size: float, ref_real_size: float,
+                    ref_sampling: float, hi_res: float, lo_res: float = 0.0, fom_type: int = 0,
+                    ctf=None, invert: bool = False):
+    """(fom, cv) of img_recip_space_fom."""
+    a = np.ascontiguousarray(img, dtype=np.complex128)
+    b = np.ascontiguousarray(ref, dtype=np.complex128)
+    c = None if ctf is None else np.ascontiguousarray(ctf, dtype=np.float64)
+    cv = np.zeros(1)
+    f = lib().orc_recip_space_fom(a.shape[0], _dp(a.view(np.float64)), _dp(b.view(np.float64)), img_real_size,
+                                  ref_real_size, ref_sampling, hi_res, lo_res, fom_type, _dp(c), int(invert),
+                                  _dp(cv))
+    return float(f), float(cv[0])

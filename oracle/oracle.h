@@ -60,15 +60,45 @@ int orc_fsc(int N, const double* vol1, const double* vol2, int nshell, double* f
 
 /* ---- projection matching (match_oracle.c) ---- */
 
-/* Central section of a complex N^3 map (standard FFT layout, origin at 0)
- * by trilinear interpolation: out = N*N complex doubles. */
-int orc_central_section(int N, const double* vol, const double* mat, double max_rad,
-                        double* out);
+/* FSI_Kernel lookup table: (512 + 1) * width doubles.  Returns the width
+ * actually used (1 for a negative power) or <0. */
+int orc_fsi_kernel(int width, int power, double* table);
 
-/* Shell-weighted Fourier ring correlation score between an image transform
- * and a reference section with the reference's per-shell normalisation. */
-double orc_frc_score(int N, const double* img, const double* ref, int rmin, int rmax,
-                     const double* ctf2d);
+/* Transform edge the reference map is cut to for a resolution limit. */
+int orc_match_diam(int N, double sampling, double hi_res);
+
+/* Reference map (real N^3, z-y-x order) -> its transform cut to diam^3
+ * (standard layout, 2*diam^3 doubles), zero-frequency term cleared, phase
+ * shifted to origin*diam/N.  spec must hold 2*N^3 doubles. */
+int orc_match_map(int N, const float* map, const double origin[3], double sampling, double hi_res,
+                  double* spec, int* diam_out);
+
+/* Kernel interpolation of a complex size^3 transform at voxel position m. */
+void orc_fspace_interpolate(int size, const double* spec, const double m[3], const double* kernel, int wd,
+                            double out[2]);
+
+/* Central section (size^2 complex doubles) of a size^3 transform for the
+ * row-major rotation `mat`, real_size = size * sampling (angstrom), pixels
+ * with s <= 1/resolution only. */
+int orc_central_section(int size, const double* spec, const double* mat, double real_size, double resolution,
+                        const double* kernel, int wd, double* out);
+
+/* Particle image (n^2 floats) -> transform of (image - avg)/std, unscaled,
+ * cut to diam^2 (2*diam^2 doubles), zero-frequency term cleared.  avg/std
+ * are the stack file's statistics (std <= 0: this image's own). */
+int orc_match_particle(int n, const float* image, int diam, double file_avg, double file_std, double* spec);
+
+/* In-place phase shift of a size^2 transform to an origin in pixels. */
+void orc_phase_shift_2d(int size, double* spec, const double origin[2]);
+
+/* img_recip_space_fom: FRC (fom_type 0) or DPR (1) figure of merit of an
+ * image transform against a reference section, both size^2 complex; ctf is
+ * NULL or the 7 aberration weights (the reference section is multiplied by
+ * the CTF, negated when invert).  The cross-validation figure goes to
+ * *cv_out. */
+double orc_recip_space_fom(int size, const double* img, const double* ref, double img_real_size,
+                           double ref_real_size, double ref_sampling, double hi_res, double lo_res,
+                           int fom_type, const double* ctf, int invert, double* cv_out);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,89 @@
+"""The CUDA matching path (libbsgpu, bsg_match_*) against the reference's
+own brefine steps (golden fixtures) and the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from tests.match_helpers import MATCH_CASES, ctf_records, hypotheses, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+# float32 kernels vs float32 reference output
+TOL_SPEC = 2e-6
+TOL_SECTION = 2e-5      # 512-tap FP32 accumulation
+TOL_FOM = 2e-5
+
+
+@pytest.fixture(scope="module", params=MATCH_CASES)
+def matcher(request):
+    from bsoft_b200.match import Matcher
+    d = load(request.param)
+    m = Matcher(n=d["n"], map=d["N"], map_sampling=d["pixel"], pixel=d["pixel"], hi_res=d["hi_res"])
+    m.set_reference(d["map"], d["map_origin"])
+    m.set_images(d["images"], ctf_records(d), float(d["file_avg"]), float(d["file_std"]))
+    yield m, d
+    m.close()
+
+
+def test_geometry(matcher):
+    m, d = matcher
+    assert m.diam == d["diam"]
+    assert abs(m.info.section_res - m.info.hi_res / 1.11) < 1e-12
+
+
+def test_reference_transform(matcher):
+    m, d = matcher
+    t = m.reference_transform()
+    assert rel_l2(t, d["map_spec"]) < TOL_SPEC
+    assert t[0, 0, 0] == 0
+
+
+def test_sections(matcher):
+    m, d = matcher
+    s = m.sections(d["mats"])
+    for a, b in zip(s, d["sections"]):
+        assert rel_l2(a, b) < TOL_SECTION
+
+
+def test_prepared_images(matcher):
+    m, d = matcher
+    p = m.prepared()
+    for a, b in zip(p, d["prepared"]):
+        assert rel_l2(a, b) < TOL_SPEC
+
+
+def test_figure_of_merit(matcher):
+    m, d = matcher
+    fom, cv = m.score(hypotheses(d))
+    assert np.max(np.abs(fom - d["fom"][:, 0])) < TOL_FOM
+    assert np.max(np.abs(cv - d["fom"][:, 1])) < TOL_FOM
+
+
+def test_own_image_statistics(matcher):
+    """file_std = 0 normalises each image by its own statistics; the figure
+    of merit is scale-invariant, so it is unchanged."""
+    m, d = matcher
+    m.set_images(d["images"], ctf_records(d))
+    fom, _ = m.score(hypotheses(d))
+    assert np.max(np.abs(fom - d["fom"][:, 0])) < TOL_FOM
+    p = m.prepared()
+    o = oracle.match_particle(d["images"][0], d["diam"])
+    assert rel_l2(p[0], o) < TOL_SPEC
+    m.set_images(d["images"], ctf_records(d), float(d["file_avg"]), float(d["file_std"]))
+
+
+def test_deterministic(matcher):
+    m, d = matcher
+    h = hypotheses(d)
+    a, _ = m.score(h)
+    b, _ = m.score(h[::-1].copy())
+    assert np.array_equal(a, b[::-1])
+
+
+def test_bad_arguments():
+    from bsoft_b200.match import Matcher
+    from bsoft_b200._lib import BsgError
+    with pytest.raises(BsgError):
+        Matcher(n=48, map=48, map_sampling=1.5, pixel=1.5, hi_res=3.75)   # not a power of two
+    with pytest.raises(BsgError):
+        Matcher(n=32, map=64, map_sampling=1.5, pixel=1.5, hi_res=3.0)    # cut edge above the box
