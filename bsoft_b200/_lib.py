@@ -40,6 +40,15 @@ class MatchInfo(C.Structure):
                 ("pixel_cut", C.c_double)]
 
 
+class MatchStats(C.Structure):
+    _fields_ = [("panel_ms", C.c_double), ("agen_ms", C.c_double), ("gemm_ms", C.c_double),
+                ("merge_ms", C.c_double), ("rescore_ms", C.c_double), ("gemm_flops", C.c_double),
+                ("hypotheses", C.c_double), ("launches", C.c_long), ("gemm_launches", C.c_long),
+                ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int)]
+
+
+MATCH_RESULT_DOUBLES = 5
+MATCH_TOPK_MAX = 8
 MATCH_APPLY_CTF = 1
 MATCH_INVERT = 2
 MATCH_CTF_DOUBLES = 8
@@ -86,6 +95,10 @@ def load():
         "bsg_match_set_images": ([vp, vp, C.c_long, dp, C.c_double, C.c_double, C.c_int], C.c_int),
         "bsg_match_prepared": ([vp, C.c_long, C.c_long, vp, C.c_int], C.c_int),
         "bsg_match_score": ([vp, dp, C.c_long, dp, dp, C.c_int], C.c_int),
+        "bsg_match_set_panel": ([vp, dp, C.c_long, C.c_int], C.c_int),
+        "bsg_match_search": ([vp, dp, C.c_int, C.c_int, dp, C.c_int], C.c_int),
+        "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
+        "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_last_error": ([], C.c_char_p),
         "bsg_version": ([], C.c_char_p),
     }

@@ -26,7 +26,7 @@
 // each of the 16 load rounds reads 4 rows of 8 consecutive x taps, so a
 // pixel costs ~160 L1 sectors instead of 512 scattered loads, and a warp
 // moves along a shell so successive pixels reuse most of their 8^3 taps.
-#include "common.cuh"
+#include "match.cuh"
 #include "fft_dev.cuh"
 
 #include <math.h>
@@ -44,72 +44,6 @@ namespace bsg {
 void set_error(const char* fmt, ...);
 
 namespace {
-
-constexpr int NDIV = 512;     // FSI_Kernel divisions (FSI_Kernel.h:42)
-constexpr int MAXW = 8;       // widest kernel the warp gather supports
-constexpr int FOM_WARPS = 8;
-
-struct MPix {
-    short h, k;     // signed frequency indices
-    int idx;        // index in the diam^2 transform
-    short shell;    // (long) sqrt(h^2 + k^2)
-    short insec;    // 1: inside the section's resolution limit
-    int pad;
-};
-static_assert(sizeof(MPix) == 16, "MPix layout");
-
-struct MHyp {
-    double m[9];    // view matrix with rows 0, 1 scaled (mg_refine.cpp:876-880)
-    double sx, sy;  // phase slopes 2 pi origin / diam (cut pixels)
-    int img;
-    int pad;
-};
-
-__device__ __forceinline__ int wrap1(int j, int D) {
-    if (j < 0) j += D;
-    if (j >= D) j -= D;
-    // only reachable for positions more than a map edge outside, which the
-    // reference would read out of bounds: keep the access inside
-    return min(max(j, 0), D - 1);
-}
-
-// FSI kernel interpolation of the diam^3 transform at voxel position m by
-// one warp (Bimage::fspace_interpolate).  Every lane returns the sum.
-// T = double reproduces the reference's FP64 accumulation (with a double
-// kernel table): near the cut edge the taps wrap onto lower frequencies that
-// are orders of magnitude stronger than the result, and FP32 weights and
-// sums lose ~1% there.  T = float serves the BF16 search panel.
-template <typename T>
-__device__ __forceinline__ void fsi_gather(const float2* __restrict__ vol, int D, double mx, double my, double mz,
-                                           const T* __restrict__ lut, int wd, int lane, T& out_re, T& out_im) {
-    const int half = (wd - 1) / 2;
-    const double fx = floor(mx), fy = floor(my), fz = floor(mz);
-    const int ikx = (int)((mx - fx) * NDIV + 0.5) * wd;
-    const int iky = (int)((my - fy) * NDIV + 0.5) * wd;
-    const int ikz = (int)((mz - fz) * NDIV + 0.5) * wd;
-    const int ibx = (int)fx - half, iby = (int)fy - half, ibz = (int)fz - half;
-    const int xl = lane & 7, rq = lane >> 3;
-    T ar = 0, ai = 0;
-    if (xl < wd) {
-        const int jx = wrap1(ibx + xl, D);
-        const T kx = lut[ikx + xl];
-        for (int r = rq; r < wd * wd; r += 4) {
-            const int zz = r / wd, yy = r - zz * wd;
-            const int jz = wrap1(ibz + zz, D), jy = wrap1(iby + yy, D);
-            const T w = kx * (lut[iky + yy] * lut[ikz + zz]);
-            const float2 v = __ldg(vol + ((size_t)jz * D + jy) * D + jx);
-            ar += (T)v.x * w;
-            ai += (T)v.y * w;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        ar += __shfl_xor_sync(0xffffffffu, ar, o);
-        ai += __shfl_xor_sync(0xffffffffu, ai, o);
-    }
-    out_re = ar;
-    out_im = ai;
-}
 
 // ---- transforms ---------------------------------------------------------
 
@@ -258,11 +192,6 @@ __global__ void img_cut_kernel(const double2* __restrict__ full, int n, int D, l
     }
 }
 
-struct ImgCtf {
-    double c[5];     // abw00 abw20 abw22 abw2m2 abw40
-    int apply;       // multiply the reference by the CTF
-    int invert;      // negate the CTF (contrast inversion)
-};
 
 // per image: CTF at the figure-of-merit pixels (ctf.h:321-365 with
 // s = index / (n * pixel)) and the image power per shell (fixed order)
@@ -454,48 +383,6 @@ double electron_lambda(double volt) {
 }
 
 }  // namespace
-
-// ---- the context ----------------------------------------------------------
-
-struct Match {
-    bsg_match_config cfg;
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int N = 0, n = 0, D = 0, wd = 8;
-    double hi_res = 0, map_samp_cut = 0, img_samp_cut = 0, sec_res = 0;
-    double real_map = 0, real_img = 0, max_rad = 0, max_rad_cv = 0;
-    double scx = 1, scy = 1;           // pref sampling / particle sampling
-    double cut_scale = 1;              // diam / n (long double in the reference)
-    int nshell = 0, nf = 0, cv0 = 0, cv1 = 0;
-    std::vector<MPix> h_pix;           // figure-of-merit pixels, shell-sorted
-    std::vector<int> h_shell_start;
-    std::vector<MPix> h_secpix;        // section pixels
-    MPix* d_pix = nullptr;
-    int* d_shell_start = nullptr;
-    MPix* d_secpix = nullptr;
-    double* d_lut = nullptr;
-    double2* d_tw_map = nullptr;
-    double2* d_tw_img = nullptr;
-    float2* d_ref = nullptr;           // diam^3
-    bool have_ref = false;
-    // images
-    long cap = 0, nimg = 0;
-    float2* d_spec = nullptr;          // cap x diam^2
-    float* d_ctf = nullptr;            // cap x npix
-    double* d_dsum = nullptr;          // cap x nshell
-    // scratch
-    float* d_real = nullptr;           // batch x n^2 (or N^3 for the map)
-    double2* d_work = nullptr;         // batch x n^2 complex (or N^3), FP64
-    size_t work_elems = 0;
-    double* d_scale = nullptr;
-    double* d_shift = nullptr;
-    ImgCtf* d_ictf = nullptr;
-    MHyp* d_hyp = nullptr;
-    long hyp_cap = 0;
-    double* d_out = nullptr;           // 2 x hyp_cap
-    float* h_pin = nullptr;            // pinned staging
-    size_t pin_bytes = 0;
-};
 
 }  // namespace bsg
 
@@ -720,7 +607,9 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
     if (M->stream) cudaStreamSynchronize(M->stream);
     void* ptrs[] = {M->d_pix, M->d_shell_start, M->d_secpix, M->d_lut, M->d_tw_map, M->d_tw_img, M->d_ref,
                     M->d_spec, M->d_ctf, M->d_dsum, M->d_real, M->d_work, M->d_scale, M->d_shift, M->d_ictf,
-                    M->d_hyp, M->d_out};
+                    M->d_hyp, M->d_out, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
+                    M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_chyp, M->d_cfom, M->d_gA, M->d_slopes,
+                    M->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);
     if (M->stream) cudaStreamDestroy(M->stream);
@@ -795,7 +684,8 @@ extern "C" int bsg_match_reference_transform(bsg_match* h, float* out, int flags
     return BSG_OK;
 }
 
-static void view_rows(const Match& M, const double* mat, double* m) {
+namespace bsg {
+void match_view_rows(const Match& M, const double* mat, double* m) {
     // img_fit_in_recip_space_grid: rows 0 and 1 multiplied componentwise by
     // (pref sampling / particle sampling) per axis, z component by 1
     for (int r = 0; r < 3; ++r)
@@ -805,6 +695,37 @@ static void view_rows(const Match& M, const double* mat, double* m) {
             m[3 * r + c] = v;
         }
 }
+
+int match_fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    set_error("%s", buf);
+    return code;
+}
+
+cudaError_t launch_fom(const Match& M, const MHyp* d_hyps, long nh, double* d_fom, double* d_cv, cudaStream_t s) {
+    FomArgs a{};
+    a.vol = M.d_ref; a.D = M.D; a.wd = M.wd; a.lut = M.d_lut;
+    a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_hyps;
+    a.spec = M.d_spec; a.ctf = M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
+    a.inv = 1.0 / M.real_map; a.real = M.real_map;
+    a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
+    a.fom = d_fom; a.cv = d_cv;
+    const size_t smem = sizeof(double) * (NDIV + 1) * MAXW + sizeof(float) * FOM_WARPS * M.nshell * 2;
+    for (long h0 = 0; h0 < nh; h0 += 65535L * 32) {
+        const long cnt = std::min(nh - h0, 65535L * 32);
+        FomArgs b = a;
+        b.hyps = d_hyps + h0; b.fom = d_fom + h0; b.cv = d_cv + h0;
+        fom_kernel<<<(unsigned)cnt, FOM_WARPS * 32, smem, s>>>(b);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+}  // namespace bsg
 
 static int ensure_hyps(Match& M, long nh) {
     if (nh <= M.hyp_cap) return BSG_OK;
@@ -831,7 +752,7 @@ extern "C" int bsg_match_sections(bsg_match* h, const double* mats, long nviews,
     std::vector<MHyp> hv(nviews);
     for (long v = 0; v < nviews; ++v) {
         memset(&hv[v], 0, sizeof(MHyp));
-        view_rows(*M, mats + 9 * v, hv[v].m);
+        match_view_rows(*M, mats + 9 * v, hv[v].m);
     }
     cudaStream_t s = M->stream;
     MCK(cudaMemcpyAsync(M->d_hyp, hv.data(), sizeof(MHyp) * nviews, cudaMemcpyHostToDevice, s));
@@ -964,7 +885,7 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
         if (img < 0 || img >= M->nimg) return mfail(BSG_ERR_ARG, "bsg_match_score: hypothesis %ld names image %ld", i, img);
         memset(&hv[i], 0, sizeof(MHyp));
         hv[i].img = (int)img;
-        view_rows(*M, r + 1, hv[i].m);
+        match_view_rows(*M, r + 1, hv[i].m);
         // origin in pixels of the uncut image, scaled with the cut
         // (Bimage_fft.cpp:433), then phase_shift_to_origin's 2 pi o / size
         const double ox = M->cut_scale * r[10], oy = M->cut_scale * r[11];
@@ -973,16 +894,7 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
     }
     cudaStream_t s = M->stream;
     MCK(cudaMemcpyAsync(M->d_hyp, hv.data(), sizeof(MHyp) * nhyp, cudaMemcpyHostToDevice, s));
-    FomArgs a{};
-    a.vol = M->d_ref; a.D = M->D; a.wd = M->wd; a.lut = M->d_lut;
-    a.pix = M->d_pix; a.npix = (int)M->h_pix.size(); a.hyps = M->d_hyp;
-    a.spec = M->d_spec; a.ctf = M->d_ctf; a.dsum = M->d_dsum; a.nshell = M->nshell;
-    a.inv = 1.0 / M->real_map; a.real = M->real_map;
-    a.nf = M->nf; a.cv0 = M->cv0; a.cv1 = M->cv1;
-    a.fom = M->d_out; a.cv = M->d_out + nhyp;
-    const size_t smem = sizeof(double) * (NDIV + 1) * MAXW + sizeof(float) * FOM_WARPS * M->nshell * 2;
-    fom_kernel<<<(unsigned)nhyp, FOM_WARPS * 32, smem, s>>>(a);
-    MCK(cudaGetLastError());
+    MCK(launch_fom(*M, M->d_hyp, nhyp, M->d_out, M->d_out + nhyp, s));
     MCK(cudaMemcpyAsync(fom, M->d_out, sizeof(double) * nhyp, cudaMemcpyDeviceToHost, s));
     if (cv) MCK(cudaMemcpyAsync(cv, M->d_out + nhyp, sizeof(double) * nhyp, cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));

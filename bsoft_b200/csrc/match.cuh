@@ -1,0 +1,158 @@
+// match.cuh - the projection-matching context shared by match.cu (transforms,
+// sections, exact scoring) and search.cu (the exhaustive BF16 search).
+#pragma once
+
+#include "common.cuh"
+
+#include <cuda_bf16.h>
+
+#include <vector>
+
+namespace bsg {
+
+constexpr int NDIV = 512;     // FSI_Kernel divisions (FSI_Kernel.h:42)
+constexpr int MAXW = 8;       // widest kernel the warp gather supports
+constexpr int FOM_WARPS = 8;
+
+struct MPix {
+    short h, k;     // signed frequency indices
+    int idx;        // index in the diam^2 transform
+    short shell;    // (long) sqrt(h^2 + k^2)
+    short insec;    // 1: inside the section's resolution limit
+    int pad;
+};
+static_assert(sizeof(MPix) == 16, "MPix layout");
+
+struct MHyp {
+    double m[9];    // view matrix with rows 0, 1 scaled (mg_refine.cpp:876-880)
+    double sx, sy;  // phase slopes 2 pi origin / diam (cut pixels)
+    int img;
+    int pad;
+};
+
+__device__ __forceinline__ int wrap1(int j, int D) {
+    if (j < 0) j += D;
+    if (j >= D) j -= D;
+    // only reachable for positions more than a map edge outside, which the
+    // reference would read out of bounds: keep the access inside
+    return min(max(j, 0), D - 1);
+}
+
+// FSI kernel interpolation of the diam^3 transform at voxel position m by
+// one warp (Bimage::fspace_interpolate).  Every lane returns the sum.
+// T = double reproduces the reference's FP64 accumulation (with a double
+// kernel table): near the cut edge the taps wrap onto lower frequencies that
+// are orders of magnitude stronger than the result, and FP32 weights and
+// sums lose ~1% there.  T = float serves the BF16 search panel.
+template <typename T>
+__device__ __forceinline__ void fsi_gather(const float2* __restrict__ vol, int D, double mx, double my, double mz,
+                                           const T* __restrict__ lut, int wd, int lane, T& out_re, T& out_im) {
+    const int half = (wd - 1) / 2;
+    const double fx = floor(mx), fy = floor(my), fz = floor(mz);
+    const int ikx = (int)((mx - fx) * NDIV + 0.5) * wd;
+    const int iky = (int)((my - fy) * NDIV + 0.5) * wd;
+    const int ikz = (int)((mz - fz) * NDIV + 0.5) * wd;
+    const int ibx = (int)fx - half, iby = (int)fy - half, ibz = (int)fz - half;
+    const int xl = lane & 7, rq = lane >> 3;
+    T ar = 0, ai = 0;
+    if (xl < wd) {
+        const int jx = wrap1(ibx + xl, D);
+        const T kx = lut[ikx + xl];
+        for (int r = rq; r < wd * wd; r += 4) {
+            const int zz = r / wd, yy = r - zz * wd;
+            const int jz = wrap1(ibz + zz, D), jy = wrap1(iby + yy, D);
+            const T w = kx * (lut[iky + yy] * lut[ikz + zz]);
+            const float2 v = __ldg(vol + ((size_t)jz * D + jy) * D + jx);
+            ar += (T)v.x * w;
+            ai += (T)v.y * w;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        ar += __shfl_xor_sync(0xffffffffu, ar, o);
+        ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    out_re = ar;
+    out_im = ai;
+}
+
+struct ImgCtf {
+    double c[5];     // abw00 abw20 abw22 abw2m2 abw40
+    int apply;       // multiply the reference by the CTF
+    int invert;      // negate the CTF (contrast inversion)
+};
+
+struct Match {
+    bsg_match_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int N = 0, n = 0, D = 0, wd = 8;
+    double hi_res = 0, map_samp_cut = 0, img_samp_cut = 0, sec_res = 0;
+    double real_map = 0, real_img = 0, max_rad = 0, max_rad_cv = 0;
+    double scx = 1, scy = 1;           // pref sampling / particle sampling
+    double cut_scale = 1;              // diam / n (long double in the reference)
+    int nshell = 0, nf = 0, cv0 = 0, cv1 = 0;
+    std::vector<MPix> h_pix;           // figure-of-merit pixels, shell-sorted
+    std::vector<int> h_shell_start;
+    std::vector<MPix> h_secpix;        // section pixels
+    MPix* d_pix = nullptr;
+    int* d_shell_start = nullptr;
+    MPix* d_secpix = nullptr;
+    double* d_lut = nullptr;
+    double2* d_tw_map = nullptr;
+    double2* d_tw_img = nullptr;
+    float2* d_ref = nullptr;           // diam^3
+    bool have_ref = false;
+    // images
+    long cap = 0, nimg = 0;
+    float2* d_spec = nullptr;          // cap x diam^2
+    float* d_ctf = nullptr;            // cap x npix
+    double* d_dsum = nullptr;          // cap x nshell
+    // scratch
+    float* d_real = nullptr;           // batch x n^2 (or N^3 for the map)
+    double2* d_work = nullptr;         // batch x n^2 complex (or N^3), FP64
+    size_t work_elems = 0;
+    double* d_scale = nullptr;
+    double* d_shift = nullptr;
+    ImgCtf* d_ictf = nullptr;
+    MHyp* d_hyp = nullptr;
+    long hyp_cap = 0;
+    double* d_out = nullptr;           // 2 x hyp_cap
+    float* h_pin = nullptr;            // pinned staging
+    size_t pin_bytes = 0;
+    // exhaustive search (search.cu)
+    std::vector<MPix> h_cpix;          // coarse pixels: half plane, shells 1 .. nf-1
+    std::vector<int> h_cstart;
+    int ncpix = 0, kpad = 0;
+    MPix* d_cpix = nullptr;
+    int* d_cstart = nullptr;
+    long nsec = 0;
+    MHyp* d_secs = nullptr;            // panel views (rows 0, 1 scaled)
+    __nv_bfloat16* d_panel = nullptr;  // nsec x kpad
+    __nv_bfloat16* d_A = nullptr;      // rows x kpad
+    size_t a_elems = 0;
+    float* d_pscore = nullptr;         // partial top-8 per (range, row)
+    int* d_pidx = nullptr;
+    size_t part_elems = 0;
+    int* d_csec = nullptr;             // candidates per image
+    int* d_corg = nullptr;
+    float* d_cscore = nullptr;
+    MHyp* d_chyp = nullptr;
+    double* d_cfom = nullptr;
+    size_t cand_elems = 0;
+    float* d_gA = nullptr;             // per image and shell: 1 / (n_f sqrt(D_j C_j))
+    size_t gA_elems = 0;
+    double2* d_slopes = nullptr;       // per trial origin
+    size_t slope_elems = 0;
+    int* d_status = nullptr;
+    bsg_match_stats sstats{};
+};
+
+
+// exact FRC scoring of nh hypotheses already on the device (match.cu)
+cudaError_t launch_fom(const Match& M, const MHyp* d_hyps, long nh, double* d_fom, double* d_cv, cudaStream_t s);
+// view matrix rows 0, 1 scaled by the sampling ratio (img_fit_in_recip_space_grid)
+void match_view_rows(const Match& M, const double* mat, double* m);
+int match_fail(int code, const char* fmt, ...);
+
+}  // namespace bsg

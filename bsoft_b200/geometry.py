@@ -112,3 +112,53 @@ def angular_distance_deg(ra: np.ndarray, rb: np.ndarray) -> np.ndarray:
     t = np.einsum("...ij,...ij->...", ra, rb)
     c = np.clip((t - 1.0) / 2.0, -1.0, 1.0)
     return np.degrees(np.arccos(c))
+
+
+def asymmetric_unit_views_c(order: int, theta_step: float, phi_step: float, full: bool = True,
+                            inplane: bool = True) -> np.ndarray:
+    """Views (x, y, z, angle) tiling the asymmetric unit of the cyclic point
+    group C<order>: asymmetric_unit_views (bsoft/src/util/symmetry.cpp:383-461)
+    for 100 < point < 200.  Steps in radians; `full` covers both halves
+    (theta up to pi), `inplane` sets each view's angle to its azimuth as the
+    reference does.  C1 at 3 degrees gives 4,586 views."""
+    if theta_step < math.pi / 1800:
+        theta_step = math.pi / 180
+    if phi_step < math.pi / 1800:
+        phi_step = math.pi / 180
+    max_theta = math.pi / 2 + 1e-6
+    nphi = int(math.pi * 2.0 / (order * phi_step) + 0.5)
+    if full:
+        max_theta = math.pi + 1e-6
+    views = [(0.0, 0.0, 1.0, 0.0)]
+    theta = theta_step
+    while theta <= max_theta:
+        nrphi = int(nphi * math.sin(theta) / 2 + 0.5)
+        phi = 0.0
+        istart = 0
+        if nrphi:
+            phi = math.pi * 1.0 / (order * nrphi)
+            istart = -nrphi
+            if order < 2:
+                nrphi -= 1
+        for j in range(istart, nrphi + 1):
+            v = np.array([math.sin(theta) * math.cos(j * phi), math.sin(theta) * math.sin(j * phi), math.cos(theta)])
+            nv = np.linalg.norm(v)
+            v = v / nv if nv > 0 else np.array([0.0, 0.0, 1.0])
+            a = j * phi if inplane else 0.0
+            if a <= -math.pi:       # the view angle is kept in (-pi, pi]
+                a += 2 * math.pi
+            views.append((v[0], v[1], v[2], a))
+        theta += theta_step
+    if full and views[-1][2] > -0.999999:
+        views.append((0.0, 0.0, -1.0, 0.0))
+    return np.array(views, dtype=np.float64)
+
+
+def search_views(directions: np.ndarray, n_inplane: int) -> np.ndarray:
+    """Every direction at n_inplane in-plane angles 2 pi i / n_inplane added
+    to its own angle: (ndir * n_inplane, 4), direction-major."""
+    d = np.asarray(directions, dtype=np.float64)
+    psi = 2 * math.pi * np.arange(n_inplane) / n_inplane
+    out = np.repeat(d, n_inplane, axis=0)
+    out[:, 3] = np.array([angle_set_negpi_to_pi(a) for a in (out[:, 3] + np.tile(psi, len(d)))])
+    return out

@@ -124,6 +124,31 @@ class Matcher:
         return fom, cv
 
 
+    # ---- exhaustive search ----
+    def set_panel(self, mats) -> None:
+        """Search panel of central sections for row-major view matrices (nsec, 3, 3)."""
+        m = np.ascontiguousarray(mats, dtype=np.float64).reshape(-1, 9)
+        _lib.check(_lib.load().bsg_match_set_panel(self._h, _dp(m), len(m), 0), "bsg_match_set_panel")
+        self.nsec = len(m)
+
+    def search(self, origins, topk: int = 8) -> np.ndarray:
+        """Every held image at every trial origin (norigin, 2) against the
+        panel; returns (nimg, topk, 5): section, origin index, correlation
+        score, FRC figure of merit, cross-validation figure, best first."""
+        o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 2)
+        out = np.empty((self.nimg, topk, _lib.MATCH_RESULT_DOUBLES))
+        _lib.check(_lib.load().bsg_match_search(self._h, _dp(o), len(o), topk, _dp(out), 0), "bsg_match_search")
+        return out
+
+    def stats(self) -> dict:
+        st = _lib.MatchStats()
+        _lib.check(_lib.load().bsg_match_get_stats(self._h, C.byref(st)), "bsg_match_get_stats")
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def reset_stats(self) -> None:
+        _lib.check(_lib.load().bsg_match_reset_stats(self._h), "bsg_match_reset_stats")
+
+
 def ctf_record(volt: float, coefs, apply: bool = True, invert: bool = False) -> np.ndarray:
     """CTF record from the aberration weights [abw00, abw20, abw22, abw2m2, abw40, ...]."""
     c = np.asarray(coefs, dtype=np.float64)

@@ -231,6 +231,49 @@ int  bsg_match_prepared(bsg_match* m, long first, long count, float* out, int fl
 /* FRC figure of merit (and cross-validation figure) of nhyp hypotheses. */
 int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, double* cv, int flags);
 
+/* Exhaustive search (no counterpart in the reference, which refines locally
+ * with img_refine_grid and scores with img_recip_space_fom; this is the
+ * global search that scoring generalises to).
+ *
+ * bsg_match_set_panel: the search panel for nsec views (row-major matrices):
+ * the central section of each at the coarse pixels (Hermitian half plane,
+ * shells 1 .. ceil(max_rad) - 1), every shell normalised to unit power,
+ * stored as BF16 (nsec x ~2 npix/2 x 2 bytes on the device).
+ *
+ * bsg_match_search: every held image at each of norigin trial origins
+ * (origins: norigin x 2 doubles, pixels of the particle image) against every
+ * panel section, by a BF16 correlation with FP32 accumulation on the tensor
+ * cores: the per-shell FRC with the shell power of the CTF-weighted section
+ * taken as (shell power of the section) x (shell mean of CTF^2).  The topk
+ * best (section, origin) pairs of each image are rescored with the exact
+ * figure of merit (bsg_match_score) and returned best first:
+ * out = nimg x topk records of BSG_MATCH_RESULT_DOUBLES doubles:
+ * section index, origin index, correlation score, FRC figure of merit,
+ * cross-validation figure (section -1 if fewer candidates exist). */
+#define BSG_MATCH_RESULT_DOUBLES 5
+#define BSG_MATCH_TOPK_MAX 8
+int  bsg_match_set_panel(bsg_match* m, const double* mats, long nsec, int flags);
+int  bsg_match_search(bsg_match* m, const double* origins, int norigin, int topk, double* out, int flags);
+
+/* Device times of the search stages (CUDA events on the context's stream). */
+typedef struct {
+    double panel_ms;       /* panel construction                           */
+    double agen_ms;        /* image rows (origin phase, CTF, shell norms)  */
+    double gemm_ms;        /* tensor-core correlation with top-8 selection */
+    double merge_ms;       /* per-image candidate merge                    */
+    double rescore_ms;     /* exact figure of merit of the candidates      */
+    double gemm_flops;     /* algorithmic: 2 x rows x sections x K         */
+    double hypotheses;     /* image x origin x section triples scored      */
+    long   launches;       /* kernels launched by the search calls         */
+    long   gemm_launches;
+    long   images;
+    long   rescored;
+    int    coarse_k;       /* real K of the correlation (2 x coarse pixels) */
+    int    kpad;           /* K padded to the 64-element stage width        */
+} bsg_match_stats;
+int  bsg_match_get_stats(bsg_match* m, bsg_match_stats* st);
+int  bsg_match_reset_stats(bsg_match* m);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 

@@ -10,6 +10,9 @@ hypotheses with and without the CTF.
 
     python tests/golden/make_match_golden.py
 
+``views_probe`` lists the views of ``asymmetric_unit_views`` for a few point
+groups and steps (views.npz).
+
 The fixture keeps the inputs (map, images, views, CTF rows, hypotheses, and
 the stack header's average and standard deviation, which the reference's
 particle normalisation uses) and
@@ -105,8 +108,25 @@ def _isnum(t: str) -> bool:
         return False
 
 
+# asymmetric_unit_views (views_probe): point group order, theta and phi steps
+# in degrees, flag (1 full sphere, 2 no in-plane angle)
+VIEW_CASES = [(1, 3.0, 3.0, 1), (1, 7.5, 7.5, 1), (1, 10.0, 5.0, 0), (3, 6.0, 6.0, 1), (1, 3.0, 3.0, 3)]
+
+
+def make_views() -> str:
+    out = {}
+    for order, t, p, f in VIEW_CASES:
+        r = subprocess.run([os.path.join(REF, "views_probe"), f"C{order}", repr(t), repr(p), str(f)],
+                           capture_output=True, text=True, check=True)
+        out[f"C{order}_{t}_{p}_{f}"] = np.loadtxt(r.stdout.splitlines()).reshape(-1, 4)
+    path = os.path.join(OUT, "views.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
 if __name__ == "__main__":
     if not os.path.exists(os.path.join(REF, "match_probe")):
         sys.exit("build the reference first: make -C oracle ref")
     for name, case in CASES.items():
         print(make(name, case))
+    print(make_views())

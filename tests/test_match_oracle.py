@@ -82,3 +82,19 @@ def test_true_view_scores_best(case):
     ctf = d["ctf_rows"][:, 6] > 0
     assert np.all(f[ctf, 0] > f[ctf, 3]) and np.all(f[ctf, 0] > f[ctf, 4])
     assert np.all(f[ctf, 0] > 0.15)
+
+
+def test_asymmetric_unit_views():
+    """The view grid restatement against asymmetric_unit_views of the reference."""
+    import math
+    import os
+    from bsoft_b200.geometry import asymmetric_unit_views_c
+    from tests.match_helpers import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "views.npz"))
+    for key in z.files:
+        sym, t, p, f = key.split("_")
+        v = asymmetric_unit_views_c(int(sym[1:]), math.radians(float(t)), math.radians(float(p)),
+                                    full=bool(int(f) & 1), inplane=not (int(f) & 2))
+        assert v.shape == z[key].shape
+        assert np.abs(v - z[key]).max() < 1e-12
+    assert len(z["C1_3.0_3.0_1"]) == 4586
