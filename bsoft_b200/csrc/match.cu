@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(256) section_kernel(const float2* __restrict__
         const double my = (V.m[3] * ix + V.m[4] * iy) * real;
         const double mz = (V.m[6] * ix + V.m[7] * iy) * real;
         double vr, vi;
-        fsi_gather<double>(vol, D, mx, my, mz, lut, wd, lane, vr, vi);
+        fsi_gather<double>(PtrSrc{vol, D}, D, mx, my, mz, lut, wd, lane, vr, vi);
         if (lane == 0) o[q.idx] = make_float2((float)vr, (float)vi);
     }
 }
@@ -260,9 +260,9 @@ __global__ void __launch_bounds__(256) section_kernel(const float2* __restrict__
 // summed by a fixed shuffle tree into the warp's shell slots.  The shell
 // totals are folded over the warps in FP64, in order.
 struct FomArgs {
-    const float2* vol;
+    cudaTextureObject_t tex;
     int D, wd;
-    const double* lut;
+    const float* lut;
     const MPix* pix;
     int npix;
     const MHyp* hyps;
@@ -278,9 +278,9 @@ struct FomArgs {
 };
 
 __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
-    extern __shared__ double dsm[];
-    double* lut = dsm;                                                     // (NDIV+1)*wd
-    float* wsum = reinterpret_cast<float*>(dsm + (NDIV + 1) * MAXW);       // FOM_WARPS x nshell x 2
+    extern __shared__ float fsm[];
+    float* lut = fsm;                                                      // (NDIV+1)*wd
+    float* wsum = fsm + (NDIV + 1) * MAXW;                                 // FOM_WARPS x nshell x 2
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < (NDIV + 1) * a.wd; i += blockDim.x) lut[i] = a.lut[i];
     for (int i = threadIdx.x; i < FOM_WARPS * a.nshell * 2; i += blockDim.x) wsum[i] = 0.f;
@@ -300,10 +300,9 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             const double mx = (H.m[0] * ix + H.m[1] * iy) * a.real;
             const double myy = (H.m[3] * ix + H.m[4] * iy) * a.real;
             const double mz = (H.m[6] * ix + H.m[7] * iy) * a.real;
-            double vr, vi;
-            fsi_gather<double>(a.vol, a.D, mx, myy, mz, lut, a.wd, lane, vr, vi);
-            // the reference stores the section as float (Complex<float>)
-            if (lane == q) R = make_float2((float)vr, (float)vi);
+            float vr, vi;
+            fsi_gather<float>(TexSrc{a.tex}, a.D, mx, myy, mz, lut, a.wd, lane, vr, vi);
+            if (lane == q) R = make_float2(vr, vi);
         }
         const int p = base + lane;
         float f = 0.f, m = 0.f;
@@ -579,6 +578,7 @@ extern "C" int bsg_match_create(const bsg_match_config* cfg, bsg_match** out) {
     ALLOC(M->d_shell_start, sizeof(int) * M->h_shell_start.size());
     ALLOC(M->d_secpix, sizeof(MPix) * std::max<size_t>(1, M->h_secpix.size()));
     ALLOC(M->d_lut, sizeof(double) * lut.size());
+    ALLOC(M->d_lutf, sizeof(float) * lut.size());
     ALLOC(M->d_tw_map, sizeof(double2) * twm.size());
     ALLOC(M->d_tw_img, sizeof(double2) * twi.size());
     ALLOC(M->d_ref, sizeof(float2) * (size_t)D * D * D);
@@ -590,6 +590,10 @@ extern "C" int bsg_match_create(const bsg_match_config* cfg, bsg_match** out) {
     if (e == cudaSuccess)
         e = cudaMemcpy(M->d_secpix, M->h_secpix.data(), sizeof(MPix) * M->h_secpix.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(M->d_lut, lut.data(), sizeof(double) * lut.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        std::vector<float> lf(lut.begin(), lut.end());
+        e = cudaMemcpy(M->d_lutf, lf.data(), sizeof(float) * lf.size(), cudaMemcpyHostToDevice);
+    }
     if (e == cudaSuccess) e = cudaMemcpy(M->d_tw_map, twm.data(), sizeof(double2) * twm.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(M->d_tw_img, twi.data(), sizeof(double2) * twi.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -605,13 +609,15 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
     if (!M) return;
     cudaSetDevice(M->device);
     if (M->stream) cudaStreamSynchronize(M->stream);
-    void* ptrs[] = {M->d_pix, M->d_shell_start, M->d_secpix, M->d_lut, M->d_tw_map, M->d_tw_img, M->d_ref,
+    void* ptrs[] = {M->d_pix, M->d_shell_start, M->d_secpix, M->d_lut, M->d_lutf, M->d_tw_map, M->d_tw_img, M->d_ref,
                     M->d_spec, M->d_ctf, M->d_dsum, M->d_real, M->d_work, M->d_scale, M->d_shift, M->d_ictf,
                     M->d_hyp, M->d_out, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
                     M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_chyp, M->d_cfom, M->d_gA, M->d_slopes,
                     M->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);
+    if (M->ref_tex) cudaDestroyTextureObject(M->ref_tex);
+    if (M->ref_array) cudaFreeArray(M->ref_array);
     if (M->stream) cudaStreamDestroy(M->stream);
     delete M;
 }
@@ -668,6 +674,31 @@ extern "C" int bsg_match_set_reference(bsg_match* h, const float* map, const dou
     map_cut_kernel<<<148 * 8, 256, 0, s>>>(M->d_work, N, D, 1.0 / sqrt((double)n3), sx, sy, sz, M->d_ref);
     MCK(cudaGetLastError());
     MCK(cudaStreamSynchronize(s));
+    // the same transform behind a 3-D texture (point sampling, integer
+    // coordinates: every fetch returns a stored value unchanged)
+    if (!M->ref_array) {
+        const cudaChannelFormatDesc ch = cudaCreateChannelDesc<float2>();
+        MCK(cudaMalloc3DArray(&M->ref_array, &ch, make_cudaExtent(D, D, D)));
+        cudaResourceDesc rd;
+        memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = M->ref_array;
+        cudaTextureDesc td;
+        memset(&td, 0, sizeof(td));
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        MCK(cudaCreateTextureObject(&M->ref_tex, &rd, &td, nullptr));
+    }
+    cudaMemcpy3DParms cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.srcPtr = make_cudaPitchedPtr(M->d_ref, sizeof(float2) * D, D, D);
+    cp.dstArray = M->ref_array;
+    cp.extent = make_cudaExtent(D, D, D);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    MCK(cudaMemcpy3DAsync(&cp, s));
+    MCK(cudaStreamSynchronize(s));
     M->have_ref = true;
     return BSG_OK;
 }
@@ -708,13 +739,13 @@ int match_fail(int code, const char* fmt, ...) {
 
 cudaError_t launch_fom(const Match& M, const MHyp* d_hyps, long nh, double* d_fom, double* d_cv, cudaStream_t s) {
     FomArgs a{};
-    a.vol = M.d_ref; a.D = M.D; a.wd = M.wd; a.lut = M.d_lut;
+    a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_hyps;
     a.spec = M.d_spec; a.ctf = M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
     a.fom = d_fom; a.cv = d_cv;
-    const size_t smem = sizeof(double) * (NDIV + 1) * MAXW + sizeof(float) * FOM_WARPS * M.nshell * 2;
+    const size_t smem = sizeof(float) * ((NDIV + 1) * MAXW + FOM_WARPS * M.nshell * 2);
     for (long h0 = 0; h0 < nh; h0 += 65535L * 32) {
         const long cnt = std::min(nh - h0, 65535L * 32);
         FomArgs b = a;

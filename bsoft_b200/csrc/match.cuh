@@ -38,14 +38,32 @@ __device__ __forceinline__ int wrap1(int j, int D) {
     return min(max(j, 0), D - 1);
 }
 
+// Sources of the cut reference transform for the gather: the linear array
+// (reference index order) or a 3-D texture over the same values.  The
+// texture's block-linear layout keeps an 8^3 tap neighbourhood on far fewer
+// cache lines than z-major rows, which is what limits the gather when many
+// warps work on different rotations at once.
+struct PtrSrc {
+    const float2* __restrict__ p;
+    int D;
+    __device__ __forceinline__ float2 operator()(int x, int y, int z) const {
+        return __ldg(p + ((size_t)z * D + y) * D + x);
+    }
+};
+struct TexSrc {
+    cudaTextureObject_t t;
+    __device__ __forceinline__ float2 operator()(int x, int y, int z) const {
+        return tex3D<float2>(t, (float)x, (float)y, (float)z);
+    }
+};
+
 // FSI kernel interpolation of the diam^3 transform at voxel position m by
 // one warp (Bimage::fspace_interpolate).  Every lane returns the sum.
-// T = double reproduces the reference's FP64 accumulation (with a double
-// kernel table): near the cut edge the taps wrap onto lower frequencies that
-// are orders of magnitude stronger than the result, and FP32 weights and
-// sums lose ~1% there.  T = float serves the BF16 search panel.
-template <typename T>
-__device__ __forceinline__ void fsi_gather(const float2* __restrict__ vol, int D, double mx, double my, double mz,
+// T = double (with an FP64 kernel table) accumulates as the reference does;
+// T = float agrees with it to ~1e-8 in the figure of merit (the transforms
+// themselves are computed in FP64, which is what the outer shells need).
+template <typename T, typename Src>
+__device__ __forceinline__ void fsi_gather_any(const Src& src, int D, double mx, double my, double mz,
                                            const T* __restrict__ lut, int wd, int lane, T& out_re, T& out_im) {
     const int half = (wd - 1) / 2;
     const double fx = floor(mx), fy = floor(my), fz = floor(mz);
@@ -62,7 +80,7 @@ __device__ __forceinline__ void fsi_gather(const float2* __restrict__ vol, int D
             const int zz = r / wd, yy = r - zz * wd;
             const int jz = wrap1(ibz + zz, D), jy = wrap1(iby + yy, D);
             const T w = kx * (lut[iky + yy] * lut[ikz + zz]);
-            const float2 v = __ldg(vol + ((size_t)jz * D + jy) * D + jx);
+            const float2 v = src(jx, jy, jz);
             ar += (T)v.x * w;
             ai += (T)v.y * w;
         }
@@ -74,6 +92,51 @@ __device__ __forceinline__ void fsi_gather(const float2* __restrict__ vol, int D
     }
     out_re = ar;
     out_im = ai;
+}
+
+// The reference's default width 8: lane = (x tap, row group rq); the lane's
+// rows are y = rq and rq + 4 at every z, so the wraps and the y weights are
+// computed once and the z loop unrolls.  Same taps, weights and summation
+// order as fsi_gather_any.
+template <typename T, typename Src>
+__device__ __forceinline__ void fsi_gather8(const Src& src, int D, double mx, double my, double mz,
+                                            const T* __restrict__ lut, int lane, T& out_re, T& out_im) {
+    const double fx = floor(mx), fy = floor(my), fz = floor(mz);
+    const int ikx = (int)((mx - fx) * NDIV + 0.5) * 8;
+    const int iky = (int)((my - fy) * NDIV + 0.5) * 8;
+    const int ikz = (int)((mz - fz) * NDIV + 0.5) * 8;
+    const int ibx = (int)fx - 3, iby = (int)fy - 3, ibz = (int)fz - 3;
+    const int xl = lane & 7, rq = lane >> 3;
+    const int jx = wrap1(ibx + xl, D);
+    const int jy0 = wrap1(iby + rq, D), jy1 = wrap1(iby + rq + 4, D);
+    const T kx = lut[ikx + xl], ky0 = lut[iky + rq], ky1 = lut[iky + rq + 4];
+    T ar = 0, ai = 0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+        const int jz = wrap1(ibz + z, D);
+        const T kz = lut[ikz + z];
+        const float2 v0 = src(jx, jy0, jz);
+        const float2 v1 = src(jx, jy1, jz);
+        const T wa = kx * (ky0 * kz), wb = kx * (ky1 * kz);
+        ar += (T)v0.x * wa;
+        ai += (T)v0.y * wa;
+        ar += (T)v1.x * wb;
+        ai += (T)v1.y * wb;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        ar += __shfl_xor_sync(0xffffffffu, ar, o);
+        ai += __shfl_xor_sync(0xffffffffu, ai, o);
+    }
+    out_re = ar;
+    out_im = ai;
+}
+
+template <typename T, typename Src>
+__device__ __forceinline__ void fsi_gather(const Src& src, int D, double mx, double my, double mz,
+                                           const T* __restrict__ lut, int wd, int lane, T& out_re, T& out_im) {
+    if (wd == 8) fsi_gather8<T, Src>(src, D, mx, my, mz, lut, lane, out_re, out_im);
+    else fsi_gather_any<T, Src>(src, D, mx, my, mz, lut, wd, lane, out_re, out_im);
 }
 
 struct ImgCtf {
@@ -98,10 +161,13 @@ struct Match {
     MPix* d_pix = nullptr;
     int* d_shell_start = nullptr;
     MPix* d_secpix = nullptr;
-    double* d_lut = nullptr;
+    double* d_lut = nullptr;           // FSI table, FP64 (sections output)
+    float* d_lutf = nullptr;           // FSI table, FP32 (scoring and search panel)
     double2* d_tw_map = nullptr;
     double2* d_tw_img = nullptr;
     float2* d_ref = nullptr;           // diam^3
+    cudaArray_t ref_array = nullptr;   // the same values behind a 3-D texture
+    cudaTextureObject_t ref_tex = 0;
     bool have_ref = false;
     // images
     long cap = 0, nimg = 0;

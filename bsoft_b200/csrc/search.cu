@@ -343,14 +343,14 @@ search_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constan
 
 // one CTA per section: FSI-kernel gather of the coarse pixels (FP64
 // accumulation), per-shell norms, BF16 row of interleaved (re, im)
-__global__ void __launch_bounds__(256) panel_kernel(const float2* __restrict__ vol, int D,
-                                                    const double* __restrict__ lut_g, int wd,
+__global__ void __launch_bounds__(256) panel_kernel(cudaTextureObject_t tex, int D,
+                                                    const float* __restrict__ lut_g, int wd,
                                                     const MPix* __restrict__ cpix, int ncpix,
                                                     const int* __restrict__ cstart, int nf,
                                                     const MHyp* __restrict__ secs, double inv, double real, int kpad,
                                                     __nv_bfloat16* __restrict__ panel) {
-    extern __shared__ double psm[];
-    double* lut = psm;                                               // (NDIV+1)*MAXW
+    extern __shared__ float psm[];
+    float* lut = psm;                                                // (NDIV+1)*MAXW
     float2* vals = reinterpret_cast<float2*>(psm + (NDIV + 1) * MAXW);   // ncpix
     float* gn = reinterpret_cast<float*>(vals + ncpix);              // nf
     for (int i = threadIdx.x; i < (NDIV + 1) * wd; i += blockDim.x) lut[i] = lut_g[i];
@@ -363,9 +363,9 @@ __global__ void __launch_bounds__(256) panel_kernel(const float2* __restrict__ v
         const double mx = (V.m[0] * ix + V.m[1] * iy) * real;
         const double my = (V.m[3] * ix + V.m[4] * iy) * real;
         const double mz = (V.m[6] * ix + V.m[7] * iy) * real;
-        double vr, vi;
-        fsi_gather<double>(vol, D, mx, my, mz, lut, wd, lane, vr, vi);
-        if (lane == 0) vals[p] = make_float2((float)vr, (float)vi);
+        float vr, vi;
+        fsi_gather<float>(TexSrc{tex}, D, mx, my, mz, lut, wd, lane, vr, vi);
+        if (lane == 0) vals[p] = make_float2(vr, vi);
     }
     __syncthreads();
     for (int j = threadIdx.x; j < nf; j += blockDim.x) {
@@ -563,7 +563,7 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     if (g_search_attr_err != cudaSuccess)
         return match_fail(BSG_ERR_CUDA, "bsg_match_set_panel: %s", cudaGetErrorString(g_search_attr_err));
     coarse_pixels(*M);
-    const size_t psmem = sizeof(double) * (NDIV + 1) * MAXW + sizeof(float2) * M->ncpix + sizeof(float) * M->nf;
+    const size_t psmem = sizeof(float) * (NDIV + 1) * MAXW + sizeof(float2) * M->ncpix + sizeof(float) * M->nf;
     if (psmem > 200 * 1024) return match_fail(BSG_ERR_ARG, "bsg_match_set_panel: %d coarse pixels exceed the panel kernel's shared memory", M->ncpix);
     cudaStream_t s = M->stream;
     // release an older panel first
@@ -591,7 +591,7 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     cudaEventRecord(e0, s);
     for (long v0 = 0; e == cudaSuccess && v0 < nsec; v0 += 1L << 20) {
         const long cnt = std::min(nsec - v0, 1L << 20);
-        panel_kernel<<<(unsigned)cnt, 256, psmem, s>>>(M->d_ref, M->D, M->d_lut, M->wd, M->d_cpix, M->ncpix, M->d_cstart,
+        panel_kernel<<<(unsigned)cnt, 256, psmem, s>>>(M->ref_tex, M->D, M->d_lutf, M->wd, M->d_cpix, M->ncpix, M->d_cstart,
                                                        M->nf, M->d_secs + v0, 1.0 / M->real_map, M->real_map, M->kpad,
                                                        M->d_panel + (size_t)v0 * M->kpad);
         e = cudaGetLastError();
