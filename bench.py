@@ -26,6 +26,17 @@ Legs reported on one JSON line:
               oracle/_ref) on a bounded sample of the same workload, all host
               threads
 
+Search leg (the "search" object of the same line): 128x128 noisy CTF images
+(SNR 0.1) of a 128^3 blob phantom against 4,586 view directions (the
+reference's asymmetric_unit_views, C1, 3 degrees) x 120 in-plane angles =
+550,320 central sections, 5 x 5 trial origins (+-2 pixels), shells up to
+0.8 Nyquist.  A step = one batch of `--search-batch` images: preparation
+(FFT, CTF, shell norms), the BF16 tensor-core correlation with top-8
+selection, and exact rescoring of the 8 candidates.  Its roofline is the
+correlation kernel against the measured sustained BF16 rate; its CPU
+baseline is the reference's own central_section + img_recip_space_fom per
+hypothesis (oracle/_ref/match_probe), extrapolated to the exhaustive search.
+
 `--impl reference` times only the reference CPU implementation (rank 0).
 Multi-GPU (`torchrun --nproc-per-node N`): each rank reconstructs its own
 shard of particles (weak scaling) and the partial maps are summed with one
@@ -200,6 +211,166 @@ def run_reference(args):
         "vs_baseline": None}))
 
 
+SEARCH_BOX = 128
+SEARCH_PIXEL = 1.5
+SEARCH_RES = 3.75            # 0.8 Nyquist at 1.5 angstrom/pixel
+SEARCH_PSI = 120             # in-plane angles (3 degrees)
+SEARCH_ORIGINS = [(SEARCH_BOX // 2 + dx, SEARCH_BOX // 2 + dy) for dy in range(-2, 3) for dx in range(-2, 3)]
+
+
+def search_workload(n_images, seed=21):
+    from bsoft_b200.synth import DatasetSpec, generate, phantom_volume
+    spec = DatasetSpec(box=SEARCH_BOX, n_particles=n_images, n_blobs=100, pixel=SEARCH_PIXEL, snr=0.1, seed=seed,
+                       defocus_range=(1.0e4, 3.0e4), shift_range=2.0)
+    ph, imgs, meta = generate(spec)
+    return dict(spec=spec, volume=phantom_volume(ph).astype(np.float32), images=imgs, meta=meta)
+
+
+def search_views_mats():
+    from bsoft_b200.geometry import asymmetric_unit_views_c, search_views, views_to_matrices
+    dirs = asymmetric_unit_views_c(1, math.radians(3.0), math.radians(3.0))
+    return len(dirs), views_to_matrices(search_views(dirs, SEARCH_PSI))
+
+
+def search_reference_sample(sw, n_views: int = 160):
+    """Per-hypothesis time of the reference's own scoring (match_probe:
+    central_section once per view, then phase shift + img_recip_space_fom per
+    trial origin), one thread, on the search workload's map and images."""
+    import oracle
+    from bsoft_b200.io import mrc
+    exe = oracle.ref_binary("match_probe")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/match_probe not built"
+    d = tempfile.mkdtemp(prefix="bench_match_")
+    N = SEARCH_BOX
+    mrc.write_stack(os.path.join(d, "ref.mrc"), sw["volume"], SEARCH_PIXEL, origin_pixels=(N // 2,) * 3, volume=True)
+    nimg = 4
+    mrc.write_stack(os.path.join(d, "p.mrcs"), sw["images"][:nimg], SEARCH_PIXEL)
+    views = sw["meta"]["views"][np.arange(n_views) % len(sw["meta"]["views"])]
+    np.savetxt(os.path.join(d, "views.txt"), views, fmt="%.17g")
+    coefs = sw["meta"]["coefs"]
+    np.savetxt(os.path.join(d, "ctf.txt"), np.array([[200000.0, *coefs[i][:5], 1] for i in range(nimg)]), fmt="%.17g")
+    hyps = [[v % nimg, v, ox, oy] for v in range(n_views) for ox, oy in SEARCH_ORIGINS]
+    np.savetxt(os.path.join(d, "hyps.txt"), np.array(hyps, float), fmt="%.17g")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, os.path.join(d, "ref.mrc"), os.path.join(d, "p.mrcs"), repr(SEARCH_PIXEL),
+                        repr(SEARCH_RES), os.path.join(d, "views.txt"), os.path.join(d, "ctf.txt"),
+                        os.path.join(d, "hyps.txt"), os.path.join(d, "out")], capture_output=True, text=True)
+    dt = time.perf_counter() - t0
+    if r.returncode != 0:
+        return None, f"match_probe failed: {r.stderr[-200:]}"
+    return dt / len(hyps), (f"{len(hyps)} hypotheses ({n_views} central sections x {len(SEARCH_ORIGINS)} origins, "
+                            f"img_recip_space_fom each), one thread, wall {dt:.1f} s including map preparation")
+
+
+def search_leg(args, local, dist, world, rank, torch):
+    """Exhaustive orientation search; returns the "search" object (rank 0)."""
+    from bsoft_b200.match import Matcher, ctf_record
+    from bsoft_b200.geometry import angular_distance_deg
+    B = args.search_batch
+    nsteps, nwarm = args.search_steps, args.search_warmup
+    pool = 2 * B
+    sw = search_workload(pool, seed=21 + rank)
+    imgs = sw["images"]
+    meta = sw["meta"]
+    ctf = np.stack([ctf_record(sw["spec"].volt, c) for c in meta["coefs"]])
+    ndir, mats = search_views_mats()
+    origins = np.array(SEARCH_ORIGINS, float)
+    m = Matcher(n=SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL, pixel=SEARCH_PIXEL, hi_res=SEARCH_RES,
+                device=local)
+    m.set_reference(sw["volume"], (SEARCH_BOX // 2,) * 3)
+    m.set_panel(mats)
+    panel_ms = m.stats()["panel_ms"]
+    host = [torch.from_numpy(np.ascontiguousarray(imgs[i * B:(i + 1) * B])).pin_memory() for i in range(2)]
+    dev = [h.cuda() for h in host]
+    s = torch.cuda.ExternalStream(m.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    results = []
+    for i in range(nwarm):
+        m.set_images(dev[i % 2], ctf[(i % 2) * B:(i % 2 + 1) * B])
+        m.search(origins, topk=8)
+    m.reset_stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(s)
+        for i in range(nsteps):
+            j = (nwarm + i) % 2
+            m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+            results.append((j, m.search(origins, topk=8)))
+        ev1.record(s)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    st = m.stats()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    images = B * nsteps * world
+    value = images / (ms / 1e3)
+    # e2e: pinned host images through the C ABI, results back on the host
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(nsteps):
+        j = (nwarm + i) % 2
+        m.set_images(host[j].numpy(), ctf[j * B:(j + 1) * B])
+        m.search(origins, topk=8)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    m.close()
+    if rank != 0:
+        return None
+    errs = []
+    for j, res in results:
+        best = res[:, 0, 0].astype(int)
+        errs.append(angular_distance_deg(mats[best], meta["mats"][j * B:(j + 1) * B]))
+    errs = np.concatenate(errs)
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+        pk = json.load(f)
+    tpeak = float(pk.get("bf16_tflops_sustained", 1411.5))
+    achieved = st["gemm_flops"] / (st["gemm_ms"] / 1e3) / 1e12
+    hyp_per_image = len(mats) * len(origins)
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        us, sample = search_reference_sample(sw)
+        if us is not None:
+            cpu = {"value": 1.0 / (us * hyp_per_image), "unit": "particles/s", "cores": 1, "kind": "reference",
+                   "sample": sample, "seconds_per_hypothesis": us,
+                   "extrapolation": f"{hyp_per_image} hypotheses per particle x measured seconds per hypothesis"}
+        else:
+            cpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference", "sample": sample}
+    return {
+        "metric": "particles/s (exhaustive orientation search)", "value": round(value, 1), "unit": "particles/s",
+        "steps": nsteps, "warmup": nwarm, "ms_per_step": round(ms / nsteps, 2), "dtype": "bf16 (correlation), f32",
+        "config": {"workload": "projection-matching-128", "images_per_step": B, "box": SEARCH_BOX,
+                   "map": SEARCH_BOX, "pixel": SEARCH_PIXEL, "hi_res": SEARCH_RES, "directions": ndir,
+                   "in_plane": SEARCH_PSI, "sections": len(mats), "origins": len(origins),
+                   "hypotheses_per_image": hyp_per_image, "topk_rescored": 8, "snr": 0.1,
+                   "l2": "inputs larger than L2 (the 9.4 GB panel is streamed every step)"},
+        "e2e": {"value": round(images / e2e_s, 1), "unit": "particles/s", "h2d_bytes_per_step": B * SEARCH_BOX ** 2 * 4,
+                "d2h_bytes_per_step": B * 8 * 5 * 8},
+        "roofline": {"kernel": "search_gemm_kernel", "bound": "tensor", "achieved": round(achieved, 1),
+                     "peak": tpeak, "unit": "TFLOP/s", "frac": round(achieved / tpeak, 4), "traffic": None,
+                     "peak_source": "measured (bf16_tflops_sustained)",
+                     "flops_per_hypothesis": 2 * st["coarse_k"], "gemm_ms": round(st["gemm_ms"], 2)},
+        "stages_ms": {k: round(st[k], 2) for k in ("agen_ms", "gemm_ms", "merge_ms", "rescore_ms")},
+        "panel_ms": round(panel_ms, 1),
+        "accuracy": {"median_angular_error_deg": round(float(np.median(errs)), 3),
+                     "frac_within_5_deg": round(float(np.mean(errs < 5)), 4)},
+        "cpu_baseline": cpu, "gpu_launches": int(st["launches"]), "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,6 +379,10 @@ def main():
     ap.add_argument("--batch", type=int, default=2000)
     ap.add_argument("--impl", default="gpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--search-batch", type=int, default=2048)
+    ap.add_argument("--search-steps", type=int, default=3)
+    ap.add_argument("--search-warmup", type=int, default=3)
+    ap.add_argument("--legs", default="insert,search")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -314,6 +489,8 @@ def main():
     e2e = particles / e2e_s
     rec.close()
 
+    search = search_leg(args, local, dist, world, rank, torch) if "search" in args.legs else None
+
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
@@ -352,6 +529,9 @@ def main():
         "roofline": roof, "cpu_baseline": cpu, "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if search is not None:
+        line["search"] = search
+        line["gpu_launches"] = int(launches) + search["gpu_launches"]
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -99,6 +99,7 @@ def load():
         "bsg_match_search": ([vp, dp, C.c_int, C.c_int, dp, C.c_int], C.c_int),
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
+        "bsg_match_stream": ([vp], vp),
         "bsg_last_error": ([], C.c_char_p),
         "bsg_version": ([], C.c_char_p),
     }

@@ -814,3 +814,8 @@ extern "C" int bsg_match_reset_stats(bsg_match* h) {
     memset(&M->sstats, 0, sizeof(M->sstats));
     return BSG_OK;
 }
+
+extern "C" void* bsg_match_stream(bsg_match* h) {
+    Match* M = reinterpret_cast<Match*>(h);
+    return M ? static_cast<void*>(M->stream) : nullptr;
+}

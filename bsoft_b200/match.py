@@ -68,6 +68,11 @@ class Matcher:
         except Exception:
             pass
 
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t (for events around its work)."""
+        return int(_lib.load().bsg_match_stream(self._h) or 0)
+
     def set_reference(self, volume, origin=None) -> None:
         if origin is None:
             origin = (self.N // 2,) * 3

@@ -273,6 +273,7 @@ typedef struct {
 } bsg_match_stats;
 int  bsg_match_get_stats(bsg_match* m, bsg_match_stats* st);
 int  bsg_match_reset_stats(bsg_match* m);
+void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
 
 const char* bsg_last_error(void);
 const char* bsg_version(void);
