@@ -253,19 +253,21 @@ __global__ void __launch_bounds__(256) section_kernel(const float2* __restrict__
     }
 }
 
-// FRC figure of merit of one hypothesis per CTA (img_recip_space_fom,
-// fom_type 0, unit weights).  Warps take 32 consecutive pixels of the
-// shell-sorted list: the section value of each is gathered by the whole
-// warp, then every lane scores its own pixel and the lanes of one shell are
-// summed by a fixed shuffle tree into the warp's shell slots.  The shell
-// totals are folded over the warps in FP64, in order.
+// FRC figure of merit of one hypothesis group per CTA (img_recip_space_fom,
+// fom_type 0, unit weights): one image, one view, up to MAXORG trial
+// origins.  Warps take 32 consecutive pixels of the shell-sorted list: the
+// section value of each is gathered once by the whole warp, then every lane
+// scores its own pixel at every origin (only the image phase depends on the
+// origin) and the lanes of one shell are summed by a fixed shuffle tree into
+// the warp's shell slots.  The shell totals are folded over the warps in
+// FP64, in order, so results do not depend on the grouping.
 struct FomArgs {
     cudaTextureObject_t tex;
     int D, wd;
     const float* lut;
     const MPix* pix;
     int npix;
-    const MHyp* hyps;
+    const MHypG* hyps;
     const float2* spec;      // prepared images, diam^2 each
     const float* ctf;        // per image x npix
     const double* dsum;      // per image x nshell
@@ -273,23 +275,25 @@ struct FomArgs {
     double inv, real;        // section frequency step and real size
     int nf;                  // shells j < max_rad
     int cv0, cv1;            // cross-validation shells [cv0, cv1)
-    double* fom;
+    double* fom;             // per group x MAXORG
     double* cv;
 };
 
 __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
     extern __shared__ float fsm[];
     float* lut = fsm;                                                      // (NDIV+1)*wd
-    float* wsum = fsm + (NDIV + 1) * MAXW;                                 // FOM_WARPS x nshell x 2
+    float* wsum = fsm + (NDIV + 1) * MAXW;                                 // FOM_WARPS x nshell x (1+MAXORG)
+    constexpr int NV = 1 + MAXORG;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < (NDIV + 1) * a.wd; i += blockDim.x) lut[i] = a.lut[i];
-    for (int i = threadIdx.x; i < FOM_WARPS * a.nshell * 2; i += blockDim.x) wsum[i] = 0.f;
+    for (int i = threadIdx.x; i < FOM_WARPS * a.nshell * NV; i += blockDim.x) wsum[i] = 0.f;
     __syncthreads();
-    const MHyp& H = a.hyps[blockIdx.x];
+    const MHypG& H = a.hyps[blockIdx.x];
+    const int norg = H.norg;
     const long img = H.img;
     const float2* X = a.spec + img * (long)a.D * a.D;
     const float* C = a.ctf + img * (long)a.npix;
-    float* my = wsum + warp * a.nshell * 2;
+    float* my = wsum + warp * a.nshell * NV;
     for (int base = warp * 32; base < a.npix; base += FOM_WARPS * 32) {
         float2 R = make_float2(0.f, 0.f);
         const int cnt = min(32, a.npix - base);
@@ -305,21 +309,28 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             if (lane == q) R = make_float2(vr, vi);
         }
         const int p = base + lane;
-        float f = 0.f, m = 0.f;
+        float v[NV];
+#pragma unroll
+        for (int o = 0; o < NV; ++o) v[o] = 0.f;
         int shell = -1;
         if (lane < cnt) {
             const MPix pq = a.pix[p];
             shell = pq.shell;
             const float2 x = X[pq.idx];
-            double phi = pq.h * H.sx + pq.k * H.sy;
-            phi -= 6.283185307179586 * rint(phi * 0.15915494309189535);
-            float sn, cs;
-            sincosf((float)phi, &sn, &cs);
-            const float xr = x.x * cs - x.y * sn, xi = x.x * sn + x.y * cs;
             const float c = C[p];
             const float rr = R.x * c, ri = R.y * c;
-            f = xr * rr + xi * ri;
-            m = rr * rr + ri * ri;
+            v[0] = rr * rr + ri * ri;
+#pragma unroll
+            for (int o = 0; o < MAXORG; ++o) {
+                if (o < norg) {
+                    double phi = pq.h * H.sx[o] + pq.k * H.sy[o];
+                    phi -= 6.283185307179586 * rint(phi * 0.15915494309189535);
+                    float sn, cs;
+                    sincosf((float)phi, &sn, &cs);
+                    const float xr = x.x * cs - x.y * sn, xi = x.x * sn + x.y * cs;
+                    v[1 + o] = xr * rr + xi * ri;
+                }
+            }
         }
         // segmented sums over the lanes of each shell present in this group
         unsigned left = __ballot_sync(0xffffffffu, shell >= 0);
@@ -327,27 +338,29 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             const int lead = __ffs(left) - 1;
             const int s = __shfl_sync(0xffffffffu, shell, lead);
             const bool in = shell == s;
-            float fv = in ? f : 0.f, mv = in ? m : 0.f;
 #pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                fv += __shfl_xor_sync(0xffffffffu, fv, o);
-                mv += __shfl_xor_sync(0xffffffffu, mv, o);
+            for (int o = 0; o < NV; ++o) {
+                if (o > norg) break;
+                float t = in ? v[o] : 0.f;
+#pragma unroll
+                for (int k = 16; k; k >>= 1) t += __shfl_xor_sync(0xffffffffu, t, k);
+                if (lane == 0) my[s * NV + o] += t;
             }
-            if (lane == 0) { my[2 * s] += fv; my[2 * s + 1] += mv; }
             left &= ~__ballot_sync(0xffffffffu, in);
         }
     }
     __syncthreads();
-    if (warp == 0) {
-        // shells j (lane-strided), folded over warps in order, then summed in
-        // order of j by a fixed shuffle tree per range
+    // one warp per origin: shells j (lane-strided), folded over warps in
+    // order, then summed over j by a fixed shuffle tree
+    if (warp < norg) {
+        const int o = warp;
         const double* ds = a.dsum + img * (long)a.nshell;
         double tf = 0, tc = 0;
         for (int j = lane; j < a.nshell; j += 32) {
             double fj = 0, mj = 0;
             for (int w = 0; w < FOM_WARPS; ++w) {
-                fj += wsum[(w * a.nshell + j) * 2];
-                mj += wsum[(w * a.nshell + j) * 2 + 1];
+                mj += wsum[(w * a.nshell + j) * NV];
+                fj += wsum[(w * a.nshell + j) * NV + 1 + o];
             }
             const double den = ds[j] * mj;
             const double t = den > 0 ? fj / sqrt(den) : 0.0;
@@ -355,13 +368,13 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             if (j >= a.cv0 && j < a.cv1) tc += t;
         }
 #pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            tf += __shfl_xor_sync(0xffffffffu, tf, o);
-            tc += __shfl_xor_sync(0xffffffffu, tc, o);
+        for (int k = 16; k; k >>= 1) {
+            tf += __shfl_xor_sync(0xffffffffu, tf, k);
+            tc += __shfl_xor_sync(0xffffffffu, tc, k);
         }
         if (lane == 0) {
-            a.fom[blockIdx.x] = a.nf > 0 ? tf / a.nf : 0.0;
-            a.cv[blockIdx.x] = (a.cv1 > a.cv0) ? tc / (a.cv1 - a.cv0) : 0.0;
+            a.fom[(long)blockIdx.x * MAXORG + o] = a.nf > 0 ? tf / a.nf : 0.0;
+            a.cv[(long)blockIdx.x * MAXORG + o] = (a.cv1 > a.cv0) ? tc / (a.cv1 - a.cv0) : 0.0;
         }
     }
 }
@@ -415,7 +428,7 @@ void set_attributes() {
     const int big = 100 * 1024;
     cudaError_t e = cudaFuncSetAttribute(strided64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        e = cudaFuncSetAttribute(fom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     g_attr_err = e;
 }
 
@@ -611,8 +624,8 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
     if (M->stream) cudaStreamSynchronize(M->stream);
     void* ptrs[] = {M->d_pix, M->d_shell_start, M->d_secpix, M->d_lut, M->d_lutf, M->d_tw_map, M->d_tw_img, M->d_ref,
                     M->d_spec, M->d_ctf, M->d_dsum, M->d_real, M->d_work, M->d_scale, M->d_shift, M->d_ictf,
-                    M->d_hyp, M->d_out, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
-                    M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_chyp, M->d_cfom, M->d_gA, M->d_slopes,
+                    M->d_hyp, M->d_out, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
+                    M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_gA, M->d_slopes,
                     M->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);
@@ -737,24 +750,51 @@ int match_fail(int code, const char* fmt, ...) {
     return code;
 }
 
-cudaError_t launch_fom(const Match& M, const MHyp* d_hyps, long nh, double* d_fom, double* d_cv, cudaStream_t s) {
+cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s) {
     FomArgs a{};
     a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf;
-    a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_hyps;
+    a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
     a.spec = M.d_spec; a.ctf = M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
     a.fom = d_fom; a.cv = d_cv;
-    const size_t smem = sizeof(float) * ((NDIV + 1) * MAXW + FOM_WARPS * M.nshell * 2);
-    for (long h0 = 0; h0 < nh; h0 += 65535L * 32) {
-        const long cnt = std::min(nh - h0, 65535L * 32);
-        FomArgs b = a;
-        b.hyps = d_hyps + h0; b.fom = d_fom + h0; b.cv = d_cv + h0;
-        fom_kernel<<<(unsigned)cnt, FOM_WARPS * 32, smem, s>>>(b);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
+    const size_t smem = sizeof(float) * ((NDIV + 1) * MAXW + FOM_WARPS * M.nshell * (1 + MAXORG));
+    if (ng > 0) fom_kernel<<<(unsigned)ng, FOM_WARPS * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// hypotheses (image, view, origin) -> groups of one image and view with up
+// to MAXORG origins; slot[i] = group * MAXORG + position of hypothesis i
+void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups, std::vector<long>& slot) {
+    std::vector<long> order(hyps.size());
+    for (size_t i = 0; i < hyps.size(); ++i) order[i] = (long)i;
+    auto key_less = [&](long x, long y) {
+        const MHyp &a = hyps[x], &b = hyps[y];
+        if (a.img != b.img) return a.img < b.img;
+        const int c = memcmp(a.m, b.m, sizeof(a.m));
+        if (c) return c < 0;
+        return x < y;
+    };
+    std::stable_sort(order.begin(), order.end(), key_less);
+    groups.clear();
+    slot.assign(hyps.size(), 0);
+    for (size_t k = 0; k < order.size(); ++k) {
+        const MHyp& h = hyps[order[k]];
+        bool same = !groups.empty() && groups.back().img == h.img && groups.back().norg < MAXORG &&
+                    memcmp(groups.back().m, h.m, sizeof(h.m)) == 0;
+        if (!same) {
+            MHypG g;
+            memset(&g, 0, sizeof(g));
+            memcpy(g.m, h.m, sizeof(g.m));
+            g.img = h.img;
+            groups.push_back(g);
+        }
+        MHypG& g = groups.back();
+        g.sx[g.norg] = h.sx;
+        g.sy[g.norg] = h.sy;
+        slot[order[k]] = (long)(groups.size() - 1) * MAXORG + g.norg;
+        g.norg++;
     }
-    return cudaSuccess;
 }
 }  // namespace bsg
 
@@ -770,6 +810,21 @@ static int ensure_hyps(Match& M, long nh) {
     M.hyp_cap = nh;
     return BSG_OK;
 }
+
+namespace bsg {
+int ensure_groups(Match& M, long ng) {
+    if (ng <= M.grp_cap) return BSG_OK;
+    cudaFree(M.d_grp);
+    cudaFree(M.d_gout);
+    M.d_grp = nullptr;
+    M.d_gout = nullptr;
+    M.grp_cap = 0;
+    MCK(cudaMalloc(&M.d_grp, sizeof(MHypG) * ng));
+    MCK(cudaMalloc(&M.d_gout, sizeof(double) * 2 * MAXORG * ng));
+    M.grp_cap = ng;
+    return BSG_OK;
+}
+}  // namespace bsg
 
 extern "C" int bsg_match_sections(bsg_match* h, const double* mats, long nviews, float* out, int flags) {
     Match* M = reinterpret_cast<Match*>(h);
@@ -923,11 +978,22 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
         hv[i].sx = ox / M->D * 2 * M_PI;
         hv[i].sy = oy / M->D * 2 * M_PI;
     }
+    std::vector<MHypG> groups;
+    std::vector<long> slot;
+    group_hypotheses(hv, groups, slot);
+    const long ng = (long)groups.size();
+    int rc2 = ensure_groups(*M, ng);
+    if (rc2) return rc2;
     cudaStream_t s = M->stream;
-    MCK(cudaMemcpyAsync(M->d_hyp, hv.data(), sizeof(MHyp) * nhyp, cudaMemcpyHostToDevice, s));
-    MCK(launch_fom(*M, M->d_hyp, nhyp, M->d_out, M->d_out + nhyp, s));
-    MCK(cudaMemcpyAsync(fom, M->d_out, sizeof(double) * nhyp, cudaMemcpyDeviceToHost, s));
-    if (cv) MCK(cudaMemcpyAsync(cv, M->d_out + nhyp, sizeof(double) * nhyp, cudaMemcpyDeviceToHost, s));
+    MCK(cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s));
+    MCK(launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s));
+    std::vector<double> go(2 * ng * MAXORG);
+    MCK(cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));
+    for (long i = 0; i < nhyp; ++i) {
+        fom[i] = go[slot[i]];
+        if (cv) cv[i] = go[ng * MAXORG + slot[i]];
+    }
     return BSG_OK;
 }
+

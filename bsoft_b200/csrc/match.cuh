@@ -23,12 +23,24 @@ struct MPix {
 };
 static_assert(sizeof(MPix) == 16, "MPix layout");
 
+constexpr int MAXORG = 9;     // trial origins scored per gathered section
+
 struct MHyp {
     double m[9];    // view matrix with rows 0, 1 scaled (mg_refine.cpp:876-880)
     double sx, sy;  // phase slopes 2 pi origin / diam (cut pixels)
     int img;
     int pad;
 };
+
+// one image and view with up to MAXORG origins (the exact figure of merit
+// gathers the section once and scores every origin from it)
+struct MHypG {
+    double m[9];
+    double sx[MAXORG], sy[MAXORG];
+    int img;
+    int norg;
+};
+
 
 __device__ __forceinline__ int wrap1(int j, int D) {
     if (j < 0) j += D;
@@ -184,6 +196,9 @@ struct Match {
     MHyp* d_hyp = nullptr;
     long hyp_cap = 0;
     double* d_out = nullptr;           // 2 x hyp_cap
+    MHypG* d_grp = nullptr;            // hypothesis groups for the exact score
+    double* d_gout = nullptr;          // 2 x MAXORG x grp_cap
+    long grp_cap = 0;
     float* h_pin = nullptr;            // pinned staging
     size_t pin_bytes = 0;
     // exhaustive search (search.cu)
@@ -194,6 +209,7 @@ struct Match {
     int* d_cstart = nullptr;
     long nsec = 0;
     MHyp* d_secs = nullptr;            // panel views (rows 0, 1 scaled)
+    std::vector<MHyp> h_secs;          // host copy
     __nv_bfloat16* d_panel = nullptr;  // nsec x kpad
     __nv_bfloat16* d_A = nullptr;      // rows x kpad
     size_t a_elems = 0;
@@ -203,8 +219,6 @@ struct Match {
     int* d_csec = nullptr;             // candidates per image
     int* d_corg = nullptr;
     float* d_cscore = nullptr;
-    MHyp* d_chyp = nullptr;
-    double* d_cfom = nullptr;
     size_t cand_elems = 0;
     float* d_gA = nullptr;             // per image and shell: 1 / (n_f sqrt(D_j C_j))
     size_t gA_elems = 0;
@@ -215,8 +229,11 @@ struct Match {
 };
 
 
-// exact FRC scoring of nh hypotheses already on the device (match.cu)
-cudaError_t launch_fom(const Match& M, const MHyp* d_hyps, long nh, double* d_fom, double* d_cv, cudaStream_t s);
+// exact FRC scoring of ng hypothesis groups already on the device (match.cu):
+// d_fom / d_cv get MAXORG slots per group
+cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s);
+void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups, std::vector<long>& slot);
+int ensure_groups(Match& M, long ng);
 // view matrix rows 0, 1 scaled by the sampling ratio (img_fit_in_recip_space_grid)
 void match_view_rows(const Match& M, const double* mat, double* m);
 int match_fail(int code, const char* fmt, ...);

@@ -478,19 +478,6 @@ __global__ void merge_kernel(const float* __restrict__ ps, const int* __restrict
     }
 }
 
-__global__ void cand_hyps_kernel(const int* __restrict__ cand_sec, const int* __restrict__ cand_org, long ncand,
-                                 int topk, const MHyp* __restrict__ secs, const double2* __restrict__ slopes,
-                                 MHyp* __restrict__ hyps) {
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncand; c += (long)gridDim.x * blockDim.x) {
-        MHyp h = secs[max(cand_sec[c], 0)];
-        const double2 sl = slopes[max(cand_org[c], 0)];
-        h.sx = sl.x;
-        h.sy = sl.y;
-        h.img = (int)(c / topk);
-        hyps[c] = h;
-    }
-}
-
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -604,6 +591,7 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     cudaEventDestroy(e1);
     if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_set_panel: %s", cudaGetErrorString(e));
     M->nsec = nsec;
+    M->h_secs.swap(sv);
     M->sstats.panel_ms += ms;
     M->sstats.launches += (nsec + (1L << 20) - 1) >> 20;
     return BSG_OK;
@@ -651,14 +639,12 @@ extern "C" int bsg_match_search(bsg_match* h, const double* origins, int norigin
         M->part_elems = need_part;
     }
     if (need_cand > M->cand_elems) {
-        cudaFree(M->d_csec); cudaFree(M->d_corg); cudaFree(M->d_cscore); cudaFree(M->d_chyp); cudaFree(M->d_cfom);
-        M->d_csec = nullptr; M->d_corg = nullptr; M->d_cscore = nullptr; M->d_chyp = nullptr; M->d_cfom = nullptr;
+        cudaFree(M->d_csec); cudaFree(M->d_corg); cudaFree(M->d_cscore);
+        M->d_csec = nullptr; M->d_corg = nullptr; M->d_cscore = nullptr;
         M->cand_elems = 0;
         e = cudaMalloc(&M->d_csec, sizeof(int) * need_cand);
         if (e == cudaSuccess) e = cudaMalloc(&M->d_corg, sizeof(int) * need_cand);
         if (e == cudaSuccess) e = cudaMalloc(&M->d_cscore, sizeof(float) * need_cand);
-        if (e == cudaSuccess) e = cudaMalloc(&M->d_chyp, sizeof(MHyp) * need_cand);
-        if (e == cudaSuccess) e = cudaMalloc(&M->d_cfom, sizeof(double) * 2 * need_cand);
         if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search: %s", cudaGetErrorString(e));
         M->cand_elems = need_cand;
     }
@@ -746,25 +732,48 @@ extern "C" int bsg_match_search(bsg_match* h, const double* origins, int norigin
         }
         M->sstats.gemm_flops += 2.0 * (double)rows * (double)M->nsec * (double)(2 * M->ncpix);
     }
-    // exact rescoring of every candidate
+    // exact rescoring of every candidate: candidates of one image that share
+    // a section are one group (one gather, several origins)
     const long ncand = M->nimg * topk;
-    cudaEventRecord(ev[0], s);
-    if (e == cudaSuccess) {
-        cand_hyps_kernel<<<148 * 4, 256, 0, s>>>(M->d_csec, M->d_corg, ncand, topk, M->d_secs, M->d_slopes, M->d_chyp);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = launch_fom(*M, M->d_chyp, ncand, M->d_cfom, M->d_cfom + ncand, s);
-    cudaEventRecord(ev[1], s);
     std::vector<int> csec(ncand), corg(ncand);
     std::vector<float> cscore(ncand);
-    std::vector<double> cf(2 * ncand);
     if (e == cudaSuccess) e = cudaMemcpyAsync(csec.data(), M->d_csec, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(corg.data(), M->d_corg, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(cscore.data(), M->d_cscore, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(cf.data(), M->d_cfom, sizeof(double) * 2 * ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    std::vector<MHyp> hv;
+    std::vector<long> hidx;
+    hv.reserve(ncand);
+    for (long c = 0; e == cudaSuccess && c < ncand; ++c) {
+        if (csec[c] < 0) continue;
+        MHyp hh = M->h_secs[csec[c]];
+        hh.sx = sl[corg[c]].x;
+        hh.sy = sl[corg[c]].y;
+        hh.img = (int)(c / topk);
+        hv.push_back(hh);
+        hidx.push_back(c);
+    }
+    std::vector<MHypG> groups;
+    std::vector<long> slot;
+    group_hypotheses(hv, groups, slot);
+    const long ng = (long)groups.size();
+    std::vector<double> cf(2 * ncand, 0.0);
     float tres = 0;
-    cudaEventElapsedTime(&tres, ev[0], ev[1]);
+    if (e == cudaSuccess && ng > 0) {
+        if (ensure_groups(*M, ng) != BSG_OK) { for (auto& x : ev) cudaEventDestroy(x); return BSG_ERR_NOMEM; }
+        std::vector<double> go(2 * ng * MAXORG);
+        e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
+        cudaEventRecord(ev[0], s);
+        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s);
+        cudaEventRecord(ev[1], s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaEventElapsedTime(&tres, ev[0], ev[1]);
+        for (size_t k = 0; k < hidx.size(); ++k) {
+            cf[hidx[k]] = go[slot[k]];
+            cf[ncand + hidx[k]] = go[ng * MAXORG + slot[k]];
+        }
+    }
     for (auto& x : ev) cudaEventDestroy(x);
     if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search: %s", cudaGetErrorString(e));
     // per image: candidates ordered by the exact figure of merit
@@ -791,7 +800,7 @@ extern "C" int bsg_match_search(bsg_match* h, const double* origins, int norigin
     M->sstats.gemm_ms += gemm;
     M->sstats.merge_ms += merge;
     M->sstats.rescore_ms += tres;
-    M->sstats.launches += launches + 2;
+    M->sstats.launches += launches + (ng > 0 ? 1 : 0);
     M->sstats.gemm_launches += launches / 4;
     M->sstats.images += M->nimg;
     M->sstats.hypotheses += (double)M->nimg * norigin * (double)M->nsec;
