@@ -95,6 +95,7 @@ def load():
         "bsg_match_set_images": ([vp, vp, C.c_long, dp, C.c_double, C.c_double, C.c_int], C.c_int),
         "bsg_match_prepared": ([vp, C.c_long, C.c_long, vp, C.c_int], C.c_int),
         "bsg_match_score": ([vp, dp, C.c_long, dp, dp, C.c_int], C.c_int),
+        "bsg_match_project": ([vp, dp, C.c_long, C.c_double, dp, dp, vp, C.c_int], C.c_int),
         "bsg_match_set_panel": ([vp, dp, C.c_long, C.c_int], C.c_int),
         "bsg_match_search": ([vp, dp, C.c_int, C.c_int, dp, C.c_int], C.c_int),
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),

@@ -179,6 +179,87 @@ __global__ void map_cut_kernel(const double2* __restrict__ full, int N, int D, d
     }
 }
 
+// the uncut transform for the projector (Bimage::project: fft with
+// 1/sqrt(N^3), phase shift to the map origin, nothing cleared)
+__global__ void map_full_kernel(const double2* __restrict__ full, int N, double norm, double sx, double sy, double sz,
+                                float2* __restrict__ out) {
+    const long total = (long)N * N * N;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % N), y = (int)((i / N) % N), z = (int)(i / ((long)N * N));
+        const double2 f = full[i];
+        const double re = (float)(f.x * norm), im = (float)(f.y * norm);
+        const double phi = sfreq(x, N) * sx + sfreq(y, N) * sy + sfreq(z, N) * sz;
+        double sn, cs;
+        sincos(phi, &sn, &cs);
+        out[i] = make_float2((float)(re * cs - im * sn), (float)(re * sn + im * cs));
+    }
+}
+
+// projections (Bimage::project, Bimage_project.cpp:362-443): one CTA per
+// view gathers the section pixels within the resolution limit from the
+// uncut transform, optionally multiplies by a CTF (data synthesis), shifts
+// the phases to the image origin (phase_shift_to_center when the origin is
+// N/2: exp(-2 pi i (h ox + k oy) / N), Bimage_complex.cpp:443-478) and
+// stores the conjugate, so that the forward transform that follows yields the
+// inverse transform's real part
+struct ProjArgs {
+    const float2* vol;
+    int N, wd;
+    const double* lut;
+    const MPix* pix;
+    int npix;
+    const MHyp* views;          // m, sx/sy = -2 pi origin / N
+    const ImgCtf* ctf;          // per view or NULL
+    double inv, real, fs;       // fs: CTF frequency step 1/(N pixel)
+    double2* out;               // per view N^2
+};
+
+__global__ void __launch_bounds__(256) project_kernel(ProjArgs a) {
+    __shared__ double lut[(NDIV + 1) * MAXW];
+    for (int i = threadIdx.x; i < (NDIV + 1) * a.wd; i += blockDim.x) lut[i] = a.lut[i];
+    __syncthreads();
+    const MHyp& V = a.views[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2* o = a.out + (size_t)blockIdx.x * a.N * a.N;
+    for (int p = warp; p < a.npix; p += 8) {
+        const MPix q = a.pix[p];
+        const double ix = q.h * a.inv, iy = q.k * a.inv;
+        const double mx = (V.m[0] * ix + V.m[1] * iy) * a.real;
+        const double my = (V.m[3] * ix + V.m[4] * iy) * a.real;
+        const double mz = (V.m[6] * ix + V.m[7] * iy) * a.real;
+        double vr, vi;
+        fsi_gather<double>(PtrSrc{a.vol, a.N}, a.N, mx, my, mz, lut, a.wd, lane, vr, vi);
+        if (lane == 0) {
+            // the section is stored as float (Complex<float>)
+            vr = (float)vr;
+            vi = (float)vi;
+            if (a.ctf && a.ctf[blockIdx.x].apply) {
+                const ImgCtf& C = a.ctf[blockIdx.x];
+                double sx2 = a.fs * q.h; sx2 *= sx2;
+                double sy2 = a.fs * q.k; sy2 *= sy2;
+                const double s2 = sx2 + sy2, ang = atan2((double)q.k, (double)q.h);
+                const double chi = C.c[0] + s2 * (C.c[3] * sin(2 * ang) + C.c[1] + C.c[2] * cos(2 * ang)) + s2 * s2 * C.c[4];
+                double c = sin(chi);
+                if (C.invert) c = -c;
+                vr *= c;
+                vi *= c;
+            }
+            const double phi = q.h * V.sx + q.k * V.sy;
+            double sn, cs;
+            sincos(phi, &sn, &cs);
+            const double rr = vr * cs - vi * sn, ri = vr * sn + vi * cs;
+            o[q.idx] = make_double2(rr, -ri);
+        }
+    }
+}
+
+// real part of the inverse transform: (forward transform of the conjugate)
+// real part x 1/N (norm 1 of fft(FFTW_BACKWARD, 1), Bimage_fft.cpp:141-146)
+__global__ void proj_real_kernel(const double2* __restrict__ in, long count, double norm, float* __restrict__ out) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x)
+        out[i] = (float)(in[i].x * norm);
+}
+
 // full n^2 transforms -> cut diam^2 with the zero-frequency term cleared
 __global__ void img_cut_kernel(const double2* __restrict__ full, int n, int D, long nimg, float2* __restrict__ out) {
     const long per = (long)D * D, total = per * nimg;
@@ -624,7 +705,7 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
     if (M->stream) cudaStreamSynchronize(M->stream);
     void* ptrs[] = {M->d_pix, M->d_shell_start, M->d_secpix, M->d_lut, M->d_lutf, M->d_tw_map, M->d_tw_img, M->d_ref,
                     M->d_spec, M->d_ctf, M->d_dsum, M->d_real, M->d_work, M->d_scale, M->d_shift, M->d_ictf,
-                    M->d_hyp, M->d_out, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
+                    M->d_hyp, M->d_out, M->d_full, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
                     M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_gA, M->d_slopes,
                     M->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
@@ -686,6 +767,12 @@ extern "C" int bsg_match_set_reference(bsg_match* h, const float* map, const dou
     const double sx = origin[0] * sc / D * 2 * M_PI, sy = origin[1] * sc / D * 2 * M_PI, sz = origin[2] * sc / D * 2 * M_PI;
     map_cut_kernel<<<148 * 8, 256, 0, s>>>(M->d_work, N, D, 1.0 / sqrt((double)n3), sx, sy, sz, M->d_ref);
     MCK(cudaGetLastError());
+    if (!M->d_full) MCK(cudaMalloc(&M->d_full, sizeof(float2) * n3));
+    {
+        const double fx = origin[0] / N * 2 * M_PI, fy = origin[1] / N * 2 * M_PI, fz = origin[2] / N * 2 * M_PI;
+        map_full_kernel<<<148 * 8, 256, 0, s>>>(M->d_work, N, 1.0 / sqrt((double)n3), fx, fy, fz, M->d_full);
+        MCK(cudaGetLastError());
+    }
     MCK(cudaStreamSynchronize(s));
     // the same transform behind a 3-D texture (point sampling, integer
     // coordinates: every fetch returns a stored value unchanged)
@@ -997,3 +1084,85 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
     return BSG_OK;
 }
 
+
+extern "C" int bsg_match_project(bsg_match* h, const double* mats, long nviews, double resolution,
+                                 const double* origins, const double* ctf, float* out, int flags) {
+    Match* M = reinterpret_cast<Match*>(h);
+    if (!M || !mats || !out || nviews < 1) return mfail(BSG_ERR_ARG, "bsg_match_project: bad argument");
+    if (!M->have_ref) return mfail(BSG_ERR_STATE, "bsg_match_project: no reference set");
+    MCK(cudaSetDevice(M->device));
+    const int N = M->N;
+    const double u = M->cfg.map_sampling, real = N * u;
+    if (!(resolution > 0)) resolution = u;                 // Bimage_project.cpp:291
+    // section pixels of the uncut map within the limit, reference order
+    std::vector<MPix> px;
+    const double inv = 1.0 / real, maxs2 = 1.0 / (resolution * resolution);
+    for (int yy = 0; yy < N; ++yy)
+        for (int xx = 0; xx < N; ++xx) {
+            const int hh = sfreq(xx, N), kk = sfreq(yy, N);
+            const double ix = hh * inv, iy = kk * inv;
+            if (ix * ix + iy * iy > maxs2) continue;
+            MPix q{};
+            q.h = (short)hh; q.k = (short)kk; q.idx = yy * N + xx; q.insec = 1;
+            px.push_back(q);
+        }
+    const long per = (long)N * N;
+    const long chunk = std::max(1L, std::min<long>(nviews, (512L << 20) / (long)(sizeof(double2) * per)));
+    int rc = ensure_work(*M, (size_t)per * chunk);
+    if (rc) return rc;
+    cudaStream_t s = M->stream;
+    MPix* d_px = nullptr;
+    MHyp* d_v = nullptr;
+    ImgCtf* d_c = nullptr;
+    float* d_o = nullptr;
+    cudaError_t e = cudaMalloc(&d_px, sizeof(MPix) * std::max<size_t>(1, px.size()));
+    if (e == cudaSuccess) e = cudaMalloc(&d_v, sizeof(MHyp) * chunk);
+    if (e == cudaSuccess && ctf) e = cudaMalloc(&d_c, sizeof(ImgCtf) * chunk);
+    if (e == cudaSuccess && !(flags & BSG_DEVICE_PTR)) e = cudaMalloc(&d_o, sizeof(float) * per * chunk);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_px, px.data(), sizeof(MPix) * px.size(), cudaMemcpyHostToDevice, s);
+    std::vector<MHyp> hv(chunk);
+    std::vector<ImgCtf> hc(ctf ? chunk : 0);
+    for (long v0 = 0; e == cudaSuccess && v0 < nviews; v0 += chunk) {
+        const long cnt = std::min(chunk, nviews - v0);
+        for (long i = 0; i < cnt; ++i) {
+            memset(&hv[i], 0, sizeof(MHyp));
+            memcpy(hv[i].m, mats + 9 * (v0 + i), sizeof(double) * 9);
+            const double ox = origins ? origins[2 * (v0 + i)] : (double)(N / 2);
+            const double oy = origins ? origins[2 * (v0 + i) + 1] : (double)(N / 2);
+            hv[i].sx = -2 * M_PI * ox / N;
+            hv[i].sy = -2 * M_PI * oy / N;
+            if (ctf) {
+                const double* r = ctf + BSG_MATCH_CTF_DOUBLES * (v0 + i);
+                memset(&hc[i], 0, sizeof(ImgCtf));
+                for (int j = 0; j < 5; ++j) hc[i].c[j] = r[1 + j];
+                const int f = (int)r[6];
+                const double t2 = -M_PI * electron_lambda(r[0]);
+                hc[i].apply = (f & BSG_MATCH_APPLY_CTF) && t2 != 0 && r[2] / t2 >= 1 ? 1 : 0;
+                hc[i].invert = (f & BSG_MATCH_INVERT) ? 1 : 0;
+            }
+        }
+        e = cudaMemcpyAsync(d_v, hv.data(), sizeof(MHyp) * cnt, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && ctf) e = cudaMemcpyAsync(d_c, hc.data(), sizeof(ImgCtf) * cnt, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(M->d_work, 0, sizeof(double2) * per * cnt, s);
+        if (e == cudaSuccess) {
+            ProjArgs a{};
+            a.vol = M->d_full; a.N = N; a.wd = M->wd; a.lut = M->d_lut; a.pix = d_px; a.npix = (int)px.size();
+            a.views = d_v; a.ctf = ctf ? d_c : nullptr; a.inv = inv; a.real = real; a.fs = 1.0 / (N * M->cfg.pixel);
+            a.out = M->d_work;
+            project_kernel<<<(unsigned)cnt, 256, 0, s>>>(a);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = fft2_forward(M->d_work, N, cnt, M->d_tw_map, s);
+        float* dst = (flags & BSG_DEVICE_PTR) ? out + per * v0 : d_o;
+        if (e == cudaSuccess) {
+            proj_real_kernel<<<148 * 8, 256, 0, s>>>(M->d_work, per * cnt, 1.0 / N, dst);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && !(flags & BSG_DEVICE_PTR))
+            e = cudaMemcpyAsync(out + per * v0, d_o, sizeof(float) * per * cnt, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaFree(d_px); cudaFree(d_v); cudaFree(d_c); cudaFree(d_o);
+    if (e != cudaSuccess) return mfail(BSG_ERR_CUDA, "bsg_match_project: %s", cudaGetErrorString(e));
+    return BSG_OK;
+}

@@ -178,6 +178,7 @@ struct Match {
     double2* d_tw_map = nullptr;
     double2* d_tw_img = nullptr;
     float2* d_ref = nullptr;           // diam^3
+    float2* d_full = nullptr;          // uncut N^3 transform for the projector
     cudaArray_t ref_array = nullptr;   // the same values behind a 3-D texture
     cudaTextureObject_t ref_tex = 0;
     bool have_ref = false;

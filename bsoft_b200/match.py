@@ -98,6 +98,20 @@ class Matcher:
                    "bsg_match_sections")
         return out
 
+    def project(self, mats, resolution: float = 0.0, origins=None, ctf=None, out=None):
+        """Real-space projections (nviews, N, N) of the reference through its
+        transform (Bimage::project); `out` may be a CUDA tensor."""
+        m = np.ascontiguousarray(mats, dtype=np.float64).reshape(-1, 9)
+        o = None if origins is None else np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 2)
+        c = None if ctf is None else np.ascontiguousarray(ctf, dtype=np.float64).reshape(-1, MATCH_CTF_DOUBLES)
+        if out is None:
+            out = np.empty((len(m), self.N, self.N), dtype=np.float32)
+        p, dev = _ptr(out)
+        _lib.check(_lib.load().bsg_match_project(self._h, _dp(m), len(m), float(resolution),
+                                                 None if o is None else _dp(o), None if c is None else _dp(c), p,
+                                                 _lib.BSG_DEVICE_PTR if dev else 0), "bsg_match_project")
+        return out
+
     def set_images(self, images, ctf, file_avg: float = 0.0, file_std: float = 0.0) -> None:
         """Prepare particle images (nimg, n, n) with their CTF records
         (nimg, 8).  file_std > 0: normalise by the stack file's statistics,

@@ -168,6 +168,8 @@ int  bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const float* d_im
  *                              (hi_res / 1.11, mg_refine.cpp:885)
  *   bsg_match_set_images    <- part_refine_orientation's particle preparation
  *                              (mg_refine.cpp:509-563)
+ *   bsg_match_project       <- Bimage::project (Bimage.h:996,
+ *                              bsoft/src/img/Bimage_project.cpp:362-443)
  *   bsg_match_score         <- one hypothesis of img_fit_in_recip_space_grid:
  *                              origin, phase_shift_to_origin, central_section,
  *                              img_recip_space_fom (mg_refine.cpp:660-781,
@@ -220,6 +222,15 @@ int  bsg_match_set_reference(bsg_match* m, const float* map, const double* origi
 int  bsg_match_reference_transform(bsg_match* m, float* out, int flags);
 /* Central sections for nviews row-major matrices: nviews x diam^2 complex64. */
 int  bsg_match_sections(bsg_match* m, const double* mats, long nviews, float* out, int flags);
+/* Projections (Bimage::project with the FSI kernel, Bimage.h:996,
+ * bsoft/src/img/Bimage_project.cpp:362-443, back-transformed, real part):
+ * nviews x N x N float32 of the UNCUT reference transform, pixels within
+ * `resolution` (angstrom; <= 0: the sampling).  origins (nviews x 2 pixels,
+ * NULL = N/2, the reference's phase_shift_to_center) place each projection;
+ * ctf (nviews CTF records, NULL = none) multiplies each section by its CTF
+ * first - an addition for synthesising particle images. */
+int  bsg_match_project(bsg_match* m, const double* mats, long nviews, double resolution,
+                       const double* origins, const double* ctf, float* out, int flags);
 /* Particle images (nimg x n x n float32) with their CTF records; file_avg /
  * file_std are the statistics rescale_to_avg_std divides by (for a stack
  * read by the reference: the file header's), file_std <= 0 uses each

@@ -10,6 +10,7 @@ hypotheses with and without the CTF.
 
     python tests/golden/make_match_golden.py
 
+``project_probe`` adds Bimage::project of the map for the same views.
 ``views_probe`` lists the views of ``asymmetric_unit_views`` for a few point
 groups and steps (views.npz).
 
@@ -90,12 +91,18 @@ def make(name: str, case: dict) -> str:
         secs = np.fromfile(out + ".sec", dtype=np.complex64).reshape(len(views), diam, diam)
         prep = np.fromfile(out + ".img", dtype=np.complex64).reshape(nimg, diam, diam)
         fom = np.loadtxt(out + ".fom").reshape(-1, 2)
+        # Bimage::project of the same map for the same views (project_probe)
+        pres = spec.pixel * 2.0
+        rp = subprocess.run([os.path.join(REF, "project_probe"), mapf, repr(pres), os.path.join(td, "views.txt"),
+                             out + ".proj"], capture_output=True, text=True, check=True)
+        proj = np.fromfile(out + ".proj", dtype=np.float32).reshape(len(views), N, N)
     path = os.path.join(OUT, f"{name}.npz")
     np.savez_compressed(path, map=vol, images=imgs, pixel=spec.pixel, hi_res=case["hi_res"], views=views,
                         ctf_rows=ctf_rows, hyps=hyps, diam=diam, map_origin=map_origin,
                         true_views=meta["views"], true_origins=meta["origins"],
                         map_spec=map_spec, sections=secs, prepared=prep, fom=fom,
                         file_avg=float(imgs.mean()), file_std=float(imgs.std()),
+                        proj=proj, proj_res=pres,
                         probe_stdout=r.stdout)
     return path
 

@@ -87,3 +87,11 @@ def test_bad_arguments():
         Matcher(n=48, map=48, map_sampling=1.5, pixel=1.5, hi_res=3.75)   # not a power of two
     with pytest.raises(BsgError):
         Matcher(n=32, map=64, map_sampling=1.5, pixel=1.5, hi_res=3.0)    # cut edge above the box
+
+
+def test_projections(matcher):
+    """Bimage::project (Fourier projector with the FSI kernel) of the uncut map."""
+    m, d = matcher
+    p = m.project(d["mats"], resolution=float(d["proj_res"]))
+    for a, b in zip(p, d["proj"]):
+        assert rel_l2(a, b) < 1e-5
