@@ -47,6 +47,12 @@ class MatchStats(C.Structure):
                 ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int)]
 
 
+class CnnConfig(C.Structure):
+    _fields_ = [("box", C.c_int), ("channels", C.c_int * 6), ("hidden", C.c_int), ("batch", C.c_int),
+                ("shift_weight", C.c_float), ("device", C.c_int), ("seed", C.c_ulonglong)]
+
+
+CNN_RESULT_FLOATS = 11
 MATCH_RESULT_DOUBLES = 5
 MATCH_TOPK_MAX = 8
 MATCH_APPLY_CTF = 1
@@ -101,6 +107,14 @@ def load():
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_match_stream": ([vp], vp),
+        "bsg_cnn_create": ([C.POINTER(CnnConfig), C.POINTER(vp)], C.c_int),
+        "bsg_cnn_destroy": ([vp], None),
+        "bsg_cnn_num_params": ([vp], C.c_long),
+        "bsg_cnn_get_params": ([vp, fp], C.c_int),
+        "bsg_cnn_set_params": ([vp, fp], C.c_int),
+        "bsg_cnn_predict": ([vp, vp, C.c_long, vp, C.c_int], C.c_int),
+        "bsg_cnn_loss_grad": ([vp, fp, fp, C.c_long, dp, fp], C.c_int),
+        "bsg_cnn_train": ([vp, vp, vp, C.c_long, C.c_int, C.c_float, fp, C.c_int], C.c_int),
         "bsg_last_error": ([], C.c_char_p),
         "bsg_version": ([], C.c_char_p),
     }

@@ -286,6 +286,46 @@ int  bsg_match_get_stats(bsg_match* m, bsg_match_stats* st);
 int  bsg_match_reset_stats(bsg_match* m);
 void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
 
+/* ---- learned orientation proposer ------------------------------------------
+ * No counterpart in the reference.  A convolutional network maps a particle
+ * image to a rotation and a shift; bsg_match_search_local then searches
+ * only the panel sections near each proposal.  6 convolutions (3x3, stride
+ * 2, ReLU), two dense layers, a 6-D rotation head (Gram-Schmidt); weights
+ * held in FP32, used rounded to BF16, FP32 accumulation.
+ * Parameter order: for each convolution W[cout][3][3][cin], b[cout]; then
+ * fc1 W[hidden][(box/64)^2 * c6] (input flattened y, x, channel), b; fc2
+ * W[8][hidden], b.  Outputs per image (BSG_CNN_RESULT_FLOATS): rotation
+ * matrix row-major (9, columns b1 b2 b3), shift x, y (pixels from the box
+ * centre). */
+#define BSG_CNN_RESULT_FLOATS 11
+typedef struct {
+    int    box;            /* image edge: power of two, 64..512             */
+    int    channels[6];    /* output channels of the 6 convolutions         */
+    int    hidden;         /* width of the dense layer                      */
+    int    batch;          /* mini-batch (training) / chunk (inference)     */
+    float  shift_weight;   /* lambda of the shift term of the loss          */
+    int    device;
+    unsigned long long seed;   /* initialisation and batch sampling         */
+} bsg_cnn_config;
+
+typedef struct bsg_cnn bsg_cnn;
+
+int  bsg_cnn_create(const bsg_cnn_config* cfg, bsg_cnn** out);
+void bsg_cnn_destroy(bsg_cnn* c);
+long bsg_cnn_num_params(const bsg_cnn* c);
+int  bsg_cnn_get_params(bsg_cnn* c, float* out);
+int  bsg_cnn_set_params(bsg_cnn* c, const float* in);      /* resets the optimiser */
+/* n images (box^2 float32 each) -> n x BSG_CNN_RESULT_FLOATS */
+int  bsg_cnn_predict(bsg_cnn* c, const float* images, long n, float* out, int flags);
+/* mean loss and its gradient (all parameters) for n host images with host
+ * targets (n x BSG_CNN_RESULT_FLOATS: true rotation and shift) */
+int  bsg_cnn_loss_grad(bsg_cnn* c, const float* images, const float* targets, long n, double* loss, float* grads);
+/* `steps` Adam steps on mini-batches drawn without replacement from ndata
+ * device-resident images and targets (BSG_DEVICE_PTR required); losses
+ * (host, optional) receives the mean loss of each step */
+int  bsg_cnn_train(bsg_cnn* c, const float* images, const float* targets, long ndata, int steps, float lr,
+                   float* losses, int flags);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 
