@@ -115,6 +115,7 @@ def load():
         "bsg_cnn_predict": ([vp, vp, C.c_long, vp, C.c_int], C.c_int),
         "bsg_cnn_loss_grad": ([vp, fp, fp, C.c_long, dp, fp], C.c_int),
         "bsg_cnn_train": ([vp, vp, vp, C.c_long, C.c_int, C.c_float, fp, C.c_int], C.c_int),
+        "bsg_add_noise": ([vp, C.c_long, C.c_int, C.c_double, C.c_ulonglong, vp], C.c_int),
         "bsg_last_error": ([], C.c_char_p),
         "bsg_version": ([], C.c_char_p),
     }

@@ -111,3 +111,10 @@ def pose_targets(mats: np.ndarray, shifts: np.ndarray) -> np.ndarray:
     """Targets (n, 11) from rotation matrices (n, 3, 3) and shifts (n, 2)."""
     m = np.asarray(mats, dtype=np.float64).reshape(-1, 9)
     return np.concatenate([m, np.asarray(shifts, dtype=np.float64).reshape(-1, 2)], axis=1).astype(np.float32)
+
+
+def add_noise(images, snr: float, seed: int = 1) -> None:
+    """Add Gaussian noise in place to CUDA images (n, box, box) at `snr`."""
+    n, box = images.shape[0], images.shape[1]
+    _lib.check(_lib.load().bsg_add_noise(C.c_void_p(images.data_ptr()), n, box, float(snr), seed, None),
+               "bsg_add_noise")

@@ -807,3 +807,57 @@ extern "C" int bsg_cnn_train(bsg_cnn* h, const float* images, const float* targe
     if (e != cudaSuccess) return cfail(BSG_ERR_CUDA, "bsg_cnn_train: %s", cudaGetErrorString(e));
     return BSG_OK;
 }
+
+namespace bsg {
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// per image: variance of the signal inside the inscribed circle, then
+// Gaussian noise of variance var / snr (Box-Muller on a counter-based hash
+// of seed, image and pixel, so the result does not depend on the launch)
+__global__ void __launch_bounds__(256) add_noise_kernel(float* __restrict__ img, int box, double snr, uint64_t seed) {
+    __shared__ double s1[256], s2[256], s3[256];
+    float* p = img + (size_t)blockIdx.x * box * box;
+    const double c = box / 2.0, r2 = c * c;
+    double a = 0, b = 0, n = 0;
+    for (int i = threadIdx.x; i < box * box; i += 256) {
+        const double dx = i % box - c, dy = i / box - c;
+        if (dx * dx + dy * dy <= r2) { const double v = p[i]; a += v; b += v * v; n += 1; }
+    }
+    s1[threadIdx.x] = a; s2[threadIdx.x] = b; s3[threadIdx.x] = n;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o]; s2[threadIdx.x] += s2[threadIdx.x + o]; s3[threadIdx.x] += s3[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    const double mean = s1[0] / s3[0], var = s2[0] / s3[0] - mean * mean;
+    const double sd = var > 0 ? sqrt(var / snr) : 0.0;
+    for (int i = threadIdx.x; i < box * box; i += 256) {
+        const uint64_t h = mix64(seed ^ mix64(((uint64_t)blockIdx.x << 32) + (uint64_t)i + 0x9E3779B97F4A7C15ull));
+        const double u1 = ((h >> 11) + 1.0) / 9007199254740993.0;
+        const double u2 = (mix64(h) >> 11) / 9007199254740992.0;
+        p[i] += (float)(sd * sqrt(-2.0 * log(u1)) * cos(2 * M_PI * u2));
+    }
+}
+
+}  // namespace
+}  // namespace bsg
+
+extern "C" int bsg_add_noise(float* d_images, long n, int box, double snr, unsigned long long seed, void* stream) {
+    if (!d_images || n < 1 || box < 2 || !(snr > 0)) return cfail(BSG_ERR_ARG, "bsg_add_noise: bad argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (long b0 = 0; b0 < n; b0 += 65535) {
+        const long cnt = std::min(65535L, n - b0);
+        add_noise_kernel<<<(unsigned)cnt, 256, 0, s>>>(d_images + (size_t)b0 * box * box, box, snr, seed + (uint64_t)b0);
+        CCK(cudaGetLastError());
+    }
+    CCK(cudaStreamSynchronize(s));
+    return BSG_OK;
+}

@@ -326,6 +326,11 @@ int  bsg_cnn_loss_grad(bsg_cnn* c, const float* images, const float* targets, lo
 int  bsg_cnn_train(bsg_cnn* c, const float* images, const float* targets, long ndata, int steps, float lr,
                    float* losses, int flags);
 
+/* Data synthesis: Gaussian noise added to n device images (box^2 each) at a
+ * signal-to-noise ratio relative to each image's variance inside the
+ * inscribed circle; counter-based, reproducible for a seed. */
+int  bsg_add_noise(float* d_images, long n, int box, double snr, unsigned long long seed, void* stream);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 
