@@ -42,7 +42,8 @@ class MatchInfo(C.Structure):
 
 class MatchStats(C.Structure):
     _fields_ = [("panel_ms", C.c_double), ("agen_ms", C.c_double), ("gemm_ms", C.c_double),
-                ("merge_ms", C.c_double), ("rescore_ms", C.c_double), ("gemm_flops", C.c_double),
+                ("merge_ms", C.c_double), ("rescore_ms", C.c_double), ("local_ms", C.c_double),
+                ("gemm_flops", C.c_double),
                 ("hypotheses", C.c_double), ("launches", C.c_long), ("gemm_launches", C.c_long),
                 ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int)]
 
@@ -104,6 +105,7 @@ def load():
         "bsg_match_project": ([vp, dp, C.c_long, C.c_double, dp, dp, vp, C.c_int], C.c_int),
         "bsg_match_set_panel": ([vp, dp, C.c_long, C.c_int], C.c_int),
         "bsg_match_search": ([vp, dp, C.c_int, C.c_int, dp, C.c_int], C.c_int),
+        "bsg_match_search_local": ([vp, vp, C.c_double, dp, C.c_int, C.c_double, C.c_int, dp, C.c_int], C.c_int),
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_match_stream": ([vp], vp),

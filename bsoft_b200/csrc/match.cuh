@@ -211,6 +211,7 @@ struct Match {
     long nsec = 0;
     MHyp* d_secs = nullptr;            // panel views (rows 0, 1 scaled)
     std::vector<MHyp> h_secs;          // host copy
+    float* d_rots = nullptr;           // panel rotations (unscaled, float) for local selection
     __nv_bfloat16* d_panel = nullptr;  // nsec x kpad
     __nv_bfloat16* d_A = nullptr;      // rows x kpad
     size_t a_elems = 0;

@@ -478,6 +478,158 @@ __global__ void merge_kernel(const float* __restrict__ ps, const int* __restrict
     }
 }
 
+
+// ---- local search around proposals -----------------------------------------
+
+constexpr int LOCAL_MAXC = 1024;    // candidate sections per image
+constexpr int LOCAL_MAXO = 9;       // trial origins per image
+
+// per image: the panel sections whose rotation lies within the angle whose
+// cosine bound is `tr_min` of trace(R_p^T R_s) - in panel order (ordered
+// compaction over 256-section chunks)
+__global__ void __launch_bounds__(256) local_select_kernel(const float* __restrict__ prop, const float* __restrict__ rots,
+                                                           long nsec, float tr_min, long img0,
+                                                           int* __restrict__ cand, int* __restrict__ count) {
+    __shared__ int wsum[8];
+    __shared__ float Rp[9];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long img = img0 + blockIdx.x;
+    if (threadIdx.x < 9) Rp[threadIdx.x] = prop[img * 11 + threadIdx.x];
+    __syncthreads();
+    int base_out = 0;
+    int* my = cand + (long)blockIdx.x * LOCAL_MAXC;
+    for (long c0 = 0; c0 < nsec; c0 += 256) {
+        const long j = c0 + threadIdx.x;
+        bool in = false;
+        if (j < nsec) {
+            const float* r = rots + j * 9;
+            float t = 0.f;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) t = fmaf(Rp[k], r[k], t);
+            in = t >= tr_min;
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) wsum[warp] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < 8; ++w) { if (w < warp) before += wsum[w]; total += wsum[w]; }
+        const int pos = base_out + before + __popc(b & ((1u << lane) - 1u));
+        if (in && pos < LOCAL_MAXC) my[pos] = (int)j;
+        base_out += total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) count[blockIdx.x] = base_out;
+}
+
+__device__ __forceinline__ float2 bf2f(uint32_t u) {
+    return make_float2(__uint_as_float(u << 16), __uint_as_float(u & 0xFFFF0000u));
+}
+
+// per image: its A rows at its local origins in shared memory (BF16, as
+// rows_kernel writes them), then every candidate section's panel row dotted
+// with each of them by one warp; the topk (section, origin) pairs by score
+// go to the candidate arrays in (score desc, section, origin) order
+__global__ void __launch_bounds__(256) local_score_kernel(
+    const float2* __restrict__ spec, int D, const float* __restrict__ ctf, int npix, const MPix* __restrict__ cpix,
+    int ncpix, int nf, const float* __restrict__ gA, const double2* __restrict__ slopes,
+    const int* __restrict__ lorg, const int* __restrict__ nlorg, const int* __restrict__ cand,
+    const int* __restrict__ count, const __nv_bfloat16* __restrict__ panel, int kpad, int topk, long img0,
+    int* __restrict__ out_sec, int* __restrict__ out_org, float* __restrict__ out_score) {
+    extern __shared__ uint4 lsm[];
+    const int b = blockIdx.x;
+    const long img = img0 + b;
+    const int no = nlorg[b];
+    const int nc = min(count[b], LOCAL_MAXC);
+    __nv_bfloat162* A = reinterpret_cast<__nv_bfloat162*>(lsm);           // no x kpad/2
+    float* sc = reinterpret_cast<float*>(A + (size_t)LOCAL_MAXO * (kpad / 2));   // LOCAL_MAXC x LOCAL_MAXO
+    const float2* X = spec + img * (long)D * D;
+    const float* C = ctf + img * (long)npix;
+    const float* g = gA + (long)b * nf;
+    for (int o = 0; o < no; ++o) {
+        const double2 sl = slopes[lorg[b * LOCAL_MAXO + o]];
+        for (int p = threadIdx.x; p < kpad / 2; p += blockDim.x) {
+            float2 v = make_float2(0.f, 0.f);
+            if (p < ncpix) {
+                const MPix q = cpix[p];
+                const float2 x = X[q.idx];
+                double phi = q.h * sl.x + q.k * sl.y;
+                phi -= 6.283185307179586 * rint(phi * 0.15915494309189535);
+                float sn, cs;
+                sincosf((float)phi, &sn, &cs);
+                const float f = C[q.pad] * g[q.shell];
+                v = make_float2((x.x * cs - x.y * sn) * f, (x.x * sn + x.y * cs) * f);
+            }
+            A[(size_t)o * (kpad / 2) + p] = __floats2bfloat162_rn(v.x, v.y);
+        }
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint4* As = reinterpret_cast<const uint4*>(A);
+    const int k8 = kpad / 8;                 // 16-byte chunks per row
+    for (int ci = warp; ci < nc; ci += 8) {
+        const int sec = cand[(long)b * LOCAL_MAXC + ci];
+        const uint4* row = reinterpret_cast<const uint4*>(panel + (size_t)sec * kpad);
+        float acc[LOCAL_MAXO];
+#pragma unroll
+        for (int o = 0; o < LOCAL_MAXO; ++o) acc[o] = 0.f;
+        for (int p = lane; p < k8; p += 32) {
+            const uint4 pb = __ldg(row + p);
+            const float2 b0 = bf2f(pb.x), b1 = bf2f(pb.y), b2 = bf2f(pb.z), b3 = bf2f(pb.w);
+#pragma unroll
+            for (int o = 0; o < LOCAL_MAXO; ++o) {
+                if (o < no) {
+                    const uint4 ab = As[(size_t)o * k8 + p];
+                    const float2 a0 = bf2f(ab.x), a1 = bf2f(ab.y), a2 = bf2f(ab.z), a3 = bf2f(ab.w);
+                    float t = acc[o];
+                    t = fmaf(a0.x, b0.x, t); t = fmaf(a0.y, b0.y, t);
+                    t = fmaf(a1.x, b1.x, t); t = fmaf(a1.y, b1.y, t);
+                    t = fmaf(a2.x, b2.x, t); t = fmaf(a2.y, b2.y, t);
+                    t = fmaf(a3.x, b3.x, t); t = fmaf(a3.y, b3.y, t);
+                    acc[o] = t;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 0; o < LOCAL_MAXO; ++o) {
+            float t = acc[o];
+#pragma unroll
+            for (int k = 16; k; k >>= 1) t += __shfl_xor_sync(0xffffffffu, t, k);
+            if (lane == 0 && o < no) sc[ci * LOCAL_MAXO + o] = t;
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int n = nc * no;
+        float prev_s = 3.0e38f;
+        long prev_k = -1;
+        for (int t = 0; t < topk; ++t) {
+            float bs = -3.0e38f;
+            long bk = -1;
+            for (int e = lane; e < n; e += 32) {
+                const int ci = e / no, o = e - ci * no;
+                const float v = sc[ci * LOCAL_MAXO + o];
+                const long key = (long)cand[(long)b * LOCAL_MAXC + ci] * LOCAL_MAXO + o;
+                const bool after = v < prev_s || (v == prev_s && key > prev_k);
+                if (!after) continue;
+                if (v > bs || (v == bs && (bk < 0 || key < bk))) { bs = v; bk = key; }
+            }
+            for (int k = 16; k; k >>= 1) {
+                const float os = __shfl_xor_sync(0xffffffffu, bs, k);
+                const long ok = __shfl_xor_sync(0xffffffffu, bk, k);
+                if (ok >= 0 && (os > bs || (os == bs && (bk < 0 || ok < bk)))) { bs = os; bk = ok; }
+            }
+            if (lane == 0) {
+                const long c = img * topk + t;
+                out_sec[c] = bk >= 0 ? (int)(bk / LOCAL_MAXO) : -1;
+                out_org[c] = bk >= 0 ? lorg[b * LOCAL_MAXO + (int)(bk % LOCAL_MAXO)] : -1;
+                out_score[c] = bs;
+            }
+            prev_s = bk >= 0 ? bs : -3.0e38f;
+            prev_k = bk;
+        }
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -531,6 +683,86 @@ static void coarse_pixels(Match& M) {
     M.kpad = ((2 * M.ncpix + BK - 1) / BK) * BK;
 }
 
+
+// exact rescoring of the candidates in d_csec / d_corg / d_cscore (topk per
+// held image): candidates of one image that share a section form one group
+// (one gather, several origins); out gets each image's candidates ordered
+// by the exact figure of merit
+static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<double2>& sl, double* out, float* tres,
+                                      long* ngroups) {
+    Match* M = &Mr;
+    cudaStream_t s = M->stream;
+    cudaError_t e = cudaSuccess;
+    const long ncand = M->nimg * topk;
+    std::vector<int> csec(ncand), corg(ncand);
+    std::vector<float> cscore(ncand);
+    e = cudaMemcpyAsync(csec.data(), M->d_csec, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(corg.data(), M->d_corg, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cscore.data(), M->d_cscore, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    std::vector<MHyp> hv;
+    std::vector<long> hidx;
+    hv.reserve(ncand);
+    for (long c = 0; c < ncand; ++c) {
+        if (csec[c] < 0) continue;
+        MHyp hh = M->h_secs[csec[c]];
+        hh.sx = sl[corg[c]].x;
+        hh.sy = sl[corg[c]].y;
+        hh.img = (int)(c / topk);
+        hv.push_back(hh);
+        hidx.push_back(c);
+    }
+    std::vector<MHypG> groups;
+    std::vector<long> slot;
+    group_hypotheses(hv, groups, slot);
+    const long ng = (long)groups.size();
+    *ngroups = ng;
+    std::vector<double> cf(2 * ncand, 0.0);
+    *tres = 0;
+    if (ng > 0) {
+        if (ensure_groups(*M, ng) != BSG_OK) return cudaErrorMemoryAllocation;
+        std::vector<double> go(2 * ng * MAXORG);
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
+        cudaEventRecord(e0, s);
+        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s);
+        cudaEventRecord(e1, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        cudaEventElapsedTime(tres, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (e != cudaSuccess) return e;
+        for (size_t k = 0; k < hidx.size(); ++k) {
+            cf[hidx[k]] = go[slot[k]];
+            cf[ncand + hidx[k]] = go[ng * MAXORG + slot[k]];
+        }
+    }
+    for (long i = 0; i < M->nimg; ++i) {
+        std::vector<int> ord(topk);
+        for (int t = 0; t < topk; ++t) ord[t] = t;
+        const long b = i * topk;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
+            const bool vx = csec[b + x] >= 0, vy = csec[b + y] >= 0;
+            if (vx != vy) return vx;
+            return cf[b + x] > cf[b + y];
+        });
+        for (int t = 0; t < topk; ++t) {
+            const long c = b + ord[t];
+            double* o = out + (b + t) * BSG_MATCH_RESULT_DOUBLES;
+            o[0] = csec[c];
+            o[1] = corg[c];
+            o[2] = cscore[c];
+            o[3] = csec[c] >= 0 ? cf[c] : 0.0;
+            o[4] = csec[c] >= 0 ? cf[ncand + c] : 0.0;
+        }
+    }
+    return cudaSuccess;
+}
+
 }  // namespace bsg
 
 using namespace bsg;
@@ -558,6 +790,7 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     cudaFree(M->d_secs); M->d_secs = nullptr;
     cudaFree(M->d_cpix); M->d_cpix = nullptr;
     cudaFree(M->d_cstart); M->d_cstart = nullptr;
+    cudaFree(M->d_rots); M->d_rots = nullptr;
     M->nsec = 0;
     std::vector<MHyp> sv(nsec);
     for (long v = 0; v < nsec; ++v) {
@@ -568,10 +801,17 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     if (e == cudaSuccess) e = cudaMalloc(&M->d_secs, sizeof(MHyp) * nsec);
     if (e == cudaSuccess) e = cudaMalloc(&M->d_cpix, sizeof(MPix) * std::max(1, M->ncpix));
     if (e == cudaSuccess) e = cudaMalloc(&M->d_cstart, sizeof(int) * (M->nf + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&M->d_rots, sizeof(float) * 9 * nsec);
     if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_set_panel: %ld sections: %s", nsec, cudaGetErrorString(e));
     e = cudaMemcpyAsync(M->d_secs, sv.data(), sizeof(MHyp) * nsec, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(M->d_cpix, M->h_cpix.data(), sizeof(MPix) * M->ncpix, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(M->d_cstart, M->h_cstart.data(), sizeof(int) * (M->nf + 1), cudaMemcpyHostToDevice, s);
+    {
+        std::vector<float> rf((size_t)9 * nsec);
+        for (long i = 0; i < 9 * nsec; ++i) rf[i] = (float)mats[i];
+        if (e == cudaSuccess) e = cudaMemcpyAsync(M->d_rots, rf.data(), sizeof(float) * rf.size(), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -732,70 +972,13 @@ extern "C" int bsg_match_search(bsg_match* h, const double* origins, int norigin
         }
         M->sstats.gemm_flops += 2.0 * (double)rows * (double)M->nsec * (double)(2 * M->ncpix);
     }
-    // exact rescoring of every candidate: candidates of one image that share
-    // a section are one group (one gather, several origins)
-    const long ncand = M->nimg * topk;
-    std::vector<int> csec(ncand), corg(ncand);
-    std::vector<float> cscore(ncand);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(csec.data(), M->d_csec, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(corg.data(), M->d_corg, sizeof(int) * ncand, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(cscore.data(), M->d_cscore, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    std::vector<MHyp> hv;
-    std::vector<long> hidx;
-    hv.reserve(ncand);
-    for (long c = 0; e == cudaSuccess && c < ncand; ++c) {
-        if (csec[c] < 0) continue;
-        MHyp hh = M->h_secs[csec[c]];
-        hh.sx = sl[corg[c]].x;
-        hh.sy = sl[corg[c]].y;
-        hh.img = (int)(c / topk);
-        hv.push_back(hh);
-        hidx.push_back(c);
-    }
-    std::vector<MHypG> groups;
-    std::vector<long> slot;
-    group_hypotheses(hv, groups, slot);
-    const long ng = (long)groups.size();
-    std::vector<double> cf(2 * ncand, 0.0);
-    float tres = 0;
-    if (e == cudaSuccess && ng > 0) {
-        if (ensure_groups(*M, ng) != BSG_OK) { for (auto& x : ev) cudaEventDestroy(x); return BSG_ERR_NOMEM; }
-        std::vector<double> go(2 * ng * MAXORG);
-        e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
-        cudaEventRecord(ev[0], s);
-        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s);
-        cudaEventRecord(ev[1], s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        cudaEventElapsedTime(&tres, ev[0], ev[1]);
-        for (size_t k = 0; k < hidx.size(); ++k) {
-            cf[hidx[k]] = go[slot[k]];
-            cf[ncand + hidx[k]] = go[ng * MAXORG + slot[k]];
-        }
-    }
     for (auto& x : ev) cudaEventDestroy(x);
     if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search: %s", cudaGetErrorString(e));
-    // per image: candidates ordered by the exact figure of merit
-    for (long i = 0; i < M->nimg; ++i) {
-        std::vector<int> ord(topk);
-        for (int t = 0; t < topk; ++t) ord[t] = t;
-        const long b = i * topk;
-        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) {
-            const bool vx = csec[b + x] >= 0, vy = csec[b + y] >= 0;
-            if (vx != vy) return vx;
-            return cf[b + x] > cf[b + y];
-        });
-        for (int t = 0; t < topk; ++t) {
-            const long c = b + ord[t];
-            double* o = out + (b + t) * BSG_MATCH_RESULT_DOUBLES;
-            o[0] = csec[c];
-            o[1] = corg[c];
-            o[2] = cscore[c];
-            o[3] = csec[c] >= 0 ? cf[c] : 0.0;
-            o[4] = csec[c] >= 0 ? cf[ncand + c] : 0.0;
-        }
-    }
+    float tres = 0;
+    long ng = 0;
+    e = rescore_candidates(*M, topk, sl, out, &tres, &ng);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search: %s", cudaGetErrorString(e));
+    const long ncand = M->nimg * topk;
     M->sstats.agen_ms += agen;
     M->sstats.gemm_ms += gemm;
     M->sstats.merge_ms += merge;
@@ -827,4 +1010,129 @@ extern "C" int bsg_match_reset_stats(bsg_match* h) {
 extern "C" void* bsg_match_stream(bsg_match* h) {
     Match* M = reinterpret_cast<Match*>(h);
     return M ? static_cast<void*>(M->stream) : nullptr;
+}
+
+extern "C" int bsg_match_search_local(bsg_match* h, const float* proposals, double radius, const double* origins,
+                                      int norigin, double origin_radius, int topk, double* out, int flags) {
+    (void)flags;
+    Match* M = reinterpret_cast<Match*>(h);
+    if (!M || !proposals || !origins || !out || norigin < 1 || topk < 1 || topk > TOPK || !(radius > 0))
+        return match_fail(BSG_ERR_ARG, "bsg_match_search_local: bad argument (topk must be 1..%d)", TOPK);
+    if (M->nsec < 1 || M->nimg < 1) return match_fail(BSG_ERR_STATE, "bsg_match_search_local: set the panel and the images first");
+    cudaError_t e = cudaSetDevice(M->device);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search_local: %s", cudaGetErrorString(e));
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(local_score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    const size_t lsmem = sizeof(__nv_bfloat16) * (size_t)LOCAL_MAXO * M->kpad + sizeof(float) * LOCAL_MAXC * LOCAL_MAXO;
+    if (attr != cudaSuccess || lsmem > 227 * 1024)
+        return match_fail(BSG_ERR_ARG, "bsg_match_search_local: %d coarse values per row exceed the kernel's shared memory",
+                          M->kpad);
+    cudaStream_t s = M->stream;
+    const long nimg = M->nimg;
+    const int nf = M->nf;
+    // local trial origins of each image: those within origin_radius of the
+    // proposed origin (box centre + proposed shift), nearest first, at most 9
+    std::vector<float> prop((size_t)nimg * 11);
+    e = cudaMemcpy(prop.data(), proposals, sizeof(float) * prop.size(),
+                   (flags & BSG_DEVICE_PTR) ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search_local: %s", cudaGetErrorString(e));
+    std::vector<int> lorg((size_t)nimg * LOCAL_MAXO, 0), nlorg(nimg, 0);
+    for (long i = 0; i < nimg; ++i) {
+        const double px = M->n / 2 + prop[i * 11 + 9], py = M->n / 2 + prop[i * 11 + 10];
+        std::vector<std::pair<double, int>> d;
+        for (int o = 0; o < norigin; ++o) {
+            const double dx = origins[2 * o] - px, dy = origins[2 * o + 1] - py;
+            d.push_back({dx * dx + dy * dy, o});
+        }
+        std::stable_sort(d.begin(), d.end());
+        int k = 0;
+        for (auto& t : d) {
+            if (k >= LOCAL_MAXO || (t.first > origin_radius * origin_radius && k > 0)) break;
+            lorg[i * LOCAL_MAXO + k++] = t.second;
+        }
+        nlorg[i] = k;
+    }
+    std::vector<double2> sl(norigin);
+    for (int i = 0; i < norigin; ++i)
+        sl[i] = make_double2(M->cut_scale * origins[2 * i] / M->D * 2 * M_PI, M->cut_scale * origins[2 * i + 1] / M->D * 2 * M_PI);
+    const long nb = std::max(1L, std::min<long>(nimg, M->cfg.batch > 0 ? M->cfg.batch : 4096));
+    // scratch
+    const size_t need_cand = (size_t)nimg * topk;
+    if (need_cand > M->cand_elems) {
+        cudaFree(M->d_csec); cudaFree(M->d_corg); cudaFree(M->d_cscore);
+        M->d_csec = nullptr; M->d_corg = nullptr; M->d_cscore = nullptr;
+        M->cand_elems = 0;
+        e = cudaMalloc(&M->d_csec, sizeof(int) * need_cand);
+        if (e == cudaSuccess) e = cudaMalloc(&M->d_corg, sizeof(int) * need_cand);
+        if (e == cudaSuccess) e = cudaMalloc(&M->d_cscore, sizeof(float) * need_cand);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
+        M->cand_elems = need_cand;
+    }
+    if (M->gA_elems < (size_t)nb * nf) {
+        cudaFree(M->d_gA); M->d_gA = nullptr;
+        e = cudaMalloc(&M->d_gA, sizeof(float) * nb * nf);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
+        M->gA_elems = (size_t)nb * nf;
+    }
+    if (M->slope_elems < (size_t)norigin) {
+        cudaFree(M->d_slopes); M->d_slopes = nullptr;
+        e = cudaMalloc(&M->d_slopes, sizeof(double2) * norigin);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
+        M->slope_elems = norigin;
+    }
+    float* d_prop = nullptr;
+    int *d_lorg = nullptr, *d_nlorg = nullptr, *d_cand = nullptr, *d_count = nullptr;
+    e = cudaMalloc(&d_prop, sizeof(float) * prop.size());
+    if (e == cudaSuccess) e = cudaMalloc(&d_lorg, sizeof(int) * lorg.size());
+    if (e == cudaSuccess) e = cudaMalloc(&d_nlorg, sizeof(int) * nimg);
+    if (e == cudaSuccess) e = cudaMalloc(&d_cand, sizeof(int) * nb * LOCAL_MAXC);
+    if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(int) * nb);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_prop, prop.data(), sizeof(float) * prop.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_lorg, lorg.data(), sizeof(int) * lorg.size(), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_nlorg, nlorg.data(), sizeof(int) * nimg, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(M->d_slopes, sl.data(), sizeof(double2) * norigin, cudaMemcpyHostToDevice, s);
+    const float tr_min = (float)(1.0 + 2.0 * cos(radius));
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], s);
+    long launches = 0, considered = 0;
+    std::vector<int> cnt_h(nb);
+    for (long i0 = 0; e == cudaSuccess && i0 < nimg; i0 += nb) {
+        const long cnt = std::min(nb, nimg - i0);
+        local_select_kernel<<<(unsigned)cnt, 256, 0, s>>>(d_prop, M->d_rots, M->nsec, tr_min, i0, d_cand, d_count);
+        coarse_norm_kernel<<<(unsigned)cnt, 64, 0, s>>>(M->d_spec, M->D, M->d_ctf, (int)M->h_pix.size(), M->d_cpix,
+                                                         M->d_cstart, nf, i0, M->d_gA);
+        local_score_kernel<<<(unsigned)cnt, 256, lsmem, s>>>(
+            M->d_spec, M->D, M->d_ctf, (int)M->h_pix.size(), M->d_cpix, M->ncpix, nf, M->d_gA, M->d_slopes,
+            d_lorg + i0 * LOCAL_MAXO, d_nlorg + i0, d_cand, d_count, M->d_panel, M->kpad, topk, i0, M->d_csec,
+            M->d_corg, M->d_cscore);
+        e = cudaGetLastError();
+        launches += 3;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(cnt_h.data(), d_count, sizeof(int) * cnt, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        for (long i = 0; i < cnt; ++i) considered += (long)std::min(cnt_h[i], LOCAL_MAXC) * nlorg[i0 + i];
+    }
+    cudaEventRecord(ev[1], s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+    float lms = 0;
+    cudaEventElapsedTime(&lms, ev[0], ev[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    cudaFree(d_prop); cudaFree(d_lorg); cudaFree(d_nlorg); cudaFree(d_cand); cudaFree(d_count);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search_local: %s", cudaGetErrorString(e));
+    float tres = 0;
+    long ng = 0;
+    e = rescore_candidates(*M, topk, sl, out, &tres, &ng);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search_local: %s", cudaGetErrorString(e));
+    M->sstats.local_ms += lms;
+    M->sstats.rescore_ms += tres;
+    M->sstats.launches += launches + (ng > 0 ? 1 : 0);
+    M->sstats.images += nimg;
+    M->sstats.hypotheses += (double)considered;
+    M->sstats.rescored += nimg * topk;
+    return BSG_OK;
 }

@@ -159,6 +159,23 @@ class Matcher:
         _lib.check(_lib.load().bsg_match_search(self._h, _dp(o), len(o), topk, _dp(out), 0), "bsg_match_search")
         return out
 
+    def search_local(self, proposals, origins, radius_deg: float = 10.0, origin_radius: float = 1.5,
+                     topk: int = 8) -> np.ndarray:
+        """Like search(), restricted per image to the panel sections within
+        radius_deg of its proposed rotation and the trial origins within
+        origin_radius pixels of its proposed origin; proposals (nimg, 11) as
+        the proposer predicts them (host array or CUDA tensor)."""
+        import math
+        o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 2)
+        if not (hasattr(proposals, "data_ptr") and getattr(proposals, "is_cuda", False)):
+            proposals = np.ascontiguousarray(proposals, dtype=np.float32)
+        p, dev = _ptr(proposals)
+        out = np.empty((self.nimg, topk, _lib.MATCH_RESULT_DOUBLES))
+        _lib.check(_lib.load().bsg_match_search_local(self._h, p, math.radians(radius_deg), _dp(o), len(o),
+                                                      float(origin_radius), topk, _dp(out),
+                                                      _lib.BSG_DEVICE_PTR if dev else 0), "bsg_match_search_local")
+        return out
+
     def stats(self) -> dict:
         st = _lib.MatchStats()
         _lib.check(_lib.load().bsg_match_get_stats(self._h, C.byref(st)), "bsg_match_get_stats")

@@ -265,6 +265,15 @@ int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, d
 #define BSG_MATCH_TOPK_MAX 8
 int  bsg_match_set_panel(bsg_match* m, const double* mats, long nsec, int flags);
 int  bsg_match_search(bsg_match* m, const double* origins, int norigin, int topk, double* out, int flags);
+/* The same scoring restricted to the neighbourhood of a proposal per held
+ * image (proposals: nimg x BSG_CNN_RESULT_FLOATS floats, host or with
+ * BSG_DEVICE_PTR device: rotation row-major and shift from the box centre):
+ * panel sections within `radius` (radians) of the proposed rotation and the
+ * (at most 9) trial origins within origin_radius pixels of the proposed
+ * origin, nearest first (the nearest is always kept).  At most 1,024
+ * sections per image are considered.  Same output as bsg_match_search. */
+int  bsg_match_search_local(bsg_match* m, const float* proposals, double radius, const double* origins, int norigin,
+                            double origin_radius, int topk, double* out, int flags);
 
 /* Device times of the search stages (CUDA events on the context's stream). */
 typedef struct {
@@ -273,6 +282,7 @@ typedef struct {
     double gemm_ms;        /* tensor-core correlation with top-8 selection */
     double merge_ms;       /* per-image candidate merge                    */
     double rescore_ms;     /* exact figure of merit of the candidates      */
+    double local_ms;       /* local search: selection and scoring          */
     double gemm_flops;     /* algorithmic: 2 x rows x sections x K         */
     double hypotheses;     /* image x origin x section triples scored      */
     long   launches;       /* kernels launched by the search calls         */

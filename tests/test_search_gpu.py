@@ -157,3 +157,38 @@ def test_stats(setup):
     st = m.stats()
     assert st["gemm_flops"] > 0 and st["gemm_ms"] > 0 and st["gemm_launches"] >= 2
     assert st["kpad"] % 64 == 0 and st["coarse_k"] <= st["kpad"]
+
+
+def _perturb(R, deg, rng):
+    ax = rng.normal(size=3)
+    ax /= np.linalg.norm(ax)
+    a = math.radians(deg)
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    return (np.eye(3) + math.sin(a) * K + (1 - math.cos(a)) * K @ K) @ R
+
+
+def test_local_search_around_proposals(setup):
+    """Proposals a few degrees and ~0.5 pixel off the truth: the local
+    search finds the generating view, and its correlation scores equal the
+    exhaustive search's for the same (section, origin) pairs."""
+    m, d, mats, origins, ctf, res, ref = setup
+    rng = np.random.default_rng(11)
+    nimg = len(d["images"])
+    prop = np.zeros((nimg, 11), np.float32)
+    for i in range(nimg):
+        prop[i, :9] = _perturb(d["mats"][i], 4.0, rng).reshape(9)
+        prop[i, 9:] = d["true_origins"][i][:2] - d["n"] // 2 + rng.uniform(-0.5, 0.5, 2)
+    loc = m.search_local(prop, origins, radius_deg=10.0, origin_radius=1.5, topk=8)
+    scale = np.abs(ref).max()
+    for i in range(nimg):
+        for sec, org, score, fom, cv in loc[i]:
+            if sec < 0:
+                continue
+            assert abs(score - ref[i, int(org), int(sec)]) < 1e-2 * scale
+        if int(ctf[i, 6]) & 1:
+            assert int(loc[i, 0, 0]) == i
+    # exact rescoring as in the exhaustive search
+    hyps = [[i, *mats[int(s)].reshape(9), *origins[int(o)]] for i in range(nimg) for s, o, *_ in loc[i] if s >= 0]
+    fom, _ = m.score(np.array(hyps))
+    got = np.array([f for i in range(nimg) for s, o, sc, f, cv in loc[i] if s >= 0])
+    assert np.max(np.abs(fom - got)) < 1e-12
