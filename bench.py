@@ -263,6 +263,90 @@ def search_reference_sample(sw, n_views: int = 160):
                             f"img_recip_space_fom each), one thread, wall {dt:.1f} s including map preparation")
 
 
+def train_proposer(sw, local, torch, n_train: int, epochs: float):
+    """The learned proposer for the search map: n_train projections through
+    the library's own projector (random views, shifts U[-2, 2] pixels, CTF
+    with defocus U[1, 3] um, noise at SNR 0.1), then Adam on the GPU."""
+    from bsoft_b200.cnn import Proposer, pose_targets, add_noise
+    from bsoft_b200.ctf import CTFParams
+    from bsoft_b200.geometry import random_views, views_to_matrices
+    from bsoft_b200.match import Matcher, ctf_record
+    rng = np.random.default_rng(11)
+    mats = views_to_matrices(random_views(rng, n_train))
+    shifts = rng.uniform(-2, 2, size=(n_train, 2))
+    defocus = rng.uniform(1e4, 3e4, size=n_train)
+    ctf = np.stack([ctf_record(200000.0, CTFParams.from_amp_contrast(200000.0, 2.7e7, 0.07, d).coefficients())
+                    for d in defocus])
+    t0 = time.perf_counter()
+    proj = Matcher(n=SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL, pixel=SEARCH_PIXEL,
+                   hi_res=2 * SEARCH_PIXEL, device=local)
+    proj.set_reference(sw["volume"], (SEARCH_BOX // 2,) * 3)
+    imgs = torch.empty((n_train, SEARCH_BOX, SEARCH_BOX), dtype=torch.float32, device="cuda")
+    proj.project(mats, origins=SEARCH_BOX // 2 + shifts, ctf=ctf, out=imgs)
+    add_noise(imgs, 0.1, seed=5)
+    proj.close()
+    torch.cuda.synchronize()
+    data_s = time.perf_counter() - t0
+    tg = torch.from_numpy(pose_targets(mats, shifts)).cuda()
+    net = Proposer(box=SEARCH_BOX, batch=256, seed=1, device=local)
+    steps = int(epochs * n_train / 256)
+    t0 = time.perf_counter()
+    losses = net.train(imgs, tg, steps=steps, lr=1e-3)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del imgs, tg
+    torch.cuda.empty_cache()
+    return net, {"train_images": n_train, "epochs": epochs, "steps": steps, "params": net.nparams,
+                 "data_s": round(data_s, 2), "train_s": round(train_s, 2),
+                 "loss_first": round(float(losses[:100].mean()), 4), "loss_last": round(float(losses[-100:].mean()), 4)}
+
+
+def fsc_of_poses(sw, sel, mats_by_method, origins_by_method, local):
+    """Reconstructions (trilinear, CTF flip, pad 2) of the images `sel` with
+    each method's poses, and their Fourier shell correlation with the map
+    reconstructed from the true poses: mean over shells up to 0.8 Nyquist and
+    the first shell below 0.5."""
+    from bsoft_b200.plan import (P_CTF, P_MAP, P_MAT, P_ORIGIN, P_PIXEL, P_SCALE, P_WEIGHT, PARTICLE_DOUBLES,
+                                 ReconPlan, check_resolution)
+    from bsoft_b200.recon import Reconstructor
+    n = len(sel)
+    imgs = np.ascontiguousarray(sw["images"][sel])
+    meta = sw["meta"]
+
+    def recon(mats, origins):
+        P = np.zeros((n, PARTICLE_DOUBLES))
+        P[:, P_ORIGIN:P_ORIGIN + 2] = origins
+        P[:, P_MAT:P_MAT + 9] = mats.reshape(n, 9)
+        P[:, P_PIXEL] = SEARCH_PIXEL
+        P[:, P_SCALE] = 1.0
+        P[:, P_WEIGHT] = 1.0
+        P[:, P_CTF:P_CTF + 7] = meta["coefs"][sel][:, :7]
+        P[:, P_MAP] = np.arange(n) % 2
+        plan = ReconPlan(n=SEARCH_BOX, ft=2 * SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL,
+                         hi_res=check_resolution(SEARCH_PIXEL, SEARCH_BOX, SEARCH_PIXEL), interp=2, ctf_action=1,
+                         wiener=0.0, params=P, nmaps=1)
+        with Reconstructor(plan, device=local) as rec:
+            rec.insert(imgs, P)
+            return rec.finish()
+
+    ref = np.fft.fftn(recon(meta["mats"][sel], meta["origins"][sel][:, :2]))
+    N = SEARCH_BOX
+    f = np.fft.fftfreq(N) * N
+    r = np.sqrt(f[:, None, None] ** 2 + f[None, :, None] ** 2 + f[None, None, :] ** 2).astype(int)
+    nsh = int(0.8 * N / 2)
+    out = {}
+    for name in mats_by_method:
+        F = np.fft.fftn(recon(mats_by_method[name], origins_by_method[name]))
+        num = np.bincount(r.ravel(), (F * np.conj(ref)).real.ravel(), minlength=N)[:nsh]
+        d1 = np.bincount(r.ravel(), (np.abs(F) ** 2).ravel(), minlength=N)[:nsh]
+        d2 = np.bincount(r.ravel(), (np.abs(ref) ** 2).ravel(), minlength=N)[:nsh]
+        fsc = num / np.sqrt(np.maximum(d1 * d2, 1e-300))
+        below = np.nonzero(fsc[1:] < 0.5)[0]
+        out[name] = {"fsc_mean_to_0.8_nyquist": round(float(fsc[1:].mean()), 4),
+                     "first_shell_below_0.5": int(below[0] + 1) if len(below) else None}
+    return out
+
+
 def search_leg(args, local, dist, world, rank, torch):
     """Exhaustive orientation search; returns the "search" object (rank 0)."""
     from bsoft_b200.match import Matcher, ctf_record
@@ -327,6 +411,37 @@ def search_leg(args, local, dist, world, rank, torch):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
+
+    # ---- learned proposal + local search on the same images
+    learned = None
+    if "learned" in args.legs:
+        net, train_info = train_proposer(sw, local, torch, args.train_images, args.train_epochs)
+        pred = torch.empty((B, 11), dtype=torch.float32, device="cuda")
+        for i in range(nwarm):
+            j = i % 2
+            net.predict(dev[j], out=pred)
+            m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+            m.search_local(pred, origins, args.local_radius, 1.5, 8)
+        m.reset_stats()
+        lres = []
+        barrier()
+        ev0.record(s)
+        for i in range(nsteps):
+            j = (nwarm + i) % 2
+            net.predict(dev[j], out=pred)
+            m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+            lres.append((j, m.search_local(pred, origins, args.local_radius, 1.5, 8), pred.cpu().numpy()))
+        ev1.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        lms = ev0.elapsed_time(ev1)
+        lst = m.stats()
+        if dist is not None:
+            t = torch.tensor([lms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            lms = float(t.item())
+        learned = {"ms": lms, "stats": lst, "results": lres, "train": train_info}
+        net.close()
     m.close()
     if rank != 0:
         return None
@@ -349,6 +464,40 @@ def search_leg(args, local, dist, world, rank, torch):
                    "extrapolation": f"{hyp_per_image} hypotheses per particle x measured seconds per hypothesis"}
         else:
             cpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference", "sample": sample}
+    learned_obj = None
+    if learned is not None:
+        lvalue = images / (learned["ms"] / 1e3)
+        lerr, perr = [], []
+        for j, res, pr in learned["results"]:
+            lerr.append(angular_distance_deg(mats[res[:, 0, 0].astype(int)], meta["mats"][j * B:(j + 1) * B]))
+            perr.append(angular_distance_deg(pr[:, :9].reshape(-1, 3, 3).astype(np.float64),
+                                             meta["mats"][j * B:(j + 1) * B]))
+        lerr = np.concatenate(lerr)
+        perr = np.concatenate(perr)
+        # reconstructions from each method's poses on the last step's images
+        j, res_l, _ = learned["results"][-1]
+        _, res_e = results[-1]
+        sel = np.arange(j * B, (j + 1) * B)
+        fsc = fsc_of_poses(sw, sel, {"exhaustive": mats[res_e[:, 0, 0].astype(int)],
+                                     "learned": mats[res_l[:, 0, 0].astype(int)]},
+                           {"exhaustive": origins[res_e[:, 0, 1].astype(int)],
+                            "learned": origins[res_l[:, 0, 1].astype(int)]}, local)
+        lst = learned["stats"]
+        learned_obj = {
+            "metric": "particles/s (learned proposal + local search)", "value": round(lvalue, 1),
+            "unit": "particles/s", "speedup_vs_exhaustive": round(lvalue / value, 2),
+            "ms_per_step": round(learned["ms"] / nsteps, 2),
+            "config": {"radius_deg": args.local_radius, "origin_radius_px": 1.5, "topk_rescored": 8,
+                       "network": "6 conv 3x3 stride 2 (32-64-64-128-128-128), fc 1024, 6-D rotation + shift"},
+            "hypotheses_per_image": round(lst["hypotheses"] / max(1, lst["images"]), 1),
+            "stages_ms": {k: round(lst[k], 2) for k in ("local_ms", "rescore_ms")},
+            "accuracy": {"median_angular_error_deg": round(float(np.median(lerr)), 3),
+                         "frac_within_5_deg": round(float(np.mean(lerr < 5)), 4),
+                         "proposal_median_error_deg": round(float(np.median(perr)), 3),
+                         "proposal_frac_within_radius": round(float(np.mean(perr < args.local_radius)), 4)},
+            "fsc_vs_true_pose_map": fsc, "training": learned["train"],
+            "gpu_launches": int(lst["launches"]),
+        }
     return {
         "metric": "particles/s (exhaustive orientation search)", "value": round(value, 1), "unit": "particles/s",
         "steps": nsteps, "warmup": nwarm, "ms_per_step": round(ms / nsteps, 2), "dtype": "bf16 (correlation), f32",
@@ -368,6 +517,7 @@ def search_leg(args, local, dist, world, rank, torch):
         "accuracy": {"median_angular_error_deg": round(float(np.median(errs)), 3),
                      "frac_within_5_deg": round(float(np.mean(errs < 5)), 4)},
         "cpu_baseline": cpu, "gpu_launches": int(st["launches"]), "clocks": clk.summary(),
+        "learned": learned_obj,
     }
 
 
@@ -382,7 +532,10 @@ def main():
     ap.add_argument("--search-batch", type=int, default=2048)
     ap.add_argument("--search-steps", type=int, default=3)
     ap.add_argument("--search-warmup", type=int, default=3)
-    ap.add_argument("--legs", default="insert,search")
+    ap.add_argument("--legs", default="insert,search,learned")
+    ap.add_argument("--train-images", type=int, default=200000)
+    ap.add_argument("--train-epochs", type=float, default=8.0)
+    ap.add_argument("--local-radius", type=float, default=10.0)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -531,7 +684,8 @@ def main():
     }
     if search is not None:
         line["search"] = search
-        line["gpu_launches"] = int(launches) + search["gpu_launches"]
+        line["gpu_launches"] = int(launches) + search["gpu_launches"] + (
+            search["learned"]["gpu_launches"] if search.get("learned") else 0)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
