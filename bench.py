@@ -226,10 +226,10 @@ def search_workload(n_images, seed=21):
     return dict(spec=spec, volume=phantom_volume(ph).astype(np.float32), images=imgs, meta=meta)
 
 
-def search_views_mats():
+def search_views_mats(npsi: int = SEARCH_PSI):
     from bsoft_b200.geometry import asymmetric_unit_views_c, search_views, views_to_matrices
     dirs = asymmetric_unit_views_c(1, math.radians(3.0), math.radians(3.0))
-    return len(dirs), views_to_matrices(search_views(dirs, SEARCH_PSI))
+    return len(dirs), views_to_matrices(search_views(dirs, npsi))
 
 
 def search_reference_sample(sw, n_views: int = 160):
@@ -358,7 +358,7 @@ def search_leg(args, local, dist, world, rank, torch):
     imgs = sw["images"]
     meta = sw["meta"]
     ctf = np.stack([ctf_record(sw["spec"].volt, c) for c in meta["coefs"]])
-    ndir, mats = search_views_mats()
+    ndir, mats = search_views_mats(args.search_psi)
     origins = np.array(SEARCH_ORIGINS, float)
     m = Matcher(n=SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL, pixel=SEARCH_PIXEL, hi_res=SEARCH_RES,
                 device=local)
@@ -503,7 +503,7 @@ def search_leg(args, local, dist, world, rank, torch):
         "steps": nsteps, "warmup": nwarm, "ms_per_step": round(ms / nsteps, 2), "dtype": "bf16 (correlation), f32",
         "config": {"workload": "projection-matching-128", "images_per_step": B, "box": SEARCH_BOX,
                    "map": SEARCH_BOX, "pixel": SEARCH_PIXEL, "hi_res": SEARCH_RES, "directions": ndir,
-                   "in_plane": SEARCH_PSI, "sections": len(mats), "origins": len(origins),
+                   "in_plane": args.search_psi, "sections": len(mats), "origins": len(origins),
                    "hypotheses_per_image": hyp_per_image, "topk_rescored": 8, "snr": 0.1,
                    "l2": "inputs larger than L2 (the 9.4 GB panel is streamed every step)"},
         "e2e": {"value": round(images / e2e_s, 1), "unit": "particles/s", "h2d_bytes_per_step": B * SEARCH_BOX ** 2 * 4,
@@ -532,6 +532,7 @@ def main():
     ap.add_argument("--search-batch", type=int, default=2048)
     ap.add_argument("--search-steps", type=int, default=3)
     ap.add_argument("--search-warmup", type=int, default=3)
+    ap.add_argument("--search-psi", type=int, default=SEARCH_PSI)
     ap.add_argument("--legs", default="insert,search,learned")
     ap.add_argument("--train-images", type=int, default=200000)
     ap.add_argument("--train-epochs", type=float, default=8.0)
@@ -555,93 +556,97 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from bsoft_b200.recon import Reconstructor
+    def insertion_leg():
+        from bsoft_b200.recon import Reconstructor
 
-    B = args.batch
-    per_rank = B * (args.warmup + args.steps)
-    w = make_workload(max(per_rank, 2 * B))
-    plan = plan_for(w)
-    P = w["params"]
-    pool = w["pool"]
-    npool = pool.shape[0]
+        B = args.batch
+        per_rank = B * (args.warmup + args.steps)
+        w = make_workload(max(per_rank, 2 * B))
+        plan = plan_for(w)
+        P = w["params"]
+        pool = w["pool"]
+        npool = pool.shape[0]
 
-    # two distinct step buffers (each > L2), alternating between steps
-    def step_images(i):
-        idx = (np.arange(B) + i * B) % npool
-        return np.ascontiguousarray(pool[idx])
+        # two distinct step buffers (each > L2), alternating between steps
+        def step_images(i):
+            idx = (np.arange(B) + i * B) % npool
+            return np.ascontiguousarray(pool[idx])
 
-    host = [torch.from_numpy(step_images(i)).pin_memory() for i in range(2)]
-    dev = [h.cuda() for h in host]
-    stream_of = lambda rec: torch.cuda.ExternalStream(rec.stream)
+        host = [torch.from_numpy(step_images(i)).pin_memory() for i in range(2)]
+        dev = [h.cuda() for h in host]
+        stream_of = lambda rec: torch.cuda.ExternalStream(rec.stream)
 
-    def barrier():
-        torch.cuda.synchronize()
+        def barrier():
+            torch.cuda.synchronize()
+            if dist is not None:
+                dist.barrier()
+
+        # ---- tile shape from the project's autotuner (untimed, on warm-up data)
+        rec = Reconstructor(plan, batch=B, device=local)
+        shape, shape_ms = rec.autotune(dev[0][: min(B, 512)], P[: min(B, 512)])
+        rec.close()
+
+        # ---- value: device-resident inputs
+        rec = Reconstructor(plan, batch=B, device=local)
+        rec.set_tile_shape(shape)
+        s = stream_of(rec)
+        for i in range(args.warmup):
+            rec.insert(dev[i % 2], P[i * B:(i + 1) * B])
+        rec.synchronize()
+        rec.set_timing(True)
+        st0 = rec.stats()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        with ClockSampler(local) as clk:
+            ev0.record(s)
+            for i in range(args.steps):
+                j = args.warmup + i
+                rec.insert(dev[j % 2], P[j * B:(j + 1) * B])
+            ev1.record(s)
+            torch.cuda.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        st1 = rec.stats()
         if dist is not None:
-            dist.barrier()
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        particles = B * args.steps * world
+        value = particles / (ms / 1e3)
+        launches = st1["launches"] - st0["launches"]
+        ins_launch = st1["insert_launches"] - st0["insert_launches"]
+        ins_ms = st1["insert_ms"] - st0["insert_ms"]
+        fft_ms = st1["fft2d_ms"] - st0["fft2d_ms"]
+        rec.close()
 
-    # ---- tile shape from the project's autotuner (untimed, on warm-up data)
-    rec = Reconstructor(plan, batch=B, device=local)
-    shape, shape_ms = rec.autotune(dev[0][: min(B, 512)], P[: min(B, 512)])
-    rec.close()
-
-    # ---- value: device-resident inputs
-    rec = Reconstructor(plan, batch=B, device=local)
-    rec.set_tile_shape(shape)
-    s = stream_of(rec)
-    for i in range(args.warmup):
-        rec.insert(dev[i % 2], P[i * B:(i + 1) * B])
-    rec.synchronize()
-    rec.set_timing(True)
-    st0 = rec.stats()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    with ClockSampler(local) as clk:
-        ev0.record(s)
+        # ---- e2e: pinned host images through the C ABI, map read back at the end
+        rec = Reconstructor(plan, batch=B, device=local)
+        rec.set_tile_shape(shape)
+        for i in range(args.warmup):
+            rec.insert(host[i % 2].numpy(), P[i * B:(i + 1) * B])
+        rec.synchronize()
+        rec.reset()
+        out = np.empty((BOX, BOX, BOX), dtype=np.float32)
+        barrier()
+        t0 = time.perf_counter()
         for i in range(args.steps):
             j = args.warmup + i
-            rec.insert(dev[j % 2], P[j * B:(j + 1) * B])
-        ev1.record(s)
-        torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    st1 = rec.stats()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    particles = B * args.steps * world
-    value = particles / (ms / 1e3)
-    launches = st1["launches"] - st0["launches"]
-    ins_launch = st1["insert_launches"] - st0["insert_launches"]
-    ins_ms = st1["insert_ms"] - st0["insert_ms"]
-    fft_ms = st1["fft2d_ms"] - st0["fft2d_ms"]
-    rec.close()
+            rec.insert(host[j % 2].numpy(), P[j * B:(j + 1) * B])
+        if dist is not None:
+            rec.synchronize()
+        rec.finish(0, out=out)
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = particles / e2e_s
+        rec.close()
+        return dict(value=value, ms=ms, e2e=e2e, launches=launches, ins_launch=ins_launch, ins_ms=ins_ms,
+                    fft_ms=fft_ms, shape=shape, shape_ms=shape_ms, clk=clk, w=w, B=B, particles=particles)
 
-    # ---- e2e: pinned host images through the C ABI, map read back at the end
-    rec = Reconstructor(plan, batch=B, device=local)
-    rec.set_tile_shape(shape)
-    for i in range(args.warmup):
-        rec.insert(host[i % 2].numpy(), P[i * B:(i + 1) * B])
-    rec.synchronize()
-    rec.reset()
-    out = np.empty((BOX, BOX, BOX), dtype=np.float32)
-    barrier()
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        j = args.warmup + i
-        rec.insert(host[j % 2].numpy(), P[j * B:(j + 1) * B])
-    if dist is not None:
-        rec.synchronize()
-    rec.finish(0, out=out)
-    barrier()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = particles / e2e_s
-    rec.close()
-
+    ins = insertion_leg() if "insert" in args.legs else None
     search = search_leg(args, local, dist, world, rank, torch) if "search" in args.legs else None
 
     if rank != 0:
@@ -649,43 +654,54 @@ def main():
             dist.destroy_process_group()
         return
 
-    # roofline of the gridding kernel
-    peak, peak_kind = peaks()
-    per_particle = 22.0 * BOX * BOX
-    avg_launch_ms = ins_ms / max(1, ins_launch)
-    achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
-    roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-            "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-            "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
-            "algorithmic_bytes_per_particle": per_particle,
-            "fft2d_ms_per_step": round(fft_ms / args.steps, 3), "tile_shape": int(shape),
-            "autotune_ms_per_shape": [round(float(x), 2) for x in shape_ms]}
+    if ins is not None:
+        value, ms, e2e, launches = ins["value"], ins["ms"], ins["e2e"], ins["launches"]
+        ins_launch, ins_ms, fft_ms = ins["ins_launch"], ins["ins_ms"], ins["fft_ms"]
+        shape, shape_ms, clk, w, B, particles = ins["shape"], ins["shape_ms"], ins["clk"], ins["w"], ins["B"], ins["particles"]
+        # roofline of the gridding kernel
+        peak, peak_kind = peaks()
+        per_particle = 22.0 * BOX * BOX
+        avg_launch_ms = ins_ms / max(1, ins_launch)
+        achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
+        roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
+                "algorithmic_bytes_per_particle": per_particle,
+                "fft2d_ms_per_step": round(fft_ms / args.steps, 3), "tile_shape": int(shape),
+                "autotune_ms_per_shape": [round(float(x), 2) for x in shape_ms]}
 
-    cpu = None
-    if world == 1 and not args.no_cpu_baseline:
-        threads = cpu_threads_for_reference()
-        v, sample = reference_sample(w, max(2 * threads, threads * 8), threads)
-        if v is not None:
-            cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
-        else:
-            cpu = {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = cpu_threads_for_reference()
+            v, sample = reference_sample(w, max(2 * threads, threads * 8), threads)
+            if v is not None:
+                cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
+            else:
+                cpu = {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
 
-    line = {
-        "metric": "particles/s (insertion)", "value": round(value, 1), "unit": "particles/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": N_PARTICLES, "particles_timed": particles,
-                   "batch_per_step": B, "box": BOX, "map": BOX, "ft": 2 * BOX, "interp": "trilinear",
-                   "ctf": "flip", "l2": "inputs larger than L2 (524 MB per step)", "parallelism": f"dp{world}"},
-        "e2e": {"value": round(e2e, 1), "unit": "particles/s", "h2d_bytes_per_step": B * BOX * BOX * 4,
-                "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps},
-        "roofline": roof, "cpu_baseline": cpu, "gpu_launches": int(launches),
-        "clocks": clk.summary(),
-    }
-    if search is not None:
-        line["search"] = search
-        line["gpu_launches"] = int(launches) + search["gpu_launches"] + (
-            search["learned"]["gpu_launches"] if search.get("learned") else 0)
+        line = {
+            "metric": "particles/s (insertion)", "value": round(value, 1), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": N_PARTICLES, "particles_timed": particles,
+                       "batch_per_step": B, "box": BOX, "map": BOX, "ft": 2 * BOX, "interp": "trilinear",
+                       "ctf": "flip", "l2": "inputs larger than L2 (524 MB per step)", "parallelism": f"dp{world}"},
+            "e2e": {"value": round(e2e, 1), "unit": "particles/s", "h2d_bytes_per_step": B * BOX * BOX * 4,
+                    "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps},
+            "roofline": roof, "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        if search is not None:
+            line["search"] = search
+            line["gpu_launches"] = int(launches) + search["gpu_launches"] + (
+                search["learned"]["gpu_launches"] if search.get("learned") else 0)
+    else:
+        line = {"metric": search["metric"], "value": search["value"], "unit": "particles/s", "n_gpus": world,
+                "steps": search["steps"], "warmup": search["warmup"], "ms_per_step": search["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": search["dtype"],
+                "data": "synthetic", "config": search["config"], "e2e": search["e2e"], "roofline": search["roofline"],
+                "cpu_baseline": search["cpu_baseline"], "gpu_launches": search["gpu_launches"],
+                "clocks": search["clocks"], "search": search}
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
