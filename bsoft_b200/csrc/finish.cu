@@ -234,33 +234,54 @@ cudaError_t launch_weigh_into(const Context& c, int imap, float2* out, cudaStrea
     return cudaGetLastError();
 }
 
-// FSC partial sums: one CTA per z-plane; thread r accumulates shell r of
-// that plane in a fixed order (rows, then columns), then fsc_reduce sums the
-// planes in order - deterministic, FP64 throughout.
-__global__ void fsc_plane_kernel(const float2* v1, const float2* v2, int N, int nshell, double* part) {
+// FSC partial sums as Bimage::fsc(Bimage*) forms them
+// (bsoft/src/img/Bimage_resolution.cpp:330-406 with fspace_radial_power,
+// Bimage_fspace.cpp:848-958): radius = real * |index / real| (wrapped at
+// (N-1)/2), a voxel adds (1 - f) to shell floor(radius) and f to the next,
+// only voxels with floor(radius) < maxrad count.  One CTA per z-plane;
+// thread r accumulates shell r of that plane in a fixed order (rows, then
+// |h|, then sign), fsc_reduce sums the planes in order - deterministic,
+// FP64 throughout.
+__device__ __forceinline__ double fsc_radius(int h, int k, int l, double real) {
+    const double fs = 1.0 / real;
+    double rx = h * fs, ry = k * fs, rz = l * fs;
+    rx *= rx; ry *= ry; rz *= rz;
+    return real * sqrt(rx + ry + rz);
+}
+
+__global__ void fsc_plane_kernel(const float2* v1, const float2* v2, int N, int nshell, int maxrad, double real,
+                                 double* part) {
     const int z = blockIdx.x;
     const int l = sfreq(z, N);
     for (int r = threadIdx.x; r < nshell; r += blockDim.x) {
         double num = 0, d1 = 0, d2 = 0;
-        const double rlo = r - 0.5, rhi = r + 0.5;
-        for (int y = 0; y < N; ++y) {
-            const int k = sfreq(y, N);
-            const double kl = (double)k * k + (double)l * l;
-            if (kl >= rhi * rhi) continue;
-            // |h| range that can land in shell r = round(sqrt(h^2 + kl))
-            const int hlo = rlo * rlo > kl ? (int)floor(sqrt(rlo * rlo - kl)) : 0;
-            const int hhi = min(N / 2, (int)ceil(sqrt(rhi * rhi - kl)));
-            for (int hh = hlo; hh <= hhi; ++hh) {
-                const double r2 = (double)hh * hh + kl;
-                if ((int)floor(sqrt(r2) + 0.5) != r) continue;
-                for (int sgn = 0; sgn < 2; ++sgn) {
-                    if (sgn && (hh == 0 || hh == N / 2)) continue;
-                    const int x = sgn ? (N - hh) % N : hh;
-                    const size_t i = ((size_t)z * N + y) * N + x;
-                    const float2 a = v1[i], b = v2[i];
-                    num += (double)a.x * b.x + (double)a.y * b.y;
-                    d1 += (double)a.x * a.x + (double)a.y * a.y;
-                    d2 += (double)b.x * b.x + (double)b.y * b.y;
+        if (r < maxrad) {
+            // voxels with floor(radius) in {r - 1, r}: radius in [r - 1, r + 1)
+            const double rlo = r - 1.5, rhi = r + 1.5;      // index-space bounds with margin
+            for (int y = 0; y < N; ++y) {
+                const int k = sfreq(y, N);
+                const double kl = (double)k * k + (double)l * l;
+                if (kl >= rhi * rhi) continue;
+                const int hlo = (rlo > 0 && rlo * rlo > kl) ? (int)floor(sqrt(rlo * rlo - kl)) : 0;
+                const int hhi = min(N / 2, (int)ceil(sqrt(rhi * rhi - kl)));
+                for (int hh = hlo; hh <= hhi; ++hh) {
+                    for (int sgn = 0; sgn < 2; ++sgn) {
+                        if (sgn && (hh == 0 || hh == N / 2)) continue;
+                        const int x = sgn ? (N - hh) % N : hh;
+                        const int h = sfreq(x, N);
+                        const double rad = fsc_radius(h, k, l, real);
+                        const int ir = (int)rad;
+                        if (ir >= maxrad) continue;
+                        double w;
+                        if (ir == r) w = 1.0 - (rad - ir);
+                        else if (ir + 1 == r) w = rad - ir;
+                        else continue;
+                        const size_t i = ((size_t)z * N + y) * N + x;
+                        const float2 a = v1[i], b = v2[i];
+                        num += w * ((double)a.x * b.x + (double)a.y * b.y);
+                        d1 += w * ((double)a.x * a.x + (double)a.y * a.y);
+                        d2 += w * ((double)b.x * b.x + (double)b.y * b.y);
+                    }
                 }
             }
         }
@@ -269,7 +290,9 @@ __global__ void fsc_plane_kernel(const float2* v1, const float2* v2, int N, int 
     }
 }
 
-__global__ void fsc_reduce_kernel(const double* part, int N, int nshell, double* fsc) {
+// FSC[0] = 1 (the reference sets it), FSC[r] = num / sqrt(d1 d2), 0 where
+// not finite or beyond maxrad
+__global__ void fsc_reduce_kernel(const double* part, int N, int nshell, int maxrad, double* fsc) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nshell) return;
     double num = 0, d1 = 0, d2 = 0;
@@ -277,7 +300,13 @@ __global__ void fsc_reduce_kernel(const double* part, int N, int nshell, double*
         const double* o = part + ((size_t)z * nshell + r) * 3;
         num += o[0]; d1 += o[1]; d2 += o[2];
     }
-    fsc[r] = (d1 > 0 && d2 > 0) ? num / sqrt(d1 * d2) : 0.0;
+    double v = 0;
+    if (r == 0) v = 1;
+    else if (r < maxrad) {
+        v = num / sqrt(d1 * d2);
+        if (!isfinite(v)) v = 0;
+    }
+    fsc[r] = v;
 }
 
 cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream_t s) {
@@ -285,10 +314,14 @@ cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream
     if (e != cudaSuccess) return e;
     e = launch_weigh_into(c, 2, c.d_half_weighed[1], s);
     if (e != cudaSuccess) return e;
-    fsc_plane_kernel<<<c.g.map, 128, 0, s>>>(c.d_half_weighed[0], c.d_half_weighed[1], c.g.map, nshell, c.d_fsc);
+    // fspace_maximum_radius (Bimage_fspace.cpp:26-38), sampling ratio 1
+    const double real = c.g.map * c.cfg.map_sampling;
+    const int maxrad = c.cfg.hi_res > 0.1 ? (int)(long)(real / c.cfg.hi_res) : c.g.map / 2;
+    fsc_plane_kernel<<<c.g.map, 128, 0, s>>>(c.d_half_weighed[0], c.d_half_weighed[1], c.g.map, nshell, maxrad, real,
+                                             c.d_fsc);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    fsc_reduce_kernel<<<(nshell + 127) / 128, 128, 0, s>>>(c.d_fsc, c.g.map, nshell, out_dev);
+    fsc_reduce_kernel<<<(nshell + 127) / 128, 128, 0, s>>>(c.d_fsc, c.g.map, nshell, maxrad, out_dev);
     return cudaGetLastError();
 }
 

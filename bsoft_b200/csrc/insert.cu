@@ -9,7 +9,7 @@
 //
 // Decomposition: one warp owns one tile of the map (8 x 8 x 8, 16 x 16 x 4,
 // 16 x 8 x 8 or 16 x 16 x 8 voxels; the autotuner picks the shape) and keeps its
-// sums in shared memory in FP64 (each contribution is the float product
+// sums in shared memory in FP32 (each contribution is the float product
 // F * w, as the reference forms it), adding them to the FP64 accumulators in
 // HBM at the end of the batch.  Nothing else writes the tile, so there are
 // no atomics and no block-wide barriers.  The warp tests 32 particles at a
@@ -95,22 +95,28 @@ __device__ __forceinline__ float pixel_weight_gate(const InsertArgs& a, const De
     return d < 1.0 ? (float)sqrt(d > 0 ? d : 0.0) : 1.0f;
 }
 
+// Tile sums are FP32: one batch adds at most a few thousand contributions
+// to a voxel, each the float product F * w the reference forms; the batch's
+// sums are folded into the FP64 map accumulators, which carry the long
+// reduction over all particles.
+typedef float tacc_t;
+
 struct TileAcc {
-    double* re;
-    double* im;
-    double* w;
-    double* p;
-    double* q;
+    tacc_t* re;
+    tacc_t* im;
+    tacc_t* w;
+    tacc_t* p;
+    tacc_t* q;
 };
 
 template <bool FOM>
 __device__ __forceinline__ void add_voxel(const TileAcc& A, int i, float2 f, float w) {
-    A.re[i] += (double)(f.x * w);
-    A.im[i] += (double)(f.y * w);
-    A.w[i] += (double)w;
+    A.re[i] += f.x * w;
+    A.im[i] += f.y * w;
+    A.w[i] += w;
     if (FOM) {
-        A.p[i] += (double)(w * (f.x * f.x + f.y * f.y));
-        A.q[i] += (double)(w * w);
+        A.p[i] += w * (f.x * f.x + f.y * f.y);
+        A.q[i] += w * w;
     }
 }
 
@@ -287,8 +293,8 @@ __device__ __forceinline__ void fold_tile(const InsertArgs& a, const TileAcc& A,
                 if (FOM) { a.pow[idx] += A.p[i]; a.w2[idx] += A.q[i]; }
             }
         }
-        A.re[i] = 0.0; A.im[i] = 0.0; A.w[i] = 0.0;
-        if (FOM) { A.p[i] = 0.0; A.q[i] = 0.0; }
+        A.re[i] = 0; A.im[i] = 0; A.w[i] = 0;
+        if (FOM) { A.p[i] = 0; A.q[i] = 0; }
     }
     __syncwarp();
 }
@@ -297,8 +303,8 @@ template <bool FOM, bool GATE, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     constexpr int NCH = FOM ? 5 : 3;
     constexpr int TV = TX * TY * TZ;
-    extern __shared__ double s_dacc[];                 // WARPS x NCH x TV
-    double* const my_acc = s_dacc + (size_t)(threadIdx.x >> 5) * NCH * TV;
+    extern __shared__ tacc_t s_dacc[];                 // WARPS x NCH x TV
+    tacc_t* const my_acc = s_dacc + (size_t)(threadIdx.x >> 5) * NCH * TV;
     __shared__ int s_rows[WARPS][96];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gw = blockIdx.x * WARPS + warp;
@@ -314,7 +320,7 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     TileAcc A;
     A.re = my_acc; A.im = A.re + TV; A.w = A.im + TV;
     A.p = FOM ? A.w + TV : nullptr; A.q = FOM ? A.p + TV : nullptr;
-    for (int i = lane; i < NCH * TV; i += 32) my_acc[i] = 0.0;
+    for (int i = lane; i < NCH * TV; i += 32) my_acc[i] = 0;
     __syncwarp();
 
     for (int base = p_lo; base < p_hi; base += 32) {
@@ -372,7 +378,7 @@ void insert_shape(int i, int* tx, int* ty, int* tz) { *tx = kShapes[i].tx; *ty =
 
 template <int TX, int TY, int TZ>
 static cudaError_t set_smem_shape() {
-    const int smem = (int)(WARPS * 5 * TX * TY * TZ * sizeof(double));
+    const int smem = (int)(WARPS * 5 * TX * TY * TZ * sizeof(tacc_t));
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(insert_kernel<true, true, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(insert_kernel<true, false, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
@@ -385,9 +391,9 @@ cudaError_t prepare_insert_attributes() {
     if ((e = set_smem_shape<8, 8, 8>()) != cudaSuccess) return e;
     if ((e = set_smem_shape<16, 16, 4>()) != cudaSuccess) return e;
     if ((e = set_smem_shape<16, 8, 8>()) != cudaSuccess) return e;
-    // 16 x 16 x 8 in FP64 needs 5 x 2048 x 8 B per warp with FOM: beyond one
-    // SM's shared memory for 4 warps, so only the non-FOM variants exist
-    const int smem = (int)(WARPS * 3 * 16 * 16 * 8 * sizeof(double));
+    // 16 x 16 x 8 with FOM needs 5 x 2048 x 4 B per warp (160 KB for 4
+    // warps); only the non-FOM variants are used
+    const int smem = (int)(WARPS * 3 * 16 * 16 * 8 * sizeof(tacc_t));
     if ((e = cudaFuncSetAttribute(insert_kernel<false, true, 16, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
     return cudaFuncSetAttribute(insert_kernel<false, false, 16, 16, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -401,7 +407,7 @@ static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStre
     a.ntz = (N + TZ - 1) / TZ;
     const int ntiles = a.ntx * a.nty * a.ntz;
     const unsigned blocks = (unsigned)(((long)ntiles * a.R + WARPS - 1) / WARPS);
-    const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TX * TY * TZ * sizeof(double);
+    const size_t smem = (size_t)WARPS * (c.g.fom ? 5 : 3) * TX * TY * TZ * sizeof(tacc_t);
     if (c.g.fom) {
         if (c.g.gate) insert_kernel<true, true, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);
         else insert_kernel<true, false, TX, TY, TZ><<<blocks, WARPS * 32, smem, s>>>(a);

@@ -109,8 +109,10 @@ int  bsg_recon_finish(bsg_recon* r, int imap, float* map_out, float* fom_out, in
  * accumulators are kept in FP64 on the device). */
 int  bsg_recon_accumulators(bsg_recon* r, int half, double* vol_out, double* weight_out, int flags);
 
-/* Fourier shell correlation of the two weighed half maps (nmaps >= 2):
- * nshell doubles, shell r = round(|frequency|). */
+/* Fourier shell correlation of the two weighed half-map transforms
+ * (nmaps >= 2) as Bimage::fsc(Bimage*) forms it: shells linearly
+ * interpolated, sampling ratio 1, FSC[0] = 1, shells from
+ * map * sampling / hi_res on are 0.  nshell doubles. */
 int  bsg_recon_fsc(bsg_recon* r, int nshell, double* fsc_out);
 
 /* The 2-D stage alone: padded FFT, origin shift and CTF of nparts images;

@@ -50,7 +50,8 @@ def lib():
         L.orc_particle_transform.restype = C.c_int
         L.orc_finish.argtypes = [C.POINTER(ReconCfg), dp, dp, dp, dp, dp, C.c_int]
         L.orc_finish.restype = C.c_long
-        L.orc_fsc.argtypes = [C.c_int, dp, dp, C.c_int, dp]
+        L.orc_fsc.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, C.c_int, dp]
+        L.orc_fsc.restype = C.c_int
         L.orc_fsi_kernel.argtypes = [C.c_int, C.c_int, dp]
         L.orc_fsi_kernel.restype = C.c_int
         L.orc_match_diam.argtypes = [C.c_int, C.c_double, C.c_double]
@@ -220,3 +221,12 @@ def recip_space_fom(img: np.ndarray, ref: np.ndarray, img_real_size: float, ref_
                                   ref_real_size, ref_sampling, hi_res, lo_res, fom_type, _dp(c), int(invert),
                                   _dp(cv))
     return float(f), float(cv[0])
+
+
+def fsc(vol1: np.ndarray, vol2: np.ndarray, real_size: float, hi_res: float, nshell: int) -> np.ndarray:
+    """Bimage::fsc of two complex (N, N, N) transforms."""
+    a = np.ascontiguousarray(vol1, dtype=np.complex128)
+    b = np.ascontiguousarray(vol2, dtype=np.complex128)
+    out = np.zeros(nshell)
+    lib().orc_fsc(a.shape[0], _dp(a.view(np.float64)), _dp(b.view(np.float64)), real_size, hi_res, nshell, _dp(out))
+    return out

@@ -55,8 +55,10 @@ int orc_particle_transform(const orc_recon_cfg* cfg, const float* image,
 long orc_finish(const orc_recon_cfg* cfg, double* vol, double* weight, double* power,
                 double* weight2, double* map_out, int sinc);
 
-/* Half-map FSC over radial shells (Bimage::fsc): nshell values. */
-int orc_fsc(int N, const double* vol1, const double* vol2, int nshell, double* fsc);
+/* FSC of two complex N^3 transforms as Bimage::fsc(Bimage*) forms it
+ * (linearly interpolated shells, sampling ratio 1, shells below
+ * real_size / hi_res): nshell values, FSC[0] = 1.  Returns the shell count. */
+int orc_fsc(int N, const double* vol1, const double* vol2, double real_size, double hi_res, int nshell, double* fsc);
 
 /* ---- projection matching (match_oracle.c) ---- */
 

@@ -254,28 +254,55 @@ long orc_finish(const orc_recon_cfg* cfg, double* vol, double* weight, double* p
     return cov;
 }
 
-int orc_fsc(int N, const double* v1, const double* v2, int nshell, double* fsc)
+int orc_fsc(int N, const double* v1, const double* v2, double real_size, double hi_res, int nshell, double* fsc)
 {
-    double* num = (double*)calloc(nshell, sizeof(double));
-    double* d1 = (double*)calloc(nshell, sizeof(double));
-    double* d2 = (double*)calloc(nshell, sizeof(double));
+    /* Bimage::fsc(Bimage*) (bsoft/src/img/Bimage_resolution.cpp:330-406)
+     * with fspace_radial_power (bsoft/src/img/Bimage_fspace.cpp:848-958) on
+     * two complex N^3 transforms (standard layout), sampling ratio 1:
+     * radius = real_size * |s|, s = index / real_size (wrapped at (N-1)/2);
+     * a voxel adds (1 - f) to shell floor(radius) and f to the next, f the
+     * fraction, shells below maxrad = (long)(real_size / hi_res)
+     * (fspace_maximum_radius, hi_res > 0.1); FSC[0] = 1, FSC[i] =
+     * sum Re(F1 F2*) / sqrt(sum |F1|^2 sum |F2|^2) per shell (the shell
+     * averages' common normalisation cancels), 0 where not finite.
+     * Returns maxrad. */
+    long maxrad = hi_res > 0.1 ? (long)(real_size / hi_res) : (long)(N / 2.0);
+    double* num = (double*)calloc(maxrad + 1, sizeof(double));
+    double* d1 = (double*)calloc(maxrad + 1, sizeof(double));
+    double* d2 = (double*)calloc(maxrad + 1, sizeof(double));
+    const double fs = 1.0 / real_size;
+    const long half = (N - 1) / 2;
     for (long z = 0; z < N; ++z) {
-        long l = sfreq(z, N);
+        double rz = (double)(z > half ? z - N : z) * fs;
+        rz *= rz;
         for (long y = 0; y < N; ++y) {
-            long k = sfreq(y, N);
+            double ry = (double)(y > half ? y - N : y) * fs;
+            ry *= ry;
             for (long x = 0; x < N; ++x) {
-                long h = sfreq(x, N);
-                long r = (long)floor(sqrt((double)(h*h + k*k + l*l)) + 0.5);
-                if (r >= nshell) continue;
-                long j = 2*((z*N + y)*N + x);
-                num[r] += v1[j]*v2[j] + v1[j+1]*v2[j+1];
-                d1[r] += v1[j]*v1[j] + v1[j+1]*v1[j+1];
-                d2[r] += v2[j]*v2[j] + v2[j+1]*v2[j+1];
+                double rx = (double)(x > half ? x - N : x) * fs;
+                rx *= rx;
+                const double radius = real_size * sqrt(rx + ry + rz);
+                const long ir = (long)radius;
+                if (ir >= maxrad) continue;
+                const double f = radius - ir, f1 = 1 - f;
+                const long j = 2 * ((z * N + y) * N + x);
+                const double p = v1[j] * v2[j] + v1[j + 1] * v2[j + 1];
+                const double a = v1[j] * v1[j] + v1[j + 1] * v1[j + 1];
+                const double b = v2[j] * v2[j] + v2[j + 1] * v2[j + 1];
+                num[ir] += f1 * p; d1[ir] += f1 * a; d2[ir] += f1 * b;
+                if (ir + 1 < maxrad) { num[ir + 1] += f * p; d1[ir + 1] += f * a; d2[ir + 1] += f * b; }
             }
         }
     }
-    for (int r = 0; r < nshell; ++r)
-        fsc[r] = (d1[r] > 0 && d2[r] > 0) ? num[r] / sqrt(d1[r]*d2[r]) : 0.0;
+    for (int r = 0; r < nshell; ++r) {
+        double v = 0;
+        if (r == 0) v = 1;
+        else if (r < maxrad) {
+            v = num[r] / sqrt(d1[r] * d2[r]);
+            if (!isfinite(v)) v = 0;
+        }
+        fsc[r] = v;
+    }
     free(num); free(d1); free(d2);
-    return 0;
+    return (int)maxrad;
 }

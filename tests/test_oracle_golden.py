@@ -43,3 +43,17 @@ def test_oracle_particle_stages(probe, tmp_path):
     rv = z["vol"].reshape(-1, 2)
     assert rel_l2(vol.reshape(-1, 2), rv) < 1e-6
     assert rel_l2(w, z["w"]) < 1e-6
+
+
+def test_fsc_matches_reference():
+    """orc_fsc against Bimage::fsc of the compiled reference (its shell sums
+    are float, hence the tolerance)."""
+    z = np.load(os.path.join(GOLDEN, "fsc32.npz"))
+    a = np.fft.fftn(z["map1"].astype(np.float64))
+    b = np.fft.fftn(z["map2"].astype(np.float64))
+    N, u = z["map1"].shape[0], float(z["sampling"])
+    for key, res in (("res5", 5.0), ("res3", 3.0)):
+        ref = z[key]
+        f = oracle.fsc(a, b, N * u, res, len(ref))
+        assert len(ref) == int(N * u / res)
+        assert np.abs(f - ref[:, 1]).max() < 1e-5

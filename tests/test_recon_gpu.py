@@ -130,8 +130,13 @@ def test_gpu_half_maps_fsc(tmp_path):
         rec.insert(images, plan.params)
         full = rec.finish(0)
         f = rec.fsc()
+        halves = [rec.accumulators(h) for h in (0, 1)]
     assert rel_l2(full, oracle.reconstruct(plan, images)) < TOL
-    assert f.shape == (16,) and f[1] > 0.5 and np.all(f <= 1.0 + 1e-9)
+    assert f.shape == (16,) and f[0] == 1.0 and f[1] > 0.5 and np.all(f <= 1.0 + 1e-9)
+    # Bimage::fsc of the two weighed half-map transforms (F / w where w > 1e-30)
+    wv = [np.where(w > 1e-30, v / np.where(w > 1e-30, w, 1.0), 0.0) for v, w in halves]
+    ref = oracle.fsc(wv[0], wv[1], plan.map * plan.map_sampling, plan.hi_res, 16)
+    assert np.abs(f - ref).max() < 1e-6
 
 
 def test_gpu_rejects_bad_sizes(tmp_path):
