@@ -45,7 +45,8 @@ class MatchStats(C.Structure):
                 ("merge_ms", C.c_double), ("rescore_ms", C.c_double), ("local_ms", C.c_double),
                 ("gemm_flops", C.c_double),
                 ("hypotheses", C.c_double), ("launches", C.c_long), ("gemm_launches", C.c_long),
-                ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int)]
+                ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int),
+                ("refine_ms", C.c_double), ("refine_launches", C.c_long)]
 
 
 class CnnConfig(C.Structure):
@@ -60,6 +61,9 @@ MATCH_APPLY_CTF = 1
 MATCH_INVERT = 2
 MATCH_CTF_DOUBLES = 8
 MATCH_HYP_DOUBLES = 12
+MATCH_REFINE_START_DOUBLES = 7
+MATCH_SCORE_FP64 = 4
+MATCH_REFINE_RESULT_DOUBLES = 9
 
 
 class BsgError(RuntimeError):
@@ -109,6 +113,8 @@ def load():
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_match_stream": ([vp], vp),
+        "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, dp, C.c_int],
+                             C.c_int),
         "bsg_cnn_create": ([C.POINTER(CnnConfig), C.POINTER(vp)], C.c_int),
         "bsg_cnn_destroy": ([vp], None),
         "bsg_cnn_num_params": ([vp], C.c_long),

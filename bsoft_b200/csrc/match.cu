@@ -345,7 +345,8 @@ __global__ void __launch_bounds__(256) section_kernel(const float2* __restrict__
 struct FomArgs {
     cudaTextureObject_t tex;
     int D, wd;
-    const float* lut;
+    const float* lut;        // FSI table, FP32 (T = float)
+    const double* lutd;      // the same, FP64 (T = double)
     const MPix* pix;
     int npix;
     const MHypG* hyps;
@@ -360,23 +361,30 @@ struct FomArgs {
     double* cv;
 };
 
+// T = float: the search's rescoring (agrees with the reference's figure of
+// merit to ~1e-7); T = double: gather, products and shell sums in FP64, as
+// the reference accumulates (~1e-8), for refinement whose decisions compare
+// figures of merit against a 1e-6 threshold.
+template <typename T>
 __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
-    extern __shared__ float fsm[];
-    float* lut = fsm;                                                      // (NDIV+1)*wd
-    float* wsum = fsm + (NDIV + 1) * MAXW;                                 // FOM_WARPS x nshell x (1+MAXORG)
+    extern __shared__ __align__(16) unsigned char fom_smem[];
+    T* lut = reinterpret_cast<T*>(fom_smem);                                // (NDIV+1)*wd
+    T* wsum = lut + (NDIV + 1) * MAXW;                                      // FOM_WARPS x nshell x (1+MAXORG)
     constexpr int NV = 1 + MAXORG;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int i = threadIdx.x; i < (NDIV + 1) * a.wd; i += blockDim.x) lut[i] = a.lut[i];
-    for (int i = threadIdx.x; i < FOM_WARPS * a.nshell * NV; i += blockDim.x) wsum[i] = 0.f;
+    const T* glut;
+    if constexpr (sizeof(T) == 8) glut = a.lutd; else glut = a.lut;
+    for (int i = threadIdx.x; i < (NDIV + 1) * a.wd; i += blockDim.x) lut[i] = glut[i];
+    for (int i = threadIdx.x; i < FOM_WARPS * a.nshell * NV; i += blockDim.x) wsum[i] = (T)0;
     __syncthreads();
     const MHypG& H = a.hyps[blockIdx.x];
     const int norg = H.norg;
     const long img = H.img;
     const float2* X = a.spec + img * (long)a.D * a.D;
     const float* C = a.ctf + img * (long)a.npix;
-    float* my = wsum + warp * a.nshell * NV;
+    T* my = wsum + warp * a.nshell * NV;
     for (int base = warp * 32; base < a.npix; base += FOM_WARPS * 32) {
-        float2 R = make_float2(0.f, 0.f);
+        T Rx = 0, Ry = 0;
         const int cnt = min(32, a.npix - base);
         for (int q = 0; q < cnt; ++q) {
             const MPix pq = a.pix[base + q];
@@ -385,30 +393,37 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             const double mx = (H.m[0] * ix + H.m[1] * iy) * a.real;
             const double myy = (H.m[3] * ix + H.m[4] * iy) * a.real;
             const double mz = (H.m[6] * ix + H.m[7] * iy) * a.real;
-            float vr, vi;
-            fsi_gather<float>(TexSrc{a.tex}, a.D, mx, myy, mz, lut, a.wd, lane, vr, vi);
-            if (lane == q) R = make_float2(vr, vi);
+            T vr, vi;
+            fsi_gather<T>(TexSrc{a.tex}, a.D, mx, myy, mz, lut, a.wd, lane, vr, vi);
+            if (lane == q) {
+                Rx = vr;
+                Ry = vi;
+            }
         }
         const int p = base + lane;
-        float v[NV];
+        T v[NV];
 #pragma unroll
-        for (int o = 0; o < NV; ++o) v[o] = 0.f;
+        for (int o = 0; o < NV; ++o) v[o] = 0;
         int shell = -1;
         if (lane < cnt) {
             const MPix pq = a.pix[p];
             shell = pq.shell;
             const float2 x = X[pq.idx];
-            const float c = C[p];
-            const float rr = R.x * c, ri = R.y * c;
+            const T c = C[p];
+            const T rr = Rx * c, ri = Ry * c;
             v[0] = rr * rr + ri * ri;
 #pragma unroll
             for (int o = 0; o < MAXORG; ++o) {
                 if (o < norg) {
                     double phi = pq.h * H.sx[o] + pq.k * H.sy[o];
-                    phi -= 6.283185307179586 * rint(phi * 0.15915494309189535);
-                    float sn, cs;
-                    sincosf((float)phi, &sn, &cs);
-                    const float xr = x.x * cs - x.y * sn, xi = x.x * sn + x.y * cs;
+                    T sn, cs;
+                    if constexpr (sizeof(T) == 8) {
+                        sincos(phi, &sn, &cs);
+                    } else {
+                        phi -= 6.283185307179586 * rint(phi * 0.15915494309189535);
+                        sincosf((float)phi, &sn, &cs);
+                    }
+                    const T xr = (T)x.x * cs - (T)x.y * sn, xi = (T)x.x * sn + (T)x.y * cs;
                     v[1 + o] = xr * rr + xi * ri;
                 }
             }
@@ -422,7 +437,7 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
 #pragma unroll
             for (int o = 0; o < NV; ++o) {
                 if (o > norg) break;
-                float t = in ? v[o] : 0.f;
+                T t = in ? v[o] : (T)0;
 #pragma unroll
                 for (int k = 16; k; k >>= 1) t += __shfl_xor_sync(0xffffffffu, t, k);
                 if (lane == 0) my[s * NV + o] += t;
@@ -433,8 +448,8 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
     __syncthreads();
     // one warp per origin: shells j (lane-strided), folded over warps in
     // order, then summed over j by a fixed shuffle tree
-    if (warp < norg) {
-        const int o = warp;
+    // (MAXORG may exceed the warp count: warps take origins in turn)
+    for (int o = warp; o < norg; o += FOM_WARPS) {
         const double* ds = a.dsum + img * (long)a.nshell;
         double tf = 0, tc = 0;
         for (int j = lane; j < a.nshell; j += 32) {
@@ -509,7 +524,9 @@ void set_attributes() {
     const int big = 100 * 1024;
     cudaError_t e = cudaFuncSetAttribute(strided64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(fom_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        e = cudaFuncSetAttribute(fom_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fom_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     g_attr_err = e;
 }
 
@@ -837,16 +854,21 @@ int match_fail(int code, const char* fmt, ...) {
     return code;
 }
 
-cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s) {
+cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
+                       bool fp64) {
     FomArgs a{};
-    a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf;
+    a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf; a.lutd = M.d_lut;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
     a.spec = M.d_spec; a.ctf = M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
     a.fom = d_fom; a.cv = d_cv;
-    const size_t smem = sizeof(float) * ((NDIV + 1) * MAXW + FOM_WARPS * M.nshell * (1 + MAXORG));
-    if (ng > 0) fom_kernel<<<(unsigned)ng, FOM_WARPS * 32, smem, s>>>(a);
+    const size_t words = (NDIV + 1) * MAXW + FOM_WARPS * M.nshell * (1 + MAXORG);
+    if (fp64 && sizeof(double) * words > 220 * 1024) return cudaErrorInvalidValue;
+    if (ng > 0) {
+        if (fp64) fom_kernel<double><<<(unsigned)ng, FOM_WARPS * 32, sizeof(double) * words, s>>>(a);
+        else fom_kernel<float><<<(unsigned)ng, FOM_WARPS * 32, sizeof(float) * words, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -1044,7 +1066,6 @@ extern "C" int bsg_match_prepared(bsg_match* h, long first, long count, float* o
 }
 
 extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, double* fom, double* cv, int flags) {
-    (void)flags;
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !hyps || !fom || nhyp < 1) return mfail(BSG_ERR_ARG, "bsg_match_score: bad argument");
     if (!M->have_ref || M->nimg < 1) return mfail(BSG_ERR_STATE, "bsg_match_score: set the reference and images first");
@@ -1073,7 +1094,7 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
     if (rc2) return rc2;
     cudaStream_t s = M->stream;
     MCK(cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s));
-    MCK(launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s));
+    MCK(launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, (flags & BSG_MATCH_SCORE_FP64) != 0));
     std::vector<double> go(2 * ng * MAXORG);
     MCK(cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));

@@ -232,8 +232,9 @@ struct Match {
 
 
 // exact FRC scoring of ng hypothesis groups already on the device (match.cu):
-// d_fom / d_cv get MAXORG slots per group
-cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s);
+// d_fom / d_cv get MAXORG slots per group; fp64: FP64 gather and sums
+cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
+                       bool fp64 = false);
 void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups, std::vector<long>& slot);
 int ensure_groups(Match& M, long ng);
 // view matrix rows 0, 1 scaled by the sampling ratio (img_fit_in_recip_space_grid)

@@ -135,12 +135,28 @@ class Matcher:
                    "bsg_match_prepared")
         return out
 
-    def score(self, hyps):
+    def score(self, hyps, fp64: bool = False):
         h = np.ascontiguousarray(hyps, dtype=np.float64).reshape(-1, MATCH_HYP_DOUBLES)
         fom = np.empty(len(h))
         cv = np.empty(len(h))
-        _lib.check(_lib.load().bsg_match_score(self._h, _dp(h), len(h), _dp(fom), _dp(cv), 0), "bsg_match_score")
+        _lib.check(_lib.load().bsg_match_score(self._h, _dp(h), len(h), _dp(fom), _dp(cv),
+                                               _lib.MATCH_SCORE_FP64 if fp64 else 0), "bsg_match_score")
         return fom, cv
+
+    def refine(self, start, alpha_step: float, accuracy: float, shift_step: float = 0.4,
+               shift_accuracy: float = 0.1) -> np.ndarray:
+        """img_refine_grid for every start record (n, 7): image index, view
+        x, y, z, angle (radians), origin x, y (particle pixels).  Angular
+        step and accuracy in radians, shift step and accuracy in pixels of
+        the cut transform (the reference's arguments).  Returns (n, 9): view
+        x, y, z, angle, origin x, y, figure of merit, cross-validation
+        figure, hypotheses scored."""
+        s = np.ascontiguousarray(start, dtype=np.float64).reshape(-1, _lib.MATCH_REFINE_START_DOUBLES)
+        out = np.empty((len(s), _lib.MATCH_REFINE_RESULT_DOUBLES))
+        _lib.check(_lib.load().bsg_match_refine(self._h, _dp(s), len(s), float(alpha_step), float(accuracy),
+                                                float(shift_step), float(shift_accuracy), _dp(out), 0),
+                   "bsg_match_refine")
+        return out
 
 
     # ---- exhaustive search ----

@@ -241,7 +241,10 @@ int  bsg_match_set_images(bsg_match* m, const float* images, long nimg, const do
                           double file_avg, double file_std, int flags);
 /* Prepared particle transforms [first, first+count): diam^2 complex64 each. */
 int  bsg_match_prepared(bsg_match* m, long first, long count, float* out, int flags);
-/* FRC figure of merit (and cross-validation figure) of nhyp hypotheses. */
+/* FRC figure of merit (and cross-validation figure) of nhyp hypotheses.
+ * flags: BSG_MATCH_SCORE_FP64 gathers and sums in FP64 (the reference's
+ * accumulation; ~1e-8 from its figures of merit, the FP32 default ~1e-7). */
+#define BSG_MATCH_SCORE_FP64 4
 int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, double* cv, int flags);
 
 /* Exhaustive search (no counterpart in the reference, which refines locally
@@ -293,10 +296,35 @@ typedef struct {
     long   rescored;
     int    coarse_k;       /* real K of the correlation (2 x coarse pixels) */
     int    kpad;           /* K padded to the 64-element stage width        */
+    double refine_ms;      /* grid refinement: figure-of-merit launches     */
+    long   refine_launches;
 } bsg_match_stats;
 int  bsg_match_get_stats(bsg_match* m, bsg_match_stats* st);
 int  bsg_match_reset_stats(bsg_match* m);
 void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
+
+/* Grid refinement of orientations and origins: brefine without -monte, i.e.
+ * img_refine_grid (bsoft/src/mg/mg_refine.cpp:1086-1195) with its shift
+ * search img_fit_in_recip_space_grid (:862-950) and the view grid of
+ * views_for_refinement (bsoft/src/util/View.cpp:371-424), for every start
+ * record at once.  start: nstart records of BSG_MATCH_REFINE_START_DOUBLES
+ * doubles: held image index, view x, y, z, angle (radians), origin x, y
+ * (pixels of the particle image); an image may appear in several records
+ * (part_refine_orientation refines from each symmetry-related view).
+ * alpha_step, accuracy: angular step and final accuracy (radians; the
+ * reference's checks: both >= 1e-30, step >= accuracy); shift_step,
+ * shift_accuracy: origin grid step and accuracy (pixels of the cut
+ * transform, as img_fit_in_recip_space_grid uses them; accuracy > 0).
+ * out: nstart records of BSG_MATCH_REFINE_RESULT_DOUBLES doubles: view x,
+ * y, z, angle, origin x, y (pixels of the particle image), figure of merit,
+ * cross-validation figure, hypotheses scored (the reference's `number`).
+ * The held images' CTF records apply as set_images gave them; the
+ * reference's defocus search (-defocus) and magnification search
+ * (max_mag > 0) are not part of this call. */
+#define BSG_MATCH_REFINE_START_DOUBLES 7
+#define BSG_MATCH_REFINE_RESULT_DOUBLES 9
+int  bsg_match_refine(bsg_match* m, const double* start, long nstart, double alpha_step, double accuracy,
+                      double shift_step, double shift_accuracy, double* out, int flags);
 
 /* ---- learned orientation proposer ------------------------------------------
  * No counterpart in the reference.  A convolutional network maps a particle

@@ -95,3 +95,26 @@ def test_projections(matcher):
     p = m.project(d["mats"], resolution=float(d["proj_res"]))
     for a, b in zip(p, d["proj"]):
         assert rel_l2(a, b) < 1e-5
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_full_origin_groups(matcher, fp64):
+    """Nine origins of one image and view share one gathered section (a full
+    group): each scores as it does alone, in FP32 and in FP64."""
+    m, d = matcher
+    ox, oy = d["n"] / 2, d["n"] / 2
+    hyps = np.array([[0, *d["mats"][0].reshape(9), ox + dx, oy + dy]
+                     for dy in (-0.4, 0.0, 0.4) for dx in (-0.4, 0.0, 0.4)])
+    f, cv = m.score(hyps, fp64=fp64)
+    for i, h in enumerate(hyps):
+        f1, cv1 = m.score(h[None], fp64=fp64)
+        assert abs(f1[0] - f[i]) < 1e-12 and abs(cv1[0] - cv[i]) < 1e-12
+    assert np.all(f != 0)
+
+
+def test_fp64_scores_match_reference(matcher):
+    m, d = matcher
+    f, cv = m.score(hypotheses(d), fp64=True)
+    f32, _ = m.score(hypotheses(d))
+    assert np.abs(f - d["fom"][:, 0]).max() < 1e-6
+    assert np.abs(f - f32).max() < 1e-5

@@ -1,0 +1,87 @@
+"""bsg_match_refine (the reference's img_refine_grid on the GPU) against the
+reference's own refinement (golden fixtures) and the grid-refinement oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from tests.refine_helpers import REFINE_CASES, load
+
+pytestmark = pytest.mark.gpu
+
+TOL_FOM = 2e-5       # float32 gather and shell sums in the figure-of-merit kernel
+
+
+@pytest.fixture(scope="module", params=REFINE_CASES)
+def setup(request):
+    from bsoft_b200.match import Matcher
+    d = load(request.param)
+    m = Matcher(n=d["n"], map=d["N"], map_sampling=d["pixel"], pixel=d["pixel"], hi_res=d["hi_res"])
+    m.set_reference(d["map"], (d["N"] / 2,) * 3)
+    ctf = np.zeros((len(d["images"]), 8))
+    ctf[:, 0] = 300.0
+    m.set_images(d["images"], ctf, d["file_avg"], d["file_std"])
+    d["start_rec"] = np.column_stack([np.arange(len(d["images"])), d["start"]])
+    yield m, d
+    m.close()
+
+
+def _refine(m, d, start=None, **kw):
+    args = dict(alpha_step=d["alpha"], accuracy=d["accuracy"], shift_step=d["shift_step"],
+                shift_accuracy=d["shift_accuracy"])
+    args.update(kw)
+    return m.refine(d["start_rec"] if start is None else start, **args)
+
+
+def test_matches_reference(setup):
+    m, d = setup
+    out = _refine(m, d)
+    ref = d["result"]
+    assert np.array_equal(out[:, 8], ref[:, 8]), (out[:, 8], ref[:, 8])     # same hypotheses scored
+    assert np.abs(out[:, :4] - ref[:, :4]).max() < 1e-12                     # same views chosen
+    assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9                    # same origins
+    assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
+    assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+
+
+def test_batch_invariant_and_repeated_images(setup):
+    m, d = setup
+    whole = _refine(m, d)
+    for i in range(len(d["start_rec"])):
+        one = _refine(m, d, start=d["start_rec"][i:i + 1])
+        assert np.array_equal(one[0], whole[i])
+    # an image may be refined from several starts (symmetry-related views)
+    two = _refine(m, d, start=np.concatenate([d["start_rec"][:1], d["start_rec"][:1]]))
+    assert np.array_equal(two[0], two[1]) and np.array_equal(two[0], whole[0])
+
+
+def test_no_shift_levels_returns_start(setup):
+    m, d = setup
+    out = _refine(m, d, shift_step=0.05, shift_accuracy=0.1)
+    assert np.all(out[:, 6] == -1) and np.all(out[:, 8] == 0) and np.all(out[:, 7] == 0)
+    assert np.allclose(out[:, 4:6], d["start"][:, 4:6], atol=1e-12)
+    v = d["start"][:, :3] / np.linalg.norm(d["start"][:, :3], axis=1, keepdims=True)
+    assert np.allclose(out[:, :3], v, atol=1e-15)
+
+
+def test_rejects_bad_steps(setup):
+    from bsoft_b200._lib import BsgError
+    m, d = setup
+    with pytest.raises(BsgError):
+        _refine(m, d, alpha_step=math.radians(0.1), accuracy=math.radians(0.5))
+    with pytest.raises(BsgError):
+        _refine(m, d, accuracy=0.0)
+    with pytest.raises(BsgError):
+        _refine(m, d, shift_accuracy=0.0)
+    bad = d["start_rec"].copy()
+    bad[0, 0] = len(d["images"])
+    with pytest.raises(BsgError):
+        _refine(m, d, start=bad)
+
+
+def test_stats_count_refinement(setup):
+    m, d = setup
+    m.reset_stats()
+    _refine(m, d)
+    st = m.stats()
+    assert st["refine_launches"] >= 3 and st["refine_ms"] > 0
