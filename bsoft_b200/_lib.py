@@ -63,7 +63,7 @@ MATCH_CTF_DOUBLES = 8
 MATCH_HYP_DOUBLES = 12
 MATCH_REFINE_START_DOUBLES = 7
 MATCH_SCORE_FP64 = 4
-MATCH_REFINE_RESULT_DOUBLES = 9
+MATCH_REFINE_RESULT_DOUBLES = 10
 
 
 class BsgError(RuntimeError):
@@ -113,7 +113,8 @@ def load():
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_match_stream": ([vp], vp),
-        "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, dp, C.c_int],
+        "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
+                              C.c_int],
                              C.c_int),
         "bsg_cnn_create": ([C.POINTER(CnnConfig), C.POINTER(vp)], C.c_int),
         "bsg_cnn_destroy": ([vp], None),

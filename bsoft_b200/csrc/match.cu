@@ -284,21 +284,7 @@ __global__ void __launch_bounds__(256) img_shells_kernel(const float2* __restric
     const long b = blockIdx.x;
     const float2* X = spec + b * (long)D * D;
     const ImgCtf C = ctf[b];
-    for (int p = threadIdx.x; p < npix; p += blockDim.x) {
-        float v = 1.f;
-        if (C.apply) {
-            const MPix q = pix[p];
-            double sx2 = fs * q.h; sx2 *= sx2;
-            double sy2 = fs * q.k; sy2 *= sy2;
-            const double s2 = sx2 + sy2;
-            const double a = atan2((double)q.k, (double)q.h);
-            const double chi = C.c[0] + s2 * (C.c[3] * sin(2 * a) + C.c[1] + C.c[2] * cos(2 * a)) + s2 * s2 * C.c[4];
-            double s = sin(chi);
-            if (C.invert) s = -s;
-            v = (float)s;
-        }
-        ctf_out[b * npix + p] = v;
-    }
+    for (int p = threadIdx.x; p < npix; p += blockDim.x) ctf_out[b * npix + p] = ctf_factor(C, pix[p], fs);
     for (int j = threadIdx.x; j < nshell; j += blockDim.x) {
         double d = 0;
         for (int p = shell_start[j]; p < shell_start[j + 1]; ++p) {
@@ -307,6 +293,14 @@ __global__ void __launch_bounds__(256) img_shells_kernel(const float2* __restric
         }
         dsum[b * nshell + j] = d;
     }
+}
+
+// CTF rows for arbitrary records (the refinement's defocus trials)
+__global__ void __launch_bounds__(256) ctf_rows_kernel(const ImgCtf* __restrict__ rec, const MPix* __restrict__ pix,
+                                                       int npix, double fs, float* __restrict__ out) {
+    const long b = blockIdx.x;
+    const ImgCtf C = rec[b];
+    for (int p = threadIdx.x; p < npix; p += blockDim.x) out[b * npix + p] = ctf_factor(C, pix[p], fs);
 }
 
 // central sections for output: one CTA per view over the pixel list of the
@@ -381,7 +375,7 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
     const int norg = H.norg;
     const long img = H.img;
     const float2* X = a.spec + img * (long)a.D * a.D;
-    const float* C = a.ctf + img * (long)a.npix;
+    const float* C = a.ctf + (long)H.ctf * a.npix;
     T* my = wsum + warp * a.nshell * NV;
     for (int base = warp * 32; base < a.npix; base += FOM_WARPS * 32) {
         T Rx = 0, Ry = 0;
@@ -854,12 +848,18 @@ int match_fail(int code, const char* fmt, ...) {
     return code;
 }
 
+cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, float* d_out, cudaStream_t s) {
+    if (nrec > 0)
+        ctf_rows_kernel<<<(unsigned)nrec, 256, 0, s>>>(d_rec, M.d_pix, (int)M.h_pix.size(), 1.0 / M.real_img, d_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64) {
+                       bool fp64, const float* ctf_table) {
     FomArgs a{};
     a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf; a.lutd = M.d_lut;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
-    a.spec = M.d_spec; a.ctf = M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
+    a.spec = M.d_spec; a.ctf = ctf_table ? ctf_table : M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
     a.fom = d_fom; a.cv = d_cv;
@@ -896,6 +896,7 @@ void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups,
             memset(&g, 0, sizeof(g));
             memcpy(g.m, h.m, sizeof(g.m));
             g.img = h.img;
+            g.ctf = h.img;
             groups.push_back(g);
         }
         MHypG& g = groups.back();
@@ -1007,6 +1008,9 @@ extern "C" int bsg_match_set_images(bsg_match* h, const float* images, long nimg
         ic[i].apply = (f & BSG_MATCH_APPLY_CTF) && def >= 1 ? 1 : 0;
         ic[i].invert = (f & BSG_MATCH_INVERT) ? 1 : 0;
     }
+    M->h_ictf = ic;
+    M->h_volt.assign(nimg, 0.0);
+    for (long i = 0; i < nimg; ++i) M->h_volt[i] = ctf[8 * i];
     MCK(cudaMemcpyAsync(M->d_ictf, ic.data(), sizeof(ImgCtf) * nimg, cudaMemcpyHostToDevice, s));
     if (file_std > 0) {
         std::vector<double> sc(nimg, 1.0 / file_std), sh(nimg, -file_avg / file_std);

@@ -39,6 +39,8 @@ struct MHypG {
     double sx[MAXORG], sy[MAXORG];
     int img;
     int norg;
+    int ctf;        // row of the CTF table the launch scores with (the image's own: img)
+    int pad;
 };
 
 
@@ -157,6 +159,21 @@ struct ImgCtf {
     int invert;      // negate the CTF (contrast inversion)
 };
 
+// sin(chi) of one figure-of-merit pixel (img_recip_space_fom's CTF factor,
+// mg_refine.cpp:700-740; chi as CTFparam::calculate_aberration_even,
+// ctf.h:321-334); 1 when the record does not apply
+__device__ __forceinline__ float ctf_factor(const ImgCtf& C, const MPix& q, double fs) {
+    if (!C.apply) return 1.f;
+    double sx2 = fs * q.h; sx2 *= sx2;
+    double sy2 = fs * q.k; sy2 *= sy2;
+    const double s2 = sx2 + sy2;
+    const double a = atan2((double)q.k, (double)q.h);
+    const double chi = C.c[0] + s2 * (C.c[3] * sin(2 * a) + C.c[1] + C.c[2] * cos(2 * a)) + s2 * s2 * C.c[4];
+    double s = sin(chi);
+    if (C.invert) s = -s;
+    return (float)s;
+}
+
 struct Match {
     bsg_match_config cfg;
     int device = 0;
@@ -194,6 +211,8 @@ struct Match {
     double* d_scale = nullptr;
     double* d_shift = nullptr;
     ImgCtf* d_ictf = nullptr;
+    std::vector<ImgCtf> h_ictf;        // host copy of the held images' CTF records
+    std::vector<double> h_volt;        // and their accelerating voltages
     MHyp* d_hyp = nullptr;
     long hyp_cap = 0;
     double* d_out = nullptr;           // 2 x hyp_cap
@@ -234,7 +253,9 @@ struct Match {
 // exact FRC scoring of ng hypothesis groups already on the device (match.cu):
 // d_fom / d_cv get MAXORG slots per group; fp64: FP64 gather and sums
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64 = false);
+                       bool fp64 = false, const float* ctf_table = nullptr);
+// CTF table rows (npix floats each) for nrec records on the device
+cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, float* d_out, cudaStream_t s);
 void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups, std::vector<long>& slot);
 int ensure_groups(Match& M, long ng);
 // view matrix rows 0, 1 scaled by the sampling ratio (img_fit_in_recip_space_grid)

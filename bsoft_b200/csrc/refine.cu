@@ -229,6 +229,26 @@ Level origin_level(double ox, double oy, double step) {
     return L;
 }
 
+// CTFparam's defocus accessors (bsoft/include/ctf.h:133-134): abw[2,0] =
+// t2 * defocus with the wavelength term t2 = -pi lambda held as a long
+// double (ctf.h:48, 76-79) and lambda from ctf.h:309-317 (constants of
+// bsoft/include/utilities.h:55-58).  The defocus search's floating loop
+// visits def - 5 sigma .. def + 5 sigma; whether its last step is taken
+// depends on the last bit of def, so the long double rounding is kept.
+struct DefocusTerm {
+    long double t2 = 0;
+    explicit DefocusTerm(double volt) {
+        const double planck = 6.626070E-34, emass = 9.109384E-31, echarge = 1.602177E-19, light = 299792458;
+        const double root = sqrt(2.0 * emass * echarge * volt * (1.0 + echarge * volt / (2.0 * emass * light * light)));
+        const double wl = (double)((long double)planck * 1e10L / (long double)root);
+        t2 = (long double)(-M_PI * wl);
+    }
+    double abw20(double defocus) const { return (double)(t2 * (long double)defocus); }
+    double defocus(double abw20) const { return (double)((long double)abw20 / t2); }
+};
+
+constexpr int MAX_DEF = 64;          // defocus trials per view (the reference's loop makes 10 or 11)
+
 struct Particle {
     long img;
     double ox, oy;                 // original origin, pixels of the cut transform
@@ -239,6 +259,13 @@ struct Particle {
     long rounds;
     bool done;
     View4 views[NVIEW];            // this round's views
+    // defocus search (brefine -defocus)
+    double def0 = 0;               // img_refine_grid's `def`: the particle's defocus
+    double bestdef = 0;
+    std::vector<double> dvals;     // the fit's defocus trials; row dvals.size() = no trial won
+    long row0 = 0;                 // first row of this particle in the call's CTF table
+    int vk[NVIEW];                 // this round: chosen trial per view
+    double vfom[NVIEW], vcv[NVIEW];
 };
 
 }  // namespace
@@ -247,7 +274,7 @@ struct Particle {
 using namespace bsg;
 
 extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, double alpha_step, double accuracy,
-                                double shift_step, double shift_accuracy, double* out, int flags) {
+                                double shift_step, double shift_accuracy, double def_std, double* out, int flags) {
     (void)flags;
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !start || !out || nstart < 1) return match_fail(BSG_ERR_ARG, "bsg_match_refine: bad argument");
@@ -263,6 +290,8 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
     // the reference's shift loop never ends for a non-positive accuracy
     if (!(shift_accuracy > 0) || !isfinite(shift_step))
         return match_fail(BSG_ERR_ARG, "bsg_match_refine: shift accuracy must be positive (got %g)", shift_accuracy);
+    if (!(def_std >= 0) || !isfinite(def_std))
+        return match_fail(BSG_ERR_ARG, "bsg_match_refine: bad defocus step %g", def_std);
     std::vector<double> steps;
     for (double st = shift_step; st >= shift_accuracy; st /= 2) {
         if ((int)steps.size() >= MAX_LEVELS)
@@ -271,6 +300,7 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         steps.push_back(st);
     }
     const int nlev = (int)steps.size();
+    const bool dsearch = def_std > 0;
     cudaError_t ce = cudaSetDevice(M->device);
     if (ce != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(ce));
 
@@ -302,13 +332,36 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         P.boy = P.oy;
         P.number = 0;
         P.rounds = 0;
-        P.done = nlev == 0;    // nothing is scored: the start pose is returned
+        P.done = nlev == 0 && !dsearch;    // nothing is scored: the start pose is returned
+        if (dsearch) {
+            // img_refine_grid :1105-1106, the view loop's reset :1118 and the
+            // fit's defocus trials :866-871, 892, 899
+            const double volt = M->h_volt[img];
+            if (!(volt > 0))
+                return match_fail(BSG_ERR_ARG, "bsg_match_refine: image %ld has no voltage for the defocus search", img);
+            const DefocusTerm dz(volt);
+            P.def0 = P.bestdef = dz.defocus(M->h_ictf[img].c[1]);
+            if (P.def0 == 0)
+                return match_fail(BSG_ERR_ARG, "bsg_match_refine: image %ld has no defocus to search around", img);
+            const double b = dz.defocus(dz.abw20(P.def0));
+            const double d0 = b - 5 * def_std, d1 = b + 5 * def_std;
+            for (double d = d0; d <= d1; d += def_std) {
+                if ((int)P.dvals.size() >= MAX_DEF || d + def_std == d)
+                    return match_fail(BSG_ERR_ARG, "bsg_match_refine: defocus step %g too small for defocus %g",
+                                      def_std, P.def0);
+                P.dvals.push_back(d);
+            }
+            P.dvals.push_back(b);    // the row used when no trial improves on -1
+        }
     }
 
-    // rounds: every active particle's 27 views x nlev levels in one launch;
-    // particles are taken in chunks so that a launch holds at most ~64k groups
-    const long per_part = (long)NVIEW * nlev;
-    const long chunk = std::max(1L, (long)(65536 / std::max(1L, per_part)));
+    // rounds: every active particle's views in one launch per pass (defocus
+    // trials, then shift levels); particles are taken in chunks so that a
+    // launch holds at most ~64k groups
+    const long per_b = (long)NVIEW * std::max(nlev, 1);
+    const long per_a = dsearch ? (long)NVIEW * (MAX_DEF / 4) : 0;
+    const long chunk = std::max(1L, (long)(65536 / std::max(per_a, per_b)));
+    const int npix = (int)M->h_pix.size();
     cudaStream_t s = M->stream;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
@@ -316,13 +369,80 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
     float tsum = 0;
     long launches = 0;
     std::vector<MHypG> groups;
-    std::vector<long> owner;
+    std::vector<long> owner, gfirst;
     std::vector<double> go;
+    float* d_rctf = nullptr;
+    ImgCtf* d_rrec = nullptr;
     int rc = BSG_OK;
+
+    // score `groups` (FP64) with the given CTF table; results in go
+    auto score = [&](const float* table) -> int {
+        const long ng = (long)groups.size();
+        int r = ensure_groups(*M, ng);
+        if (r != BSG_OK) return r;
+        go.resize(2 * ng * MAXORG);
+        cudaError_t e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(e));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        tsum += ms;
+        ++launches;
+        return BSG_OK;
+    };
+    auto view_group = [&](const Particle& P, int v) {
+        // Bimage::view stores a twice-copied view; the fit reads it back (one
+        // more) and View::matrix normalises once more
+        double mat[9];
+        view_matrix(renormalised(P.views[v], 3), mat);
+        MHypG g;
+        memset(&g, 0, sizeof(g));
+        match_view_rows(*M, mat, g.m);
+        g.img = (int)P.img;
+        g.ctf = (int)P.img;
+        return g;
+    };
+    // phase_shift_to_origin's slopes, as bsg_match_score forms them
+    auto slope = [&](double o) { return o / M->D * 2 * M_PI; };
+
     for (long c0 = 0; c0 < nstart && rc == BSG_OK; c0 += chunk) {
         const long c1 = std::min(nstart, c0 + chunk);
+        if (dsearch) {
+            // CTF rows of every defocus trial of this chunk's particles
+            std::vector<ImgCtf> recs;
+            for (long i = c0; i < c1; ++i) {
+                Particle& P = parts[i];
+                P.row0 = (long)recs.size();
+                const DefocusTerm dz(M->h_volt[P.img]);
+                for (double d : P.dvals) {
+                    ImgCtf C = M->h_ictf[P.img];
+                    C.c[1] = dz.abw20(d);
+                    // APPLY_CTF is set with -defocus (mg_refine.cpp:575); the
+                    // figure of merit drops the CTF below 1 angstrom (:685-686)
+                    C.apply = dz.defocus(C.c[1]) >= 1 ? 1 : 0;
+                    recs.push_back(C);
+                }
+            }
+            cudaFree(d_rctf);
+            cudaFree(d_rrec);
+            d_rctf = nullptr;
+            d_rrec = nullptr;
+            ce = cudaMalloc(&d_rctf, sizeof(float) * npix * recs.size());
+            if (ce == cudaSuccess) ce = cudaMalloc(&d_rrec, sizeof(ImgCtf) * recs.size());
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(d_rrec, recs.data(), sizeof(ImgCtf) * recs.size(), cudaMemcpyHostToDevice, s);
+            if (ce == cudaSuccess) ce = launch_ctf_rows(*M, d_rrec, (long)recs.size(), d_rctf, s);
+            if (ce != cudaSuccess) {
+                rc = match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(ce));
+                break;
+            }
+        }
         for (;;) {
-            groups.clear();
             owner.clear();
             for (long i = c0; i < c1; ++i) {
                 Particle& P = parts[i];
@@ -332,60 +452,90 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
                     rc = match_fail(BSG_ERR_STATE, "bsg_match_refine: %d refinement views", nv);
                     break;
                 }
+                owner.push_back(i);
+            }
+            if (rc != BSG_OK || owner.empty()) break;
+            // pass A: the fit's defocus trials at the original origin
+            // (img_fit_in_recip_space_grid :895-911)
+            for (long i : owner)
                 for (int v = 0; v < NVIEW; ++v) {
-                    // Bimage::view stores a twice-copied view; the fit reads it
-                    // back (one more) and View::matrix normalises once more
-                    double mat[9];
-                    view_matrix(renormalised(P.views[v], 3), mat);
-                    MHypG g;
-                    memset(&g, 0, sizeof(g));
-                    match_view_rows(*M, mat, g.m);
-                    g.img = (int)P.img;
+                    parts[i].vk[v] = (int)parts[i].dvals.size() - 1;
+                    parts[i].vfom[v] = -1;
+                    parts[i].vcv[v] = 0;
+                }
+            if (dsearch) {
+                groups.clear();
+                gfirst.clear();
+                for (long i : owner) {
+                    Particle& P = parts[i];
+                    gfirst.push_back((long)groups.size());
+                    for (int v = 0; v < NVIEW; ++v) {
+                        MHypG g = view_group(P, v);
+                        g.norg = 1;
+                        g.sx[0] = slope(P.ox);
+                        g.sy[0] = slope(P.oy);
+                        for (size_t k = 0; k + 1 < P.dvals.size(); ++k) {
+                            g.ctf = (int)(P.row0 + (long)k);
+                            groups.push_back(g);
+                        }
+                    }
+                }
+                rc = score(d_rctf);
+                if (rc != BSG_OK) break;
+                for (size_t t = 0; t < owner.size(); ++t) {
+                    Particle& P = parts[owner[t]];
+                    const long nd = (long)P.dvals.size() - 1;
+                    for (int v = 0; v < NVIEW; ++v)
+                        for (long k = 0; k < nd; ++k) {
+                            const long g = gfirst[t] + (long)v * nd + k;
+                            const double f = go[g * MAXORG];
+                            P.number++;
+                            if (P.vfom[v] < f) {
+                                P.vfom[v] = f;
+                                P.vk[v] = (int)k;
+                                P.vcv[v] = go[(long)groups.size() * MAXORG + g * MAXORG];
+                            }
+                        }
+                }
+            }
+            // pass B: every shift level of every view (:914-944), with the
+            // defocus each view's trials chose
+            groups.clear();
+            for (long i : owner) {
+                Particle& P = parts[i];
+                for (int v = 0; v < NVIEW; ++v) {
+                    MHypG g = view_group(P, v);
+                    if (dsearch) g.ctf = (int)(P.row0 + P.vk[v]);
                     for (int k = 0; k < nlev; ++k) {
                         const Level& L = P.levels[k];
                         g.norg = L.n;
                         for (int o = 0; o < L.n; ++o) {
-                            // phase_shift_to_origin's slopes, as bsg_match_score
-                            g.sx[o] = L.x[o] / M->D * 2 * M_PI;
-                            g.sy[o] = L.y[o] / M->D * 2 * M_PI;
+                            g.sx[o] = slope(L.x[o]);
+                            g.sy[o] = slope(L.y[o]);
                         }
                         groups.push_back(g);
                     }
                 }
-                owner.push_back(i);
             }
-            if (rc != BSG_OK || owner.empty()) break;
+            if (!groups.empty()) {
+                rc = score(dsearch ? d_rctf : nullptr);
+                if (rc != BSG_OK) break;
+            }
             const long ng = (long)groups.size();
-            rc = ensure_groups(*M, ng);
-            if (rc != BSG_OK) break;
-            go.resize(2 * ng * MAXORG);
-            ce = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
-            if (ce == cudaSuccess) ce = cudaEventRecord(e0, s);
-            if (ce == cudaSuccess) ce = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true);
-            if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
-            if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-            if (ce != cudaSuccess) {
-                rc = match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(ce));
-                break;
-            }
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            tsum += ms;
-            ++launches;
             const double* gfom = go.data();
             const double* gcv = go.data() + ng * MAXORG;
             for (size_t t = 0; t < owner.size(); ++t) {
                 Particle& P = parts[owner[t]];
-                const long gbase = (long)t * per_part;
+                const long gbase = (long)t * NVIEW * nlev;
+                const DefocusTerm dz(dsearch ? M->h_volt[P.img] : 0.0);
                 // img_refine_grid's angular round (mg_refine.cpp:1112-1136)
                 P.prefom = P.bestfom;
                 P.bestfom = -1;
                 int ibest = 0;
                 for (int v = 0; v < NVIEW; ++v) {
-                    // img_fit_in_recip_space_grid's shift levels (:914-944)
-                    double bestfom = -1, prevfom, bestcv = 0, bx = P.ox, by = P.oy;
+                    // img_fit_in_recip_space_grid's shift levels (:914-944),
+                    // starting from the defocus trials' best
+                    double bestfom = P.vfom[v], prevfom, bestcv = P.vcv[v], bx = P.ox, by = P.oy;
                     int k = 0;
                     while (k < nlev) {
                         const Level& L = P.levels[k];
@@ -413,6 +563,8 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
                         P.box = bx;
                         P.boy = by;
                         P.bestcv = bestcv;
+                        // the defocus the fit left in the CTF (:1133)
+                        if (dsearch) P.bestdef = dz.defocus(dz.abw20(P.dvals[P.vk[v]]));
                     }
                 }
                 if (ibest == NVIEW / 2 || fabs(P.prefom - P.bestfom) < 1e-6) P.alpha /= 2;
@@ -420,6 +572,8 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
             }
         }
     }
+    cudaFree(d_rctf);
+    cudaFree(d_rrec);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != BSG_OK) return rc;
@@ -437,6 +591,13 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         o[6] = P.bestfom;
         o[7] = P.bestcv;
         o[8] = (double)P.number;
+        o[9] = 0;
+        if (dsearch) {
+            // the final defocus check (:1186-1191), read back through the CTF
+            const DefocusTerm dz(M->h_volt[P.img]);
+            const double d = (P.bestdef > P.def0 - 5 * def_std && P.bestdef < P.def0 + 5 * def_std) ? P.bestdef : P.def0;
+            o[9] = dz.defocus(dz.abw20(d));
+        }
     }
     M->sstats.refine_ms += tsum;
     M->sstats.refine_launches += launches;

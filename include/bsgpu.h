@@ -315,16 +315,22 @@ void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
  * reference's checks: both >= 1e-30, step >= accuracy); shift_step,
  * shift_accuracy: origin grid step and accuracy (pixels of the cut
  * transform, as img_fit_in_recip_space_grid uses them; accuracy > 0).
+ * def_std > 0 (angstrom): brefine -defocus: for every view the CTF is
+ * applied at the 10 or 11 defoci d - 5 def_std .. d + 5 def_std around the
+ * image's defocus d (its CTF record's abw20) at the original origin, and
+ * the best of them is used for the view's shift grid (mg_refine.cpp:866-911,
+ * 1105-1191); every held image needs a voltage and a non-zero defocus.
+ * def_std = 0: the held images' CTF records apply as set_images gave them
+ * (in the reference the grid refinement applies a CTF only with -defocus).
  * out: nstart records of BSG_MATCH_REFINE_RESULT_DOUBLES doubles: view x,
  * y, z, angle, origin x, y (pixels of the particle image), figure of merit,
- * cross-validation figure, hypotheses scored (the reference's `number`).
- * The held images' CTF records apply as set_images gave them; the
- * reference's defocus search (-defocus) and magnification search
- * (max_mag > 0) are not part of this call. */
+ * cross-validation figure, hypotheses scored (the reference's `number`),
+ * defocus after refinement (angstrom; 0 without the defocus search).  The
+ * magnification search (max_mag > 0) is not part of this call. */
 #define BSG_MATCH_REFINE_START_DOUBLES 7
-#define BSG_MATCH_REFINE_RESULT_DOUBLES 9
+#define BSG_MATCH_REFINE_RESULT_DOUBLES 10
 int  bsg_match_refine(bsg_match* m, const double* start, long nstart, double alpha_step, double accuracy,
-                      double shift_step, double shift_accuracy, double* out, int flags);
+                      double shift_step, double shift_accuracy, double def_std, double* out, int flags);
 
 /* ---- learned orientation proposer ------------------------------------------
  * No counterpart in the reference.  A convolutional network maps a particle

@@ -5,11 +5,15 @@
 // part_refine_orientation (bsoft/src/mg/mg_refine.cpp:279-365, 509-563) and
 // img_refine_grid (:1086-1195, with img_fit_in_recip_space_grid :862-950).
 // Prints per particle: view x y z angle, origin x y (pixels of the uncut
-// image), figure of merit, cross-validation figure, hypotheses scored.
+// image), figure of merit, cross-validation figure, hypotheses scored,
+// defocus after refinement (angstrom).
 // Usage:
-//   refine_probe map.mrc stack.mrc pixel hi_res start.txt ctf.txt alpha_step_deg accuracy_deg shift_step shift_accuracy
+//   refine_probe map.mrc stack.mrc pixel hi_res start.txt ctf.txt alpha_step_deg accuracy_deg shift_step shift_accuracy [verbose [def_std]]
 // start.txt: "x y z angle(rad) origin_x origin_y" per particle; ctf.txt as
-// for match_probe ("volt abw00 abw20 abw22 abw2m2 abw40 apply").
+// for match_probe ("volt abw00 abw20 abw22 abw2m2 abw40 apply").  def_std > 0
+// turns on the defocus search with the CTF applied, as brefine -defocus does
+// (part_refine_orientation, mg_refine.cpp:569-576).  Without it the CTF must
+// not be applied: the reference's defocus loop would not end (def += 0).
 #include "rwimg.h"
 #include "mg_processing.h"
 #include "Bimage.h"
@@ -32,6 +36,7 @@ double img_refine_grid(Bimage* p, Bimage* pref, double hi_res, double lo_res, in
 int main(int argc, char** argv) {
 	if ( argc < 11 ) { fprintf(stderr, "usage: refine_probe map stack pixel hi_res start ctf alpha acc step step_acc\n"); return 1; }
 	verbose = argc > 11 ? atoi(argv[11]) : 0;
+	double def_std = argc > 12 ? atof(argv[12]) : 0;
 	double pixel = atof(argv[3]), hi_res = atof(argv[4]);
 	double alpha_step = atof(argv[7])*M_PI/180.0, accuracy = atof(argv[8])*M_PI/180.0;
 	double shift_step = atof(argv[9]), shift_accuracy = atof(argv[10]);
@@ -86,13 +91,15 @@ int main(int argc, char** argv) {
 		c.aberration_weight(2, -2, ctfs[i][4]);
 		c.aberration_weight(4, 0, ctfs[i][5]);
 		int flags = ctfs[i][6] > 0 ? APPLY_CTF : 0;
+		if ( def_std > 0 ) flags |= APPLY_CTF;
+		else if ( flags ) { fprintf(stderr, "refine_probe: a CTF needs def_std > 0\n"); return 4; }
 		long number = 0;
 		double fom = img_refine_grid(p, pref, hi_res, 0, flags, alpha_step, accuracy, shift_step, shift_accuracy,
-			0, 0, weight, &c, 0, kernel, number);
+			0, 0, weight, &c, def_std, kernel, number);
 		View v = p->image->view();
 		Vector3<double> o = p->image->origin() / scale;
-		printf("%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %ld\n", v[0], v[1], v[2], v[3], o[0], o[1],
-			fom, p->image->FOM(), number);
+		printf("%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %ld %.17g\n", v[0], v[1], v[2], v[3], o[0], o[1],
+			fom, p->image->FOM(), number, c.defocus_average());
 		delete p;
 	}
 	return 0;

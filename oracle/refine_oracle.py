@@ -14,6 +14,12 @@ Follows, one particle at a time:
 with every hypothesis scored by the FP64 oracle's central section and
 img_recip_space_fom (match_oracle.c).  Floating-point loops are written as
 the reference writes them, so ragged origin grids come out the same.
+
+The defocus search (brefine -defocus: img_fit_in_recip_space_grid
+:866-911, img_refine_grid :1105-1106, 1118, 1133, 1186-1191) goes through
+CTFparam's defocus accessors (bsoft/include/ctf.h:133-134, 76-79, 309-317),
+whose wavelength term t2 is a long double: np.longdouble (x87 extended on
+x86-64, as the reference's build) reproduces their rounding.
 """
 from __future__ import annotations
 
@@ -24,6 +30,25 @@ import numpy as np
 from . import central_section, fsi_kernel, phase_shift_2d, recip_space_fom
 
 TRIG = 1e-30
+
+# bsoft/include/utilities.h:55-58
+PLANCK, EMASS, ECHARGE, LIGHTSPEED = 6.626070E-34, 9.109384E-31, 1.602177E-19, 299792458
+
+
+class Defocus:
+    """CTFparam's defocus_average set/get for one accelerating voltage."""
+
+    def __init__(self, volt: float):
+        LD = np.longdouble
+        root = math.sqrt(2.0 * EMASS * ECHARGE * volt * (1.0 + ECHARGE * volt / (2.0 * EMASS * LIGHTSPEED * LIGHTSPEED)))
+        wl = float(LD(PLANCK) * LD(1e10) / LD(root))        # ctf.h:311, stored as double
+        self.t2 = LD(-math.pi * wl)                         # ctf.h:78, double product held as long double
+
+    def abw20(self, defocus: float) -> float:
+        return float(self.t2 * np.longdouble(defocus))
+
+    def defocus(self, abw20: float) -> float:
+        return float(np.longdouble(abw20) / self.t2)
 
 
 def _angle_neg_pi_to_pi(a: float) -> float:
@@ -173,7 +198,8 @@ class Scorer:
         self._sec = {}
         self._img = {}
 
-    def __call__(self, view, origin):
+    def __call__(self, view, origin, ctf=None):
+        """ctf: [abw00, abw20, abw22, abw2m2, abw40] applied to the section, or None."""
         mat = view_matrix(view)
         key = mat.tobytes()
         sec = self._sec.get(key)
@@ -184,18 +210,48 @@ class Scorer:
         if x is None:
             x = phase_shift_2d(self.prep, origin)
             self._img[origin] = x
-        return recip_space_fom(x, sec, self.real_img, self.D * self.samp, self.samp, self.hi_res)
+        return recip_space_fom(x, sec, self.real_img, self.D * self.samp, self.samp, self.hi_res, ctf=ctf)
 
 
-def fit_origin(score, view, ox, oy, step, accuracy, counter):
-    """img_fit_in_recip_space_grid without CTF: (fom, (x, y), cv)."""
+class CtfSearch:
+    """The particle's CTF (aberration weights) and defocus step of brefine -defocus."""
+
+    def __init__(self, volt: float, coefs, def_std: float):
+        self.dz = Defocus(volt)
+        self.coefs = [float(c) for c in coefs[:5]]
+        self.def_std = def_std
+        self.abw20 = self.coefs[1]        # the CTFparam's current abw[2,0]
+
+    def current(self):
+        c = list(self.coefs)
+        c[1] = self.abw20
+        # img_recip_space_fom applies the CTF only for a defocus >= 1 (mg_refine.cpp:685-686)
+        return c if self.dz.defocus(self.abw20) >= 1 else None
+
+
+def fit_origin(score, view, ox, oy, step, accuracy, counter, ctf=None):
+    """img_fit_in_recip_space_grid: (fom, (x, y), cv); with a CtfSearch the
+    defocus loop comes first and leaves the best defocus in ctf.abw20."""
     bestfom, bestcv, best = -1.0, 0.0, (ox, oy)
+    if ctf is not None:
+        bestdef = ctf.dz.defocus(ctf.abw20)
+        def_start, def_end = bestdef - 5 * ctf.def_std, bestdef + 5 * ctf.def_std
+        d = def_start
+        while d <= def_end:
+            ctf.abw20 = ctf.dz.abw20(d)
+            f, cv = score(view, (ox, oy), ctf.current())
+            counter[0] += 1
+            if bestfom < f:
+                bestfom, bestdef, bestcv = f, d, cv
+            d += ctf.def_std
+        ctf.abw20 = ctf.dz.abw20(bestdef)
+    cc = ctf.current() if ctf is not None else None
     while step >= accuracy:
         prevfom, bestfom = bestfom, -1.0
         pts = origin_grid(ox, oy, step)
         ibest = 0
         for i, o in enumerate(pts):
-            f, cv = score(view, o)
+            f, cv = score(view, o, cc)
             counter[0] += 1
             if bestfom < f:
                 bestfom, ibest, best, bestcv = f, i, o, cv
@@ -204,23 +260,37 @@ def fit_origin(score, view, ox, oy, step, accuracy, counter):
     return bestfom, best, bestcv
 
 
-def refine_grid(score, view, origin_cut, alpha_step, accuracy, shift_step, shift_accuracy):
-    """img_refine_grid without CTF or magnification search for one particle.
+def refine_grid(score, view, origin_cut, alpha_step, accuracy, shift_step, shift_accuracy, ctf=None):
+    """img_refine_grid without magnification search for one particle.
 
-    view: (x, y, z, angle) as given; origin_cut: origin in cut pixels.
-    Returns (view, origin_cut, fom, cv, number)."""
+    view: (x, y, z, angle) as given; origin_cut: origin in cut pixels; ctf:
+    a CtfSearch (brefine -defocus) or None (no CTF).
+    Returns (view, origin_cut, fom, cv, number, defocus)."""
     counter = [0]
     bestview = _norm_view(view, 4)          # constructed, stored, read back, copied
     bestfom, bestcv, bestorigin = -1.0, 0.0, tuple(origin_cut)
+    defocus = bestdef = 0.0
+    if ctf is not None and ctf.def_std and ctf.dz.defocus(ctf.abw20):
+        defocus = bestdef = ctf.dz.defocus(ctf.abw20)
+    elif ctf is not None:
+        ctf = None
     while alpha_step >= accuracy:
         prefom, bestfom = bestfom, -1.0
         views = views_for_refinement(_norm_view(bestview), alpha_step)
         ibest = 0
         for i, v in enumerate(views):
+            if defocus:
+                ctf.abw20 = ctf.dz.abw20(defocus)          # resets defocus to the original
             f, o, cv = fit_origin(score, _norm_view(v, 3), origin_cut[0], origin_cut[1], shift_step,
-                                  shift_accuracy, counter)
+                                  shift_accuracy, counter, ctf)
             if bestfom < f:
                 bestfom, ibest, bestview, bestorigin, bestcv = f, i, v, o, cv
+                if defocus:
+                    bestdef = ctf.dz.defocus(ctf.abw20)
         if ibest == len(views) // 2 or abs(prefom - bestfom) < 1e-6:
             alpha_step /= 2
-    return _norm_view(bestview, 3), bestorigin, bestfom, bestcv, counter[0]
+    out_def = 0.0
+    if defocus:
+        out_def = bestdef if defocus - 5 * ctf.def_std < bestdef < defocus + 5 * ctf.def_std else defocus
+        out_def = ctf.dz.defocus(ctf.dz.abw20(out_def))
+    return _norm_view(bestview, 3), bestorigin, bestfom, bestcv, counter[0], out_def

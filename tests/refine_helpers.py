@@ -5,7 +5,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REFINE_CASES = ["refine64", "refine32"]
+REFINE_CASES = ["refine64", "refine32", "refine64ctf"]
 
 
 def load(case: str):
@@ -13,6 +13,7 @@ def load(case: str):
     d = {k: z[k] for k in z.files}
     d["N"] = int(d["map"].shape[0])
     d["n"] = int(d["images"].shape[1])
-    for k in ("pixel", "hi_res", "alpha", "accuracy", "shift_step", "shift_accuracy", "file_avg", "file_std"):
+    for k in ("pixel", "hi_res", "alpha", "accuracy", "shift_step", "shift_accuracy", "file_avg", "file_std", "volt",
+              "def_std"):
         d[k] = float(d[k])
     return d

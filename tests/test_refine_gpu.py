@@ -18,8 +18,10 @@ def setup(request):
     d = load(request.param)
     m = Matcher(n=d["n"], map=d["N"], map_sampling=d["pixel"], pixel=d["pixel"], hi_res=d["hi_res"])
     m.set_reference(d["map"], (d["N"] / 2,) * 3)
+    rows = d["ctf_rows"]
     ctf = np.zeros((len(d["images"]), 8))
-    ctf[:, 0] = 300.0
+    ctf[:, :6] = rows[:, :6]
+    ctf[:, 6] = rows[:, 6]               # 1: apply (the defocus search applies it anyway)
     m.set_images(d["images"], ctf, d["file_avg"], d["file_std"])
     d["start_rec"] = np.column_stack([np.arange(len(d["images"])), d["start"]])
     yield m, d
@@ -28,7 +30,7 @@ def setup(request):
 
 def _refine(m, d, start=None, **kw):
     args = dict(alpha_step=d["alpha"], accuracy=d["accuracy"], shift_step=d["shift_step"],
-                shift_accuracy=d["shift_accuracy"])
+                shift_accuracy=d["shift_accuracy"], def_std=d["def_std"])
     args.update(kw)
     return m.refine(d["start_rec"] if start is None else start, **args)
 
@@ -42,6 +44,7 @@ def test_matches_reference(setup):
     assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9                    # same origins
     assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
     assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+    assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
 
 
 def test_batch_invariant_and_repeated_images(setup):
@@ -57,7 +60,7 @@ def test_batch_invariant_and_repeated_images(setup):
 
 def test_no_shift_levels_returns_start(setup):
     m, d = setup
-    out = _refine(m, d, shift_step=0.05, shift_accuracy=0.1)
+    out = _refine(m, d, shift_step=0.05, shift_accuracy=0.1, def_std=0.0)
     assert np.all(out[:, 6] == -1) and np.all(out[:, 8] == 0) and np.all(out[:, 7] == 0)
     assert np.allclose(out[:, 4:6], d["start"][:, 4:6], atol=1e-12)
     v = d["start"][:, :3] / np.linalg.norm(d["start"][:, :3], axis=1, keepdims=True)
@@ -77,6 +80,15 @@ def test_rejects_bad_steps(setup):
     bad[0, 0] = len(d["images"])
     with pytest.raises(BsgError):
         _refine(m, d, start=bad)
+
+
+def test_defocus_search_needs_a_defocus(setup):
+    from bsoft_b200._lib import BsgError
+    m, d = setup
+    if d["def_std"] > 0:
+        pytest.skip("the CTF-free fixtures hold images without a defocus")
+    with pytest.raises(BsgError):
+        _refine(m, d, def_std=300.0)
 
 
 def test_stats_count_refinement(setup):

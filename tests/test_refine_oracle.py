@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from oracle.refine_oracle import Scorer, origin_grid, refine_grid, views_for_refinement
+from oracle.refine_oracle import CtfSearch, Scorer, origin_grid, refine_grid, views_for_refinement
 from tests.refine_helpers import REFINE_CASES, load
 
 
@@ -22,13 +22,15 @@ def test_oracle_matches_reference(case):
         prep = oracle.match_particle(img, D, d["file_avg"], d["file_std"])
         score = Scorer(spec, prep, n, d["pixel"], N, d["hi_res"])
         st = d["start"][i]
-        v, o, f, cv, num = refine_grid(score, st[:4], (st[4] * (D / n), st[5] * (D / n)), d["alpha"],
-                                       d["accuracy"], d["shift_step"], d["shift_accuracy"])
+        ctf = CtfSearch(d["volt"], d["ctf_rows"][i, 1:6], d["def_std"]) if d["def_std"] > 0 else None
+        v, o, f, cv, num, dz = refine_grid(score, st[:4], (st[4] * (D / n), st[5] * (D / n)), d["alpha"],
+                                           d["accuracy"], d["shift_step"], d["shift_accuracy"], ctf)
         ref = d["result"][i]
         assert np.array_equal(np.array(v), ref[:4]), (i, v, ref[:4])
         assert o[0] / (D / n) == ref[4] and o[1] / (D / n) == ref[5]
         assert num == ref[8]
         assert abs(f - ref[6]) < 1e-7 and abs(cv - ref[7]) < 1e-7
+        assert dz == ref[9] or (ctf is None and ref[9] == 0)
 
 
 def test_views_for_refinement_geometry():
