@@ -37,6 +37,13 @@ correlation kernel against the measured sustained BF16 rate; its CPU
 baseline is the reference's own central_section + img_recip_space_fom per
 hypothesis (oracle/_ref/match_probe), extrapolated to the exhaustive search.
 
+Refinement leg (the search object's "refine"): `--refine-images` images of
+the last search step refined from their best search pose by the reference's
+grid refinement (img_refine_grid: 27 views, 2 -> 0.5 degrees; 3 x 3 origins,
+0.4 -> 0.1 pixel; defocus search +-5 x 100 angstrom, as brefine -defocus),
+scored in FP64 on the GPU; its CPU baseline is the reference's own
+img_refine_grid on one of those particles (oracle/_ref/refine_probe).
+
 `--impl reference` times only the reference CPU implementation (rank 0).
 Multi-GPU (`torchrun --nproc-per-node N`): each rank reconstructs its own
 shard of particles (weak scaling) and the partial maps are summed with one
@@ -229,7 +236,39 @@ def search_workload(n_images, seed=21):
 def search_views_mats(npsi: int = SEARCH_PSI):
     from bsoft_b200.geometry import asymmetric_unit_views_c, search_views, views_to_matrices
     dirs = asymmetric_unit_views_c(1, math.radians(3.0), math.radians(3.0))
-    return len(dirs), views_to_matrices(search_views(dirs, npsi))
+    views = search_views(dirs, npsi)
+    return len(dirs), views_to_matrices(views), views
+
+
+# grid refinement (brefine without -monte): 2 -> 0.5 degrees, 0.4 -> 0.1 pixel
+# of the cut transform, defocus search of +-5 x 100 angstrom (brefine -defocus)
+REFINE_ALPHA, REFINE_ACC, REFINE_STEP, REFINE_SACC, REFINE_DEF = 2.0, 0.5, 0.4, 0.1, 100.0
+
+
+def refine_reference_sample(sw, start_row, ctf_row):
+    """The reference's img_refine_grid (refine_probe, one thread) on one
+    particle of the search workload with the bench's parameters."""
+    import oracle
+    from bsoft_b200.io import mrc
+    exe = oracle.ref_binary("refine_probe")
+    if not os.path.exists(exe):
+        return None, None, "oracle/_ref/refine_probe not built"
+    d = tempfile.mkdtemp(prefix="bench_refine_")
+    N = SEARCH_BOX
+    mrc.write_stack(os.path.join(d, "ref.mrc"), sw["volume"], SEARCH_PIXEL, origin_pixels=(N // 2,) * 3, volume=True)
+    mrc.write_stack(os.path.join(d, "p.mrcs"), sw["images"][int(start_row[0]):int(start_row[0]) + 1], SEARCH_PIXEL)
+    np.savetxt(os.path.join(d, "start.txt"), np.asarray(start_row[1:7])[None], fmt="%.17g")
+    np.savetxt(os.path.join(d, "ctf.txt"), np.asarray(ctf_row)[None], fmt="%.17g")
+    t0 = time.perf_counter()
+    r = subprocess.run([exe, os.path.join(d, "ref.mrc"), os.path.join(d, "p.mrcs"), repr(SEARCH_PIXEL),
+                        repr(SEARCH_RES), os.path.join(d, "start.txt"), os.path.join(d, "ctf.txt"),
+                        repr(REFINE_ALPHA), repr(REFINE_ACC), repr(REFINE_STEP), repr(REFINE_SACC), "0",
+                        repr(REFINE_DEF)], capture_output=True, text=True)
+    dt = time.perf_counter() - t0
+    if r.returncode != 0:
+        return None, None, f"refine_probe failed: {r.stderr[-200:]}"
+    out = np.array([float(t) for t in r.stdout.split()])
+    return dt, out, f"1 particle (img_refine_grid with the defocus search), one thread, wall {dt:.1f} s including map preparation"
 
 
 def search_reference_sample(sw, n_views: int = 160):
@@ -358,7 +397,7 @@ def search_leg(args, local, dist, world, rank, torch):
     imgs = sw["images"]
     meta = sw["meta"]
     ctf = np.stack([ctf_record(sw["spec"].volt, c) for c in meta["coefs"]])
-    ndir, mats = search_views_mats(args.search_psi)
+    ndir, mats, pviews = search_views_mats(args.search_psi)
     origins = np.array(SEARCH_ORIGINS, float)
     m = Matcher(n=SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL, pixel=SEARCH_PIXEL, hi_res=SEARCH_RES,
                 device=local)
@@ -412,6 +451,27 @@ def search_leg(args, local, dist, world, rank, torch):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # ---- grid refinement of the last step's best poses (brefine -defocus)
+    refine = None
+    if "refine" in args.legs:
+        j, res = results[-1]
+        R = min(args.refine_images, B)
+        best = res[:R, 0, 0].astype(int)
+        start = np.column_stack([np.arange(R), pviews[best], origins[res[:R, 0, 1].astype(int)]])
+        m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+        # radians as the reference's CLI converts degrees (atof(x) * M_PI / 180.0)
+        rargs = (REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP, REFINE_SACC, REFINE_DEF)
+        m.refine(start[:16], *rargs)                                # warm-up
+        m.reset_stats()
+        barrier()
+        ev0.record(s)
+        rout = m.refine(start, *rargs)
+        ev1.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        rms = ev0.elapsed_time(ev1)
+        refine = {"ms": rms, "out": rout, "start": start, "j": j, "stats": m.stats(), "R": R}
+
     # ---- learned proposal + local search on the same images
     learned = None
     if "learned" in args.legs:
@@ -464,6 +524,45 @@ def search_leg(args, local, dist, world, rank, torch):
                    "extrapolation": f"{hyp_per_image} hypotheses per particle x measured seconds per hypothesis"}
         else:
             cpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference", "sample": sample}
+    refine_obj = None
+    if refine is not None:
+        from bsoft_b200.geometry import views_to_matrices
+        from bsoft_b200.ctf import electron_wavelength
+        R, j, rout, start = refine["R"], refine["j"], refine["out"], refine["start"]
+        truth = meta["mats"][j * B:j * B + R]
+        e0 = angular_distance_deg(views_to_matrices(start[:, 1:5]), truth)
+        e1 = angular_distance_deg(views_to_matrices(rout[:, :4]), truth)
+        t2 = -math.pi * electron_wavelength(sw["spec"].volt)
+        true_def = meta["coefs"][j * B:j * B + R, 1] / t2
+        rst = refine["stats"]
+        rvalue = R / (refine["ms"] / 1e3)
+        rcpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            ctf_row = [sw["spec"].volt, *meta["coefs"][j * B][:5], 1]
+            row = start[0].copy()
+            row[0] = j * B                         # the image's index in the workload's stack
+            dt, rref, sample = refine_reference_sample(sw, row, ctf_row)
+            if dt is not None:
+                rcpu = {"value": round(1.0 / dt, 5), "unit": "particles/s", "cores": 1, "kind": "reference",
+                        "sample": sample,
+                        "same_result_as_gpu": bool(np.abs(rref[:6] - rout[0, :6]).max() < 1e-9
+                                                   and rref[8] == rout[0, 8]),
+                        "reference_hypotheses": int(rref[8])}
+            else:
+                rcpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference", "sample": sample}
+        refine_obj = {
+            "metric": "particles/s (grid refinement, img_refine_grid with defocus search)",
+            "value": round(rvalue, 1), "unit": "particles/s", "particles": R,
+            "config": {"start": "best pose of the exhaustive search", "alpha_deg": REFINE_ALPHA,
+                       "accuracy_deg": REFINE_ACC, "shift_step_px": REFINE_STEP, "shift_accuracy_px": REFINE_SACC,
+                       "defocus_step_A": REFINE_DEF, "scoring": "FP64 figure of merit"},
+            "hypotheses_per_particle": round(float(rout[:, 8].mean()), 1),
+            "fom_ms": round(rst["refine_ms"], 2), "gpu_launches": int(rst["refine_launches"]),
+            "accuracy": {"median_angular_error_deg_search": round(float(np.median(e0)), 3),
+                         "median_angular_error_deg_refined": round(float(np.median(e1)), 3),
+                         "median_defocus_error_A_refined": round(float(np.median(np.abs(rout[:, 9] - true_def))), 1)},
+            "cpu_baseline": rcpu,
+        }
     learned_obj = None
     if learned is not None:
         lvalue = images / (learned["ms"] / 1e3)
@@ -517,7 +616,7 @@ def search_leg(args, local, dist, world, rank, torch):
         "accuracy": {"median_angular_error_deg": round(float(np.median(errs)), 3),
                      "frac_within_5_deg": round(float(np.mean(errs < 5)), 4)},
         "cpu_baseline": cpu, "gpu_launches": int(st["launches"]), "clocks": clk.summary(),
-        "learned": learned_obj,
+        "learned": learned_obj, "refine": refine_obj,
     }
 
 
@@ -533,7 +632,8 @@ def main():
     ap.add_argument("--search-steps", type=int, default=3)
     ap.add_argument("--search-warmup", type=int, default=3)
     ap.add_argument("--search-psi", type=int, default=SEARCH_PSI)
-    ap.add_argument("--legs", default="insert,search,learned")
+    ap.add_argument("--legs", default="insert,search,refine,learned")
+    ap.add_argument("--refine-images", type=int, default=512)
     ap.add_argument("--train-images", type=int, default=200000)
     ap.add_argument("--train-epochs", type=float, default=8.0)
     ap.add_argument("--local-radius", type=float, default=10.0)
@@ -694,7 +794,8 @@ def main():
         if search is not None:
             line["search"] = search
             line["gpu_launches"] = int(launches) + search["gpu_launches"] + (
-                search["learned"]["gpu_launches"] if search.get("learned") else 0)
+                search["learned"]["gpu_launches"] if search.get("learned") else 0) + (
+                search["refine"]["gpu_launches"] if search.get("refine") else 0)
     else:
         line = {"metric": search["metric"], "value": search["value"], "unit": "particles/s", "n_gpus": world,
                 "steps": search["steps"], "warmup": search["warmup"], "ms_per_step": search["ms_per_step"],
