@@ -34,14 +34,31 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
+HOST = os.path.join(HERE, "host", "breconstruct.cpp")
+HOST_OUT = os.path.join(HERE, "_build", "breconstruct")
+
+
+def build_host(force: bool = False) -> str:
+    """The C++ drop-in breconstruct over libbsgpu (bsoft_b200/host)."""
+    if not force and os.path.exists(HOST_OUT) and os.path.getmtime(HOST_OUT) >= max(
+            os.path.getmtime(HOST), os.path.getmtime(OUT)):
+        return HOST_OUT
+    cxx = shutil.which("g++") or "g++"
+    tmp = HOST_OUT + ".tmp"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"), HOST,
+                    "-L", os.path.dirname(OUT), "-lbsgpu", "-Wl,-rpath,$ORIGIN", "-o", tmp], check=True)
+    os.replace(tmp, HOST_OUT)
+    return HOST_OUT
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and up_to_date():
-        return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    tmp = OUT + ".tmp"
-    cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", tmp] + sources()
-    subprocess.run(cmd, check=True)
-    os.replace(tmp, OUT)
+    if force or not up_to_date():
+        os.makedirs(os.path.dirname(OUT), exist_ok=True)
+        tmp = OUT + ".tmp"
+        cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", tmp] + sources()
+        subprocess.run(cmd, check=True)
+        os.replace(tmp, OUT)
+    build_host(force)
     return OUT
 
 

@@ -72,12 +72,14 @@ def _dataset(tmp_path, **kw):
     return star
 
 
-def test_gpu_c1_scale_against_oracle(tmp_path):
-    # configs[0] geometry (64^2 images -> 64^3, CTF flip, trilinear), 300 particles
+@pytest.mark.parametrize("shape", [0, 2])
+def test_gpu_c1_scale_against_oracle(tmp_path, shape):
+    # 64^2 images -> 64^3, CTF flip, trilinear, 300 particles
     star = _dataset(tmp_path, box=64, n_particles=300, n_blobs=50, seed=21, snr=0.1)
     plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
     images = load_images(plan)
     with Reconstructor(plan) as rec:
+        rec.set_tile_shape(shape)
         rec.insert(images, plan.params)
         m = rec.finish()
     orc = oracle.reconstruct(plan, images)
@@ -85,18 +87,21 @@ def test_gpu_c1_scale_against_oracle(tmp_path):
     assert fsc(m, orc).min() > 0.999
 
 
-def test_gpu_bitwise_deterministic_and_batch_invariant(tmp_path):
+@pytest.mark.parametrize("shape", [0, 1, 3])
+def test_gpu_bitwise_deterministic_and_batch_invariant(tmp_path, shape):
     star = _dataset(tmp_path, box=32, n_particles=120, n_blobs=12, seed=22, snr=0.3)
     plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
     images = load_images(plan)
     outs = []
     for _ in range(2):
         with Reconstructor(plan) as rec:
+            rec.set_tile_shape(shape)
             rec.insert(images, plan.params)
             outs.append(rec.accumulators(0))
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
     # different device batch sizes and split insert calls: same sums within rounding
     with Reconstructor(plan, batch=7) as rec:
+        rec.set_tile_shape(shape)
         rec.insert(images[:50], plan.params[:50])
         rec.insert(images[50:], plan.params[50:])
         v, w = rec.accumulators(0)
@@ -104,6 +109,30 @@ def test_gpu_bitwise_deterministic_and_batch_invariant(tmp_path):
     # and the FP64 oracle's accumulators
     ov, ow, _, _ = oracle.insert(plan, images, plan.params)
     assert rel_l2(v.reshape(-1), ov.view(np.complex128)) < 1e-6 and rel_l2(w.reshape(-1), ow) < 1e-6
+
+
+@pytest.mark.parametrize("shape", range(4))
+@pytest.mark.parametrize("case", ["ctf16_tri_flip", "ctf16_tri_flip_res", "plain24_tri", "ctf16_near_apply"])
+def test_gpu_tile_shapes_match_reference(case, shape, tmp_path):
+    """Every gridding tile shape against the compiled reference's map."""
+    plan, images, refs = load_case(case, str(tmp_path))
+    with Reconstructor(plan) as rec:
+        rec.set_tile_shape(shape)
+        rec.insert(images, plan.params)
+        m = rec.finish(0)
+    assert rel_l2(m, refs["map"]) < TOL, rel_l2(m, refs["map"])
+
+
+def test_gpu_autotune_reports_every_shape(tmp_path):
+    star = _dataset(tmp_path, box=32, n_particles=40, n_blobs=8, seed=26)
+    plan = plan_reconstruction(read_project(star), ReconOptions(interp=2, ctf_action=1))
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        best, ms = rec.autotune(images, plan.params)
+        assert len(ms) == 4 and np.all(ms > 0) and 0 <= best < 4
+        rec.insert(images, plan.params)
+        m = rec.finish()
+    assert rel_l2(m, oracle.reconstruct(plan, images)) < TOL
 
 
 def test_gpu_device_pointer_input(tmp_path):
