@@ -353,6 +353,7 @@ struct FomArgs {
     int cv0, cv1;            // cross-validation shells [cv0, cv1)
     double* fom;             // per group x MAXORG
     double* cv;
+    const double2* sec;      // gathered sections (npix per view, FP64), or null: gather here
 };
 
 // T = float: the search's rescoring (agrees with the reference's figure of
@@ -380,6 +381,13 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
     for (int base = warp * 32; base < a.npix; base += FOM_WARPS * 32) {
         T Rx = 0, Ry = 0;
         const int cnt = min(32, a.npix - base);
+        if (a.sec) {                                      // section gathered once per view
+            if (lane < cnt) {
+                const double2 r = a.sec[(long)H.sec * a.npix + base + lane];
+                Rx = (T)r.x;
+                Ry = (T)r.y;
+            }
+        } else
         for (int q = 0; q < cnt; ++q) {
             const MPix pq = a.pix[base + q];
             if (!pq.insec) continue;                      // warp-uniform
@@ -848,6 +856,50 @@ int match_fail(int code, const char* fmt, ...) {
     return code;
 }
 
+// The FP64 section values of nv views (9 doubles each, rows 0 and 1
+// scaled as in MHyp) at the figure-of-merit pixels: the same gather, in the
+// same order, as fom_kernel<double> performs for one group, so scores from
+// these values equal the gathering kernel's.
+__global__ void __launch_bounds__(FOM_WARPS * 32) secgather_kernel(cudaTextureObject_t tex, int D, int wd,
+                                                                   const double* __restrict__ lut_g,
+                                                                   const MPix* __restrict__ pix, int npix,
+                                                                   const double* __restrict__ mats, double inv,
+                                                                   double real, double2* __restrict__ out) {
+    __shared__ double lut[(NDIV + 1) * MAXW];
+    for (int i = threadIdx.x; i < (NDIV + 1) * wd; i += blockDim.x) lut[i] = lut_g[i];
+    __syncthreads();
+    const double* m = mats + 9 * (long)blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2* o = out + (long)blockIdx.x * npix;
+    for (int base = warp * 32; base < npix; base += FOM_WARPS * 32) {
+        double Rx = 0, Ry = 0;
+        const int cnt = min(32, npix - base);
+        for (int q = 0; q < cnt; ++q) {
+            const MPix pq = pix[base + q];
+            if (!pq.insec) continue;                      // warp-uniform
+            const double ix = pq.h * inv, iy = pq.k * inv;
+            const double mx = (m[0] * ix + m[1] * iy) * real;
+            const double myy = (m[3] * ix + m[4] * iy) * real;
+            const double mz = (m[6] * ix + m[7] * iy) * real;
+            double vr, vi;
+            fsi_gather<double>(TexSrc{tex}, D, mx, myy, mz, lut, wd, lane, vr, vi);
+            if (lane == q) {
+                Rx = vr;
+                Ry = vi;
+            }
+        }
+        if (lane < cnt) o[base + lane] = make_double2(Rx, Ry);
+    }
+}
+
+cudaError_t launch_secgather(const Match& M, const double* d_mats, long nv, double2* d_out, cudaStream_t s) {
+    if (nv > 0)
+        secgather_kernel<<<(unsigned)nv, FOM_WARPS * 32, 0, s>>>(M.ref_tex, M.D, M.wd, M.d_lut, M.d_pix,
+                                                                 (int)M.h_pix.size(), d_mats, 1.0 / M.real_map,
+                                                                 M.real_map, d_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, float* d_out, cudaStream_t s) {
     if (nrec > 0)
         ctf_rows_kernel<<<(unsigned)nrec, 256, 0, s>>>(d_rec, M.d_pix, (int)M.h_pix.size(), 1.0 / M.real_img, d_out);
@@ -855,14 +907,14 @@ cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, floa
 }
 
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64, const float* ctf_table) {
+                       bool fp64, const float* ctf_table, const double2* sec) {
     FomArgs a{};
     a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf; a.lutd = M.d_lut;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
     a.spec = M.d_spec; a.ctf = ctf_table ? ctf_table : M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
-    a.fom = d_fom; a.cv = d_cv;
+    a.fom = d_fom; a.cv = d_cv; a.sec = sec;
     const size_t words = (NDIV + 1) * MAXW + FOM_WARPS * M.nshell * (1 + MAXORG);
     if (fp64 && sizeof(double) * words > 220 * 1024) return cudaErrorInvalidValue;
     if (ng > 0) {

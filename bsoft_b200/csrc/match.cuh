@@ -40,7 +40,7 @@ struct MHypG {
     int img;
     int norg;
     int ctf;        // row of the CTF table the launch scores with (the image's own: img)
-    int pad;
+    int sec;        // gathered section of the launch's section buffer (when it has one)
 };
 
 
@@ -253,7 +253,10 @@ struct Match {
 // exact FRC scoring of ng hypothesis groups already on the device (match.cu):
 // d_fom / d_cv get MAXORG slots per group; fp64: FP64 gather and sums
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64 = false, const float* ctf_table = nullptr);
+                       bool fp64 = false, const float* ctf_table = nullptr, const double2* sec = nullptr);
+// FP64 section values of nv views (9 doubles each, MHyp's scaled rows) at
+// the figure-of-merit pixels: nv x npix double2
+cudaError_t launch_secgather(const Match& M, const double* d_mats, long nv, double2* d_out, cudaStream_t s);
 // CTF table rows (npix floats each) for nrec records on the device
 cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, float* d_out, cudaStream_t s);
 void group_hypotheses(const std::vector<MHyp>& hyps, std::vector<MHypG>& groups, std::vector<long>& slot);

@@ -355,13 +355,16 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         }
     }
 
-    // rounds: every active particle's views in one launch per pass (defocus
-    // trials, then shift levels); particles are taken in chunks so that a
-    // launch holds at most ~64k groups
+    // rounds: every active particle's 27 views gathered once (FP64 section
+    // values at the figure-of-merit pixels), then scored in one launch per
+    // pass (defocus trials, then shift levels); particles are taken in chunks
+    // so that a launch holds at most ~64k groups and the gathered sections
+    // at most ~1 GB
+    const int npix = (int)M->h_pix.size();
     const long per_b = (long)NVIEW * std::max(nlev, 1);
     const long per_a = dsearch ? (long)NVIEW * (MAX_DEF / 4) : 0;
-    const long chunk = std::max(1L, (long)(65536 / std::max(per_a, per_b)));
-    const int npix = (int)M->h_pix.size();
+    const long sec_views = std::max((long)NVIEW, (long)((1L << 30) / ((long)sizeof(double2) * std::max(npix, 1))));
+    const long chunk = std::max(1L, std::min((long)(65536 / std::max(per_a, per_b)), sec_views / NVIEW));
     cudaStream_t s = M->stream;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
@@ -373,7 +376,22 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
     std::vector<double> go;
     float* d_rctf = nullptr;
     ImgCtf* d_rrec = nullptr;
+    double* d_rmats = nullptr;          // chunk x 27 views, 9 doubles each
+    double2* d_sec = nullptr;           // chunk x 27 gathered sections
+    std::vector<double> mats;
     int rc = BSG_OK;
+    {
+        const long nvmax = std::min(nstart, chunk) * NVIEW;
+        ce = cudaMalloc(&d_rmats, sizeof(double) * 9 * nvmax);
+        if (ce == cudaSuccess) ce = cudaMalloc(&d_sec, sizeof(double2) * (size_t)npix * nvmax);
+        if (ce != cudaSuccess) {
+            cudaFree(d_rmats);
+            cudaFree(d_sec);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return match_fail(BSG_ERR_NOMEM, "bsg_match_refine: %s", cudaGetErrorString(ce));
+        }
+    }
 
     // score `groups` (FP64) with the given CTF table; results in go
     auto score = [&](const float* table) -> int {
@@ -383,7 +401,8 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         go.resize(2 * ng * MAXORG);
         cudaError_t e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaEventRecord(e0, s);
-        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table);
+        if (e == cudaSuccess)
+            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table, d_sec);
         if (e == cudaSuccess) e = cudaEventRecord(e1, s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
@@ -395,16 +414,14 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         ++launches;
         return BSG_OK;
     };
-    auto view_group = [&](const Particle& P, int v) {
-        // Bimage::view stores a twice-copied view; the fit reads it back (one
-        // more) and View::matrix normalises once more
-        double mat[9];
-        view_matrix(renormalised(P.views[v], 3), mat);
+    // group of the t-th active particle's view v (its gathered section t * 27 + v)
+    auto view_group = [&](const Particle& P, long t, int v) {
         MHypG g;
         memset(&g, 0, sizeof(g));
-        match_view_rows(*M, mat, g.m);
+        memcpy(g.m, &mats[9 * (t * NVIEW + v)], sizeof(g.m));
         g.img = (int)P.img;
         g.ctf = (int)P.img;
+        g.sec = (int)(t * NVIEW + v);
         return g;
     };
     // phase_shift_to_origin's slopes, as bsg_match_score forms them
@@ -455,6 +472,32 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
                 owner.push_back(i);
             }
             if (rc != BSG_OK || owner.empty()) break;
+            // the views' matrices and their sections, gathered once
+            mats.assign(9 * owner.size() * NVIEW, 0.0);
+            for (size_t t = 0; t < owner.size(); ++t)
+                for (int v = 0; v < NVIEW; ++v) {
+                    // Bimage::view stores a twice-copied view; the fit reads
+                    // it back (one more) and View::matrix normalises once more
+                    double mat[9];
+                    view_matrix(renormalised(parts[owner[t]].views[v], 3), mat);
+                    match_view_rows(*M, mat, &mats[9 * (t * NVIEW + v)]);
+                }
+            {
+                const long nv = (long)owner.size() * NVIEW;
+                cudaError_t e = cudaMemcpyAsync(d_rmats, mats.data(), sizeof(double) * 9 * nv, cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+                if (e == cudaSuccess) e = launch_secgather(*M, d_rmats, nv, d_sec, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) {
+                    rc = match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(e));
+                    break;
+                }
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tsum += ms;
+                ++launches;
+            }
             // pass A: the fit's defocus trials at the original origin
             // (img_fit_in_recip_space_grid :895-911)
             for (long i : owner)
@@ -466,11 +509,11 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
             if (dsearch) {
                 groups.clear();
                 gfirst.clear();
-                for (long i : owner) {
-                    Particle& P = parts[i];
+                for (size_t t = 0; t < owner.size(); ++t) {
+                    Particle& P = parts[owner[t]];
                     gfirst.push_back((long)groups.size());
                     for (int v = 0; v < NVIEW; ++v) {
-                        MHypG g = view_group(P, v);
+                        MHypG g = view_group(P, (long)t, v);
                         g.norg = 1;
                         g.sx[0] = slope(P.ox);
                         g.sy[0] = slope(P.oy);
@@ -501,10 +544,10 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
             // pass B: every shift level of every view (:914-944), with the
             // defocus each view's trials chose
             groups.clear();
-            for (long i : owner) {
-                Particle& P = parts[i];
+            for (size_t t = 0; t < owner.size(); ++t) {
+                Particle& P = parts[owner[t]];
                 for (int v = 0; v < NVIEW; ++v) {
-                    MHypG g = view_group(P, v);
+                    MHypG g = view_group(P, (long)t, v);
                     if (dsearch) g.ctf = (int)(P.row0 + P.vk[v]);
                     for (int k = 0; k < nlev; ++k) {
                         const Level& L = P.levels[k];
@@ -574,6 +617,8 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
     }
     cudaFree(d_rctf);
     cudaFree(d_rrec);
+    cudaFree(d_rmats);
+    cudaFree(d_sec);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != BSG_OK) return rc;
