@@ -17,11 +17,12 @@
 // walks the pixels of each particle that reaches it, in particle order.
 //
 // Conflict-free lanes: the pixels of a particle's footprint are visited on
-// a lattice of spacing L = ceil(sqrt(3)/step) pixels (step = voxels per
-// pixel), L^2 phases one after another.  Two lattice points are at least
-// sqrt(3) voxels apart in the map, so their base voxels floor(m) differ in
-// some axis, and for any one corner offset the lanes of a warp touch
-// distinct voxels: a plain read-modify-write of shared memory is exact.
+// a lattice whose points are at least sqrt(3) voxels apart in the map (a
+// square lattice of L = ceil(sqrt(3)/step) pixels, step = voxels per pixel,
+// or at step 0.5 the 12-phase lattice spanned by (4, 0) and (2, 3) pixels),
+// one phase after another.  Two such points have different base voxels
+// floor(m), so for any one corner offset the lanes of a warp touch distinct
+// voxels: a plain read-modify-write of shared memory is exact.
 // The order of every voxel's sum (particle, alias, phase, lattice point,
 // corner) is fixed, so results are bitwise reproducible.  Tiles are visited
 // heaviest first (nearest to the Fourier origin, where every particle's
@@ -197,25 +198,35 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     const int k_lo = max((int)ceil(vc - hv), -hf), k_hi = min((int)floor(vc + hv), hf - 1);
     const int h_lo = max((int)ceil(uc - hu), -hf), h_hi = min((int)floor(uc + hu), hf - 1);
     if (k_lo > k_hi || h_lo > h_hi) return;
-    // lattice spacing: points L apart are >= sqrt(3) voxels apart
-    const int L = max(1, (int)ceilf(1.7320508f * P.inv_step));
+    // Conflict-free lattice: two points of one phase are >= sqrt(3) voxels
+    // apart.  Square lattice L x L pixels (L = ceil(sqrt(3)/step)), or, where
+    // it has fewer phases, the lattice spanned by (4, 0) and (2, 3) pixels
+    // (shortest vector sqrt(13) pixels; 12 phases instead of 16 at step 0.5).
+    // Row j of phase (ph, pk) is k = k_lo + pk + Lk j, its points
+    // h = h_lo + ph + sh j + Lh i.
+    int Lh, Lk, sh;
+    {
+        const int L = max(1, (int)ceilf(1.7320508f * P.inv_step));
+        if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f) { Lh = 4; Lk = 3; sh = 2; }
+        else { Lh = L; Lk = L; sh = 0; }
+    }
     // per-axis 1 / ad (0 when the axis does not vary along h)
     double ia[3];
     for (int i = 0; i < 3; ++i) ia[i] = fabs(P.ad[i]) > 1e-12 ? 1.0 / P.ad[i] : 0.0;
-    for (int pk = 0; pk < L; ++pk) {
+    for (int pk = 0; pk < Lk; ++pk) {
         const int k0 = k_lo + pk;
         if (k0 > k_hi) break;
-        const int nrows = (k_hi - k0) / L + 1;
-        for (int ph = 0; ph < L; ++ph) {
-            const int h0 = h_lo + ph;
-            if (h0 > h_hi) break;
+        const int nrows = (k_hi - k0) / Lk + 1;
+        for (int ph = 0; ph < Lh; ++ph) {
+            if (sh == 0 && h_lo + ph > h_hi) break;
             for (int jb = 0; jb < nrows; jb += 32) {
-                // lane j: exact lattice range of row k = k0 + L (jb + j)
+                // lane j: exact lattice range of row k = k0 + Lk (jb + j)
                 const int j = jb + lane;
-                int istart = 0, cnt = 0, k = 0;
+                int hfirst = 0, cnt = 0, k = 0;
                 if (j < nrows) {
-                    k = k0 + L * j;
-                    double hl = h0, hh = h_hi;
+                    k = k0 + Lk * j;
+                    const int h0 = h_lo + ph + sh * j;
+                    double hl = h_lo, hh = h_hi;
                     bool empty = false;
                     for (int i = 0; i < 3; ++i) {
                         const double base = k * P.bd[i];
@@ -229,9 +240,9 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                         }
                     }
                     if (!empty && hl <= hh) {
-                        // lattice h = h0 + L i inside [hl, hh]
-                        const int i0 = (int)ceil((hl - h0) / L), i1 = (int)floor((hh - h0) / L);
-                        if (i1 >= i0) { istart = i0; cnt = i1 - i0 + 1; }
+                        // lattice h = h0 + Lh i inside [hl, hh]
+                        const int i0 = (int)ceil((hl - h0) / Lh), i1 = (int)floor((hh - h0) / Lh);
+                        if (i1 >= i0) { hfirst = h0 + Lh * i0; cnt = i1 - i0 + 1; }
                     }
                 }
                 // exclusive scan of the row counts
@@ -243,7 +254,7 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                 }
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
                 s_row[lane] = incl;                        // inclusive end of row j
-                s_row[32 + lane] = istart;
+                s_row[32 + lane] = hfirst;
                 s_row[64 + lane] = k;
                 __syncwarp();
                 for (int t0 = 0; t0 < total; t0 += 32) {
@@ -255,7 +266,7 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                         if (s_row[r + sft - 1] <= t) r += sft;
                     r = min(r, 31);
                     const int before = r ? s_row[r - 1] : 0;
-                    const int h = h0 + L * (s_row[32 + r] + (t - before));
+                    const int h = s_row[32 + r] + Lh * (t - before);
                     pixel<FOM, GATE, TX, TY, TZ>(a, P, S, A, ox, oy, oz, h, s_row[64 + r], act);
                 }
                 __syncwarp();
