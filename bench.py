@@ -42,7 +42,10 @@ the last search step refined from their best search pose by the reference's
 grid refinement (img_refine_grid: 27 views, 2 -> 0.5 degrees; 3 x 3 origins,
 0.4 -> 0.1 pixel; defocus search +-5 x 100 angstrom, as brefine -defocus),
 scored in FP64 on the GPU; its CPU baseline is the reference's own
-img_refine_grid on one of those particles (oracle/_ref/refine_probe).
+img_refine_grid on one of those particles at a single angular level
+(oracle/_ref/refine_probe, one thread), timed per hypothesis and
+extrapolated to the GPU leg's hypotheses per particle; the GPU refines the
+same particle with the same steps and the two results are compared.
 
 `--impl reference` times only the reference CPU implementation (rank 0).
 Multi-GPU (`torchrun --nproc-per-node N`): each rank reconstructs its own
@@ -245,9 +248,10 @@ def search_views_mats(npsi: int = SEARCH_PSI):
 REFINE_ALPHA, REFINE_ACC, REFINE_STEP, REFINE_SACC, REFINE_DEF = 2.0, 0.5, 0.4, 0.1, 100.0
 
 
-def refine_reference_sample(sw, start_row, ctf_row):
+def refine_reference_sample(sw, start_row, ctf_row, alpha=REFINE_ALPHA, accuracy=REFINE_ACC):
     """The reference's img_refine_grid (refine_probe, one thread) on one
-    particle of the search workload with the bench's parameters."""
+    particle of the search workload with the bench's shift and defocus
+    steps and the given angular steps (degrees)."""
     import oracle
     from bsoft_b200.io import mrc
     exe = oracle.ref_binary("refine_probe")
@@ -262,13 +266,14 @@ def refine_reference_sample(sw, start_row, ctf_row):
     t0 = time.perf_counter()
     r = subprocess.run([exe, os.path.join(d, "ref.mrc"), os.path.join(d, "p.mrcs"), repr(SEARCH_PIXEL),
                         repr(SEARCH_RES), os.path.join(d, "start.txt"), os.path.join(d, "ctf.txt"),
-                        repr(REFINE_ALPHA), repr(REFINE_ACC), repr(REFINE_STEP), repr(REFINE_SACC), "0",
+                        repr(alpha), repr(accuracy), repr(REFINE_STEP), repr(REFINE_SACC), "0",
                         repr(REFINE_DEF)], capture_output=True, text=True)
     dt = time.perf_counter() - t0
     if r.returncode != 0:
         return None, None, f"refine_probe failed: {r.stderr[-200:]}"
     out = np.array([float(t) for t in r.stdout.split()])
-    return dt, out, f"1 particle (img_refine_grid with the defocus search), one thread, wall {dt:.1f} s including map preparation"
+    return dt, out, (f"1 particle, img_refine_grid with the defocus search at one angular level "
+                     f"({alpha} degrees), one thread, wall {dt:.1f} s including map preparation")
 
 
 def search_reference_sample(sw, n_views: int = 160):
@@ -538,15 +543,28 @@ def search_leg(args, local, dist, world, rank, torch):
         rvalue = R / (refine["ms"] / 1e3)
         rcpu = None
         if world == 1 and not args.no_cpu_baseline:
+            # a bounded sample: one particle at a single angular level (alpha =
+            # accuracy), timed per hypothesis and extrapolated to the GPU leg's
+            # hypotheses per particle; the GPU refines the same particle with the
+            # same steps for a bitwise comparison
             ctf_row = [sw["spec"].volt, *meta["coefs"][j * B][:5], 1]
             row = start[0].copy()
             row[0] = j * B                         # the image's index in the workload's stack
-            dt, rref, sample = refine_reference_sample(sw, row, ctf_row)
+            dt, rref, sample = refine_reference_sample(sw, row, ctf_row, REFINE_ALPHA, REFINE_ALPHA)
             if dt is not None:
-                rcpu = {"value": round(1.0 / dt, 5), "unit": "particles/s", "cores": 1, "kind": "reference",
-                        "sample": sample,
-                        "same_result_as_gpu": bool(np.abs(rref[:6] - rout[0, :6]).max() < 1e-9
-                                                   and rref[8] == rout[0, 8]),
+                m2 = Matcher(n=SEARCH_BOX, map=SEARCH_BOX, map_sampling=SEARCH_PIXEL, pixel=SEARCH_PIXEL,
+                             hi_res=SEARCH_RES, device=local)
+                m2.set_reference(sw["volume"], (SEARCH_BOX // 2,) * 3)
+                m2.set_images(sw["images"][j * B:j * B + 1], ctf[j * B:j * B + 1])
+                a1 = REFINE_ALPHA * math.pi / 180.0
+                g1 = m2.refine(start[:1], a1, a1, REFINE_STEP, REFINE_SACC, REFINE_DEF)[0]
+                m2.close()
+                per_hyp = dt / max(1.0, rref[8])
+                rcpu = {"value": round(1.0 / (per_hyp * float(rout[:, 8].mean())), 5), "unit": "particles/s",
+                        "cores": 1, "kind": "reference", "sample": sample,
+                        "seconds_per_hypothesis": per_hyp,
+                        "extrapolation": "mean hypotheses per particle of the GPU leg x measured seconds per hypothesis",
+                        "same_result_as_gpu": bool(np.abs(rref[:6] - g1[:6]).max() < 1e-9 and rref[8] == g1[8]),
                         "reference_hypotheses": int(rref[8])}
             else:
                 rcpu = {"value": None, "unit": "particles/s", "cores": 1, "kind": "reference", "sample": sample}
