@@ -456,27 +456,6 @@ def search_leg(args, local, dist, world, rank, torch):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
-    # ---- grid refinement of the last step's best poses (brefine -defocus)
-    refine = None
-    if "refine" in args.legs:
-        j, res = results[-1]
-        R = min(args.refine_images, B)
-        best = res[:R, 0, 0].astype(int)
-        start = np.column_stack([np.arange(R), pviews[best], origins[res[:R, 0, 1].astype(int)]])
-        m.set_images(dev[j], ctf[j * B:(j + 1) * B])
-        # radians as the reference's CLI converts degrees (atof(x) * M_PI / 180.0)
-        rargs = (REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP, REFINE_SACC, REFINE_DEF)
-        m.refine(start[:16], *rargs)                                # warm-up
-        m.reset_stats()
-        barrier()
-        ev0.record(s)
-        rout = m.refine(start, *rargs)
-        ev1.record(s)
-        torch.cuda.synchronize()
-        barrier()
-        rms = ev0.elapsed_time(ev1)
-        refine = {"ms": rms, "out": rout, "start": start, "j": j, "stats": m.stats(), "R": R}
-
     # ---- learned proposal + local search on the same images
     learned = None
     if "learned" in args.legs:
@@ -507,6 +486,27 @@ def search_leg(args, local, dist, world, rank, torch):
             lms = float(t.item())
         learned = {"ms": lms, "stats": lst, "results": lres, "train": train_info}
         net.close()
+    # ---- grid refinement of the last step's best poses (brefine -defocus)
+    refine = None
+    if "refine" in args.legs:
+        j, res = results[-1]
+        R = min(args.refine_images, B)
+        best = res[:R, 0, 0].astype(int)
+        start = np.column_stack([np.arange(R), pviews[best], origins[res[:R, 0, 1].astype(int)]])
+        m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+        # radians as the reference's CLI converts degrees (atof(x) * M_PI / 180.0)
+        rargs = (REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP, REFINE_SACC, REFINE_DEF)
+        m.refine(start[:16], *rargs)                                # warm-up
+        m.reset_stats()
+        barrier()
+        ev0.record(s)
+        rout = m.refine(start, *rargs)
+        ev1.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        rms = ev0.elapsed_time(ev1)
+        refine = {"ms": rms, "out": rout, "start": start, "j": j, "stats": m.stats(), "R": R}
+
     m.close()
     if rank != 0:
         return None
