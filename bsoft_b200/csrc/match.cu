@@ -726,6 +726,7 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
                     M->d_spec, M->d_ctf, M->d_dsum, M->d_real, M->d_work, M->d_scale, M->d_shift, M->d_ictf,
                     M->d_hyp, M->d_out, M->d_full, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
                     M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_rots, M->d_gA, M->d_slopes,
+                    M->d_lprop, M->d_lorg, M->d_nlorg, M->d_lcand, M->d_lcount,
                     M->d_status};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);

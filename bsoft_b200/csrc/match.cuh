@@ -246,6 +246,14 @@ struct Match {
     double2* d_slopes = nullptr;       // per trial origin
     size_t slope_elems = 0;
     int* d_status = nullptr;
+    // local search scratch (grow-only)
+    float* d_lprop = nullptr;          // nimg x 11 proposals
+    int* d_lorg = nullptr;             // nimg x LOCAL_MAXO trial origins
+    int* d_nlorg = nullptr;            // nimg
+    long lscr_img = 0;
+    int* d_lcand = nullptr;            // batch x LOCAL_MAXC selected sections
+    int* d_lcount = nullptr;           // batch
+    long lscr_nb = 0;
     bsg_match_stats sstats{};
 };
 

@@ -701,21 +701,36 @@ static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<dou
     if (e == cudaSuccess) e = cudaMemcpyAsync(cscore.data(), M->d_cscore, sizeof(float) * ncand, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return e;
-    std::vector<MHyp> hv;
-    std::vector<long> hidx;
-    hv.reserve(ncand);
-    for (long c = 0; c < ncand; ++c) {
-        if (csec[c] < 0) continue;
-        MHyp hh = M->h_secs[csec[c]];
-        hh.sx = sl[corg[c]].x;
-        hh.sy = sl[corg[c]].y;
-        hh.img = (int)(c / topk);
-        hv.push_back(hh);
-        hidx.push_back(c);
-    }
+    // groups of one image and one section (up to MAXORG origins), built per
+    // image from the section index (the candidates of an image are adjacent)
     std::vector<MHypG> groups;
-    std::vector<long> slot;
-    group_hypotheses(hv, groups, slot);
+    std::vector<int> gsec;
+    std::vector<long> cslot(ncand, -1);
+    groups.reserve(ncand);
+    for (long i = 0; i < M->nimg; ++i) {
+        const size_t g0 = groups.size();
+        for (int t = 0; t < topk; ++t) {
+            const long c = i * topk + t;
+            if (csec[c] < 0) continue;
+            size_t g = groups.size();
+            for (size_t q = g0; q < groups.size(); ++q)
+                if (gsec[q] == csec[c] && groups[q].norg < MAXORG) { g = q; break; }
+            if (g == groups.size()) {
+                MHypG ng;
+                memset(&ng, 0, sizeof(ng));
+                memcpy(ng.m, M->h_secs[csec[c]].m, sizeof(ng.m));
+                ng.img = (int)i;
+                ng.ctf = (int)i;
+                groups.push_back(ng);
+                gsec.push_back(csec[c]);
+            }
+            MHypG& G = groups[g];
+            G.sx[G.norg] = sl[corg[c]].x;
+            G.sy[G.norg] = sl[corg[c]].y;
+            cslot[c] = (long)g * MAXORG + G.norg;
+            G.norg++;
+        }
+    }
     const long ng = (long)groups.size();
     *ngroups = ng;
     std::vector<double> cf(2 * ncand, 0.0);
@@ -736,9 +751,10 @@ static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<dou
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (e != cudaSuccess) return e;
-        for (size_t k = 0; k < hidx.size(); ++k) {
-            cf[hidx[k]] = go[slot[k]];
-            cf[ncand + hidx[k]] = go[ng * MAXORG + slot[k]];
+        for (long c = 0; c < ncand; ++c) {
+            if (cslot[c] < 0) continue;
+            cf[c] = go[cslot[c]];
+            cf[ncand + c] = go[ng * MAXORG + cslot[c]];
         }
     }
     for (long i = 0; i < M->nimg; ++i) {
@@ -1083,14 +1099,29 @@ extern "C" int bsg_match_search_local(bsg_match* h, const float* proposals, doub
         if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
         M->slope_elems = norigin;
     }
-    float* d_prop = nullptr;
-    int *d_lorg = nullptr, *d_nlorg = nullptr, *d_cand = nullptr, *d_count = nullptr;
-    e = cudaMalloc(&d_prop, sizeof(float) * prop.size());
-    if (e == cudaSuccess) e = cudaMalloc(&d_lorg, sizeof(int) * lorg.size());
-    if (e == cudaSuccess) e = cudaMalloc(&d_nlorg, sizeof(int) * nimg);
-    if (e == cudaSuccess) e = cudaMalloc(&d_cand, sizeof(int) * nb * LOCAL_MAXC);
-    if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(int) * nb);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_prop, prop.data(), sizeof(float) * prop.size(), cudaMemcpyHostToDevice, s);
+    // scratch kept in the context (grow-only): no allocation per call
+    if (M->lscr_img < nimg) {
+        cudaFree(M->d_lprop); cudaFree(M->d_lorg); cudaFree(M->d_nlorg);
+        M->d_lprop = nullptr; M->d_lorg = nullptr; M->d_nlorg = nullptr;
+        M->lscr_img = 0;
+        e = cudaMalloc(&M->d_lprop, sizeof(float) * 11 * nimg);
+        if (e == cudaSuccess) e = cudaMalloc(&M->d_lorg, sizeof(int) * LOCAL_MAXO * nimg);
+        if (e == cudaSuccess) e = cudaMalloc(&M->d_nlorg, sizeof(int) * nimg);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
+        M->lscr_img = nimg;
+    }
+    if (M->lscr_nb < nb) {
+        cudaFree(M->d_lcand); cudaFree(M->d_lcount);
+        M->d_lcand = nullptr; M->d_lcount = nullptr;
+        M->lscr_nb = 0;
+        e = cudaMalloc(&M->d_lcand, sizeof(int) * nb * LOCAL_MAXC);
+        if (e == cudaSuccess) e = cudaMalloc(&M->d_lcount, sizeof(int) * nb);
+        if (e != cudaSuccess) return match_fail(BSG_ERR_NOMEM, "bsg_match_search_local: %s", cudaGetErrorString(e));
+        M->lscr_nb = nb;
+    }
+    float* d_prop = M->d_lprop;
+    int *d_lorg = M->d_lorg, *d_nlorg = M->d_nlorg, *d_cand = M->d_lcand, *d_count = M->d_lcount;
+    e = cudaMemcpyAsync(d_prop, prop.data(), sizeof(float) * prop.size(), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_lorg, lorg.data(), sizeof(int) * lorg.size(), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_nlorg, nlorg.data(), sizeof(int) * nimg, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(M->d_slopes, sl.data(), sizeof(double2) * norigin, cudaMemcpyHostToDevice, s);
@@ -1122,7 +1153,6 @@ extern "C" int bsg_match_search_local(bsg_match* h, const float* proposals, doub
     cudaEventElapsedTime(&lms, ev[0], ev[1]);
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
-    cudaFree(d_prop); cudaFree(d_lorg); cudaFree(d_nlorg); cudaFree(d_cand); cudaFree(d_count);
     if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_search_local: %s", cudaGetErrorString(e));
     float tres = 0;
     long ng = 0;
