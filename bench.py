@@ -652,6 +652,7 @@ def main():
     ap.add_argument("--search-psi", type=int, default=SEARCH_PSI)
     ap.add_argument("--legs", default="insert,search,refine,learned")
     ap.add_argument("--refine-images", type=int, default=512)
+    ap.add_argument("--tile-shape", type=int, default=-1, help="gridding tile shape (default: autotuned)")
     ap.add_argument("--train-images", type=int, default=200000)
     ap.add_argument("--train-epochs", type=float, default=8.0)
     ap.add_argument("--local-radius", type=float, default=10.0)
@@ -699,10 +700,14 @@ def main():
             if dist is not None:
                 dist.barrier()
 
-        # ---- tile shape from the project's autotuner (untimed, on warm-up data)
-        rec = Reconstructor(plan, batch=B, device=local)
-        shape, shape_ms = rec.autotune(dev[0][: min(B, 512)], P[: min(B, 512)])
-        rec.close()
+        # ---- tile shape from the project's autotuner (untimed, on warm-up
+        # data), or the one given (profiling runs fix it)
+        if args.tile_shape >= 0:
+            shape, shape_ms = args.tile_shape, []
+        else:
+            rec = Reconstructor(plan, batch=B, device=local)
+            shape, shape_ms = rec.autotune(dev[0][: min(B, 512)], P[: min(B, 512)])
+            rec.close()
 
         # ---- value: device-resident inputs
         rec = Reconstructor(plan, batch=B, device=local)
