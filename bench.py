@@ -786,8 +786,13 @@ def main():
         per_particle = 22.0 * BOX * BOX
         avg_launch_ms = ins_ms / max(1, ins_launch)
         achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
+        # DRAM bytes per launch from one ncu capture of this configuration (8^3
+        # tiles, 2,000 particles per launch: profiles/insert_kernel_batched-
+        # insertion-256.md); other configurations were not captured
+        traffic = 13.206e9 if (int(shape) == 0 and B == 2000 and BOX == 256) else None
         roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
                 "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
                 "algorithmic_bytes_per_particle": per_particle,
                 "fft2d_ms_per_step": round(fft_ms / args.steps, 3), "tile_shape": int(shape),
