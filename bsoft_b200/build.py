@@ -34,21 +34,25 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
 
 
-HOST = os.path.join(HERE, "host", "breconstruct.cpp")
-HOST_OUT = os.path.join(HERE, "_build", "breconstruct")
+HOSTDIR = os.path.join(HERE, "host")
+HOST_PROGRAMS = ("breconstruct", "brefine")
 
 
-def build_host(force: bool = False) -> str:
-    """The C++ drop-in breconstruct over libbsgpu (bsoft_b200/host)."""
-    if not force and os.path.exists(HOST_OUT) and os.path.getmtime(HOST_OUT) >= max(
-            os.path.getmtime(HOST), os.path.getmtime(OUT)):
-        return HOST_OUT
+def build_host(force: bool = False) -> list:
+    """The C++ drop-in executables over libbsgpu (bsoft_b200/host)."""
     cxx = shutil.which("g++") or "g++"
-    tmp = HOST_OUT + ".tmp"
-    subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"), HOST,
-                    "-L", os.path.dirname(OUT), "-lbsgpu", "-Wl,-rpath,$ORIGIN", "-o", tmp], check=True)
-    os.replace(tmp, HOST_OUT)
-    return HOST_OUT
+    out = []
+    for name in HOST_PROGRAMS:
+        src = os.path.join(HOSTDIR, name + ".cpp")
+        exe = os.path.join(os.path.dirname(OUT), name)
+        deps = [src, os.path.join(HOSTDIR, "project.hpp"), OUT, os.path.join(HERE, "..", "include", "bsgpu.h")]
+        if force or not os.path.exists(exe) or os.path.getmtime(exe) < max(os.path.getmtime(d) for d in deps):
+            tmp = exe + ".tmp"
+            subprocess.run([cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(HERE, "..", "include"), src,
+                            "-L", os.path.dirname(OUT), "-lbsgpu", "-Wl,-rpath,$ORIGIN", "-o", tmp], check=True)
+            os.replace(tmp, exe)
+        out.append(exe)
+    return out
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

@@ -21,6 +21,7 @@
 // Bimage::check_resolution (Bimage.cpp:633-648) and the per-particle set-up
 // of particle_reconstruct (mg_reconstruct.cpp:143-212).
 #include "bsgpu.h"
+#include "project.hpp"
 
 #include <cmath>
 #include <cstdint>
@@ -35,370 +36,7 @@
 
 namespace {
 
-// ---------------------------------------------------------------- STAR
-struct StarLoop {
-    std::vector<std::string> tags;
-    std::vector<std::vector<std::string>> rows;
-    int index(const std::string& t) const {
-        for (size_t i = 0; i < tags.size(); ++i)
-            if (tags[i] == t) return (int)i;
-        return -1;
-    }
-};
-
-struct StarBlock {
-    std::string name;
-    std::map<std::string, std::string> items;
-    std::vector<StarLoop> loops;
-    bool has(const std::string& t) const { return items.count(t) > 0; }
-    double real(const std::string& t, double def = 0) const {
-        auto it = items.find(t);
-        if (it == items.end()) return def;
-        char* end = nullptr;
-        const double v = strtod(it->second.c_str(), &end);
-        return end == it->second.c_str() ? def : v;
-    }
-    long integer(const std::string& t, long def = 0) const { return (long)real(t, (double)def); }
-    const StarLoop* loop_with(const std::string& t) const {
-        for (auto& l : loops)
-            if (l.index(t) >= 0) return &l;
-        return nullptr;
-    }
-};
-
-// whitespace-separated tokens; single or double quotes group
-std::vector<std::string> tokens(const std::string& line) {
-    std::vector<std::string> out;
-    size_t i = 0;
-    while (i < line.size()) {
-        while (i < line.size() && isspace((unsigned char)line[i])) ++i;
-        if (i >= line.size()) break;
-        if (line[i] == '\'' || line[i] == '"') {
-            const char q = line[i++];
-            size_t j = line.find(q, i);
-            if (j == std::string::npos) j = line.size();
-            out.push_back(line.substr(i, j - i));
-            i = j + 1;
-        } else {
-            size_t j = i;
-            while (j < line.size() && !isspace((unsigned char)line[j])) ++j;
-            out.push_back(line.substr(i, j - i));
-            i = j;
-        }
-    }
-    return out;
-}
-
-std::vector<StarBlock> read_star(const std::string& path) {
-    std::ifstream f(path);
-    if (!f) throw std::runtime_error("cannot open " + path);
-    std::vector<StarBlock> blocks;
-    StarLoop* loop = nullptr;
-    bool in_header = false;
-    std::string raw;
-    while (std::getline(f, raw)) {
-        size_t a = raw.find_first_not_of(" \t\r\n");
-        const std::string line = a == std::string::npos ? "" : raw.substr(a, raw.find_last_not_of(" \t\r\n") - a + 1);
-        if (line.empty() || line[0] == '#') {
-            if (line.empty() && loop && !in_header && !loop->rows.empty()) loop = nullptr;
-            continue;
-        }
-        if (line.compare(0, 5, "data_") == 0) {
-            blocks.push_back(StarBlock{line.substr(5), {}, {}});
-            loop = nullptr;
-            continue;
-        }
-        if (blocks.empty()) continue;
-        StarBlock& cur = blocks.back();
-        if (line.compare(0, 5, "loop_") == 0) {
-            cur.loops.emplace_back();
-            loop = &cur.loops.back();
-            in_header = true;
-            continue;
-        }
-        if (line[0] == '_') {
-            if (loop && in_header) {
-                loop->tags.push_back(tokens(line)[0].substr(1));
-                continue;
-            }
-            loop = nullptr;
-            auto t = tokens(line);
-            cur.items[t[0].substr(1)] = t.size() > 1 ? t[1] : "";
-            continue;
-        }
-        if (loop) {
-            in_header = false;
-            auto t = tokens(line);
-            if (t.size() == loop->tags.size()) loop->rows.push_back(t);
-        }
-    }
-    return blocks;
-}
-
-// ---------------------------------------------------------------- MRC
-struct MrcHeader {
-    int nx = 0, ny = 0, nz = 0, mode = 0, mx = 0, my = 0, mz = 0, nsymbt = 0, nversion = 0;
-    float cell[3] = {0, 0, 0}, origin[3] = {0, 0, 0};
-    double sampling(int i) const {
-        const int m = i == 0 ? (mx ? mx : 1) : i == 1 ? (my ? my : 1) : (mz ? mz : 1);
-        return cell[i] ? cell[i] / m : 1.0;
-    }
-    long images() const { return (nversion >= 20140 && nversion <= 20209 && mz) ? nz / mz : nz; }
-    // rwMRC.cpp:195: image origin (pixels) = -origin field / sampling
-    double image_origin(int i) const { return -origin[i] / sampling(i); }
-};
-
-MrcHeader read_mrc_header(const std::string& path) {
-    std::ifstream f(path, std::ios::binary);
-    unsigned char raw[1024];
-    if (!f.read((char*)raw, 1024)) throw std::runtime_error(path + ": short MRC header");
-    MrcHeader h;
-    int32_t iv[10];
-    memcpy(iv, raw, 40);
-    h.nx = iv[0]; h.ny = iv[1]; h.nz = iv[2]; h.mode = iv[3]; h.mx = iv[7]; h.my = iv[8]; h.mz = iv[9];
-    memcpy(h.cell, raw + 40, 12);
-    memcpy(&h.nsymbt, raw + 92, 4);
-    memcpy(&h.nversion, raw + 108, 4);
-    memcpy(h.origin, raw + 196, 12);
-    if (h.nx < 1 || h.ny < 1 || h.nz < 1 || h.mode < 0 || h.mode > 16)
-        throw std::runtime_error(path + ": not a valid little-endian MRC image");
-    return h;
-}
-
-// float32 images [first, first + count) of a mode-2 stack
-void read_mrc_images(const std::string& path, const MrcHeader& h, long first, long count, float* out) {
-    if (h.mode != 2) throw std::runtime_error(path + ": only mode 2 (float32) stacks are supported");
-    const long per = (long)h.nx * h.ny * ((h.nversion >= 20140 && h.mz) ? h.mz : 1);
-    if (first < 0 || first + count > h.images()) throw std::runtime_error(path + ": image index outside the stack");
-    std::ifstream f(path, std::ios::binary);
-    f.seekg(1024 + (long)h.nsymbt + first * per * 4);
-    if (!f.read((char*)out, sizeof(float) * per * count)) throw std::runtime_error(path + ": truncated data");
-}
-
-void write_mrc_volume(const std::string& path, const float* v, int N, double sampling, double origin) {
-    unsigned char hdr[1024];
-    memset(hdr, 0, sizeof(hdr));
-    const int32_t iv[10] = {N, N, N, 2, 0, 0, 0, N, N, N};
-    memcpy(hdr, iv, 40);
-    const float cell[6] = {(float)(N * sampling), (float)(N * sampling), (float)(N * sampling), 90.f, 90.f, 90.f};
-    memcpy(hdr + 40, cell, 24);
-    const int32_t axes[3] = {1, 2, 3};
-    memcpy(hdr + 64, axes, 12);
-    const size_t n3 = (size_t)N * N * N;
-    double mn = v[0], mx = v[0], sum = 0, sum2 = 0;
-    for (size_t i = 0; i < n3; ++i) {
-        mn = std::fmin(mn, v[i]);
-        mx = std::fmax(mx, v[i]);
-        sum += v[i];
-        sum2 += (double)v[i] * v[i];
-    }
-    const double avg = sum / n3, rms = std::sqrt(std::fmax(0.0, sum2 / n3 - avg * avg));
-    const float st[3] = {(float)mn, (float)mx, (float)avg};
-    memcpy(hdr + 76, st, 12);
-    const int32_t ver = 20140;
-    memcpy(hdr + 108, &ver, 4);
-    const float org[3] = {(float)(-origin * sampling), (float)(-origin * sampling), (float)(-origin * sampling)};
-    memcpy(hdr + 196, org, 12);
-    memcpy(hdr + 208, "MAP ", 4);
-    const unsigned char stamp[4] = {0x44, 0x44, 0, 0};
-    memcpy(hdr + 212, stamp, 4);
-    const float frms = (float)rms;
-    memcpy(hdr + 216, &frms, 4);
-    std::ofstream f(path, std::ios::binary);
-    f.write((const char*)hdr, 1024);
-    f.write((const char*)v, sizeof(float) * n3);
-    if (!f) throw std::runtime_error("cannot write " + path);
-}
-
-// ---------------------------------------------------------------- geometry and CTF
-const double TRIG = 1e-30;   // TRIGPRECISION / SMALLFLOAT
-
-// angle_set_negPI_to_PI (bsoft/src/util/utilities.cpp:606-615)
-double angle_neg_pi_to_pi(double a) {
-    if (!std::isfinite(a)) return 0;
-    const long n = (long)(a / M_PI);
-    return a - (double)(n + n % 2) * M_PI;
-}
-
-// View::normalize + View::quaternion + Matrix3(Quaternion)
-// (View.h:110-116, 131-157; Matrix3.h:21-42), row-major
-void view_matrix(double x, double y, double z, double a, double* m) {
-    const double size = std::sqrt(x * x + y * y + z * z);
-    if (size < TRIG) { x = 0; y = 0; z = 1; }
-    else { x /= size; y /= size; z /= size; }
-    if (std::fabs(x) < TRIG) x = 0;
-    if (std::fabs(y) < TRIG) y = 0;
-    if (std::fabs(z) < TRIG) z = 0;
-    a = angle_neg_pi_to_pi(a);
-    if (std::fabs(a) < TRIG) a = 0;
-    const double ang = a / 2.0, ca = std::cos(ang), sa = std::sin(ang), z1 = z + 1.0;
-    double q[4] = {ca, 0, 0, sa};
-    if (z < 1.0 - TRIG) {
-        if (z <= TRIG - 1.0) {
-            q[0] = 0; q[1] = sa; q[2] = ca; q[3] = 0;
-        } else {
-            const double f1 = std::sqrt(z1 / 2.0), f2 = std::sqrt(1.0 / (2 * z1));
-            q[0] = f1 * ca; q[1] = f2 * (x * sa - y * ca); q[2] = f2 * (x * ca + y * sa); q[3] = f1 * sa;
-        }
-    }
-    for (double& t : q)
-        if (std::fabs(t) < TRIG) t = 0;
-    m[0] = q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3];
-    m[1] = 2 * q[1] * q[2] - 2 * q[0] * q[3];
-    m[2] = 2 * q[1] * q[3] + 2 * q[0] * q[2];
-    m[3] = 2 * q[1] * q[2] + 2 * q[0] * q[3];
-    m[4] = q[0] * q[0] - q[1] * q[1] + q[2] * q[2] - q[3] * q[3];
-    m[5] = 2 * q[2] * q[3] - 2 * q[0] * q[1];
-    m[6] = 2 * q[1] * q[3] - 2 * q[0] * q[2];
-    m[7] = 2 * q[2] * q[3] + 2 * q[0] * q[1];
-    m[8] = q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3];
-    for (int i = 0; i < 9; ++i) {
-        if (std::fabs(m[i]) < 1e-12) m[i] = 0;
-        m[i] = std::fmin(1.0, std::fmax(-1.0, m[i]));
-    }
-}
-
-// CTFparam (bsoft/include/ctf.h): the aberration weights the C ABI takes
-struct Ctf {
-    double volt = 300000, cs = 2.7e7, amp_shift = 0, defocus = 20000, def_dev = 0, ast_angle = 0;
-    double btx = 0, bty = 0;
-    void coefficients(double* c) const {
-        // relativistic electron wavelength in angstrom (ctf.h:309-317)
-        const double h = 6.626070e-34, me = 9.109384e-31, e = 1.602177e-19, cl = 299792458.0;
-        const double wl = volt > 0 ? h * 1e10 / std::sqrt(2.0 * me * e * volt * (1.0 + e * volt / (2.0 * me * cl * cl))) : 0;
-        const double t1 = M_PI / 2 * wl * wl * wl, t2 = -M_PI * wl, dev = std::fabs(def_dev);
-        c[0] = -amp_shift;
-        c[1] = t2 * defocus;
-        c[2] = t2 * dev * std::cos(2 * ast_angle);
-        c[3] = t2 * dev * std::sin(2 * ast_angle);
-        c[4] = t1 * cs;
-        c[5] = 2 * M_PI * btx;
-        c[6] = 2 * M_PI * bty;
-    }
-};
-
-// ---------------------------------------------------------------- project
-struct Micrograph {
-    std::string id, particle_file;
-    int box = 0;
-    double pixel_size = 0;
-    bool has_ctf = false;
-    Ctf ctf;
-    std::vector<long> part_id;
-    std::vector<double> ox, oy, vx, vy, vz, va, defocus, mag, pixel;
-    std::vector<long> select;
-};
-
-std::string dir_of(const std::string& p) {
-    const size_t s = p.find_last_of('/');
-    return s == std::string::npos ? "." : p.substr(0, s);
-}
-
-std::vector<Micrograph> read_project(const std::string& path) {
-    auto blocks = read_star(path);
-    const std::string base = dir_of(path);
-    std::vector<Micrograph> out;
-    for (auto& b : blocks) {
-        if (!(b.has("micrograph.id") || b.has("micrograph.file_name"))) continue;
-        Micrograph mg;
-        mg.id = b.has("micrograph.id") ? b.items.at("micrograph.id") : b.items.at("micrograph.file_name");
-        mg.particle_file = b.has("particle.file_name") ? b.items.at("particle.file_name") : "";
-        if (!mg.particle_file.empty() && mg.particle_file[0] != '/') mg.particle_file = base + "/" + mg.particle_file;
-        // box size vector as micrograph_from_starblock fills it (rwmgSTAR.cpp:590-605)
-        long bs[3] = {0, 0, 0};
-        if (b.has("particle.box_radius")) bs[0] = bs[1] = bs[2] = 2 * b.integer("particle.box_radius");
-        if (b.has("particle.box_radius_x")) {
-            bs[0] = 2 * b.integer("particle.box_radius_x"); bs[1] = 2 * b.integer("particle.box_radius_y");
-            bs[2] = 2 * b.integer("particle.box_radius_z");
-        }
-        if (b.has("particle.box_size")) bs[0] = bs[1] = bs[2] = b.integer("particle.box_size");
-        if (b.has("particle.box_size_x")) {
-            bs[0] = b.integer("particle.box_size_x"); bs[1] = b.integer("particle.box_size_y");
-            bs[2] = b.integer("particle.box_size_z");
-        }
-        mg.box = (int)bs[0];
-        mg.pixel_size = b.real("micrograph.pixel_size");
-        if (mg.pixel_size == 0) mg.pixel_size = b.real("micrograph.pixel_size_x");
-        if (b.has("ctf.voltage")) {
-            mg.has_ctf = true;
-            Ctf& c = mg.ctf;
-            c.amp_shift = b.has("ctf.amplitude_phase_shift") ? b.real("ctf.amplitude_phase_shift")
-                                                              : std::asin(b.real("ctf.amp_contrast"));
-            if (b.has("ctf.defocus_average")) {
-                c.defocus = b.real("ctf.defocus_average");
-                c.def_dev = b.real("ctf.defocus_deviation");
-            } else {
-                const double dmin = b.real("ctf.defocus_min"), dmax = b.real("ctf.defocus_max");
-                c.defocus = (dmax + dmin) / 2;
-                c.def_dev = std::fabs(dmax - dmin) / 2;
-            }
-            c.volt = b.real("ctf.voltage");
-            if (c.volt < 1e3) c.volt *= 1e3;    // kV given (rwmg.cpp:641)
-            c.cs = b.real("ctf.Cs");
-            c.ast_angle = b.real("ctf.astigmatism_angle") * M_PI / 180.0;
-            c.btx = b.real("ctf.beam_tilt_x");
-            c.bty = b.real("ctf.beam_tilt_y");
-        }
-        const StarLoop* lp = b.loop_with("particle.id");
-        const size_t n = lp ? lp->rows.size() : 0;
-        auto col = [&](const char* tag, double def) {
-            std::vector<double> v(n, def);
-            const int i = lp ? lp->index(tag) : -1;
-            if (i >= 0)
-                for (size_t r = 0; r < n; ++r) v[r] = strtod(lp->rows[r][i].c_str(), nullptr);
-            return v;
-        };
-        auto ids = col("particle.id", 0);
-        mg.ox = col("particle.origin_x", 0);
-        mg.oy = col("particle.origin_y", 0);
-        auto oz = col("particle.origin_z", 0);
-        if (lp && lp->index("particle.view_angle") >= 0) {
-            mg.vx = col("particle.view_x", 0); mg.vy = col("particle.view_y", 0); mg.vz = col("particle.view_z", 1);
-            mg.va = col("particle.view_angle", 0);
-            for (auto& a : mg.va) a *= M_PI / 180.0;
-        } else if (lp && (lp->index("particle.psi") >= 0 || lp->index("particle.omega") >= 0)) {
-            // Euler (ZYZ) -> view (Euler.h:62-66)
-            const bool psi = lp->index("particle.psi") >= 0;
-            auto p = col(psi ? "particle.psi" : "particle.omega", 0);
-            auto th = col("particle.theta", 0), ph = col("particle.phi", 0);
-            for (size_t r = 0; r < n; ++r) {
-                const double ps = (psi ? p[r] : -p[r]) * M_PI / 180.0, t = th[r] * M_PI / 180.0,
-                             f = ph[r] * M_PI / 180.0;
-                mg.vx.push_back(std::cos(f) * std::sin(t));
-                mg.vy.push_back(std::sin(f) * std::sin(t));
-                mg.vz.push_back(std::cos(t));
-                mg.va.push_back(angle_neg_pi_to_pi(ps + f));
-            }
-        } else {
-            mg.vx.assign(n, 0); mg.vy.assign(n, 0); mg.vz.assign(n, 1); mg.va.assign(n, 0);
-        }
-        mg.pixel = (lp && lp->index("particle.pixel_size_x") >= 0) ? col("particle.pixel_size_x", 0)
-                                                                     : col("particle.pixel_size", 0);
-        for (auto& p : mg.pixel)
-            if (!(p > 0)) p = mg.pixel_size;
-        // read_project post-processing (rwmg.cpp:650-659): an origin further
-        // than box_x/4 from the box centre (integer halves, z included) is
-        // reset to the centre; then origin z = 0
-        const double half[3] = {(double)(bs[0] / 2), (double)(bs[1] / 2), (double)(bs[2] / 2)};
-        for (size_t r = 0; r < n; ++r) {
-            const double d0 = mg.ox[r] - half[0], d1 = mg.oy[r] - half[1], d2 = oz[r] - half[2];
-            if (std::sqrt(d0 * d0 + d1 * d1 + d2 * d2) > (double)(bs[0] / 4)) {
-                mg.ox[r] = half[0];
-                mg.oy[r] = half[1];
-            }
-        }
-        mg.defocus = col("particle.defocus", 0);
-        mg.mag = col("particle.magnification", 0);
-        auto sel = col("particle.select", 1);
-        for (size_t r = 0; r < n; ++r) {
-            mg.part_id.push_back((long)ids[r]);
-            mg.select.push_back((long)sel[r]);
-        }
-        out.push_back(std::move(mg));
-    }
-    if (out.empty()) throw std::runtime_error(path + ": no micrograph blocks found");
-    return out;
-}
+using namespace bsh;
 
 // ---------------------------------------------------------------- plan
 struct Options {

@@ -63,3 +63,57 @@ def test_maps_match_reference(case, exe, tmp_path):
         assert (h.nx, h.ny, h.nz) == z[k].shape[::-1]
         m = np.fromfile(name, dtype="<f4", offset=1024 + h.nsymbt).reshape(z[k].shape)
         assert rel_l2(m, z[k]) < 1e-5, (k, rel_l2(m, z[k]))
+
+
+# ---- brefine: the reference's grid refinement fixtures through the drop-in
+def _write_refine_project(d, tmp_path):
+    import math
+    from bsoft_b200.ctf import CTFParams, electron_wavelength
+    from bsoft_b200.project import Micrograph, Project, write_project
+    N, n = d["N"], d["n"]
+    mrc.write_stack(os.path.join(tmp_path, "ref.mrc"), d["map"], d["pixel"], origin_pixels=(N // 2,) * 3, volume=True)
+    mrc.write_stack(os.path.join(tmp_path, "parts.mrcs"), d["images"], d["pixel"])
+    proj = Project(base_dir=str(tmp_path))
+    for i, st in enumerate(d["start"]):
+        ctf = None
+        if d["def_std"] > 0:
+            r = d["ctf_rows"][i]
+            wl = electron_wavelength(r[0])
+            t1, t2 = math.pi / 2 * wl ** 3, -math.pi * wl
+            ctf = CTFParams(volt=r[0], cs=r[5] / t1, amp_shift=-r[1], defocus=r[2] / t2,
+                            def_dev=math.hypot(r[3], r[4]) / abs(t2), ast_angle=math.atan2(r[4] / t2, r[3] / t2) / 2)
+        # one micrograph per particle: each carries its own CTF
+        proj.micrographs.append(Micrograph(
+            id=f"mg{i}", particle_file="parts.mrcs", box_size=n, pixel_size=d["pixel"], ctf=ctf,
+            part_id=np.array([i + 1]), origin=np.array([[st[4], st[5], 0.0]]), view=st[None, :4].copy(),
+            defocus=np.zeros(1), magnification=np.zeros(1), select=np.ones(1, dtype=np.int64),
+            pixel=np.array([d["pixel"]])))
+    star = os.path.join(tmp_path, "in.star")
+    write_project(star, proj)
+    return star
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["refine64", "refine32", "refine64ctf"])
+def test_brefine_matches_reference(case, exe, tmp_path):
+    import math
+    from bsoft_b200.project import read_project
+    from tests.refine_helpers import load
+    d = load(case)
+    star = _write_refine_project(d, str(tmp_path))
+    out = os.path.join(str(tmp_path), "out.star")
+    deg = lambda x: repr(x * 180.0 / math.pi)
+    args = [os.path.join(ROOT, "bsoft_b200", "_build", "brefine"), "-reference", os.path.join(str(tmp_path), "ref.mrc"),
+            "-grid", f"{round(d['alpha'] * 180 / math.pi, 6)},{round(d['accuracy'] * 180 / math.pi, 6)}",
+            "-step", f"{d['shift_step']},{d['shift_accuracy']}", "-resolution", repr(d["hi_res"]), "-output", out, star]
+    if d["def_std"] > 0:
+        args[1:1] = ["-defocus", repr(d["def_std"])]
+    subprocess.run(args, capture_output=True, text=True, check=True)
+    proj = read_project(out)
+    ref = d["result"]
+    for i, mg in enumerate(proj.micrographs):
+        v = mg.view[0]
+        assert np.abs(v[:3] - ref[i, :3]).max() < 1e-9 and abs(v[3] - ref[i, 3]) < 1e-9, (i, v, ref[i, :4])
+        assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 1e-9
+        if d["def_std"] > 0:
+            assert abs(mg.defocus[0] - ref[i, 9]) < 1e-6 * ref[i, 9]
