@@ -182,7 +182,7 @@ static void free_all(Recon* r) {
         if (r->copy_done[i]) cudaEventDestroy(r->copy_done[i]);
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
-    F(r->d_part); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
+    F(r->d_part); F(r->d_psym); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
     F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax); F(r->d_tile_order); F(r->d_part_sums);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
@@ -204,7 +204,9 @@ static int run_batch_kernels(Recon* r, const float* d_img, long np, float2* spec
     if (!insert) return BSG_OK;
     for (int h = 0; h < r->nhalves; ++h) {
         if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
-        CK(launch_insert(*r, spec_out, 0, (int)np, r->nhalves == 2 ? h : -1, s));
+        const long nsym = std::max(1L, (long)r->sym.size() / 9);
+        if (nsym > 1) CK(launch_insert(*r, spec_out, r->d_psym, (int)(np * nsym), r->nhalves == 2 ? h : -1, s));
+        else CK(launch_insert(*r, spec_out, r->d_part, (int)np, r->nhalves == 2 ? h : -1, s));
         if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 0}); }
         r->stats.launches += r->replicas > 1 ? 2 : 1;     // gridding (+ replica combine)
         r->stats.insert_launches += 1;
@@ -218,7 +220,10 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
     // the staging buffer may still feed an in-flight copy from two batches ago
     CK(cudaEventSynchronize(r->compute_done[buf]));
     DevParticle* hp = r->h_partbuf[buf];
-    for (long i = 0; i < np; ++i) make_dev_particle(*r, params + i * BSG_PARTICLE_DOUBLES, hp[i]);
+    for (long i = 0; i < np; ++i) {
+        make_dev_particle(*r, params + i * BSG_PARTICLE_DOUBLES, hp[i]);
+        hp[i].spec = (int)i;
+    }
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
     // fixed-point range of the gridding sums: the largest particle weight
     // and the most contributions one voxel can take from one batch (at most
@@ -230,6 +235,40 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
     const int need = (int)ceil(log2((double)np * per + 1.0));
     r->fix_bits = std::max(20, std::min(44, 62 - need));
     CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->stream));
+    const long nsym = (long)r->sym.size() / 9;
+    if (nsym > 1) {
+        // one gridding record per (particle, operator): matrix S R, the
+        // particle's spectrum (fspace_pack_2D(p, View, sym, ...),
+        // Bimage_reconstruct.cpp:248-266)
+        const size_t need = (size_t)np * nsym;
+        if (need > r->psym_cap) {
+            if (r->d_psym) cudaFree(r->d_psym);
+            r->d_psym = nullptr;
+            r->psym_cap = 0;
+            CK(cudaMalloc((void**)&r->d_psym, sizeof(DevParticle) * need));
+            r->psym_cap = need;
+        }
+        // the pageable staging below is copied before cudaMemcpyAsync returns
+        CK(cudaStreamSynchronize(r->stream));
+        r->h_psym.resize(need);
+        double q[BSG_PARTICLE_DOUBLES];
+        for (long i = 0; i < np; ++i) {
+            const double* p0 = params + i * BSG_PARTICLE_DOUBLES;
+            for (long s = 0; s < nsym; ++s) {
+                memcpy(q, p0, sizeof(q));
+                const double* S = &r->sym[9 * s];
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        q[4 + 3 * a + b] = S[3 * a + 0] * p0[4 + 0 * 3 + b] + S[3 * a + 1] * p0[4 + 1 * 3 + b] +
+                                           S[3 * a + 2] * p0[4 + 2 * 3 + b];
+                DevParticle& d = r->h_psym[i * nsym + s];
+                make_dev_particle(*r, q, d);
+                d.spec = (int)i;
+            }
+        }
+        CK(cudaMemcpyAsync(r->d_psym, r->h_psym.data(), sizeof(DevParticle) * need, cudaMemcpyHostToDevice,
+                           r->stream));
+    }
     return BSG_OK;
 }
 
@@ -507,6 +546,24 @@ int bsg_recon_fsc(bsg_recon* h, int nshell, double* fsc_out) {
     r->stats.launches += 4;
     CK(cudaMemcpyAsync(fsc_out, d_out, sizeof(double) * nshell, cudaMemcpyDeviceToHost, r->stream));
     CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
+int bsg_recon_set_symmetry(bsg_recon* h, const double* ops, int nops) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || nops < 0 || (nops > 0 && !ops)) return fail(BSG_ERR_ARG, "bsg_recon_set_symmetry: bad argument");
+    if (nops > 4096) return fail(BSG_ERR_ARG, "bsg_recon_set_symmetry: %d operators (at most 4096)", nops);
+    for (int s = 0; s < nops; ++s) {
+        // rotations only: rows orthonormal to 1e-6
+        const double* S = ops + 9 * s;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                const double d = S[3 * a] * S[3 * b] + S[3 * a + 1] * S[3 * b + 1] + S[3 * a + 2] * S[3 * b + 2];
+                if (!(fabs(d - (a == b ? 1.0 : 0.0)) < 1e-6))
+                    return fail(BSG_ERR_ARG, "bsg_recon_set_symmetry: operator %d is not a rotation", s);
+            }
+    }
+    r->sym.assign(ops, ops + 9 * (size_t)(nops > 1 ? nops : 0));
     return BSG_OK;
 }
 

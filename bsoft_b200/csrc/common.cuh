@@ -40,7 +40,7 @@ struct alignas(16) DevParticle {
     float  slab;            // sum |nrm_i|: plane reaches a voxel cube iff |n.c| < slab
     float  step;            // |ad| = voxels per pixel step
     int    half;            // half-map index
-    int    pad_;
+    int    spec;            // index of this record's spectrum in the batch (symmetry copies share it)
 };
 
 // Run geometry shared by all kernels of one context.
@@ -69,7 +69,8 @@ struct Context;
 cudaError_t launch_background(const Context& c, const float* img, int nimg, cudaStream_t s);
 cudaError_t launch_rows(const Context& c, const float* img, int nimg, cudaStream_t s);
 cudaError_t launch_cols(const Context& c, int nimg, float2* spectra, cudaStream_t s);
-cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int np, int half, cudaStream_t s);
+cudaError_t launch_insert(const Context& c, const float2* spectra, const DevParticle* parts, int np, int half,
+                          cudaStream_t s);
 cudaError_t launch_finish(const Context& c, int imap, float* map_out, float* fom_out, bool sinc, cudaStream_t s);
 cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream_t s);
 

@@ -5,6 +5,8 @@
 
 #include <cuda.h>
 
+#include <vector>
+
 namespace bsg {
 
 struct Context {
@@ -18,6 +20,13 @@ struct Context {
     // per-batch device buffers
     float* d_img = nullptr;          // batch x n x n
     DevParticle* d_part = nullptr;   // batch
+    // point-group symmetry (fspace_pack_2D over symmetry_get_all_views):
+    // nsym operators S (row-major); particle records are gridded once per
+    // operator with matrix S R, all copies reading the particle's spectrum
+    std::vector<double> sym;          // 9 per operator; empty = C1
+    DevParticle* d_psym = nullptr;    // batch x nsym expanded records
+    size_t psym_cap = 0;
+    std::vector<DevParticle> h_psym;
     double* d_bkg = nullptr;         // batch
     float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
     float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms

@@ -45,7 +45,6 @@ constexpr int WARPS = 4;                  // warps (tiles) per block
 struct InsertArgs {
     const float2* spec;        // batch x (ft+1) x (ft+2), centred
     const DevParticle* part;   // particles of this launch
-    int p_base;                // index of part[0] in the spectra buffer
     int np;
     int half;                  // only particles of this half map (-1: all)
     int N, ft, pitch;
@@ -348,7 +347,7 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
             const unsigned am = __shfl_sync(0xffffffffu, mask, src);
             const int pi = base + src;
             const DevParticle& P = a.part[pi];
-            const float2* S = a.spec + (size_t)(a.p_base + pi) * spec_stride;
+            const float2* S = a.spec + (size_t)P.spec * spec_stride;
             for (int al = 0; al < 8; ++al)
                 if ((am >> al) & 1u)
                     scatter_particle<FOM, GATE, TX, TY, TZ>(a, P, S, A, (double)(x0 - ((al & 1) ? N : 0)),
@@ -433,11 +432,11 @@ static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_insert(const Context& c, const float2* spectra, int p0, int np, int half, cudaStream_t s) {
+cudaError_t launch_insert(const Context& c, const float2* spectra, const DevParticle* parts, int np, int half,
+                          cudaStream_t s) {
     InsertArgs a;
     a.spec = spectra;
-    a.part = c.d_part + p0;
-    a.p_base = p0;
+    a.part = parts;
     a.np = np;
     a.half = half;
     a.N = c.g.map;

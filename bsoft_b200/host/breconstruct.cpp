@@ -8,7 +8,7 @@
 //   -interpolation nearest|weighted|trilinear   (default nearest)
 //   -pad 2          -CTF none|flip|apply|correct|wiener    -wiener 0.2
 //   -resolution 4   -size 64   -sampling 1.5   -scale 1
-//   -fullmap / -halfmaps       -bootstrap
+//   -fullmap / -halfmaps       -bootstrap     -symmetry D6 (inserted during reconstruction)
 //   -reconstruction out.mrc    -fom fom.mrc    -batch 4096   -device 0
 //   -plan           print the per-particle records (no GPU work) and exit
 // Output names follow the reference: out.mrc for a full map, out_01.mrc and
@@ -43,6 +43,7 @@ struct Options {
     int interp = 0, pad = 2, ctf_action = 0, size = 0, nmaps = 0, batch = 4096, device = 0;
     double wiener = 0, resolution = 0, sampling = 0, scale = 1;
     bool bootstrap = false, plan_only = false;
+    std::string symmetry = "C1";
     std::string recons, fom;
     std::vector<std::string> inputs;
 };
@@ -167,6 +168,7 @@ Options parse(int argc, char** argv) {
         else if (a == "-fullmap") o.nmaps += 1;
         else if (a == "-halfmaps") o.nmaps += 2;
         else if (a == "-bootstrap") o.bootstrap = true;
+        else if (a == "-symmetry" || a == "-sym") o.symmetry = val();
         else if (a == "-reconstruction") o.recons = val();
         else if (a == "-fom") o.fom = val();
         else if (a == "-batch") o.batch = atoi(val().c_str());
@@ -207,9 +209,10 @@ int main(int argc, char** argv) {
         }
         const Plan p = plan_reconstruction(mgs, o);
         const long np = (long)p.src.size();
+        const std::vector<double> sym = symmetry_operators(o.symmetry);
         if (o.plan_only) {
-            printf("n %d ft %d map %d map_sampling %.17g hi_res %.17g wiener %.17g nmaps %d particles %ld\n", p.n,
-                   p.ft, p.map, p.map_sampling, p.hi_res, p.wiener, p.nmaps, np);
+            printf("n %d ft %d map %d map_sampling %.17g hi_res %.17g wiener %.17g nmaps %d particles %ld nsym %ld\n",
+                   p.n, p.ft, p.map, p.map_sampling, p.hi_res, p.wiener, p.nmaps, np, (long)(sym.size() / 9));
             for (long i = 0; i < np; ++i) {
                 for (int j = 0; j < BSG_PARTICLE_DOUBLES; ++j)
                     printf("%.17g%c", p.rec[i * BSG_PARTICLE_DOUBLES + j], j + 1 < BSG_PARTICLE_DOUBLES ? ' ' : '\n');
@@ -223,6 +226,8 @@ int main(int argc, char** argv) {
         cfg.fom = o.fom.empty() ? 0 : 1; cfg.batch = 0; cfg.device = o.device;
         bsg_recon* rec = nullptr;
         CALL(bsg_recon_create(&cfg, &rec));
+        // point-group symmetry during reconstruction (mode 0)
+        CALL(bsg_recon_set_symmetry(rec, sym.data(), (int)(sym.size() / 9)));
         // stream the particles in host batches (the library uploads and
         // overlaps them with the device work)
         const long n2 = (long)p.n * p.n;

@@ -7,6 +7,8 @@
 // weights (ctf.h).
 #pragma once
 
+#include <array>
+#include <cctype>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -396,6 +398,78 @@ inline std::vector<Micrograph> read_project(const std::string& path) {
     }
     if (out.empty()) throw std::runtime_error(path + ": no micrograph blocks found");
     return out;
+}
+
+// Point-group operators as rotation matrices (row-major, identity first) in
+// the order of symmetry_get_all_views (bsoft/src/util/symmetry.cpp:277-319),
+// from the generating operations of Bsymmetry::Bsymmetry (:42-115) and the
+// label rules of clean_symstring (bsoft/include/symmetry.h:73-99): Cn, Dn,
+// T, O, I and their -2/-3/-4/-5 variants.  Helical and I90 are rejected.
+inline std::vector<double> symmetry_operators(const std::string& sym) {
+    std::string lbl;
+    for (char ch : sym)
+        if (!isspace((unsigned char)ch)) lbl += ch;
+    if (lbl.empty()) lbl = "C1";
+    if (isdigit((unsigned char)lbl[0])) {
+        const int j = atoi(lbl.c_str());
+        if (lbl.find("532") != std::string::npos) lbl = lbl.find("90") != std::string::npos ? "I90" : "I";
+        else if (lbl.find("432") != std::string::npos) lbl = "O";
+        else if (lbl.find("23") != std::string::npos) lbl = "T";
+        else if (j > 1 && lbl.size() > 1 && lbl[1] == '2') lbl = "D" + std::to_string(j);
+        else if (j > 0) lbl = "C" + std::to_string(j);
+        else lbl = "C1";
+    }
+    lbl[0] = (char)toupper((unsigned char)lbl[0]);
+    auto has = [&](const char* t) { return lbl.find(t) != std::string::npos; };
+    const double gold = 1.61803398874989484820458683436563811772;
+    struct Op { double a[3]; int order; };
+    std::vector<Op> ops;
+    if (lbl[0] == 'C') ops.push_back({{0, 0, 1}, lbl == "Cs" ? 1 : std::max(1, atoi(lbl.c_str() + 1))});
+    else if (lbl[0] == 'D') { ops.push_back({{0, 0, 1}, atoi(lbl.c_str() + 1)}); ops.push_back({{1, 0, 0}, 2}); }
+    else if (lbl[0] == 'T') {
+        if (!has("-3")) ops.push_back({{1, 1, 1}, 3});
+        ops.push_back({{0, 0, 1}, 2});
+        ops.push_back({{1, 0, 0}, 2});
+    } else if (lbl[0] == 'O') {
+        if (!has("-3")) ops.push_back({{1, 1, 1}, 3});
+        if (has("-4")) ops.push_back({{1, -1, 0}, 2});
+        else if (has("-2")) ops.push_back({{0, 0, 1}, 4});
+        else { ops.push_back({{0, 0, 1}, 4}); ops.push_back({{1, 0, 0}, 2}); }
+    } else if (lbl[0] == 'I' && !has("90")) {
+        if (!has("-3")) ops.push_back({{1, 1, 1}, 3});
+        if (has("-5")) ops.push_back({{1, 0, 0}, 2});
+        else if (has("-2")) ops.push_back({{1, -1, 0}, 2});
+        else ops.push_back({{1, 1.0 / gold, gold}, 2});
+        if (!has("-5")) ops.push_back({{1.0 / gold, 1, 0}, 5});
+        if (!has("-2")) ops.push_back({{0, 0, 1}, 2});
+    } else {
+        throw std::runtime_error("unsupported symmetry " + sym);
+    }
+    std::vector<std::array<double, 4>> q{{1, 0, 0, 0}};
+    for (const Op& op : ops) {
+        const double n = std::sqrt(op.a[0] * op.a[0] + op.a[1] * op.a[1] + op.a[2] * op.a[2]);
+        const size_t nv = q.size();
+        for (int j = 1; j < op.order; ++j) {
+            const double ang = j * 2.0 * M_PI / op.order, s = std::sin(ang / 2);
+            const std::array<double, 4> g{std::cos(ang / 2), op.a[0] / n * s, op.a[1] / n * s, op.a[2] / n * s};
+            for (size_t k = 0; k < nv; ++k) {
+                const auto& p = q[k];
+                q.push_back({g[0] * p[0] - g[1] * p[1] - g[2] * p[2] - g[3] * p[3],
+                             g[0] * p[1] + g[1] * p[0] + g[2] * p[3] - g[3] * p[2],
+                             g[0] * p[2] + g[2] * p[0] + g[3] * p[1] - g[1] * p[3],
+                             g[0] * p[3] + g[3] * p[0] + g[1] * p[2] - g[2] * p[1]});
+            }
+        }
+    }
+    std::vector<double> m;
+    for (const auto& t : q) {
+        const double q0 = t[0], q1 = t[1], q2 = t[2], q3 = t[3];
+        const double r[9] = {q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3, 2 * q1 * q2 - 2 * q0 * q3, 2 * q1 * q3 + 2 * q0 * q2,
+                             2 * q1 * q2 + 2 * q0 * q3, q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3, 2 * q2 * q3 - 2 * q0 * q1,
+                             2 * q1 * q3 - 2 * q0 * q2, 2 * q2 * q3 + 2 * q0 * q1, q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3};
+        m.insert(m.end(), r, r + 9);
+    }
+    return m;
 }
 
 // STAR project with the particle parameters the readers above take, plus

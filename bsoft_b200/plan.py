@@ -78,6 +78,7 @@ class ReconOptions:
     bootstrap: bool = False
     fom: bool = False             # keep power / weight^2 channels
     threads: int = 2              # reference partial maps (only sets half-map parity)
+    symmetry: str = ""            # point group (-symmetry; "" = C1)
 
 
 @dataclass
@@ -93,6 +94,7 @@ class ReconPlan:
     params: np.ndarray            # (P, 32) float64 per-particle records
     stack_index: list = field(default_factory=list)   # (stack file, image index) per particle
     nmaps: int = 1
+    symmetry: str = "C1"          # point group inserted during reconstruction (mode 0)
 
 
 def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
@@ -159,7 +161,7 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
     return ReconPlan(n=hdr.nx, ft=ft, map=size, map_sampling=map_sampling, hi_res=hi_res,
                      interp=opt.interp, ctf_action=opt.ctf_action, wiener=wiener,
                      params=np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES),
-                     stack_index=index, nmaps=opt.nmaps)
+                     stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1")
 
 
 def load_images(plan: ReconPlan, sel=None) -> np.ndarray:

@@ -42,6 +42,9 @@ class Reconstructor:
         h = C.c_void_p()
         _lib.check(L.bsg_recon_create(C.byref(cfg), C.byref(h)), "bsg_recon_create")
         self._h = h
+        sym = getattr(plan, "symmetry", "C1") or "C1"
+        if sym != "C1":
+            self.set_symmetry(sym)
         self.fom = fom
 
     # context management
@@ -146,6 +149,15 @@ class Reconstructor:
                    "bsg_recon_autotune")
         del keep
         return best.value, ms[:4]
+
+    def set_symmetry(self, sym):
+        """Point group (label, or (n, 3, 3) operator matrices) inserted during
+        reconstruction, as breconstruct -symmetry does."""
+        from .symmetry import operators
+        ops = operators(sym) if isinstance(sym, str) else np.asarray(sym, dtype=np.float64)
+        ops = np.ascontiguousarray(ops, dtype=np.float64).reshape(-1, 9)
+        _lib.check(_lib.load().bsg_recon_set_symmetry(self._h, ops.ctypes.data_as(C.POINTER(C.c_double)), len(ops)),
+                   "bsg_recon_set_symmetry")
 
     def set_tile_shape(self, shape: int):
         _lib.check(_lib.load().bsg_recon_set_tile_shape(self._h, shape), "bsg_recon_set_tile_shape")

@@ -127,6 +127,17 @@ int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* param
  * (-1 where the shape does not apply); best_out the chosen shape.  The
  * reference has no counterpart (it has no tunable tiling). */
 int  bsg_recon_set_tile_shape(bsg_recon* r, int shape);
+
+/* Point-group symmetry during reconstruction (breconstruct -symmetry, mode
+ * 0): Bimage::fspace_pack_2D(p, View, sym, ...) (bsoft/src/img/
+ * Bimage_reconstruct.cpp:248-266) inserts each particle once per view of
+ * symmetry_get_all_views (bsoft/src/util/symmetry.cpp:277-319); the view
+ * made by the group element q from the particle's view v has the matrix
+ * M(q) M(v).  ops: nops rotation matrices M(q) (row-major, the identity
+ * first, in the reference's generation order); every later insert grids
+ * each particle with matrix M(q) R for every operator, all copies from the
+ * particle's one transform.  nops <= 1 restores C1. */
+int  bsg_recon_set_symmetry(bsg_recon* r, const double* ops, int nops);
 int  bsg_recon_autotune(bsg_recon* r, const float* images, const double* params, long nparts,
                         int flags, double* ms_out, int* best_out);
 

@@ -122,10 +122,58 @@ def finish(plan, vol, weight, power=None, weight2=None, sinc=None):
     return out.reshape(plan.map, plan.map, plan.map), cov
 
 
+def symmetry_matrices(sym: str) -> np.ndarray:
+    """Group elements of a point group as rotation matrices, in the order of
+    symmetry_get_all_views (bsoft/src/util/symmetry.cpp:277-319) with the
+    generating operations of Bsymmetry::Bsymmetry (symmetry.cpp:53-99):
+    Cn, Dn, T, O, I."""
+    g = (sym or "C1").strip().upper()
+    phi = (1 + 5 ** 0.5) / 2
+    if g[0] == "C":
+        ops = [((0, 0, 1), int(g[1:] or 1))]
+    elif g[0] == "D":
+        ops = [((0, 0, 1), int(g[1:])), ((1, 0, 0), 2)]
+    elif g == "T":
+        ops = [((1, 1, 1), 3), ((0, 0, 1), 2), ((1, 0, 0), 2)]
+    elif g == "O":
+        ops = [((1, 1, 1), 3), ((0, 0, 1), 4), ((1, 0, 0), 2)]
+    elif g == "I":
+        ops = [((1, 1, 1), 3), ((1, 1 / phi, phi), 2), ((1 / phi, 1, 0), 5), ((0, 0, 1), 2)]
+    else:
+        raise ValueError(sym)
+
+    def rot(axis, ang):
+        a = np.asarray(axis, float) / np.linalg.norm(axis)
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        return np.eye(3) + np.sin(ang) * K + (1 - np.cos(ang)) * K @ K     # Rodrigues
+
+    mats = [np.eye(3)]
+    for axis, order in ops:
+        n = len(mats)
+        for j in range(1, order):
+            r = rot(axis, j * 2 * np.pi / order)
+            mats += [r @ mats[k] for k in range(n)]
+    return np.stack(mats)
+
+
+def expand_symmetry(plan, images: np.ndarray, params: np.ndarray):
+    """Every particle once per symmetry-related view (fspace_pack_2D over
+    symmetry_get_all_views, Bimage_reconstruct.cpp:248-266): matrix S R."""
+    sym = getattr(plan, "symmetry", "C1") or "C1"
+    if sym == "C1":
+        return images, params
+    S = symmetry_matrices(sym)
+    P = np.repeat(params, len(S), axis=0).copy()
+    R = params[:, 4:13].reshape(-1, 3, 3)
+    P[:, 4:13] = np.einsum("sab,pbc->psac", S, R).reshape(-1, 9)
+    return np.repeat(images, len(S), axis=0), P
+
+
 def reconstruct(plan, images: np.ndarray, sel=None):
     """Full-map FP64 reconstruction of the selected particles (all by default)."""
     params = plan.params if sel is None else plan.params[sel]
     imgs = images if sel is None else images[sel]
+    imgs, params = expand_symmetry(plan, imgs, params)
     vol, w, _, _ = insert(plan, imgs, params)
     m, _ = finish(plan, vol, w)
     return m

@@ -51,6 +51,10 @@ CASES = [
     ("ctf16_tri_flip_half", "ctf16", "-interp trilinear -CTF flip -halfmaps", ("_01", "_02")),
     ("plain24_tri", "plain24", "-interp trilinear", None),
     ("plain24_near", "plain24", "-interp nearest", None),
+    # point-group symmetry inserted during reconstruction (-symmetry, mode 0)
+    ("ctf16_tri_flip_d3", "ctf16", "-interp trilinear -CTF flip -symmetry D3", None),
+    ("plain24_tri_t", "plain24", "-interp trilinear -symmetry T", None),
+    ("plain24_near_c4", "plain24", "-interp nearest -symmetry C4", None),
 ]
 
 PROBES = [("ctf16", 0, 2, 1), ("ctf16", 37, 2, 1)]
@@ -63,8 +67,11 @@ def run(cmd, cwd):
 
 
 def main():
+    """All fixtures, or only the cases named on the command line (then the
+    dataset fixtures and the probes are left as they are)."""
     if not os.path.exists(os.path.join(REF, "breconstruct")):
         sys.exit("build the reference first: make -C oracle ref")
+    only = set(sys.argv[1:])
     tmp = tempfile.mkdtemp(prefix="golden_")
     data = {}
     for name, spec in DATASETS.items():
@@ -75,9 +82,13 @@ def main():
             star_text = f.read()
         stacks = {fn: mrc.read_stack(os.path.join(d, fn))[0] for fn in sorted(os.listdir(d)) if fn.endswith(".mrcs")}
         data[name] = (d, star_text, stacks)
+        if only:
+            continue
         np.savez_compressed(os.path.join(OUT, f"ds_{name}.npz"), star=np.array(star_text),
                             stack_names=np.array(list(stacks)), **{"stack_" + k: v for k, v in stacks.items()})
     for fname, ds, opts, suffixes in CASES:
+        if only and fname not in only:
+            continue
         d, star_text, stacks = data[ds]
         run(f"{REF}/breconstruct {opts} -threads 2 -recon ref.mrc particles.star", d)
         outs = {}
@@ -88,7 +99,7 @@ def main():
         np.savez_compressed(os.path.join(OUT, fname + ".npz"), dataset=np.array(ds), options=np.array(opts),
                             **outs)
         print("wrote", fname, list(outs))
-    for ds, idx, interp, ctf in PROBES:
+    for ds, idx, interp, ctf in ([] if only else PROBES):
         d, star_text, stacks = data[ds]
         run(f"{REF}/recon_probe particles.star {idx} {interp} {ctf} probe", d)
         ft = int(np.sqrt(os.path.getsize(os.path.join(d, "probe.fft")) // 8))

@@ -13,7 +13,16 @@ from bsoft_b200.project import read_project
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 CASES = ["ctf16_tri_none", "ctf16_tri_flip", "ctf16_near_apply", "ctf16_wtd_correct",
-         "ctf16_tri_flip_res", "ctf16_tri_flip_half", "plain24_tri", "plain24_near"]
+         "ctf16_tri_flip_res", "ctf16_tri_flip_half", "plain24_tri", "plain24_near",
+         "ctf16_tri_flip_d3", "plain24_tri_t", "plain24_near_c4"]
+
+
+def ref_tol(case: str) -> float:
+    """Agreement bar with the reference's map: 1e-5, or 3e-5 for the 12-fold
+    tetrahedral case, where the reference's own FP32 accumulation of ~12x
+    more contributions per voxel reaches ~1.3e-5 against the FP64 oracle
+    (the error is largest at low resolution, where contributions pile up)."""
+    return 3e-5 if case == "plain24_tri_t" else 1e-5
 
 
 def rel_l2(a, b) -> float:
@@ -60,6 +69,8 @@ def options_from_args(args: str) -> ReconOptions:
             opt.nmaps = 2
         elif t == "pad":
             opt.pad = int(val)
+        elif "symmetry".startswith(t) and len(t) >= 3:
+            opt.symmetry = val
         i += 2 if val is not None else 1
     return opt
 

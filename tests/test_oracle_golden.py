@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from tests.helpers import CASES, GOLDEN, load_case, materialize_dataset, rel_l2
+from tests.helpers import CASES, GOLDEN, load_case, materialize_dataset, ref_tol, rel_l2
 from bsoft_b200.plan import P_MAP, ReconOptions, load_images, plan_reconstruction
 from bsoft_b200.project import read_project
 
@@ -21,10 +21,10 @@ def test_oracle_matches_reference(case, tmp_path):
         for h, key in ((0, "map_01"), (1, "map_02")):
             sel = np.nonzero(plan.params[:, P_MAP] == h)[0]
             m = oracle.reconstruct(plan, images, sel)
-            assert rel_l2(m, refs[key]) < TOL, key
+            assert rel_l2(m, refs[key]) < ref_tol(case), key
     else:
         m = oracle.reconstruct(plan, images)
-        assert rel_l2(m, refs["map"]) < TOL
+        assert rel_l2(m, refs["map"]) < ref_tol(case)
 
 
 @pytest.mark.parametrize("probe", ["probe_ctf16_0", "probe_ctf16_37"])
