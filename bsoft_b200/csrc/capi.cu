@@ -46,6 +46,7 @@ struct Recon : Context {
     cudaEvent_t compute_done[2] = {nullptr, nullptr};
     std::vector<Timed> timed;
     bool broken = false;
+    long seq = 0;                    // batches issued over the context's life (staging buffer = seq & 1)
 };
 
 static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
@@ -248,8 +249,8 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
             CK(cudaMalloc((void**)&r->d_psym, sizeof(DevParticle) * need));
             r->psym_cap = need;
         }
-        // the pageable staging below is copied before cudaMemcpyAsync returns
-        CK(cudaStreamSynchronize(r->stream));
+        // pageable staging: cudaMemcpyAsync has copied it when it returns,
+        // and the device buffer is rewritten in stream order
         r->h_psym.resize(need);
         double q[BSG_PARTICLE_DOUBLES];
         for (long i = 0; i < np; ++i) {
@@ -276,9 +277,11 @@ static int process(Recon* r, const float* images, const double* params, long npa
                    float* spectra_out) {
     const size_t img_elems = (size_t)r->g.n * r->g.n;
     const bool dev = flags & BSG_DEVICE_PTR;
-    for (long off = 0, bi = 0; off < nparts; off += r->batch, ++bi) {
+    for (long off = 0; off < nparts; off += r->batch) {
         const long np = std::min<long>(r->batch, nparts - off);
-        const int buf = (int)(bi & 1);
+        // alternate the staging buffers across calls too, so that one call's
+        // upload overlaps the previous call's kernels
+        const int buf = (int)(r->seq++ & 1);
         int rc = upload_params(r, buf, params + off * BSG_PARTICLE_DOUBLES, np);
         if (rc) return rc;
         const float* d_img;
