@@ -96,15 +96,15 @@ rows_kernel(const float* __restrict__ img, const double* __restrict__ bkg, const
     for (int x = lane; x < ft; x += 32) {
         float re = (x < n) ? r0[x] : fill;
         float im = (y1 < n && x < n) ? r1[x] : fill;
-        buf[bitrev(x, logft)] = make_float2(re, im);
+        buf[swz(bitrev(x, logft))] = make_float2(re, im);
     }
     __syncwarp();
-    warp_fft<false>(buf, ft, logft, stw);
+    warp_fft<false, true>(buf, ft, logft, stw);
     const int hw = ft / 2 + 1;
     float2* o0 = rows + ((size_t)b * n + y0) * hw;
     float2* o1 = o0 + hw;
     for (int h = lane; h < hw; h += 32) {
-        float2 z = buf[h], zm = buf[(ft - h) & (ft - 1)];
+        float2 z = buf[swz(h)], zm = buf[swz((ft - h) & (ft - 1))];
         o0[h] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
         if (y1 < n) o1[h] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
     }
@@ -112,6 +112,10 @@ rows_kernel(const float* __restrict__ img, const double* __restrict__ bkg, const
 
 // ------------------------------------------------------------------ columns + epilogue
 constexpr int COL_W = 16;   // columns per CTA, one warp each
+
+// Column buffers are ft + 1 apart, so the 16 columns' copies of one row fall
+// in 16 different bank slots; within a column the line is swizzled (swz).
+__host__ __device__ constexpr int col_stride(int ft) { return ft + 1; }
 
 struct ColArgs {
     const float2* rows;
@@ -165,7 +169,8 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
     extern __shared__ float2 smem[];
     const int ft = a.ft, n = a.n, logft = a.logft;
     float2* stw = smem;
-    float2* cols = smem + ft / 2;                // COL_W x ft
+    float2* cols = smem + ft / 2;                // COL_W x col_stride(ft)
+    const int cs = col_stride(ft);
     const int b = blockIdx.y;
     const int h0 = blockIdx.x * COL_W;
     const int hw = ft / 2 + 1;
@@ -181,11 +186,11 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
             if (y < n) v = rows[(size_t)y * hw + h];
             else if (h == 0) v = make_float2(dc, 0.f);
         }
-        cols[c * ft + bitrev(y, logft)] = v;
+        cols[c * cs + swz(bitrev(y, logft))] = v;
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5;
-    if (h0 + warp < hw) warp_fft<false>(cols + warp * ft, ft, logft, stw);
+    if (h0 + warp < hw) warp_fft<false, true>(cols + warp * cs, ft, logft, stw);
     __syncthreads();
     const DevParticle& P = a.part[b];
     const float2* ex = a.phase + (size_t)b * 2 * ft;
@@ -201,14 +206,14 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
         if (hidx >= hw) continue;
         const int k = sfreq(kk, ft);
         const int h = sfreq(hidx, ft);            // hidx == ft/2 -> -ft/2
-        float2 g = cols[c * ft + kk];
+        float2 g = cols[c * cs + swz(kk)];
         float2* row = out + (size_t)(k + hf) * pitch + hf;
         const float2 v = cmul(g, pixel_factor(a, P, ex, ey, h, k));
         row[h] = v;
         vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
         if (hidx >= 1 && hidx < ft / 2) {
             // F(-h, k) = conj(G(h, -k)) * factor(-h, k)
-            float2 gm = cols[c * ft + ((-kk) & fm)];
+            float2 gm = cols[c * cs + swz((-kk) & fm)];
             gm.y = -gm.y;
             const float2 vm = cmul(gm, pixel_factor(a, P, ex, ey, -h, k));
             row[-h] = vm;
@@ -240,7 +245,7 @@ cudaError_t launch_cols(const Context& c, int nimg, float2* spectra, cudaStream_
     a.ctf_action = c.g.ctf_action; a.wiener = c.g.wiener; a.shi2 = c.g.ctf_shi2;
     const int hw = c.g.ft / 2 + 1;
     dim3 grid((hw + COL_W - 1) / COL_W, nimg);
-    size_t smem = sizeof(float2) * ((size_t)c.g.ft / 2 + (size_t)COL_W * c.g.ft);
+    size_t smem = sizeof(float2) * ((size_t)c.g.ft / 2 + (size_t)COL_W * col_stride(c.g.ft));
     cols_kernel<<<grid, COL_W * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
@@ -250,7 +255,7 @@ cudaError_t prepare_fft2d_attributes() {
                                          (int)(sizeof(float2) * (512 + ROW_WARPS * 1024)));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(float2) * (512 + COL_W * 1024)));
+                                (int)(sizeof(float2) * (512 + COL_W * col_stride(1024))));
 }
 
 }  // namespace bsg

@@ -25,9 +25,28 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {   // a * conj(b)
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
+// Bank swizzle of a line in shared memory: element i moves within its
+// aligned block of 16 (one 128-byte row of the 32 banks) by XOR with a
+// function of the block number, so a power-of-two line of L >= 16 maps onto
+// itself.  Unswizzled, the radix-4 stages of span 1 and 4 put 8 lanes on the
+// same banks, and the bit-reversed stores of 32 consecutive inputs all land
+// in one bank pair; swizzled, both spread over all 16 slots (the minimum of
+// two wavefronts for 32 eight-byte accesses).
+__device__ __forceinline__ int swz(int i) {
+    const int row = i >> 4;
+    return i ^ (((row & 3) * 5) ^ ((row >> 2) & 3));
+}
+
+template <bool SWZ>
+__device__ __forceinline__ int line_at(int i) {
+    return SWZ ? swz(i) : i;
+}
+
 // In-place radix-2 DIT over x[0..L) by the calling warp.  Radix-4 fusion:
-// two radix-2 stages per shared-memory round trip where possible.
-template <bool INVERSE>
+// two radix-2 stages per shared-memory round trip where possible.  With SWZ
+// the line is stored swizzled (element i at x[swz(i)]), inputs and outputs
+// included.
+template <bool INVERSE, bool SWZ = false>
 __device__ __forceinline__ void warp_fft(float2* x, int L, int logL, const float2* tw) {
     const int lane = threadIdx.x & 31;
     int s = 1;
@@ -46,7 +65,9 @@ __device__ __forceinline__ void warp_fft(float2* x, int L, int logL, const float
             float2 w2a = tw[j * tstride2];
             float2 w2b = tw[(j + half) * tstride2];
             if (INVERSE) { w1.y = -w1.y; w2a.y = -w2a.y; w2b.y = -w2b.y; }
-            float2 a0 = x[i0], a1 = x[i1], a2 = x[i2], a3 = x[i3];
+            const int p0 = line_at<SWZ>(i0), p1 = line_at<SWZ>(i1), p2 = line_at<SWZ>(i2),
+                      p3 = line_at<SWZ>(i3);
+            float2 a0 = x[p0], a1 = x[p1], a2 = x[p2], a3 = x[p3];
             // stage s: (a0,a1) and (a2,a3) with twiddle w1
             float2 t1 = cmul(a1, w1), t3 = cmul(a3, w1);
             float2 b0 = make_float2(a0.x + t1.x, a0.y + t1.y);
@@ -55,10 +76,10 @@ __device__ __forceinline__ void warp_fft(float2* x, int L, int logL, const float
             float2 b3 = make_float2(a2.x - t3.x, a2.y - t3.y);
             // stage s+1: (b0,b2) with w2a, (b1,b3) with w2b
             float2 u2 = cmul(b2, w2a), u3 = cmul(b3, w2b);
-            x[i0] = make_float2(b0.x + u2.x, b0.y + u2.y);
-            x[i2] = make_float2(b0.x - u2.x, b0.y - u2.y);
-            x[i1] = make_float2(b1.x + u3.x, b1.y + u3.y);
-            x[i3] = make_float2(b1.x - u3.x, b1.y - u3.y);
+            x[p0] = make_float2(b0.x + u2.x, b0.y + u2.y);
+            x[p2] = make_float2(b0.x - u2.x, b0.y - u2.y);
+            x[p1] = make_float2(b1.x + u3.x, b1.y + u3.y);
+            x[p3] = make_float2(b1.x - u3.x, b1.y - u3.y);
         }
         __syncwarp();
     }
@@ -71,9 +92,10 @@ __device__ __forceinline__ void warp_fft(float2* x, int L, int logL, const float
             const int i0 = (grp << s) + j, i1 = i0 + half;
             float2 w = tw[j * tstride];
             if (INVERSE) w.y = -w.y;
-            float2 u = x[i0], t = cmul(x[i1], w);
-            x[i0] = make_float2(u.x + t.x, u.y + t.y);
-            x[i1] = make_float2(u.x - t.x, u.y - t.y);
+            const int p0 = line_at<SWZ>(i0), p1 = line_at<SWZ>(i1);
+            float2 u = x[p0], t = cmul(x[p1], w);
+            x[p0] = make_float2(u.x + t.x, u.y + t.y);
+            x[p1] = make_float2(u.x - t.x, u.y - t.y);
         }
         __syncwarp();
     }
