@@ -131,38 +131,58 @@ struct ColArgs {
     double shi2;
 };
 
-// Per-pixel factor 1/ft * exp(i phi) * CTF for signed frequency (h, k).
-__device__ __forceinline__ float2 pixel_factor(const ColArgs& a, const DevParticle& P, const float2* ex,
-                                               const float2* ey, int h, int k) {
-    const int fm = a.ft - 1;
-    float2 ph = cmul(ex[h & fm], ey[k & fm]);
+// CTF weight of one pixel from its reduced even aberration r in (-pi, pi].
+__device__ __forceinline__ float ctf_weight(const ColArgs& a, double r) {
+    if (a.ctf_action == 1) return (r < 0.0) ? -1.f : 1.f;
+    float w = sinf((float)r);
+    if (a.wiener != 0.0) w = (float)((a.wiener + 1.0) * w / ((double)w * w + a.wiener));
+    return w;
+}
+
+// Factors 1/ft * exp(i phi) * CTF of pixel (h, k) and, with MIRROR, of its
+// mirror (-h, k).  exh = exp(i h shx) and eyk = exp(i k shy); the mirror's
+// phase is conj(exh) * eyk.  img_ctf_calculate: s = (h, k) * fs, inside
+// [0, shi2]; even aberration chi = c00 + s2 (c20 + c22 cos2a + c2m2 sin2a) +
+// c40 s2^2 with s2 cos2a = sx^2 - sy^2, s2 sin2a = 2 sx sy (ctf.h:321-334),
+// in double.  Mirroring h changes only the sign of the 2 sx sy term (and of
+// sx in the odd, beam-tilt aberration psi = c1m1 sy + c11 sx).
+template <bool MIRROR>
+__device__ __forceinline__ void pixel_factors(const ColArgs& a, const DevParticle& P, float2 exh, float2 eyk,
+                                              int h, int k, float2& f, float2& fm) {
     const float sc = 1.0f / (float)a.ft;
-    if (!a.ctf_action) return make_float2(ph.x * sc, ph.y * sc);
-    // img_ctf_calculate: s = (h, k) * fs, inside [0, shi2]; even aberration
-    // chi = c00 + s2 (c20 + c22 cos2a + c2m2 sin2a) + c40 s2^2 with
-    // s2 cos2a = sx^2 - sy^2, s2 sin2a = 2 sx sy (ctf.h:321-334), in double.
+    const float2 ph = cmul(exh, eyk);
+    const float2 phm = cmulc(eyk, exh);
+    f = make_float2(ph.x * sc, ph.y * sc);
+    if (MIRROR) fm = make_float2(phm.x * sc, phm.y * sc);
+    if (!a.ctf_action) return;
     const double sx = (double)h * P.fs, sy = (double)k * P.fs;
     const double s2 = sx * sx + sy * sy;
-    if (!(s2 <= a.shi2)) return make_float2(0.f, 0.f);
-    const double chi = P.c00 + P.c20 * s2 + P.c22 * (sx * sx - sy * sy) + P.c2m2 * (2.0 * sx * sy) +
-                       P.c40 * s2 * s2;
-    // reduce to (-pi, pi] in double so the sign of sin(chi) is exact
-    const double r = chi - 6.283185307179586 * rint(chi * 0.15915494309189535);
-    float w;
-    if (a.ctf_action == 1) {
-        w = (r < 0.0) ? -1.f : 1.f;
-    } else {
-        w = sinf((float)r);
-        if (a.wiener != 0.0) w = (float)((a.wiener + 1.0) * w / ((double)w * w + a.wiener));
+    if (!(s2 <= a.shi2)) {
+        f = make_float2(0.f, 0.f);
+        if (MIRROR) fm = f;
+        return;
     }
-    // odd aberrations (beam tilt): psi = c1m1 |s| sin a + c11 |s| cos a
-    float2 f = make_float2(ph.x * sc * w, ph.y * sc * w);
+    const double even = P.c00 + P.c20 * s2 + P.c22 * (sx * sx - sy * sy) + P.c40 * s2 * s2;
+    const double cross = P.c2m2 * (2.0 * sx * sy);
+    // reduce to (-pi, pi] in double so the sign of sin(chi) is exact
+    const double chi = even + cross;
+    const float w = ctf_weight(a, chi - 6.283185307179586 * rint(chi * 0.15915494309189535));
+    f.x *= w; f.y *= w;
+    float wm = 0.f;
+    if (MIRROR) {
+        const double chim = even - cross;
+        wm = ctf_weight(a, chim - 6.283185307179586 * rint(chim * 0.15915494309189535));
+        fm.x *= wm; fm.y *= wm;
+    }
     if (P.c11 != 0.0 || P.c1m1 != 0.0) {
         float sp, cp;
         sincosf((float)(P.c1m1 * sy + P.c11 * sx), &sp, &cp);
         f = cmulc(f, make_float2(cp, sp));
+        if (MIRROR) {
+            sincosf((float)(P.c1m1 * sy - P.c11 * sx), &sp, &cp);
+            fm = cmulc(fm, make_float2(cp, sp));
+        }
     }
-    return f;
 }
 
 __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
@@ -208,17 +228,21 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
         const int h = sfreq(hidx, ft);            // hidx == ft/2 -> -ft/2
         float2 g = cols[c * cs + swz(kk)];
         float2* row = out + (size_t)(k + hf) * pitch + hf;
-        const float2 v = cmul(g, pixel_factor(a, P, ex, ey, h, k));
-        row[h] = v;
-        vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
+        float2 f, fmr;
         if (hidx >= 1 && hidx < ft / 2) {
+            pixel_factors<true>(a, P, ex[hidx], ey[kk], h, k, f, fmr);
             // F(-h, k) = conj(G(h, -k)) * factor(-h, k)
             float2 gm = cols[c * cs + swz((-kk) & fm)];
             gm.y = -gm.y;
-            const float2 vm = cmul(gm, pixel_factor(a, P, ex, ey, -h, k));
+            const float2 vm = cmul(gm, fmr);
             row[-h] = vm;
             vmax = fmaxf(vmax, fmaxf(fabsf(vm.x), fabsf(vm.y)));
+        } else {
+            pixel_factors<false>(a, P, ex[hidx], ey[kk], h, k, f, fmr);
         }
+        const float2 v = cmul(g, f);
+        row[h] = v;
+        vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
     }
     // batch maximum for the fixed-point scale of the gridding sums
     for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
