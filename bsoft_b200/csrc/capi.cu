@@ -38,12 +38,26 @@ struct Timed {
     int kind;   // 0 insert, 1 fft2d, 2 h2d
 };
 
+// Batches alternate between two sets of buffers (buf = seq & 1).  Three
+// streams: copy_stream uploads batch i's images, fft_stream runs batch i's
+// 2-D transforms and `stream` grids batch i - 1.  The transforms' blocks
+// are dispatched once the gridding kernel has dispatched all of its own, so
+// they fill the SMs its last (lightest) tiles leave idle.  (At high stream
+// priority they displace gridding blocks instead and the step is slower.)
+// Gridding stays in batch order on `stream`: the accumulation order does
+// not change.
 struct Recon : Context {
     cudaStream_t copy_stream = nullptr;
+    cudaStream_t fft_stream = nullptr;
     float* d_imgbuf[2] = {nullptr, nullptr};
     DevParticle* h_partbuf[2] = {nullptr, nullptr};
+    DevParticle* d_partbuf[2] = {nullptr, nullptr};
+    DevParticle* d_psymbuf[2] = {nullptr, nullptr};
+    size_t psymbuf_cap[2] = {0, 0};
+    float2* d_specbuf[2] = {nullptr, nullptr};
     cudaEvent_t copy_done[2] = {nullptr, nullptr};
-    cudaEvent_t compute_done[2] = {nullptr, nullptr};
+    cudaEvent_t fft_done[2] = {nullptr, nullptr};       // batch's spectra written
+    cudaEvent_t compute_done[2] = {nullptr, nullptr};   // batch gridded: its buffers are free
     std::vector<Timed> timed;
     bool broken = false;
     long seq = 0;                    // batches issued over the context's life (staging buffer = seq & 1)
@@ -179,29 +193,38 @@ static void free_all(Recon* r) {
     for (int i = 0; i < 2; ++i) {
         F(r->d_imgbuf[i]); F(r->d_vol[i]); F(r->d_w[i]); F(r->d_pow[i]); F(r->d_w2[i]);
         F(r->d_half_weighed[i]);
+        F(r->d_partbuf[i]); F(r->d_psymbuf[i]); F(r->d_specbuf[i]);
         if (r->h_partbuf[i]) cudaFreeHost(r->h_partbuf[i]);
         if (r->copy_done[i]) cudaEventDestroy(r->copy_done[i]);
+        if (r->fft_done[i]) cudaEventDestroy(r->fft_done[i]);
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
-    F(r->d_part); F(r->d_psym); F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_spec); F(r->d_tw); F(r->d_twmap);
-    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_fmax); F(r->d_tile_order); F(r->d_part_sums);
+    F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_tw); F(r->d_twmap);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_tile_order); F(r->d_part_sums);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();
     if (r->stream) cudaStreamDestroy(r->stream);
     if (r->copy_stream) cudaStreamDestroy(r->copy_stream);
+    if (r->fft_stream) cudaStreamDestroy(r->fft_stream);
 }
 
-static int run_batch_kernels(Recon* r, const float* d_img, long np, float2* spec_out, bool insert) {
-    cudaStream_t s = r->stream;
+// The batch's 2-D transforms on fft_stream into the spectra buffer `buf`,
+// then (insert) its gridding on `stream` once they are done.
+static int run_batch_kernels(Recon* r, int buf, const float* d_img, long np, bool insert) {
+    cudaStream_t f = r->fft_stream, s = r->stream;
+    float2* spec_out = r->d_specbuf[buf];
     cudaEvent_t a = nullptr, b = nullptr;
-    if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
-    CK(cudaMemsetAsync(r->d_fmax, 0, sizeof(unsigned), s));
-    CK(launch_background(*r, d_img, (int)np, s));
-    CK(launch_rows(*r, d_img, (int)np, s));
-    CK(launch_cols(*r, (int)np, spec_out, s));
+    // the spectra buffer is free once the batch two back has been gridded
+    CK(cudaStreamWaitEvent(f, r->compute_done[buf], 0));
+    if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, f); }
+    CK(launch_background(*r, d_img, (int)np, f));
+    CK(launch_rows(*r, d_img, (int)np, f));
+    CK(launch_cols(*r, (int)np, spec_out, f));
     r->stats.launches += 3;
-    if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 1}); }
+    if (r->timing) { cudaEventRecord(b, f); r->timed.push_back({a, b, 1}); }
+    CK(cudaEventRecord(r->fft_done[buf], f));
+    CK(cudaStreamWaitEvent(s, r->fft_done[buf], 0));
     if (!insert) return BSG_OK;
     for (int h = 0; h < r->nhalves; ++h) {
         if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
@@ -226,29 +249,22 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
         hp[i].spec = (int)i;
     }
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
-    // fixed-point range of the gridding sums: the largest particle weight
-    // and the most contributions one voxel can take from one batch (at most
-    // (2/step + 1)^2 pixels per plane crossing, up to 4 wrap-around aliases)
-    float pwm = 0.f, smin = 1e30f;
-    for (long i = 0; i < np; ++i) { pwm = std::max(pwm, hp[i].pw); smin = std::min(smin, hp[i].step); }
-    r->pw_max = pwm;
-    const double per = 4.0 * pow(2.0 / std::max(1e-3f, smin) + 1.0, 2.0);
-    const int need = (int)ceil(log2((double)np * per + 1.0));
-    r->fix_bits = std::max(20, std::min(44, 62 - need));
-    CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->stream));
+    r->d_part = r->d_partbuf[buf];
+    CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->fft_stream));
     const long nsym = (long)r->sym.size() / 9;
     if (nsym > 1) {
         // one gridding record per (particle, operator): matrix S R, the
         // particle's spectrum (fspace_pack_2D(p, View, sym, ...),
         // Bimage_reconstruct.cpp:248-266)
         const size_t need = (size_t)np * nsym;
-        if (need > r->psym_cap) {
-            if (r->d_psym) cudaFree(r->d_psym);
-            r->d_psym = nullptr;
-            r->psym_cap = 0;
-            CK(cudaMalloc((void**)&r->d_psym, sizeof(DevParticle) * need));
-            r->psym_cap = need;
+        if (need > r->psymbuf_cap[buf]) {
+            if (r->d_psymbuf[buf]) cudaFree(r->d_psymbuf[buf]);
+            r->d_psymbuf[buf] = nullptr;
+            r->psymbuf_cap[buf] = 0;
+            CK(cudaMalloc((void**)&r->d_psymbuf[buf], sizeof(DevParticle) * need));
+            r->psymbuf_cap[buf] = need;
         }
+        r->d_psym = r->d_psymbuf[buf];
         // pageable staging: cudaMemcpyAsync has copied it when it returns,
         // and the device buffer is rewritten in stream order
         r->h_psym.resize(need);
@@ -268,7 +284,7 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
             }
         }
         CK(cudaMemcpyAsync(r->d_psym, r->h_psym.data(), sizeof(DevParticle) * need, cudaMemcpyHostToDevice,
-                           r->stream));
+                           r->fft_stream));
     }
     return BSG_OK;
 }
@@ -296,10 +312,11 @@ static int process(Recon* r, const float* images, const double* params, long npa
                                cudaMemcpyHostToDevice, r->copy_stream));
             if (r->timing) { cudaEventRecord(b, r->copy_stream); r->timed.push_back({a, b, 2}); }
             CK(cudaEventRecord(r->copy_done[buf], r->copy_stream));
-            CK(cudaStreamWaitEvent(r->stream, r->copy_done[buf], 0));
+            CK(cudaStreamWaitEvent(r->fft_stream, r->copy_done[buf], 0));
             d_img = r->d_imgbuf[buf];
         }
-        rc = run_batch_kernels(r, d_img, np, r->d_spec, spectra_out == nullptr);
+        r->d_spec = r->d_specbuf[buf];
+        rc = run_batch_kernels(r, buf, d_img, np, spectra_out == nullptr);
         if (rc) return rc;
         if (spectra_out) {
             // centred device layout -> the reference's pixel order (the four
@@ -386,7 +403,8 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     int rc = BSG_OK;
     auto A = [&](void** p, size_t bytes) { if (!rc) rc = alloc(p, bytes); };
     if (cudaStreamCreateWithFlags(&r->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaStreamCreateWithFlags(&r->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&r->fft_stream, cudaStreamNonBlocking) != cudaSuccess) {
         free_all(r); delete r;
         return fail(BSG_ERR_CUDA, "bsg_recon_create: stream creation failed");
     }
@@ -395,15 +413,18 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
         A((void**)&r->d_imgbuf[i], sizeof(float) * (size_t)n * n * batch);
         if (!rc && cudaMallocHost((void**)&r->h_partbuf[i], sizeof(DevParticle) * batch) != cudaSuccess)
             rc = fail(BSG_ERR_NOMEM, "bsg_recon_create: pinned host allocation");
+        A((void**)&r->d_partbuf[i], sizeof(DevParticle) * batch);
+        A((void**)&r->d_specbuf[i], sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch);
+        if (!rc && cudaMemset(r->d_specbuf[i], 0, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch) != cudaSuccess)
+            rc = fail(BSG_ERR_CUDA, "bsg_recon_create: clearing the spectra buffer");
         if (!rc && (cudaEventCreateWithFlags(&r->copy_done[i], cudaEventDisableTiming) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&r->fft_done[i], cudaEventDisableTiming) != cudaSuccess ||
                     cudaEventCreateWithFlags(&r->compute_done[i], cudaEventDisableTiming) != cudaSuccess))
             rc = fail(BSG_ERR_CUDA, "bsg_recon_create: event creation failed");
     }
-    A((void**)&r->d_part, sizeof(DevParticle) * batch);
     A((void**)&r->d_bkg, sizeof(double) * batch);
     A((void**)&r->d_phase, sizeof(float2) * 2 * ft * (size_t)batch);
     A((void**)&r->d_rows, sizeof(float2) * (size_t)n * (ft / 2 + 1) * batch);
-    A((void**)&r->d_spec, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch);
     A((void**)&r->d_tw, sizeof(float2) * std::max(1, ft / 2));
     A((void**)&r->d_twmap, sizeof(float2) * N);
     for (int h = 0; h < r->nhalves; ++h) {
@@ -416,9 +437,6 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
     if (!rc && cudaHostGetDevicePointer((void**)&r->d_status, r->h_status, 0) != cudaSuccess)
         rc = fail(BSG_ERR_CUDA, "bsg_recon_create: status word mapping");
     if (!rc) *r->h_status = 0;
-    if (!rc && cudaMemset(r->d_spec, 0, sizeof(float2) * (size_t)(ft + 1) * (ft + 2) * batch) != cudaSuccess)
-        rc = fail(BSG_ERR_CUDA, "bsg_recon_create: clearing the spectra buffer");
-    if (!rc) rc = alloc((void**)&r->d_fmax, sizeof(unsigned));
     if (!rc) rc = alloc((void**)&r->d_tile_order, sizeof(int) * (size_t)((N + 7) / 8) * ((N + 7) / 8) * ((N + 7) / 8));
     if (rc) { free_all(r); delete r; return rc; }
     std::vector<float2> tw;
@@ -450,6 +468,7 @@ void bsg_recon_destroy(bsg_recon* h) {
     if (!r) return;
     cudaSetDevice(r->device);
     if (r->stream) cudaStreamSynchronize(r->stream);
+    if (r->fft_stream) cudaStreamSynchronize(r->fft_stream);
     if (r->copy_stream) cudaStreamSynchronize(r->copy_stream);
     free_all(r);
     delete r;
@@ -630,6 +649,7 @@ int bsg_recon_get_stats(bsg_recon* h, bsg_recon_stats* st) {
     if (!r || !st) return fail(BSG_ERR_ARG, "bsg_recon_get_stats: bad argument");
     CK(cudaSetDevice(r->device));
     CK(cudaStreamSynchronize(r->stream));
+    CK(cudaStreamSynchronize(r->fft_stream));
     CK(cudaStreamSynchronize(r->copy_stream));
     for (auto& t : r->timed) {
         float ms = 0.f;
@@ -650,6 +670,7 @@ int bsg_recon_synchronize(bsg_recon* h) {
     if (!r) return fail(BSG_ERR_ARG, "bsg_recon_synchronize: null context");
     CK(cudaSetDevice(r->device));
     CK(cudaStreamSynchronize(r->copy_stream));
+    CK(cudaStreamSynchronize(r->fft_stream));
     CK(cudaStreamSynchronize(r->stream));
     return check_status(r);
 }

@@ -19,18 +19,17 @@ struct Context {
 
     // per-batch device buffers
     float* d_img = nullptr;          // batch x n x n
-    DevParticle* d_part = nullptr;   // batch
+    DevParticle* d_part = nullptr;   // batch (the current batch's buffer)
     // point-group symmetry (fspace_pack_2D over symmetry_get_all_views):
     // nsym operators S (row-major); particle records are gridded once per
     // operator with matrix S R, all copies reading the particle's spectrum
     std::vector<double> sym;          // 9 per operator; empty = C1
-    DevParticle* d_psym = nullptr;    // batch x nsym expanded records
-    size_t psym_cap = 0;
+    DevParticle* d_psym = nullptr;    // batch x nsym expanded records (current batch)
     std::vector<DevParticle> h_psym;
     double* d_bkg = nullptr;         // batch
     float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
     float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms
-    float2* d_spec = nullptr;        // batch x (ft+1) x (ft+2): centred, padded particle spectra
+    float2* d_spec = nullptr;        // batch x (ft+1) x (ft+2): centred, padded particle spectra (current batch)
     float2* d_tw = nullptr;          // ft/2 twiddles exp(-2 pi i j / ft)
     float2* d_twmap = nullptr;       // N/2 twiddles exp(-2 pi i j / N)
 
@@ -49,10 +48,6 @@ struct Context {
     float2* d_half_weighed[2] = {nullptr, nullptr};
     double* d_fsc = nullptr;         // FSC partial sums
 
-    // batch statistics for the fixed-point gridding sums
-    unsigned* d_fmax = nullptr;      // max |Re F|, |Im F| of the batch (float bits)
-    float pw_max = 0.f;              // max particle weight of the batch
-    int fix_bits = 44;               // largest |F w| maps below 2^fix_bits
     int shape = 0;                   // gridding tile shape (insert.cu kShapes)
     int* d_tile_order = nullptr;     // tile visiting order for `shape`
     int replicas = 1;                // warps per tile, each on a slice of the particles

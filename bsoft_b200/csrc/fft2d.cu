@@ -124,7 +124,6 @@ struct ColArgs {
     const DevParticle* part;
     const float2* tw;
     float2* spec;
-    unsigned* fmax_bits;   // running max of |Re|, |Im| over the batch
     int n, ft, logft;
     int ctf_action;
     double wiener;
@@ -219,7 +218,6 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
     const int pitch = ft + 2, hf = ft / 2;
     float2* out = a.spec + (size_t)b * (ft + 1) * pitch;
     const int fm = ft - 1;
-    float vmax = 0.f;
     for (int i = threadIdx.x; i < COL_W * ft; i += blockDim.x) {
         const int c = i % COL_W, kk = i / COL_W;
         const int hidx = h0 + c;
@@ -236,17 +234,11 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
             gm.y = -gm.y;
             const float2 vm = cmul(gm, fmr);
             row[-h] = vm;
-            vmax = fmaxf(vmax, fmaxf(fabsf(vm.x), fabsf(vm.y)));
         } else {
             pixel_factors<false>(a, P, ex[hidx], ey[kk], h, k, f, fmr);
         }
-        const float2 v = cmul(g, f);
-        row[h] = v;
-        vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
+        row[h] = cmul(g, f);
     }
-    // batch maximum for the fixed-point scale of the gridding sums
-    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    if ((threadIdx.x & 31) == 0 && a.fmax_bits) atomicMax(a.fmax_bits, __float_as_uint(vmax));
 }
 
 cudaError_t launch_background(const Context& c, const float* img, int nimg, cudaStream_t s) {
@@ -265,7 +257,7 @@ cudaError_t launch_rows(const Context& c, const float* img, int nimg, cudaStream
 cudaError_t launch_cols(const Context& c, int nimg, float2* spectra, cudaStream_t s) {
     ColArgs a;
     a.rows = c.d_rows; a.bkg = c.d_bkg; a.phase = c.d_phase; a.part = c.d_part; a.tw = c.d_tw;
-    a.spec = spectra; a.fmax_bits = c.d_fmax; a.n = c.g.n; a.ft = c.g.ft; a.logft = c.g.logft;
+    a.spec = spectra; a.n = c.g.n; a.ft = c.g.ft; a.logft = c.g.logft;
     a.ctf_action = c.g.ctf_action; a.wiener = c.g.wiener; a.shi2 = c.g.ctf_shi2;
     const int hw = c.g.ft / 2 + 1;
     dim3 grid((hw + COL_W - 1) / COL_W, nimg);

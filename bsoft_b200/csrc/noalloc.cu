@@ -170,7 +170,6 @@ extern "C" int bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const f
     c.d_bkg = reinterpret_cast<double*>(sc + L.bkg);
     c.d_phase = reinterpret_cast<float2*>(sc + L.phase);
     c.d_rows = reinterpret_cast<float2*>(sc + L.rows);
-    c.d_fmax = nullptr;
     float2* spec = reinterpret_cast<float2*>(sc + L.spec);
 
     // particle records: converted on the host in small stack chunks and

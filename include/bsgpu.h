@@ -26,8 +26,9 @@
  * Conventions: every function returns 0 (BSG_OK) or a negative BSG_ERR_*
  * code and leaves a message for bsg_last_error() (thread-local), the way the
  * reference returns NULL / <0 after error_show (bsoft/src/util/utilities.cpp:745).
- * Host buffers are caller-owned; a context owns its device memory and one
- * CUDA stream, and is used by one host thread at a time.
+ * Host buffers are caller-owned; a context owns its device memory and its
+ * CUDA streams (bsg_recon_stream returns the one the gridding and finishing
+ * run on), and is used by one host thread at a time.
  */
 #ifndef BSGPU_H
 #define BSGPU_H
@@ -84,7 +85,8 @@ typedef struct {
     long   launches;          /* all kernels this library launched          */
     long   insert_launches;   /* gridding kernel launches                   */
     double insert_ms;         /* summed device time of the gridding kernel  */
-    double fft2d_ms;          /* background + row + column passes           */
+    double fft2d_ms;          /* background + row + column passes, elapsed on
+                                 their stream (they overlap the gridding)   */
     double h2d_ms;            /* host-to-device copies of particle images   */
     long   particles;         /* particles inserted                         */
 } bsg_recon_stats;
@@ -94,7 +96,12 @@ void bsg_recon_destroy(bsg_recon* r);
 
 /* Insert nparts particles: images (nparts x n x n float32, x fastest) and
  * params (nparts x BSG_PARTICLE_DOUBLES, host).  Accumulation order is fixed
- * (particle order, then pixel order), so results are bitwise reproducible. */
+ * (particle order, then pixel order), so results are bitwise reproducible.
+ * The call is asynchronous: the images (host, where pinned buffers are read
+ * by an asynchronous copy, or device with BSG_DEVICE_PTR, which must be
+ * complete when the call is made) stay unchanged until
+ * bsg_recon_synchronize.  One batch's 2-D transforms overlap the previous
+ * batch's gridding. */
 int  bsg_recon_insert(bsg_recon* r, const float* images, const double* params,
                       long nparts, int flags);
 
