@@ -216,33 +216,35 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
         const int k0 = k_lo + pk;
         if (k0 > k_hi) break;
         const int nrows = (k_hi - k0) / Lk + 1;
-        for (int ph = 0; ph < Lh; ++ph) {
-            if (sh == 0 && h_lo + ph > h_hi) break;
-            for (int jb = 0; jb < nrows; jb += 32) {
-                // lane j: exact lattice range of row k = k0 + Lk (jb + j)
-                const int j = jb + lane;
-                int hfirst = 0, cnt = 0, k = 0;
-                if (j < nrows) {
-                    k = k0 + Lk * j;
+        for (int jb = 0; jb < nrows; jb += 32) {
+            // lane j: the exact h range [hl, hh] of row k = k0 + Lk (jb + j),
+            // shared by the Lh phases that walk this row
+            const int j = jb + lane;
+            const int k = k0 + Lk * j;
+            double hl = h_lo, hh = h_hi;
+            bool live = j < nrows;
+            if (live) {
+                for (int i = 0; i < 3; ++i) {
+                    const double base = k * P.bd[i];
+                    if (ia[i] != 0.0) {
+                        double p0 = (lo[i] - base) * ia[i], p1 = (hi[i] - base) * ia[i];
+                        if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
+                        hl = fmax(hl, p0);
+                        hh = fmin(hh, p1);
+                    } else if (!(base > lo[i] && base < hi[i])) {
+                        live = false;
+                    }
+                }
+                live = live && hl <= hh;
+            }
+            for (int ph = 0; ph < Lh; ++ph) {
+                if (sh == 0 && h_lo + ph > h_hi) break;
+                int hfirst = 0, cnt = 0;
+                if (live) {
+                    // lattice h = h0 + Lh i inside [hl, hh]
                     const int h0 = h_lo + ph + sh * j;
-                    double hl = h_lo, hh = h_hi;
-                    bool empty = false;
-                    for (int i = 0; i < 3; ++i) {
-                        const double base = k * P.bd[i];
-                        if (ia[i] != 0.0) {
-                            double p0 = (lo[i] - base) * ia[i], p1 = (hi[i] - base) * ia[i];
-                            if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
-                            hl = fmax(hl, p0);
-                            hh = fmin(hh, p1);
-                        } else if (!(base > lo[i] && base < hi[i])) {
-                            empty = true;
-                        }
-                    }
-                    if (!empty && hl <= hh) {
-                        // lattice h = h0 + Lh i inside [hl, hh]
-                        const int i0 = (int)ceil((hl - h0) / Lh), i1 = (int)floor((hh - h0) / Lh);
-                        if (i1 >= i0) { hfirst = h0 + Lh * i0; cnt = i1 - i0 + 1; }
-                    }
+                    const int i0 = (int)ceil((hl - h0) / Lh), i1 = (int)floor((hh - h0) / Lh);
+                    if (i1 >= i0) { hfirst = h0 + Lh * i0; cnt = i1 - i0 + 1; }
                 }
                 // exclusive scan of the row counts
                 int incl = cnt;
@@ -252,6 +254,7 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                     if (lane >= o) incl += v;
                 }
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
+                if (total == 0) continue;
                 s_row[lane] = incl;                        // inclusive end of row j
                 s_row[32 + lane] = hfirst;
                 s_row[64 + lane] = k;
