@@ -38,12 +38,19 @@ __global__ void background_kernel(const float* __restrict__ img, const DevPartic
     const int b = blockIdx.x;
     const float* im = img + (size_t)b * n * n;
     const DevParticle& P = part[b];
-    const double h = (double)(n / 2);
+    const int hn = n / 2;
+    const double h = (double)hn;
+    // dividing by a power of two is multiplying by its exact reciprocal:
+    // the same doubles without the division sequence
+    const bool pow2 = (hn & (hn - 1)) == 0;
+    const double ih = 1.0 / h;
     double sum = 0.0;
     int cnt = 0;
     for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
         int y = i / n, x = i - y * n;
-        double x2 = (x - P.bx) / h, y2 = (y - P.by) / h;
+        double x2, y2;
+        if (pow2) { x2 = (x - P.bx) * ih; y2 = (y - P.by) * ih; }
+        else { x2 = (x - P.bx) / h; y2 = (y - P.by) / h; }
         if (x2 * x2 + y2 * y2 - 1 > 0) { sum += im[i]; ++cnt; }
     }
     // deterministic block reduction (fixed tree)
