@@ -3,7 +3,7 @@
 // pipeline (image upload, 2-D stage, gridding) and map finishing.
 #include "context.cuh"
 #include "fft_dev.cuh"
-
+#include "lattice.h"
 
 #include <math.h>
 #include <stdarg.h>
@@ -122,6 +122,7 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
     if (pad_ratio > 1) { pad_ratio *= pad_ratio * 0.6; pw /= pad_ratio; }
     d.pw = (float)pw;
     d.half = (int)q[23];
+    d.lat = pack_lattice(choose_lattice(d.ad, d.bd));
 }
 
 static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {

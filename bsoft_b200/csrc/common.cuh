@@ -41,6 +41,8 @@ struct alignas(16) DevParticle {
     float  step;            // |ad| = voxels per pixel step
     int    half;            // half-map index
     int    spec;            // index of this record's spectrum in the batch (symmetry copies share it)
+    int    lat;             // gridding phase lattice lh | lk << 12 | sh << 24 (lattice.h); 0: the
+                            // orientation-independent one
 };
 
 // Run geometry shared by all kernels of one context.

@@ -197,14 +197,19 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     const int k_lo = max((int)ceil(vc - hv), -hf), k_hi = min((int)floor(vc + hv), hf - 1);
     const int h_lo = max((int)ceil(uc - hu), -hf), h_hi = min((int)floor(uc + hu), hf - 1);
     if (k_lo > k_hi || h_lo > h_hi) return;
-    // Conflict-free lattice: two points of one phase are >= sqrt(3) voxels
-    // apart.  Square lattice L x L pixels (L = ceil(sqrt(3)/step)), or, where
-    // it has fewer phases, the lattice spanned by (4, 0) and (2, 3) pixels
-    // (shortest vector sqrt(13) pixels; 12 phases instead of 16 at step 0.5).
+    // Conflict-free lattice: two points of one phase never share a unit cell
+    // of the map.  P.lat, when set, is the smallest such lattice for this
+    // particle's orientation (lattice.h; 5 to 9 phases at step 0.5).  Else
+    // one safe for every orientation, whose points are >= sqrt(3) voxels
+    // apart: the square lattice of L x L pixels (L = ceil(sqrt(3)/step)), or,
+    // where it has fewer phases, the lattice spanned by (4, 0) and (2, 3)
+    // pixels (shortest vector sqrt(13) pixels; 12 phases at step 0.5).
     // Row j of phase (ph, pk) is k = k_lo + pk + Lk j, its points
     // h = h_lo + ph + sh j + Lh i.
     int Lh, Lk, sh;
-    {
+    if (P.lat) {
+        Lh = P.lat & 0xfff; Lk = (P.lat >> 12) & 0xfff; sh = (P.lat >> 24) & 0x7f;
+    } else {
         const int L = max(1, (int)ceilf(1.7320508f * P.inv_step));
         if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f) { Lh = 4; Lk = 3; sh = 2; }
         else { Lh = L; Lk = L; sh = 0; }
