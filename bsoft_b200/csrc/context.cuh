@@ -18,7 +18,6 @@ struct Context {
     cudaStream_t stream = nullptr;
 
     // per-batch device buffers
-    float* d_img = nullptr;          // batch x n x n
     DevParticle* d_part = nullptr;   // batch (the current batch's buffer)
     // point-group symmetry (fspace_pack_2D over symmetry_get_all_views):
     // nsym operators S (row-major); particle records are gridded once per
@@ -55,13 +54,8 @@ struct Context {
     int* d_status = nullptr;         // device view of h_status (mapped)
     int* h_status = nullptr;         // kernel-reported failures (bounded waits)
 
-    // host staging (pinned)
-    DevParticle* h_part = nullptr;
-    float* h_stage = nullptr;        // batch x n x n pinned image staging
-
     bool timing = false;
     bsg_recon_stats stats{};
-    cudaEvent_t ev[8]{};
 
     size_t spec_elems() const { return (size_t)(g.ft + 1) * (g.ft + 2); }
     int spec_pitch() const { return g.ft + 2; }
