@@ -788,7 +788,9 @@ def main():
         achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
         # DRAM bytes per launch from one ncu capture of this configuration (8^3
         # tiles, 2,000 particles per launch: profiles/insert_kernel_batched-
-        # insertion-256.md); other configurations were not captured
+        # insertion-256.md), taken with the orientation-independent 12-phase
+        # lattice; the per-particle lattice reads the same spectra in a
+        # different order. Other configurations were not captured.
         traffic = 11.947e9 if (int(shape) == 0 and B == 2000 and BOX == 256) else None
         roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
