@@ -86,7 +86,7 @@ def test_defocus_search_needs_a_defocus(setup):
     from bsoft_b200._lib import BsgError
     m, d = setup
     if d["def_std"] > 0:
-        pytest.skip("the CTF-free fixtures hold images without a defocus")
+        pytest.skip("this fixture's images have a defocus; the rejection applies to CTF-free images")
     with pytest.raises(BsgError):
         _refine(m, d, def_std=300.0)
 
