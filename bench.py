@@ -139,18 +139,15 @@ def plan_for(w):
                      ctf_action=1, wiener=0.0, params=w["params"], nmaps=1)
 
 
-def reference_sample(w, n_sample: int, threads: int):
-    """Time the reference's breconstruct on `n_sample` particles of the
-    workload written as MRC + STAR (writing is not timed)."""
-    import oracle
+def reference_project(w, n_sample: int) -> str:
+    """The first `n_sample` particles of the workload as an MRC stack and a
+    STAR project in a new temporary directory (returned); the project file
+    is p.star."""
     from bsoft_b200.ctf import CTFParams
     from bsoft_b200.geometry import matrix_to_view
     from bsoft_b200.io import mrc
     from bsoft_b200.plan import P_CTF, P_MAT, P_ORIGIN
     from bsoft_b200.project import Micrograph, Project, write_project
-    exe = oracle.ref_binary("breconstruct")
-    if not os.path.exists(exe):
-        return None, "oracle/_ref/breconstruct not built"
     d = tempfile.mkdtemp(prefix="bench_ref_")
     P = w["params"][:n_sample]
     imgs = w["pool"][np.arange(n_sample) % w["pool"].shape[0]]
@@ -169,6 +166,17 @@ def reference_sample(w, n_sample: int, threads: int):
         view=views, defocus=defocus, magnification=np.ones(n_sample), select=np.ones(n_sample, dtype=np.int64),
         pixel=np.full(n_sample, w["pixel"])))
     write_project(os.path.join(d, "p.star"), proj)
+    return d
+
+
+def reference_sample(w, n_sample: int, threads: int):
+    """Time the reference's breconstruct on `n_sample` particles of the
+    workload written as MRC + STAR (writing is not timed)."""
+    import oracle
+    exe = oracle.ref_binary("breconstruct")
+    if not os.path.exists(exe):
+        return None, "oracle/_ref/breconstruct not built"
+    d = reference_project(w, n_sample)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     t0 = time.perf_counter()
     r = subprocess.run([exe, "-interp", "trilinear", "-CTF", "flip", "-threads", str(threads), "-recon",
