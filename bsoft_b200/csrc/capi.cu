@@ -553,6 +553,56 @@ int bsg_recon_accumulators(bsg_recon* h, int half, double* vol_out, double* weig
     return BSG_OK;
 }
 
+namespace bsg {
+// dst[i] += src[i]: one shard's partial sums into the accumulators
+__global__ void add_partial_kernel(double* __restrict__ dst, const double* __restrict__ src, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+}  // namespace bsg
+
+int bsg_recon_add_partial(bsg_recon* h, int half, const double* vol, const double* weight, const double* power,
+                          const double* weight2, int flags) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || half < 0 || half >= r->nhalves) return fail(BSG_ERR_ARG, "bsg_recon_add_partial: bad half %d", half);
+    if (!vol || !weight) return fail(BSG_ERR_ARG, "bsg_recon_add_partial: vol and weight are required");
+    if ((power == nullptr) != (weight2 == nullptr))
+        return fail(BSG_ERR_ARG, "bsg_recon_add_partial: give power and weight2 together");
+    if (power && !r->g.fom) return fail(BSG_ERR_STATE, "bsg_recon_add_partial: power sums need fom = 1");
+    CK(cudaSetDevice(r->device));
+    const size_t N3 = r->vol_elems();
+    const bool dev = flags & BSG_DEVICE_PTR;
+    double* stage = nullptr;
+    if (!dev) {
+        // host sums pass through the finishing work buffer (N^3 complex
+        // floats = N^3 doubles), in stream order with the gridding
+        int rc = ensure_finish_buffers(r);
+        if (rc) return rc;
+        stage = reinterpret_cast<double*>(r->d_work);
+    }
+    auto add = [&](double* dst, const double* src, size_t n) -> int {
+        for (size_t off = 0; off < n; off += N3) {
+            const size_t cnt = std::min(N3, n - off);
+            const double* s = src + off;
+            if (!dev) {
+                CK(cudaMemcpyAsync(stage, s, sizeof(double) * cnt, cudaMemcpyHostToDevice, r->stream));
+                s = stage;
+            }
+            add_partial_kernel<<<148 * 8, 256, 0, r->stream>>>(dst + off, s, cnt);
+            CK(cudaGetLastError());
+            r->stats.launches += 1;
+        }
+        return BSG_OK;
+    };
+    int rc = add(reinterpret_cast<double*>(r->d_vol[half]), vol, 2 * N3);
+    if (!rc) rc = add(r->d_w[half], weight, N3);
+    if (!rc && power) rc = add(r->d_pow[half], power, N3);
+    if (!rc && weight2) rc = add(r->d_w2[half], weight2, N3);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(r->stream));
+    return BSG_OK;
+}
+
 int bsg_recon_fsc(bsg_recon* h, int nshell, double* fsc_out) {
     Recon* r = reinterpret_cast<Recon*>(h);
     if (!r || !fsc_out || nshell < 1) return fail(BSG_ERR_ARG, "bsg_recon_fsc: bad argument");

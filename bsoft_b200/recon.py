@@ -118,6 +118,21 @@ class Reconstructor:
                                                       C.c_void_p(w.ctypes.data), 0), "bsg_recon_accumulators")
         return vol[..., 0] + 1j * vol[..., 1], w
 
+    def add_partial(self, vol: np.ndarray, weight: np.ndarray, half: int = 0) -> None:
+        """Add another shard's accumulators (as `accumulators` returns them:
+        complex vol, weight) into half `half` of this context, the
+        reference's partial-map sum before weighing."""
+        N = self.N
+        v = np.empty((N, N, N, 2), dtype=np.float64)
+        v[..., 0] = np.real(vol)
+        v[..., 1] = np.imag(vol)
+        w = np.ascontiguousarray(weight, dtype=np.float64)
+        if w.size != N ** 3:
+            raise ValueError(f"weight has {w.size} values, the map {N ** 3}")
+        _lib.check(_lib.load().bsg_recon_add_partial(self._h, half, C.c_void_p(v.ctypes.data),
+                                                     C.c_void_p(w.ctypes.data), None, None, 0),
+                   "bsg_recon_add_partial")
+
     def fsc(self, nshell: int | None = None) -> np.ndarray:
         nshell = nshell or self.N // 2
         out = np.zeros(nshell)

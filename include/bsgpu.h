@@ -116,6 +116,18 @@ int  bsg_recon_finish(bsg_recon* r, int imap, float* map_out, float* fom_out, in
  * accumulators are kept in FP64 on the device). */
 int  bsg_recon_accumulators(bsg_recon* r, int half, double* vol_out, double* weight_out, int flags);
 
+/* Add another reconstruction's partial sums into half h of this context:
+ * the reference's partial-map sum before weighing (img_reconstruction_sum_
+ * weigh, bsoft/src/mg/mg_reconstruct.cpp:263-324, over the per-thread maps
+ * of breconstruct.cpp:268-305).  With particles split across GPUs, each
+ * shard's accumulators (bsg_recon_accumulators) are added, in shard order,
+ * into one context, which then finishes the map; the sum is FP64, so the
+ * result depends only on that order.  vol: 2*N^3 doubles, weight: N^3;
+ * power and weight2 (N^3 each, both or neither) need fom = 1.  Host or
+ * device (BSG_DEVICE_PTR) pointers; returns when the sums have been added. */
+int  bsg_recon_add_partial(bsg_recon* r, int half, const double* vol, const double* weight,
+                           const double* power, const double* weight2, int flags);
+
 /* Fourier shell correlation of the two weighed half-map transforms
  * (nmaps >= 2) as Bimage::fsc(Bimage*) forms it: shells linearly
  * interpolated, sampling ratio 1, FSC[0] = 1, shells from
