@@ -18,6 +18,8 @@
  *                           mg_reconstruct.cpp:266-361) + fft_back
  *                           (Bimage.h:903-908) + filter_sinc
  *                           (breconstruct.cpp:328-359)
+ *   bsg_recon_add_partial <- the partial-map sum in img_reconstruction_sum_weigh
+ *                           (mg_reconstruct.cpp:263-324), across GPUs
  *   bsg_recon_fsc        <- Bimage::fsc (bsoft/src/img/Bimage_resolution.cpp:330-406)
  *   bsg_particle_spectra <- the 2-D half of particle_reconstruct
  *                           (Bimage::fft + phase_shift_to_origin +
