@@ -122,25 +122,30 @@ def finish(plan, vol, weight, power=None, weight2=None, sinc=None):
     return out.reshape(plan.map, plan.map, plan.map), cov
 
 
+def symmetry_ops(sym: str):
+    """The generating operations (axis, order) of Bsymmetry::Bsymmetry
+    (bsoft/src/util/symmetry.cpp:53-99) for Cn, Dn, T, O, I, in its order."""
+    g = (sym or "C1").strip().upper()
+    phi = (1 + 5 ** 0.5) / 2
+    if g[0] == "C":
+        return [((0, 0, 1), int(g[1:] or 1))]
+    if g[0] == "D":
+        return [((0, 0, 1), int(g[1:])), ((1, 0, 0), 2)]
+    if g == "T":
+        return [((1, 1, 1), 3), ((0, 0, 1), 2), ((1, 0, 0), 2)]
+    if g == "O":
+        return [((1, 1, 1), 3), ((0, 0, 1), 4), ((1, 0, 0), 2)]
+    if g == "I":
+        return [((1, 1, 1), 3), ((1, 1 / phi, phi), 2), ((1 / phi, 1, 0), 5), ((0, 0, 1), 2)]
+    raise ValueError(sym)
+
+
 def symmetry_matrices(sym: str) -> np.ndarray:
     """Group elements of a point group as rotation matrices, in the order of
     symmetry_get_all_views (bsoft/src/util/symmetry.cpp:277-319) with the
     generating operations of Bsymmetry::Bsymmetry (symmetry.cpp:53-99):
     Cn, Dn, T, O, I."""
-    g = (sym or "C1").strip().upper()
-    phi = (1 + 5 ** 0.5) / 2
-    if g[0] == "C":
-        ops = [((0, 0, 1), int(g[1:] or 1))]
-    elif g[0] == "D":
-        ops = [((0, 0, 1), int(g[1:])), ((1, 0, 0), 2)]
-    elif g == "T":
-        ops = [((1, 1, 1), 3), ((0, 0, 1), 2), ((1, 0, 0), 2)]
-    elif g == "O":
-        ops = [((1, 1, 1), 3), ((0, 0, 1), 4), ((1, 0, 0), 2)]
-    elif g == "I":
-        ops = [((1, 1, 1), 3), ((1, 1 / phi, phi), 2), ((1 / phi, 1, 0), 5), ((0, 0, 1), 2)]
-    else:
-        raise ValueError(sym)
+    ops = symmetry_ops(sym)
 
     def rot(axis, ang):
         a = np.asarray(axis, float) / np.linalg.norm(axis)
