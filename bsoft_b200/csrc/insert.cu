@@ -17,12 +17,15 @@
 // walks the pixels of each particle that reaches it, in particle order.
 //
 // Conflict-free lanes: the pixels of a particle's footprint are visited on
-// a lattice whose points are at least sqrt(3) voxels apart in the map (a
-// square lattice of L = ceil(sqrt(3)/step) pixels, step = voxels per pixel,
-// or at step 0.5 the 12-phase lattice spanned by (4, 0) and (2, 3) pixels),
-// one phase after another.  Two such points have different base voxels
-// floor(m), so for any one corner offset the lanes of a warp touch distinct
-// voxels: a plain read-modify-write of shared memory is exact.
+// a lattice whose points never share a unit cell of the map, one phase
+// after another.  Each particle record carries the smallest such lattice
+// for its orientation (lattice.h; 5 to 9 phases at step 0.5); without one,
+// a lattice safe for every orientation is used (points at least sqrt(3)
+// voxels apart: L x L pixels with L = ceil(sqrt(3)/step), step = voxels per
+// pixel, or at step 0.5 the 12-phase lattice spanned by (4, 0) and (2, 3)
+// pixels).  Two points of a phase have different base voxels floor(m), so
+// for any one corner offset the lanes of a warp touch distinct voxels: a
+// plain read-modify-write of shared memory is exact.
 // The order of every voxel's sum (particle, alias, phase, lattice point,
 // corner) is fixed, so results are bitwise reproducible.  Tiles are visited
 // heaviest first (nearest to the Fourier origin, where every particle's
@@ -32,8 +35,8 @@
 //
 // Each phase's lattice points are enumerated exactly: lane j computes the
 // h-interval of lattice row j from the three slab constraints of the tile
-// box, a warp scan turns the row counts into offsets, and lanes take points
-// in order.
+// box (once for all phases that walk that row), a warp scan turns the row
+// counts into offsets, and lanes take points in order.
 #include "context.cuh"
 
 #include <math.h>
