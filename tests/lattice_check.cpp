@@ -68,6 +68,21 @@ int main(int argc, char** argv) {
             }
         }
     }
+    // very fine steps: the square lattice of side ceil(reach) (packable), and
+    // beyond the 12-bit fields no lattice at all (the kernel's own rule)
+    {
+        const double ad[3] = {1e-3, 0, 0}, bd[3] = {0, 1e-3, 0};
+        const bsg::PhaseLattice L = bsg::choose_lattice(ad, bd);
+        if (L.lh != L.lk || L.sh != 0 || L.lh < 1732 || bsg::pack_lattice(L) == 0) {
+            printf("fine step: lattice %d %d %d\n", L.lh, L.lk, L.sh);
+            return 1;
+        }
+        const double ad2[3] = {1e-4, 0, 0}, bd2[3] = {0, 1e-4, 0};
+        if (bsg::pack_lattice(bsg::choose_lattice(ad2, bd2)) != 0) {
+            printf("finest step: expected no lattice\n");
+            return 1;
+        }
+    }
     printf("points %ld collisions %ld more_phases_than_before %ld phases_at_step_0.5:", checked, collisions, worse);
     for (int d = 1; d <= 16; ++d)
         if (hist[d]) printf(" %d:%ld", d, hist[d]);
