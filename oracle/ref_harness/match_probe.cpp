@@ -7,7 +7,8 @@
 //   <out>.map    float[2*diam^3]          prepared reference transform
 //   <out>.sec    float[2*diam^2] per view  central sections (hi_res/1.11)
 //   <out>.img    float[2*diam^2] per image prepared particle transforms
-//   <out>.fom    text "fom cv" per hypothesis (img_recip_space_fom)
+//   <out>.fom    text "fom cv" per hypothesis (img_recip_space_fom; FRC, or
+//                DPR with MATCH_PROBE_FOM_TYPE=1 in the environment)
 // Usage:
 //   match_probe map.mrc stack.mrc pixel hi_res views.txt ctf.txt hyps.txt out [width power]
 // views.txt: "x y z angle(rad)" per view; ctf.txt: "volt abw00 abw20 abw22 abw2m2
@@ -109,6 +110,8 @@ int main(int argc, char** argv) {
 	std::ofstream fo(out + ".fom");
 	fo.precision(17);
 	vector<double> weight;
+	// MATCH_PROBE_FOM_TYPE=1 scores with the DPR form (brefine -fomtype dpr)
+	const int fom_type = getenv("MATCH_PROBE_FOM_TYPE") ? atoi(getenv("MATCH_PROBE_FOM_TYPE")) : 0;
 	for ( auto& h : hyps ) {
 		long ii = (long)h[0], vv = (long)h[1];
 		Bimage* pcopy = imgs[ii]->copy();
@@ -122,7 +125,7 @@ int main(int argc, char** argv) {
 		c.aberration_weight(2, -2, ctfs[ii][4]);
 		c.aberration_weight(4, 0, ctfs[ii][5]);
 		int flags = (ctfs[ii].size() > 6 && ctfs[ii][6] > 0) ? APPLY_CTF : 0;
-		double fom = img_recip_space_fom(pcopy, secs[vv], hi_res, 0, 0, weight, flags, &c);
+		double fom = img_recip_space_fom(pcopy, secs[vv], hi_res, 0, fom_type, weight, flags, &c);
 		fo << fom << " " << pcopy->image->FOM() << "\n";
 		delete pcopy;
 	}

@@ -13,6 +13,7 @@ MATCH_CASES = ["match64", "match32"]
 def load(case: str):
     z = np.load(os.path.join(GOLDEN, case + ".npz"))
     d = {k: z[k] for k in z.files}
+    d["name"] = case
     d["N"] = int(d["map"].shape[0])
     d["n"] = int(d["images"].shape[1])
     d["pixel"] = float(d["pixel"])

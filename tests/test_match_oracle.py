@@ -72,6 +72,26 @@ def test_figure_of_merit(case):
         assert abs(fo - f) < 1e-6 and abs(cvo - cv) < 1e-6
 
 
+def test_figure_of_merit_dpr(case):
+    """The DPR form (brefine -fomtype dpr) of the same hypotheses against the
+    reference's (tests/golden/match_dpr.npz, make_match_dpr_golden.py)."""
+    import os
+    from tests.helpers import GOLDEN
+    d = case
+    ref = np.load(os.path.join(GOLDEN, "match_dpr.npz"))[d["name"]]
+    D, N = d["diam"], d["N"]
+    samp = d["pixel"] * N / D
+    k = oracle.fsi_kernel(8, 2)
+    secs = [oracle.central_section(d["spec"], m, D * samp, d["hi_res"] / 1.11, k) for m in d["mats"]]
+    preps = [oracle.match_particle(img, D, float(d["file_avg"]), float(d["file_std"])) for img in d["images"]]
+    for (i, v, ox, oy), (f, cv) in zip(d["hyps"], ref):
+        x = oracle.phase_shift_2d(preps[int(i)], (ox * D / N, oy * D / N))
+        row = d["ctf_rows"][int(i)]
+        fo, cvo = oracle.recip_space_fom(x, secs[int(v)], d["n"] * d["pixel"], D * samp, samp, d["hi_res"],
+                                         fom_type=1, ctf=row[1:6] if row[6] > 0 else None)
+        assert abs(fo - f) < 1e-6 and abs(cvo - cv) < 1e-6, (fo, f, cvo, cv)
+
+
 def test_true_view_scores_best(case):
     """With the CTF applied to the reference, the generating view and origin
     score above the random views (without it the CTF-modulated images
