@@ -48,10 +48,12 @@ extrapolated to the GPU leg's hypotheses per particle; the GPU refines the
 same particle with the same steps and the two results are compared.
 
 `--impl reference` times only the reference CPU implementation (rank 0).
-Multi-GPU (`torchrun --nproc-per-node N`): each rank reconstructs its own
-shard of particles (weak scaling) and the partial maps are summed with one
-NCCL all-reduce before finishing, as the reference sums per-thread partial
-maps (mg_reconstruct.cpp:306-324).
+Multi-GPU (`torchrun --nproc-per-node N`): replicas only.  Every rank runs
+the same insertion workload on its own GPU (weak scaling, no collective
+while inserting); timing is the max over ranks.  The partial-map sum that a
+particle split across GPUs would need (the reference's sum of per-thread
+maps, mg_reconstruct.cpp:306-324) is bsoft_b200.shard, not part of the
+timed step.
 """
 from __future__ import annotations
 
@@ -128,8 +130,8 @@ class ClockSampler:
 def make_workload(n_particles, rank=0, world=1):
     from bsoft_b200.synth import batched_insertion_workload
     w = batched_insertion_workload(n_particles=n_particles, box=BOX, pool=512)
-    # shard: rank r takes particles r, r+world, ... (weak scaling keeps the
-    # per-rank count fixed by generating world x particles)
+    # every rank inserts the same synthetic particles (replicas; weak
+    # scaling keeps the per-rank count fixed)
     return w
 
 

@@ -521,7 +521,7 @@ int bsg_particle_spectra(bsg_recon* h, const float* images, const double* params
 int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int flags) {
     Recon* r = reinterpret_cast<Recon*>(h);
     if (!r || !map_out) return fail(BSG_ERR_ARG, "bsg_recon_finish: bad argument");
-    if (imap < 0 || imap > 2 || (imap > 0 && r->nhalves < 2) || (imap == 0 && r->cfg.nmaps == 2 && false))
+    if (imap < 0 || imap > 2 || (imap > 0 && r->nhalves < 2))
         return fail(BSG_ERR_ARG, "bsg_recon_finish: map %d not available (nmaps = %d)", imap, r->cfg.nmaps);
     if (fom_out && !r->g.fom) return fail(BSG_ERR_ARG, "bsg_recon_finish: FOM requested but fom = 0");
     CK(cudaSetDevice(r->device));

@@ -181,12 +181,11 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
 }
 
 // Walk the pixels of particle P (alias origin o) whose contributions can
-// reach the tile, phase by phase of the lattice.
-template <bool FOM, bool GATE, int TX, int TY, int TZ>
-__device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevParticle& P, const float2* S,
-                                                 const TileAcc& A, double ox, double oy, double oz, int lane,
-                                                 int* s_row) {
-    const int hf = a.ft / 2;
+// reach the tile, phase by phase of the lattice, calling pix(h, k, act) with
+// all lanes of the warp together (act false for idle lanes).
+template <int TX, int TY, int TZ, class Pix>
+__device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
+                                          int* s_row, Pix&& pix) {
     // open box of map frequencies whose tent touches the tile
     const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
     const double hi[3] = {ox + TX, oy + TY, oz + TZ};
@@ -213,8 +212,8 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
     if (P.lat) {
         Lh = P.lat & 0xfff; Lk = (P.lat >> 12) & 0xfff; sh = (P.lat >> 24) & 0x7f;
     } else {
-        const int L = max(1, (int)ceilf(1.7320508f * P.inv_step));
-        if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f) { Lh = 4; Lk = 3; sh = 2; }
+        const int L = max(1, (int)ceilf(1.7320508f * 1.0001f * P.inv_step));
+        if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f * 1.0001f) { Lh = 4; Lk = 3; sh = 2; }
         else { Lh = L; Lk = L; sh = 0; }
     }
     // per-axis 1 / ad (0 when the axis does not vary along h)
@@ -277,12 +276,126 @@ __device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevP
                     r = min(r, 31);
                     const int before = r ? s_row[r - 1] : 0;
                     const int h = s_row[32 + r] + Lh * (t - before);
-                    pixel<FOM, GATE, TX, TY, TZ>(a, P, S, A, ox, oy, oz, h, s_row[64 + r], act);
+                    pix(h, s_row[64 + r], act);
                 }
                 __syncwarp();
             }
         }
     }
+}
+
+// The same walk with the lattice phases of one row block interleaved: lane t
+// takes a group of Lh consecutive pixels of one lattice row (h = g, g + 1,
+// ..., g + Lh - 1 with g = h_lo + sh j + Lh i), one pixel of each column
+// phase, and the warp steps through the phases together: at step ph every
+// lane holds a point of phase (ph, pk), so the conflict-free property of a
+// phase still holds, and pix() ends each step with __syncwarp.  The row
+// search is done once per group instead of once per point, and neighbouring
+// lanes read neighbouring pixels of the spectrum.
+template <int TX, int TY, int TZ, class Pix>
+__device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
+                                            int* s_row, Pix&& pix) {
+    const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
+    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
+    double vc = 0, hv = 0, uc = 0, hu = 0;
+    for (int i = 0; i < 3; ++i) {
+        const double c = 0.5 * (lo[i] + hi[i]), e = 0.5 * (hi[i] - lo[i]);
+        vc += P.bd[i] * c; hv += fabs(P.bd[i]) * e;
+        uc += P.ad[i] * c; hu += fabs(P.ad[i]) * e;
+    }
+    vc *= P.inv_st2; hv *= P.inv_st2; uc *= P.inv_st2; hu *= P.inv_st2;
+    const int k_lo = max((int)ceil(vc - hv), -hf), k_hi = min((int)floor(vc + hv), hf - 1);
+    const int h_lo = max((int)ceil(uc - hu), -hf), h_hi = min((int)floor(uc + hu), hf - 1);
+    if (k_lo > k_hi || h_lo > h_hi) return;
+    int Lh, Lk, sh;
+    if (P.lat) {
+        Lh = P.lat & 0xfff; Lk = (P.lat >> 12) & 0xfff; sh = (P.lat >> 24) & 0x7f;
+    } else {
+        const int L = max(1, (int)ceilf(1.7320508f * 1.0001f * P.inv_step));
+        if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f * 1.0001f) { Lh = 4; Lk = 3; sh = 2; }
+        else { Lh = L; Lk = L; sh = 0; }
+    }
+    double ia[3];
+    for (int i = 0; i < 3; ++i) ia[i] = fabs(P.ad[i]) > 1e-12 ? 1.0 / P.ad[i] : 0.0;
+    for (int pk = 0; pk < Lk; ++pk) {
+        const int k0 = k_lo + pk;
+        if (k0 > k_hi) break;
+        const int nrows = (k_hi - k0) / Lk + 1;
+        for (int jb = 0; jb < nrows; jb += 32) {
+            const int j = jb + lane;
+            const int k = k0 + Lk * j;
+            double hl = h_lo, hh = h_hi;
+            bool live = j < nrows;
+            if (live) {
+                for (int i = 0; i < 3; ++i) {
+                    const double base = k * P.bd[i];
+                    if (ia[i] != 0.0) {
+                        double p0 = (lo[i] - base) * ia[i], p1 = (hi[i] - base) * ia[i];
+                        if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
+                        hl = fmax(hl, p0);
+                        hh = fmin(hh, p1);
+                    } else if (!(base > lo[i] && base < hi[i])) {
+                        live = false;
+                    }
+                }
+                live = live && hl <= hh;
+            }
+            // this row's pixels [hmin, hmax] in groups of Lh from its phase-0
+            // lattice point g0 = h_lo + sh j (mod Lh)
+            int gfirst = 0, cnt = 0, hmin = 0, hmax = -1;
+            if (live) {
+                hmin = (int)ceil(hl);
+                hmax = (int)floor(hh);
+                if (hmax >= hmin) {
+                    const int g0 = h_lo + sh * j;
+                    const int i0 = (int)floorf(__fdiv_rn((float)(hmin - g0), (float)Lh));
+                    const int i1 = (int)floorf(__fdiv_rn((float)(hmax - g0), (float)Lh));
+                    gfirst = g0 + Lh * i0;
+                    cnt = i1 - i0 + 1;
+                }
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            if (total == 0) continue;
+            s_row[lane] = incl;                        // inclusive end of row j's groups
+            s_row[32 + lane] = gfirst;
+            s_row[64 + lane] = k;
+            s_row[96 + lane] = hmin;
+            s_row[128 + lane] = hmax;
+            __syncwarp();
+            for (int t0 = 0; t0 < total; t0 += 32) {
+                const int t = t0 + lane;
+                const bool in = t < total;
+                int r = 0;                              // row holding group t
+#pragma unroll
+                for (int sft = 16; sft > 0; sft >>= 1)
+                    if (s_row[r + sft - 1] <= t) r += sft;
+                r = min(r, 31);
+                const int before = r ? s_row[r - 1] : 0;
+                const int g = s_row[32 + r] + Lh * (t - before);
+                const int kr = s_row[64 + r], lo_h = s_row[96 + r], hi_h = s_row[128 + r];
+                for (int ph = 0; ph < Lh; ++ph) {
+                    const int h = g + ph;
+                    pix(h, kr, in && h >= lo_h && h <= hi_h);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+template <bool FOM, bool GATE, int TX, int TY, int TZ>
+__device__ __forceinline__ void scatter_particle(const InsertArgs& a, const DevParticle& P, const float2* S,
+                                                 const TileAcc& A, double ox, double oy, double oz, int lane,
+                                                 int* s_row) {
+    walk_pair<TX, TY, TZ>(P, a.ft / 2, ox, oy, oz, lane, s_row, [&](int h, int k, bool act) {
+        pixel<FOM, GATE, TX, TY, TZ>(a, P, S, A, ox, oy, oz, h, k, act);
+    });
 }
 
 // Tile sums -> HBM: added to the map accumulators (one replica), or stored
@@ -369,6 +482,171 @@ __global__ void __launch_bounds__(WARPS * 32) insert_kernel(InsertArgs a) {
     fold_tile<FOM, TX, TY, TZ>(a, A, x0, y0, z0, rep, lane);
 }
 
+// ---- gridding without the FOM channels: float4 cells --------------------
+//
+// The map tile is an array of float4 cells {F re * w, F im * w, w, unused},
+// so a corner's read-modify-write is one 16-byte load, three adds and one
+// 16-byte store.  Cell (x, y, z) of the tile sits at slot x + PX y + PP z:
+// the plane pitch PP (PX TY plus a few unused slots) spreads the cells a
+// warp's lattice points touch over the eight 16-byte bank groups (at 8^3,
+// PP = 68 puts cell (x, y, z) in group (x + 4 z) mod 8; the pitches were
+// chosen by simulating the lattice walk over random orientations), and the
+// corner offsets stay compile-time constants.
+//
+// Map frequencies are formed in FP32 relative to the tile: per (tile,
+// particle) pair an anchor pixel (hc, kc) near the tile's projection has its
+// frequency hc ad + kc bd - o formed in FP64, and a point (h, k) adds
+// (h - hc) af + (k - kc) bf to it.  The offsets are at most ~25 pixel steps
+// at these tile sizes, so the coordinates carry < 5e-6 voxel of rounding;
+// the trilinear weights are continuous in the coordinates, so a floor that
+// lands on the other side of a cell boundary because of it moves a
+// contribution by that much, and the phase lattices keep a margin above it
+// (lattice.h).
+// One cell's read-modify-write as a single 16-byte shared load and store
+// (the unused fourth word travels with them, so the compiler cannot split the
+// access into narrower ones).
+__device__ __forceinline__ void cell_add(unsigned addr, float2 f, float w) {
+    float x, y, z, u;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(x), "=f"(y), "=f"(z), "=f"(u) : "r"(addr) : "memory");
+    x = fmaf(f.x, w, x);
+    y = fmaf(f.y, w, y);
+    z += w;
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" :: "r"(addr), "f"(x), "f"(y), "f"(z), "f"(u) : "memory");
+}
+
+template <bool GATE, int TX, int TY, int TZ, int PX, int PP>
+__device__ __forceinline__ void pixel4(const InsertArgs& a, const DevParticle& P, const float2* S, float4* cell,
+                                       unsigned cell0,
+                                       float bx, float by, float bz, int hc, int kc, int h, int k, bool act) {
+    const int hf = a.ft / 2;
+    float wt = P.pw;
+    if (GATE && act) {
+        bool keep;
+        const float tw = pixel_weight_gate(a, P, h, k, keep);
+        if (!keep) act = false;
+        wt *= tw;
+    }
+    const float dh = (float)(h - hc), dk = (float)(k - kc);
+    const float mx = fmaf(dh, P.af[0], fmaf(dk, P.bf[0], bx));
+    const float my = fmaf(dh, P.af[1], fmaf(dk, P.bf[1], by));
+    const float mz = fmaf(dh, P.af[2], fmaf(dk, P.bf[2], bz));
+    const float2 f = act ? __ldg(S + (size_t)(k + hf) * a.pitch + (h + hf)) : make_float2(0.f, 0.f);
+    if (a.interp != 2) {
+        const float fx = floorf(mx + 0.5f), fy = floorf(my + 0.5f), fz = floorf(mz + 0.5f);
+        const int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+        float w = wt;
+        if (a.interp == 1) {
+            const float dx = mx - fx, dy = my - fy, dz = mz - fz;
+            w = wt * (1.0f - sqrtf(dx * dx + dy * dy + dz * dz));
+        }
+        if (act && (unsigned)ix < TX && (unsigned)iy < TY && (unsigned)iz < TZ && w > 0.f)
+            cell_add(cell0 + 16u * (unsigned)(ix + PX * iy + PP * iz), f, w);
+        __syncwarp();
+        return;
+    }
+    const float flx = floorf(mx), fly = floorf(my), flz = floorf(mz);
+    const int ix = (int)flx, iy = (int)fly, iz = (int)flz;
+    const float rx = mx - flx, ry = my - fly, rz = mz - flz;
+    const bool vx[2] = {(unsigned)ix < TX, (unsigned)(ix + 1) < TX};
+    const bool vy[2] = {(unsigned)iy < TY, (unsigned)(iy + 1) < TY};
+    const bool vz[2] = {(unsigned)iz < TZ, (unsigned)(iz + 1) < TZ};
+    const unsigned cell_addr = cell0 + 16u * (unsigned)(ix + PX * iy + PP * iz);
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz) {
+        const float wz = (dz ? rz : 1.f - rz) * wt;
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+            const float wyz = (dy ? ry : 1.f - ry) * wz;
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                if (act && vx[dx] && vy[dy] && vz[dz]) {
+                    const float w = (dx ? rx : 1.f - rx) * wyz;
+                    cell_add(cell_addr + 16u * (unsigned)(dx + PX * dy + PP * dz), f, w);
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+template <bool GATE, int TX, int TY, int TZ, int PX, int PP, int NW>
+__global__ void __launch_bounds__(NW * 32) grid4_kernel(InsertArgs a) {
+    constexpr int SLOTS = PP * TZ;
+    constexpr int TV = TX * TY * TZ;
+    extern __shared__ float4 s_cells[];                 // NW x SLOTS
+    __shared__ int s_rows[NW][160];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float4* const cell = s_cells + (size_t)warp * SLOTS;
+    const int gw = blockIdx.x * NW + warp;
+    const int slot = gw / a.R, rep = gw % a.R;        // replicas of a tile are adjacent
+    if (slot >= a.ntx * a.nty * a.ntz) return;
+    const int tile = a.order[slot];
+    const int p_lo = (int)((long)a.np * rep / a.R), p_hi = (int)((long)a.np * (rep + 1) / a.R);
+    const int x0 = (tile % a.ntx) * TX, y0 = ((tile / a.ntx) % a.nty) * TY, z0 = (tile / (a.ntx * a.nty)) * TZ;
+    const int N = a.N;
+    const int hf = a.ft / 2;
+    const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
+    const unsigned cell0 = (unsigned)__cvta_generic_to_shared(cell);
+    for (int i = lane; i < SLOTS; i += 32) cell[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+
+    for (int base = p_lo; base < p_hi; base += 32) {
+        const int p = base + lane;
+        unsigned mask = 0;
+        if (p < p_hi) {
+            const DevParticle& P = a.part[p];
+            if (P.half == a.half || a.half < 0) mask = tile_mask<TX, TY, TZ>(P, x0, y0, z0, N, a.ft);
+        }
+        unsigned todo = __ballot_sync(0xffffffffu, mask != 0);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const unsigned am = __shfl_sync(0xffffffffu, mask, src);
+            const DevParticle& P = a.part[base + src];
+            const float2* S = a.spec + (size_t)P.spec * spec_stride;
+            for (int al = 0; al < 8; ++al) {
+                if (!((am >> al) & 1u)) continue;
+                const double ox = (double)(x0 - ((al & 1) ? N : 0));
+                const double oy = (double)(y0 - ((al & 2) ? N : 0));
+                const double oz = (double)(z0 - ((al & 4) ? N : 0));
+                // anchor pixel: the tile centre's projection on the plane
+                const double cx = ox + 0.5 * (TX - 1), cy = oy + 0.5 * (TY - 1), cz = oz + 0.5 * (TZ - 1);
+                const int hc = (int)rint((P.ad[0] * cx + P.ad[1] * cy + P.ad[2] * cz) * P.inv_st2);
+                const int kc = (int)rint((P.bd[0] * cx + P.bd[1] * cy + P.bd[2] * cz) * P.inv_st2);
+                const float bx = (float)(hc * P.ad[0] + kc * P.bd[0] - ox);
+                const float by = (float)(hc * P.ad[1] + kc * P.bd[1] - oy);
+                const float bz = (float)(hc * P.ad[2] + kc * P.bd[2] - oz);
+                walk_groups<TX, TY, TZ>(P, hf, ox, oy, oz, lane, s_rows[warp], [&](int h, int k, bool act) {
+                    pixel4<GATE, TX, TY, TZ, PX, PP>(a, P, S, cell, cell0, bx, by, bz, hc, kc, h, k, act);
+                });
+            }
+        }
+    }
+    // tile sums -> HBM (one replica: add to the map; else this replica's
+    // partial sums, combined later in replica order)
+    const size_t N3 = (size_t)N * N * N;
+    for (int i = lane; i < TV; i += 32) {
+        const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
+        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+        const float4 c = cell[lx + PX * ly + PP * lz];
+        if (x < N && y < N && z < N) {
+            const size_t idx = ((size_t)z * N + y) * N + x;
+            if (a.R > 1) {
+                double* pb = a.psum + (size_t)rep * 3 * N3 + idx;
+                pb[0] = c.x;
+                pb[N3] = c.y;
+                pb[2 * N3] = c.z;
+            } else {
+                double2 o = a.vol[idx];
+                o.x += c.x;
+                o.y += c.y;
+                a.vol[idx] = o;
+                a.w[idx] += c.z;
+            }
+        }
+    }
+}
+
 // vol += sum over replicas, in replica order.
 template <bool FOM>
 __global__ void combine_kernel(InsertArgs a) {
@@ -389,7 +667,9 @@ __global__ void combine_kernel(InsertArgs a) {
     }
 }
 
-// Tile shapes the autotuner chooses from (map voxels per warp).
+// Tile shapes the autotuner chooses from (map voxels per warp).  The float4
+// cell pitches (PX, PP) and warps per block of each shape are the template
+// arguments of its grid4_kernel launch below.
 struct Shape { int tx, ty, tz; };
 static const Shape kShapes[] = {{8, 8, 8}, {16, 16, 4}, {16, 8, 8}, {16, 16, 8}};
 constexpr int kNumShapes = 4;
@@ -407,8 +687,20 @@ static cudaError_t set_smem_shape() {
     return cudaFuncSetAttribute(insert_kernel<false, false, TX, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
+template <int TX, int TY, int TZ, int PX, int PP, int NW>
+static cudaError_t set_smem_shape4() {
+    const int smem = (int)(NW * PP * TZ * sizeof(float4));
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(grid4_kernel<true, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(grid4_kernel<false, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
 cudaError_t prepare_insert_attributes() {
     cudaError_t e;
+    if ((e = set_smem_shape4<8, 8, 8, 8, 68, 4>()) != cudaSuccess) return e;
+    if ((e = set_smem_shape4<16, 16, 4, 17, 277, 4>()) != cudaSuccess) return e;
+    if ((e = set_smem_shape4<16, 8, 8, 16, 134, 4>()) != cudaSuccess) return e;
+    if ((e = set_smem_shape4<16, 16, 8, 16, 262, 2>()) != cudaSuccess) return e;
     if ((e = set_smem_shape<8, 8, 8>()) != cudaSuccess) return e;
     if ((e = set_smem_shape<16, 16, 4>()) != cudaSuccess) return e;
     if ((e = set_smem_shape<16, 8, 8>()) != cudaSuccess) return e;
@@ -443,6 +735,24 @@ static cudaError_t launch_shape(const InsertArgs& a0, const Context& c, cudaStre
     return cudaGetLastError();
 }
 
+template <int TX, int TY, int TZ, int PX, int PP, int NW>
+static cudaError_t launch_shape4(const InsertArgs& a0, const Context& c, cudaStream_t s) {
+    InsertArgs a = a0;
+    const int N = c.g.map;
+    a.ntx = (N + TX - 1) / TX;
+    a.nty = (N + TY - 1) / TY;
+    a.ntz = (N + TZ - 1) / TZ;
+    const int ntiles = a.ntx * a.nty * a.ntz;
+    const unsigned blocks = (unsigned)(((long)ntiles * a.R + NW - 1) / NW);
+    const size_t smem = (size_t)NW * PP * TZ * sizeof(float4);
+    if (c.g.gate) grid4_kernel<true, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+    else grid4_kernel<false, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || a.R == 1) return e;
+    combine_kernel<false><<<148 * 8, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_insert(const Context& c, const float2* spectra, const DevParticle* parts, int np, int half,
                           cudaStream_t s) {
     InsertArgs a;
@@ -465,6 +775,14 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, const DevPart
     a.order = c.d_tile_order;
     a.R = c.replicas;
     a.psum = c.d_part_sums;
+    if (!c.g.fom) {
+        switch (c.shape) {
+            case 0: return launch_shape4<8, 8, 8, 8, 68, 4>(a, c, s);
+            case 2: return launch_shape4<16, 8, 8, 16, 134, 4>(a, c, s);
+            case 3: return launch_shape4<16, 16, 8, 16, 262, 2>(a, c, s);
+            default: return launch_shape4<16, 16, 4, 17, 277, 4>(a, c, s);
+        }
+    }
     switch (c.shape) {
         case 0: return launch_shape<8, 8, 8>(a, c, s);
         case 2: return launch_shape<16, 8, 8>(a, c, s);

@@ -10,7 +10,8 @@
 // in the map (ad, bd: the map displacement of one pixel step along h and k);
 // they can share a cell only if |d_x|, |d_y| and |d_z| are all below 1.  So
 // a lattice is safe when every nonzero lattice vector has max_c |d_c| >= 1
-// (with a margin for the rounding of the per-pixel FP64 coordinates).
+// (with a margin above the rounding of the per-pixel coordinates: the
+// kernel forms them in FP32 relative to its tile, < 5e-6 voxel).
 //
 // A lattice safe for every orientation needs vectors of length >= sqrt(3)
 // voxels (12 phases at half-voxel pixel steps); for one orientation the
@@ -50,7 +51,7 @@ inline double lattice_reach(const double ad[3], const double bd[3]) {
 // displacement with all three |d_c| < 1 + margin.  Only vectors shorter than
 // `reach` pixel steps need checking, and of each pair +-v only one.
 inline bool lattice_ok(const double ad[3], const double bd[3], int lh, int lk, int sh, double reach) {
-    const double margin = 1e-7;
+    const double margin = 2e-5;
     const int jmax = (int)std::floor(reach / lk);
     for (int j = 0; j <= jmax; ++j) {
         const double dk = (double)lk * j;

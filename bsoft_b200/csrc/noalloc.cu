@@ -43,6 +43,10 @@ namespace {
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mu;
 void* g_addr[MAX_DEVICES] = {};
+// host staging of the particle records: more than the scratch area can hold
+// at the smallest transform (32^2: about 10 KB of scratch per particle)
+constexpr long MAX_RECORDS = 8192;
+DevParticle g_records[MAX_RECORDS];
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
@@ -116,17 +120,25 @@ extern "C" int bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const f
                   ft, n);
         return BSG_ERR_ARG;
     }
-    const Layout L = layout(n, ft, nparts);
-    if (L.total > SCRATCH_BYTES) {
-        const size_t one = layout(n, ft, 1).total;
-        set_error("bsg_particle_spectra_noalloc: %ld particles of box %d (transform %d) need %zu bytes of scratch; "
-                  "the fixed scratch area holds %zu bytes (at most about %zu particles of this size per call)",
-                  nparts, n, ft, L.total, SCRATCH_BYTES, one ? SCRATCH_BYTES / one : 0);
+    if (cfg->interp < 0 || cfg->interp > 2 || cfg->ctf_action < 0 || !(cfg->hi_res > 0)) {
+        set_error("bsg_particle_spectra_noalloc: interp %d, ctf_action %d or resolution %g out of range",
+                  cfg->interp, cfg->ctf_action, cfg->hi_res);
         return BSG_ERR_ARG;
     }
+    // bound the particle count before multiplying it into the layout
+    const size_t one = layout(n, ft, 1).total;
+    const long fit = (long)(SCRATCH_BYTES / one);
+    const long cap = fit < MAX_RECORDS ? fit : MAX_RECORDS;
+    if (nparts > cap || layout(n, ft, nparts).total > SCRATCH_BYTES) {
+        set_error("bsg_particle_spectra_noalloc: %ld particles of box %d (transform %d) do not fit the fixed "
+                  "scratch area of %zu bytes (at most %ld particles of this size per call)",
+                  nparts, n, ft, SCRATCH_BYTES, cap);
+        return BSG_ERR_ARG;
+    }
+    const Layout L = layout(n, ft, nparts);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    if (e != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
         set_error("bsg_particle_spectra_noalloc: no current CUDA device (%s)", cudaGetErrorString(e));
         return BSG_ERR_NODEV;
     }
@@ -172,26 +184,26 @@ extern "C" int bsg_particle_spectra_noalloc(const bsg_recon_config* cfg, const f
     c.d_rows = reinterpret_cast<float2*>(sc + L.rows);
     float2* spec = reinterpret_cast<float2*>(sc + L.spec);
 
-    // particle records: converted on the host in small stack chunks and
-    // copied from pageable memory (the copy completes before it returns)
-    constexpr int CHUNK = 16;
-    DevParticle buf[CHUNK];
-    for (long off = 0; off < nparts; off += CHUNK) {
-        const long cnt = nparts - off < CHUNK ? nparts - off : CHUNK;
-        for (long i = 0; i < cnt; ++i) {
-            const double* q = params + (off + i) * BSG_PARTICLE_DOUBLES;
-            if (!(q[13] > 0)) {
-                set_error("bsg_particle_spectra_noalloc: particle %ld has pixel size %g", off + i, q[13]);
-                return BSG_ERR_ARG;
-            }
-            to_dev_particle(c.g, q, buf[i]);
+    // particle records: converted on the host into one static buffer and
+    // sent in one copy.  The buffer is ordinary (pageable) host memory, so
+    // CUDA stages the copy before cudaMemcpyAsync returns, after which the
+    // buffer may be refilled; the lock keeps two host threads from filling
+    // it at once.
+    for (long i = 0; i < nparts; ++i) {
+        const double* q = params + i * BSG_PARTICLE_DOUBLES;
+        if (!(q[13] > 0)) {
+            set_error("bsg_particle_spectra_noalloc: particle %ld has pixel size %g", i, q[13]);
+            return BSG_ERR_ARG;
         }
-        e = cudaMemcpyAsync(c.d_part + off, buf, sizeof(DevParticle) * cnt, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) {
-            set_error("bsg_particle_spectra_noalloc: copying particle records: %s", cudaGetErrorString(e));
-            return BSG_ERR_CUDA;
-        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (long i = 0; i < nparts; ++i) to_dev_particle(c.g, params + i * BSG_PARTICLE_DOUBLES, g_records[i]);
+        e = cudaMemcpyAsync(c.d_part, g_records, sizeof(DevParticle) * nparts, cudaMemcpyHostToDevice, s);
+    }
+    if (e != cudaSuccess) {
+        set_error("bsg_particle_spectra_noalloc: copying particle records: %s", cudaGetErrorString(e));
+        return BSG_ERR_CUDA;
     }
     twiddle_kernel<<<1, 256, 0, s>>>(c.d_tw, ft);
     e = cudaGetLastError();

@@ -175,7 +175,9 @@ void* bsg_recon_stream(bsg_recon* r);        /* the context's cudaStream_t  */
  *
  * d_images (nparts x n x n float32) and d_out (nparts x ft x ft complex64,
  * the same order as bsg_particle_spectra) are device pointers owned by the
- * caller; params is the host record array.  Work goes to `stream` (a
+ * caller; params is the host record array, converted and sent to the
+ * device in one copy from ordinary host memory (CUDA orders that copy with
+ * `stream` and stages it before the call returns).  Work goes to `stream` (a
  * cudaStream_t, NULL for the default stream).  The intermediate data use a
  * fixed scratch area of BSG_NOALLOC_SCRATCH_BYTES inside the library, held
  * on every GPU that loads it until exit; a call needing more (too many or
