@@ -61,6 +61,7 @@ import argparse
 import json
 import math
 import os
+import shutil
 import subprocess
 import sys
 import tempfile
@@ -172,12 +173,13 @@ def reference_project(w, n_sample: int) -> str:
 
 
 def reference_sample(w, n_sample: int, threads: int):
-    """Time the reference's breconstruct on `n_sample` particles of the
-    workload written as MRC + STAR (writing is not timed)."""
+    """Run the reference's breconstruct on `n_sample` particles of the
+    workload written as MRC + STAR (writing is not timed).  Returns
+    (wall seconds, project directory holding ref.mrc, error text)."""
     import oracle
     exe = oracle.ref_binary("breconstruct")
     if not os.path.exists(exe):
-        return None, "oracle/_ref/breconstruct not built"
+        return None, None, "oracle/_ref/breconstruct not built"
     d = reference_project(w, n_sample)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     t0 = time.perf_counter()
@@ -186,8 +188,59 @@ def reference_sample(w, n_sample: int, threads: int):
                        capture_output=True, text=True)
     dt = time.perf_counter() - t0
     if r.returncode != 0:
-        return None, f"breconstruct failed: {r.stderr[-200:]}"
-    return n_sample / dt, f"{n_sample} particles of the workload ({BOX}^2 -> {BOX}^3, trilinear, CTF flip), wall {dt:.1f} s"
+        return None, d, f"breconstruct failed: {r.stderr[-200:]}"
+    return dt, d, None
+
+
+def reference_steady(w, threads: int, per_thread=(4, 12)):
+    """Steady-state rate of the reference: two runs of per_thread[0] and
+    per_thread[1] particles per thread; the rate is the slope between them,
+    so each thread's map set-up, the partial-map sum and the final transform
+    (the intercept) are reported apart.  Returns (cpu_baseline dict, project
+    directory of the larger run)."""
+    n0, n1 = threads * per_thread[0], threads * per_thread[1]
+    t0, d0, err = reference_sample(w, n0, threads)
+    if t0 is None:
+        return {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": err}, None
+    shutil.rmtree(d0, ignore_errors=True)
+    t1, d1, err = reference_sample(w, n1, threads)
+    if t1 is None:
+        return {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": err}, None
+    slope = (n1 - n0) / max(t1 - t0, 1e-9)
+    setup = max(0.0, t0 - n0 / slope)
+    return {"value": round(slope, 2), "unit": "particles/s", "cores": threads, "kind": "reference",
+            "sample": (f"steady state: slope between {n0} and {n1} particles of the workload ({BOX}^2 -> {BOX}^3, "
+                       f"trilinear, CTF flip), walls {t0:.1f} s and {t1:.1f} s"),
+            "setup_s": round(setup, 2), "single_run_particles_per_s": round(n1 / t1, 2)}, d1
+
+
+def gpu_parity(d):
+    """The GPU path on the reference run's own STAR project and stacks,
+    against the reference's map: relative L2 and the smallest shell FSC."""
+    from bsoft_b200.io import mrc
+    from bsoft_b200.plan import ReconOptions, load_images, plan_reconstruction
+    from bsoft_b200.project import read_project
+    from bsoft_b200.recon import Reconstructor
+    ref, _ = mrc.read_volume(os.path.join(d, "ref.mrc"))
+    plan = plan_reconstruction(read_project(os.path.join(d, "p.star")), ReconOptions(interp=2, ctf_action=1))
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        m = rec.finish().reshape(ref.shape)
+    a, b = m.astype(np.float64), ref.astype(np.float64)
+    rel = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    A, Bf = np.fft.rfftn(a), np.fft.rfftn(b)
+    N = a.shape[0]
+    fz = np.fft.fftfreq(N) * N
+    fx = np.arange(N // 2 + 1)
+    r = np.rint(np.sqrt(fz[:, None, None] ** 2 + fz[None, :, None] ** 2 + fx[None, None, :] ** 2)).astype(int)
+    num = np.bincount(r.ravel(), np.real(A * np.conj(Bf)).ravel(), minlength=N)
+    da = np.bincount(r.ravel(), (np.abs(A) ** 2).ravel(), minlength=N)
+    db = np.bincount(r.ravel(), (np.abs(Bf) ** 2).ravel(), minlength=N)
+    sh = np.arange(1, N // 2)
+    fsc = num[sh] / np.sqrt(da[sh] * db[sh])
+    return {"against": "reference breconstruct map, same STAR project and stacks", "particles": int(plan.params.shape[0]),
+            "rel_l2": float(f"{rel:.3g}"), "fsc_min": round(float(fsc.min()), 7), "fsc_shells": f"1..{N // 2 - 1}"}
 
 
 def cpu_threads():
@@ -208,14 +261,16 @@ def run_reference(args):
     at least 8 per thread so the map set-up and final transform do not
     dominate); the warm-up is a separate small call."""
     threads = cpu_threads_for_reference()
-    n = threads * max(args.steps, 8)
-    w = make_workload(max(n, 2 * threads))
+    w = make_workload(threads * 12)
     if args.warmup:
-        v, sample = reference_sample(w, 2 * threads, threads)
-        if v is None:
-            print(json.dumps({"impl": "reference", "unavailable": sample}))
+        t, _, err = reference_sample(w, 2 * threads, threads)
+        if t is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
             return
-    value, sample = reference_sample(w, n, threads)
+    cpu, d = reference_steady(w, threads)
+    if d is not None:
+        shutil.rmtree(d, ignore_errors=True)
+    value, sample = cpu["value"], cpu["sample"]
     if value is None:
         print(json.dumps({"impl": "reference", "unavailable": sample}))
         return
@@ -225,8 +280,7 @@ def run_reference(args):
         "scaling": "weak", "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "particles": N_PARTICLES, "box": BOX, "map": BOX, "ft": 2 * BOX,
                    "interp": "trilinear", "ctf": "flip"},
-        "cpu_baseline": {"value": value, "unit": "particles/s", "cores": threads, "kind": "reference",
-                         "sample": sample},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "vs_baseline": None}))
 
@@ -796,28 +850,30 @@ def main():
         per_particle = 22.0 * BOX * BOX
         avg_launch_ms = ins_ms / max(1, ins_launch)
         achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
-        # DRAM bytes per launch from one ncu capture of this configuration (8^3
-        # tiles, 2,000 particles per launch: profiles/insert_kernel_batched-
-        # insertion-256.md), taken with the orientation-independent 12-phase
-        # lattice; the per-particle lattice reads the same spectra in a
-        # different order. Other configurations were not captured.
-        traffic = 11.947e9 if (int(shape) == 0 and B == 2000 and BOX == 256) else None
+        # DRAM bytes of one gridding launch, from one ncu capture of this
+        # kernel (8^3 tiles, two replicas, 256^3 map) on a 256-particle batch
+        # of this workload: reads 961.1 MB (the spectra, 3.754 MB per
+        # particle, read ~1.8 times as the tiles a particle reaches are
+        # spread over the launch) and writes 767.2 MB (the two replicas'
+        # partial sums, fixed per launch); scaled to the launch's batch
+        traffic = (3.754e6 * B + 0.767e9) if (int(shape) == 0 and BOX == 256) else None
         roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                "traffic_unit": "bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum)",
+                "traffic_unit": ("bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
+                                 "256-particle launch, reads scaled per particle)"),
                 "peak_source": peak_kind, "avg_launch_ms": round(avg_launch_ms, 3),
                 "algorithmic_bytes_per_particle": per_particle,
                 "fft2d_ms_per_step": round(fft_ms / args.steps, 3), "tile_shape": int(shape),
                 "autotune_ms_per_shape": [round(float(x), 2) for x in shape_ms]}
 
         cpu = None
+        parity = None
         if world == 1 and not args.no_cpu_baseline:
             threads = cpu_threads_for_reference()
-            v, sample = reference_sample(w, max(2 * threads, threads * 8), threads)
-            if v is not None:
-                cpu = {"value": v, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
-            else:
-                cpu = {"value": None, "unit": "particles/s", "cores": threads, "kind": "reference", "sample": sample}
+            cpu, d = reference_steady(w, threads)
+            if d is not None:
+                parity = gpu_parity(d)
+                shutil.rmtree(d, ignore_errors=True)
 
         line = {
             "metric": "particles/s (insertion)", "value": round(value, 1), "unit": "particles/s", "n_gpus": world,
@@ -828,7 +884,7 @@ def main():
                        "ctf": "flip", "l2": "inputs larger than L2 (524 MB per step)", "parallelism": f"dp{world}"},
             "e2e": {"value": round(e2e, 1), "unit": "particles/s", "h2d_bytes_per_step": B * BOX * BOX * 4,
                     "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps},
-            "roofline": roof, "cpu_baseline": cpu, "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "parity": parity, "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
         if search is not None:
