@@ -63,6 +63,7 @@ MATCH_CTF_DOUBLES = 8
 MATCH_HYP_DOUBLES = 12
 MATCH_REFINE_START_DOUBLES = 7
 MATCH_SCORE_FP64 = 4
+MATCH_SCORE_DPR = 8
 MATCH_REFINE_RESULT_DOUBLES = 10
 
 

@@ -328,8 +328,11 @@ __global__ void __launch_bounds__(256) section_kernel(const float2* __restrict__
     }
 }
 
-// FRC figure of merit of one hypothesis group per CTA (img_recip_space_fom,
-// fom_type 0, unit weights): one image, one view, up to MAXORG trial
+// Figure of merit of one hypothesis group per CTA (img_recip_space_fom,
+// unit weights; the FRC, fom_type 0, or with a.dpr the DPR form, fom_type 1,
+// mg_refine.cpp:725-772: per shell the sums of (|X| + |R c|) dphi^2 and of
+// |X| + |R c|, dphi the phase difference wrapped to [-pi, pi], and the mean
+// over shells of cos(sqrt(ratio))): one image, one view, up to MAXORG trial
 // origins.  Warps take 32 consecutive pixels of the shell-sorted list: the
 // section value of each is gathered once by the whole warp, then every lane
 // scores its own pixel at every origin (only the image phase depends on the
@@ -354,6 +357,7 @@ struct FomArgs {
     double* fom;             // per group x MAXORG
     double* cv;
     const double2* sec;      // gathered sections (npix per view, FP64), or null: gather here
+    int dpr;                 // 1: the DPR form (fom_type 1) instead of the FRC
 };
 
 // T = float: the search's rescoring (agrees with the reference's figure of
@@ -413,7 +417,14 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             const float2 x = X[pq.idx];
             const T c = C[p];
             const T rr = Rx * c, ri = Ry * c;
-            v[0] = rr * rr + ri * ri;
+            T amp = 0, pr = 0;
+            if (a.dpr) {
+                amp = sqrt((T)x.x * (T)x.x + (T)x.y * (T)x.y) + sqrt(rr * rr + ri * ri);
+                pr = atan2(ri, rr);
+                v[0] = amp;
+            } else {
+                v[0] = rr * rr + ri * ri;
+            }
 #pragma unroll
             for (int o = 0; o < MAXORG; ++o) {
                 if (o < norg) {
@@ -426,7 +437,14 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
                         sincosf((float)phi, &sn, &cs);
                     }
                     const T xr = (T)x.x * cs - (T)x.y * sn, xi = (T)x.x * sn + (T)x.y * cs;
-                    v[1 + o] = xr * rr + xi * ri;
+                    if (a.dpr) {
+                        T d = atan2(xi, xr) - pr;
+                        if (d < (T)-3.14159265358979323846) d += (T)6.28318530717958647692;
+                        else if (d > (T)3.14159265358979323846) d -= (T)6.28318530717958647692;
+                        v[1 + o] = amp * d * d;
+                    } else {
+                        v[1 + o] = xr * rr + xi * ri;
+                    }
                 }
             }
         }
@@ -460,8 +478,13 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
                 mj += wsum[(w * a.nshell + j) * NV];
                 fj += wsum[(w * a.nshell + j) * NV + 1 + o];
             }
-            const double den = ds[j] * mj;
-            const double t = den > 0 ? fj / sqrt(den) : 0.0;
+            double t;
+            if (a.dpr) {
+                t = mj != 0.0 ? cos(sqrt(fj / mj)) : 0.0;
+            } else {
+                const double den = ds[j] * mj;
+                t = den > 0 ? fj / sqrt(den) : 0.0;
+            }
             if (j < a.nf) tf += t;
             if (j >= a.cv0 && j < a.cv1) tc += t;
         }
@@ -908,8 +931,9 @@ cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, floa
 }
 
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64, const float* ctf_table, const double2* sec) {
+                       bool fp64, const float* ctf_table, const double2* sec, bool dpr) {
     FomArgs a{};
+    a.dpr = dpr ? 1 : 0;
     a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf; a.lutd = M.d_lut;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
     a.spec = M.d_spec; a.ctf = ctf_table ? ctf_table : M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
@@ -1151,7 +1175,8 @@ extern "C" int bsg_match_score(bsg_match* h, const double* hyps, long nhyp, doub
     if (rc2) return rc2;
     cudaStream_t s = M->stream;
     MCK(cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s));
-    MCK(launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, (flags & BSG_MATCH_SCORE_FP64) != 0));
+    MCK(launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, (flags & BSG_MATCH_SCORE_FP64) != 0,
+                   nullptr, nullptr, (flags & BSG_MATCH_SCORE_DPR) != 0));
     std::vector<double> go(2 * ng * MAXORG);
     MCK(cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));

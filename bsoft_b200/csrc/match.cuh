@@ -258,10 +258,12 @@ struct Match {
 };
 
 
-// exact FRC scoring of ng hypothesis groups already on the device (match.cu):
-// d_fom / d_cv get MAXORG slots per group; fp64: FP64 gather and sums
+// exact scoring of ng hypothesis groups already on the device (match.cu):
+// d_fom / d_cv get MAXORG slots per group; fp64: FP64 gather and sums; dpr:
+// the DPR figure of merit instead of the FRC
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64 = false, const float* ctf_table = nullptr, const double2* sec = nullptr);
+                       bool fp64 = false, const float* ctf_table = nullptr, const double2* sec = nullptr,
+                       bool dpr = false);
 // FP64 section values of nv views (9 doubles each, MHyp's scaled rows) at
 // the figure-of-merit pixels: nv x npix double2
 cudaError_t launch_secgather(const Match& M, const double* d_mats, long nv, double2* d_out, cudaStream_t s);

@@ -275,7 +275,7 @@ using namespace bsg;
 
 extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, double alpha_step, double accuracy,
                                 double shift_step, double shift_accuracy, double def_std, double* out, int flags) {
-    (void)flags;
+    const bool dpr = (flags & BSG_MATCH_SCORE_DPR) != 0;
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !start || !out || nstart < 1) return match_fail(BSG_ERR_ARG, "bsg_match_refine: bad argument");
     if (!M->have_ref || M->nimg < 1)
@@ -402,7 +402,7 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         cudaError_t e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaEventRecord(e0, s);
         if (e == cudaSuccess)
-            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table, d_sec);
+            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table, d_sec, dpr);
         if (e == cudaSuccess) e = cudaEventRecord(e1, s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);

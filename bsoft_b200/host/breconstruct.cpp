@@ -74,17 +74,17 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
         if (!mgs[i].part_id.empty()) { first = (int)i; break; }
     if (first < 0) throw std::runtime_error("no particles");
     const Micrograph& m0 = mgs[first];
-    const MrcHeader h0 = read_mrc_header(m0.particle_file);
+    const StackHeader h0 = read_stack_header(m0.particle_file);
     // project_set_reconstruction_size (mg_reconstruct.cpp:596-651)
     double sam = o.sampling;
     if (sam < 0.1) sam = m0.pixel[0] > 0 ? m0.pixel[0] : 0.0;
     if (sam < 0.1) sam = m0.pixel_size;
     if (sam < 0.1) sam = h0.sampling(0);
     Plan p;
-    p.n = h0.nx;
-    p.map = o.size ? o.size : (int)(h0.nx * o.scale);
+    p.n = h0.nx();
+    p.map = o.size ? o.size : (int)(h0.nx() * o.scale);
     const double resolution = o.resolution >= 0.1 ? o.resolution : sam;
-    long ft = m0.box ? m0.box : h0.nx;
+    long ft = m0.box ? m0.box : h0.nx();
     if (p.map > ft) ft = p.map;
     p.ft = (int)part_ft_size(ft, 1, o.pad);
     p.map_sampling = sam / o.scale;
@@ -101,11 +101,11 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
     for (size_t mi = 0; mi < mgs.size(); ++mi) {
         const Micrograph& mg = mgs[mi];
         if (mg.part_id.empty()) continue;
-        const MrcHeader h = read_mrc_header(mg.particle_file);
-        const double fo[2] = {h.image_origin(0), h.image_origin(1)};
+        const StackHeader h = read_stack_header(mg.particle_file);
         if (mg.has_ctf) em = mg.ctf;
         for (size_t i = 0; i < mg.part_id.size(); ++i) {
             if (mg.select[i] <= 0) continue;
+            const double fo[2] = {h.image_origin(0, mg.part_id[i] - 1), h.image_origin(1, mg.part_id[i] - 1)};
             double r[BSG_PARTICLE_DOUBLES] = {};
             double ox = mg.ox[i], oy = mg.oy[i];
             if (ox <= 0) { ox = fo[0] > 0 ? fo[0] : 0; oy = fo[0] > 0 ? fo[1] : 0; }
@@ -233,7 +233,7 @@ int main(int argc, char** argv) {
         const long n2 = (long)p.n * p.n;
         const long B = std::max(1, o.batch);
         std::vector<float> buf[2] = {std::vector<float>(B * n2), std::vector<float>(B * n2)};
-        std::map<int, MrcHeader> hdrs;
+        std::map<int, StackHeader> hdrs;
         for (long b0 = 0, bi = 0; b0 < np; b0 += B, ++bi) {
             const long cnt = std::min(B, np - b0);
             std::vector<float>& dst = buf[bi % 2];
@@ -241,8 +241,8 @@ int main(int argc, char** argv) {
             for (long i = 0; i < cnt; ++i) {
                 const auto& s = p.src[b0 + i];
                 const Micrograph& mg = mgs[s.first];
-                if (!hdrs.count(s.first)) hdrs[s.first] = read_mrc_header(mg.particle_file);
-                read_mrc_images(mg.particle_file, hdrs[s.first], s.second, 1, dst.data() + i * n2);
+                if (!hdrs.count(s.first)) hdrs[s.first] = read_stack_header(mg.particle_file);
+                read_stack_images(mg.particle_file, hdrs[s.first], s.second, 1, dst.data() + i * n2);
             }
             CALL(bsg_recon_insert(rec, dst.data(), p.rec.data() + b0 * BSG_PARTICLE_DOUBLES, cnt, 0));
         }

@@ -16,8 +16,9 @@
 //   -select 14   -all         particle selection
 //   -output out.star          output project
 //   -batch 4096  -device 0
+//   -fomtype frc|dpr          figure of merit (brefine.cpp:124-127: the first letter decides)
 // Not supported (rejected): -monte, -symmetry, -magnification, -mask, -FSC,
-// -fomtype dpr, -edge.
+// -edge.
 //
 // Flow as project_refine_orientations / part_refine_orientation
 // (bsoft/src/mg/mg_refine.cpp:249-457, 491-648): one reference preparation,
@@ -43,7 +44,7 @@ struct Options {
     double alpha = 0, accuracy = 0.5 * M_PI / 180.0;   // radians (brefine.cpp:80)
     double shift_step = 0.4, shift_accuracy = 0.1;
     double def_std = 0, hi_res = 0, lo_res = 0;
-    int kernel_w = 8, kernel_p = 2, select = -1, batch = 4096, device = 0;
+    int kernel_w = 8, kernel_p = 2, select = -1, batch = 4096, device = 0, fom_type = 0;
     bool contrast = false, all = false;
     std::vector<std::string> inputs;
 };
@@ -84,6 +85,10 @@ Options parse(int argc, char** argv) {
             values(val(), w, p);
             o.kernel_w = (int)w;
             o.kernel_p = (int)p;
+        } else if (a == "-fomtype") {
+            const std::string v = val();
+            if (!v.empty() && v[0] == 'f') o.fom_type = 0;
+            if (!v.empty() && v[0] == 'd') o.fom_type = 1;
         } else if (a == "-contrast") o.contrast = true;
         else if (a == "-select") o.select = atoi(val().c_str());
         else if (a == "-all") o.all = true;
@@ -124,9 +129,9 @@ int main(int argc, char** argv) {
         for (size_t i = 0; i < mgs.size(); ++i)
             if (!mgs[i].part_id.empty()) { first = (int)i; break; }
         if (first < 0) throw std::runtime_error("no particles");
-        const MrcHeader h0 = read_mrc_header(mgs[first].particle_file);
+        const StackHeader h0 = read_stack_header(mgs[first].particle_file);
         bsg_match_config cfg = {};
-        cfg.n = h0.nx;
+        cfg.n = h0.nx();
         cfg.map = mh.nx;
         cfg.map_sampling = mh.sampling(0);
         cfg.pixel = mgs[first].pixel[0] > 0 ? mgs[first].pixel[0] : h0.sampling(0);
@@ -138,7 +143,7 @@ int main(int argc, char** argv) {
         bsg_match* m = nullptr;
         CALL(bsg_match_create(&cfg, &m));
         CALL(bsg_match_set_reference(m, map.data(), map_origin, 0));
-        const long n2 = (long)h0.nx * h0.ny;
+        const long n2 = (long)h0.nx() * h0.ny();
         std::vector<std::vector<double>> fom(mgs.size()), fcv(mgs.size());
         long done = 0;
         Ctf em;
@@ -151,15 +156,15 @@ int main(int argc, char** argv) {
             for (size_t i = 0; i < mg.part_id.size(); ++i)
                 if (o.select >= 0 ? mg.select[i] == o.select : mg.select[i] > 0) sel.push_back((long)i);
             if (sel.empty()) continue;
-            const MrcHeader h = read_mrc_header(mg.particle_file);
-            if (h.nx != cfg.n || h.ny != cfg.n) throw std::runtime_error(mg.particle_file + ": particle size differs");
+            const StackHeader h = read_stack_header(mg.particle_file);
+            if (h.nx() != cfg.n || h.ny() != cfg.n) throw std::runtime_error(mg.particle_file + ": particle size differs");
             for (size_t b0 = 0; b0 < sel.size(); b0 += (size_t)std::max(1, o.batch)) {
                 const size_t cnt = std::min(sel.size() - b0, (size_t)std::max(1, o.batch));
                 std::vector<float> imgs(cnt * n2);
                 std::vector<double> ctf(cnt * BSG_MATCH_CTF_DOUBLES, 0.0), start(cnt * BSG_MATCH_REFINE_START_DOUBLES);
                 for (size_t j = 0; j < cnt; ++j) {
                     const long i = sel[b0 + j];
-                    read_mrc_images(mg.particle_file, h, mg.part_id[i] - 1, 1, imgs.data() + j * n2);
+                    read_stack_images(mg.particle_file, h, mg.part_id[i] - 1, 1, imgs.data() + j * n2);
                     // the particle's CTF: the micrograph's, at the particle's
                     // defocus when it has one (part_refine_orientation :567-598)
                     Ctf c = em;
@@ -175,10 +180,10 @@ int main(int argc, char** argv) {
                     s[1] = mg.vx[i]; s[2] = mg.vy[i]; s[3] = mg.vz[i]; s[4] = mg.va[i];
                     s[5] = mg.ox[i]; s[6] = mg.oy[i];
                 }
-                CALL(bsg_match_set_images(m, imgs.data(), (long)cnt, ctf.data(), h.dmean, h.rms, 0));
+                CALL(bsg_match_set_images(m, imgs.data(), (long)cnt, ctf.data(), h.mean(), h.stddev(), 0));
                 std::vector<double> out(cnt * BSG_MATCH_REFINE_RESULT_DOUBLES);
                 CALL(bsg_match_refine(m, start.data(), (long)cnt, o.alpha, o.accuracy, o.shift_step, o.shift_accuracy,
-                                      o.def_std, out.data(), 0));
+                                      o.def_std, out.data(), o.fom_type == 1 ? BSG_MATCH_SCORE_DPR : 0));
                 for (size_t j = 0; j < cnt; ++j) {
                     const long i = sel[b0 + j];
                     const double* r = &out[j * BSG_MATCH_REFINE_RESULT_DOUBLES];

@@ -175,6 +175,128 @@ inline std::vector<float> read_mrc_volume(const std::string& path, const MrcHead
     return v;
 }
 
+// ---------------------------------------------------------------- SPIDER
+// Real-space float stacks as the reference's SPIDER reader reads them
+// (bsoft/src/rwimg/rwSPIDER.cpp:82-243): header words as floats (nslice 0,
+// nrow 1, iform 4, av 8, sig 9, nsam 11, xoff/yoff/zoff 17-19, scale 20,
+// labbyt 21, istack 23, maxim 25); the words (and the data) are byte-swapped
+// when |nslice| or |iform| exceeds 65535 or |nslice| < 1; a stack
+// (istack > 0) holds maxim images, image i being a labbyt-byte header and
+// its data at labbyt + i (labbyt + 4 nsam nrow nslice); sampling = scale;
+// each image's origin is its own header's.
+struct SpiderHeader {
+    int nx = 0, ny = 0, nz = 0;
+    float iform = 0, istack = 0, scale = 1, av = 0, sig = 0;
+    long labbyt = 0, maxim = 0;
+    bool swap = false;
+    std::vector<double> ox, oy;      // per image origin (pixels)
+    long images() const { return istack > 0 ? maxim : 1; }
+    long image_bytes() const { return labbyt + 4L * nx * ny * nz; }
+    long data_offset(long i) const { return istack > 0 ? labbyt + i * image_bytes() + labbyt : labbyt; }
+};
+
+inline bool is_spider(const std::string& path) {
+    auto ends = [&](const char* e) {
+        const size_t n = strlen(e);
+        if (path.size() < n) return false;
+        for (size_t i = 0; i < n; ++i)
+            if (tolower((unsigned char)path[path.size() - n + i]) != e[i]) return false;
+        return true;
+    };
+    return ends(".spi") || ends(".spider");
+}
+
+inline void spider_words(const unsigned char* raw, bool swap, float* w) {
+    for (int i = 0; i < 36; ++i) {
+        unsigned char b[4] = {raw[4 * i], raw[4 * i + 1], raw[4 * i + 2], raw[4 * i + 3]};
+        if (swap) { std::swap(b[0], b[3]); std::swap(b[1], b[2]); }
+        memcpy(&w[i], b, 4);
+    }
+}
+
+inline SpiderHeader read_spider_header(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    unsigned char raw[1024];
+    if (!f.read((char*)raw, 1024)) throw std::runtime_error(path + ": short SPIDER header");
+    float w[36];
+    spider_words(raw, false, w);
+    SpiderHeader h;
+    h.swap = fabsf(w[0]) > 65535 || fabsf(w[4]) > 65535 || fabsf(w[0]) < 1;
+    if (h.swap) spider_words(raw, true, w);
+    h.nz = (int)w[0]; h.ny = (int)w[1]; h.nx = (int)w[11];
+    h.iform = w[4]; h.av = w[8]; h.sig = w[9]; h.scale = w[20];
+    h.labbyt = (long)w[21]; h.istack = w[23]; h.maxim = (long)w[25];
+    if (h.nx < 1 || h.ny < 1 || h.nz < 1 || h.labbyt < 144)
+        throw std::runtime_error(path + ": not a valid SPIDER image");
+    if (h.iform < 0) throw std::runtime_error(path + ": SPIDER Fourier transforms are not particle stacks");
+    const long n = h.images();
+    h.ox.assign(n, w[17]);
+    h.oy.assign(n, w[18]);
+    if (h.istack > 0)
+        for (long i = 0; i < n; ++i) {
+            f.seekg(h.labbyt + i * h.image_bytes());
+            if (!f.read((char*)raw, 144)) throw std::runtime_error(path + ": truncated image header");
+            spider_words(raw, h.swap, w);
+            h.ox[i] = w[17];
+            h.oy[i] = w[18];
+        }
+    return h;
+}
+
+inline void read_spider_images(const std::string& path, const SpiderHeader& h, long first, long count, float* out) {
+    if (first < 0 || first + count > h.images()) throw std::runtime_error(path + ": image index outside the stack");
+    const long per = (long)h.nx * h.ny * h.nz;
+    std::ifstream f(path, std::ios::binary);
+    for (long j = 0; j < count; ++j) {
+        f.seekg(h.data_offset(first + j));
+        float* o = out + j * per;
+        if (!f.read((char*)o, sizeof(float) * per)) throw std::runtime_error(path + ": truncated data");
+        if (h.swap)
+            for (long k = 0; k < per; ++k) {
+                unsigned char* b = (unsigned char*)(o + k);
+                std::swap(b[0], b[3]);
+                std::swap(b[1], b[2]);
+            }
+    }
+}
+
+// ---------------------------------------------------------------- stacks
+// Particle stacks by format, as read_img picks the reader from the file
+// extension (bsoft/src/rwimg/rwimg.cpp:79-130): .spi / .spider -> SPIDER,
+// else MRC.
+struct StackHeader {
+    bool spider = false;
+    MrcHeader mrc;
+    SpiderHeader spi;
+    int nx() const { return spider ? spi.nx : mrc.nx; }
+    int ny() const { return spider ? spi.ny : mrc.ny; }
+    double sampling(int i) const { return spider ? (double)spi.scale : mrc.sampling(i); }
+    long images() const { return spider ? spi.images() : mrc.images(); }
+    // origin (pixels) of image img: the MRC header's for every image, a
+    // SPIDER stack's per image
+    double image_origin(int axis, long img) const {
+        if (!spider) return mrc.image_origin(axis);
+        const std::vector<double>& v = axis == 0 ? spi.ox : spi.oy;
+        return v.empty() ? 0.0 : v[std::min<long>(std::max<long>(img, 0), (long)v.size() - 1)];
+    }
+    // the file statistics read_img attaches (MRC dmean/rms, SPIDER av/sig)
+    double mean() const { return spider ? spi.av : mrc.dmean; }
+    double stddev() const { return spider ? spi.sig : mrc.rms; }
+};
+
+inline StackHeader read_stack_header(const std::string& path) {
+    StackHeader h;
+    h.spider = is_spider(path);
+    if (h.spider) h.spi = read_spider_header(path);
+    else h.mrc = read_mrc_header(path);
+    return h;
+}
+
+inline void read_stack_images(const std::string& path, const StackHeader& h, long first, long count, float* out) {
+    if (h.spider) read_spider_images(path, h.spi, first, count, out);
+    else read_mrc_images(path, h.mrc, first, count, out);
+}
+
 inline void write_mrc_volume(const std::string& path, const float* v, int N, double sampling, double origin) {
     unsigned char hdr[1024];
     memset(hdr, 0, sizeof(hdr));

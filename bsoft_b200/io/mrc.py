@@ -55,6 +55,10 @@ class MRCHeader:
         s = self.sampling
         return tuple(-self.origin[i] / s[i] for i in range(3))
 
+    def image_origin_of(self, i: int):
+        """The origin of image i of the stack: the header's, for every image."""
+        return self.image_origin
+
 
 def read_header(path: str) -> MRCHeader:
     with open(path, "rb") as f:

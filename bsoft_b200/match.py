@@ -135,28 +135,31 @@ class Matcher:
                    "bsg_match_prepared")
         return out
 
-    def score(self, hyps, fp64: bool = False):
+    def score(self, hyps, fp64: bool = False, dpr: bool = False):
+        """Figure of merit and cross-validation figure of each hypothesis: the
+        FRC form, or with dpr the DPR form (brefine -fomtype dpr)."""
         h = np.ascontiguousarray(hyps, dtype=np.float64).reshape(-1, MATCH_HYP_DOUBLES)
         fom = np.empty(len(h))
         cv = np.empty(len(h))
-        _lib.check(_lib.load().bsg_match_score(self._h, _dp(h), len(h), _dp(fom), _dp(cv),
-                                               _lib.MATCH_SCORE_FP64 if fp64 else 0), "bsg_match_score")
+        flags = (_lib.MATCH_SCORE_FP64 if fp64 else 0) | (_lib.MATCH_SCORE_DPR if dpr else 0)
+        _lib.check(_lib.load().bsg_match_score(self._h, _dp(h), len(h), _dp(fom), _dp(cv), flags), "bsg_match_score")
         return fom, cv
 
     def refine(self, start, alpha_step: float, accuracy: float, shift_step: float = 0.4,
-               shift_accuracy: float = 0.1, def_std: float = 0.0) -> np.ndarray:
+               shift_accuracy: float = 0.1, def_std: float = 0.0, dpr: bool = False) -> np.ndarray:
         """img_refine_grid for every start record (n, 7): image index, view
         x, y, z, angle (radians), origin x, y (particle pixels).  Angular
         step and accuracy in radians, shift step and accuracy in pixels of
         the cut transform (the reference's arguments); def_std > 0 adds
         brefine's defocus search (angstrom).  Returns (n, 10): view x, y, z,
         angle, origin x, y, figure of merit, cross-validation figure,
-        hypotheses scored, defocus (0 without the search)."""
+        hypotheses scored, defocus (0 without the search).  dpr scores with
+        the DPR figure of merit (brefine -fomtype dpr)."""
         s = np.ascontiguousarray(start, dtype=np.float64).reshape(-1, _lib.MATCH_REFINE_START_DOUBLES)
         out = np.empty((len(s), _lib.MATCH_REFINE_RESULT_DOUBLES))
         _lib.check(_lib.load().bsg_match_refine(self._h, _dp(s), len(s), float(alpha_step), float(accuracy),
                                                 float(shift_step), float(shift_accuracy), float(def_std), _dp(out),
-                                                0), "bsg_match_refine")
+                                                _lib.MATCH_SCORE_DPR if dpr else 0), "bsg_match_refine")
         return out
 
 

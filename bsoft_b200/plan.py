@@ -19,7 +19,7 @@ import numpy as np
 
 from .ctf import CTFParams
 from .geometry import view_to_matrix
-from .io import mrc
+from .io import mrc, stacks  # noqa: F401
 from .project import Project
 
 # interpolation / CTF action codes (breconstruct.cpp:131-135; options.h:418-442)
@@ -103,7 +103,7 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
         raise ValueError("no particles")
     first = mgs[0]
     first_file = project.resolve(first.particle_file)
-    hdr = mrc.read_header(first_file)
+    hdr = stacks.read_header(first_file)
 
     # project_set_reconstruction_size
     sam = opt.sampling
@@ -132,14 +132,14 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
     em = CTFParams()       # CTFparam defaults when a micrograph has no CTF block
     for mg in mgs:
         path = project.resolve(mg.particle_file)
-        h = mrc.read_header(path)
-        file_origin = h.image_origin
+        h = stacks.read_header(path)
         if mg.ctf is not None:
             em = CTFParams(**vars(mg.ctf))
         for i in range(mg.n):
             if mg.select[i] <= 0:
                 continue
             r = np.zeros(PARTICLE_DOUBLES)
+            file_origin = h.image_origin_of(int(mg.part_id[i]) - 1)
             ori = mg.origin[i].copy()
             if ori[0] <= 0:
                 ori = np.array(file_origin) if file_origin[0] > 0 else np.zeros(3)
@@ -171,6 +171,6 @@ def load_images(plan: ReconPlan, sel=None) -> np.ndarray:
     cache = {}
     for j, (path, num) in enumerate(idx):
         if path not in cache:
-            cache[path] = mrc.read_stack(path)[0]
+            cache[path] = stacks.read_stack(path)[0]
         out[j] = cache[path][num]
     return out

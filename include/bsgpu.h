@@ -275,10 +275,13 @@ int  bsg_match_set_images(bsg_match* m, const float* images, long nimg, const do
                           double file_avg, double file_std, int flags);
 /* Prepared particle transforms [first, first+count): diam^2 complex64 each. */
 int  bsg_match_prepared(bsg_match* m, long first, long count, float* out, int flags);
-/* FRC figure of merit (and cross-validation figure) of nhyp hypotheses.
+/* Figure of merit (and cross-validation figure) of nhyp hypotheses: the
+ * FRC form (img_recip_space_fom fom_type 0), or with BSG_MATCH_SCORE_DPR the
+ * DPR form (fom_type 1, brefine -fomtype dpr, mg_refine.cpp:725-772).
  * flags: BSG_MATCH_SCORE_FP64 gathers and sums in FP64 (the reference's
  * accumulation; ~1e-8 from its figures of merit, the FP32 default ~1e-7). */
 #define BSG_MATCH_SCORE_FP64 4
+#define BSG_MATCH_SCORE_DPR  8
 int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, double* cv, int flags);
 
 /* Exhaustive search (no counterpart in the reference, which refines locally
@@ -359,8 +362,10 @@ void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
  * out: nstart records of BSG_MATCH_REFINE_RESULT_DOUBLES doubles: view x,
  * y, z, angle, origin x, y (pixels of the particle image), figure of merit,
  * cross-validation figure, hypotheses scored (the reference's `number`),
- * defocus after refinement (angstrom; 0 without the defocus search).  The
- * magnification search (max_mag > 0) is not part of this call. */
+ * defocus after refinement (angstrom; 0 without the defocus search).
+ * flags: BSG_MATCH_SCORE_DPR scores with the DPR figure of merit (brefine
+ * -fomtype dpr).  The magnification search (max_mag > 0) is not part of
+ * this call. */
 #define BSG_MATCH_REFINE_START_DOUBLES 7
 #define BSG_MATCH_REFINE_RESULT_DOUBLES 10
 int  bsg_match_refine(bsg_match* m, const double* start, long nstart, double alpha_step, double accuracy,

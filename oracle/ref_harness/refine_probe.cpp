@@ -34,9 +34,12 @@ double img_refine_grid(Bimage* p, Bimage* pref, double hi_res, double lo_res, in
                        CTFparam* em_ctf, double def_std, FSI_Kernel* kernel, long &number);
 
 int main(int argc, char** argv) {
-	if ( argc < 11 ) { fprintf(stderr, "usage: refine_probe map stack pixel hi_res start ctf alpha acc step step_acc\n"); return 1; }
+	if ( argc < 11 ) { fprintf(stderr, "usage: refine_probe map stack pixel hi_res start ctf alpha acc step step_acc"
+		" [verbose [def_std [fom_type [max_mag]]]]\n"); return 1; }
 	verbose = argc > 11 ? atoi(argv[11]) : 0;
 	double def_std = argc > 12 ? atof(argv[12]) : 0;
+	int fom_type = argc > 13 ? atoi(argv[13]) : 0;        // 1: DPR (brefine -fomtype dpr)
+	double max_mag = argc > 14 ? atof(argv[14]) : 0;      // brefine -magnification
 	double pixel = atof(argv[3]), hi_res = atof(argv[4]);
 	double alpha_step = atof(argv[7])*M_PI/180.0, accuracy = atof(argv[8])*M_PI/180.0;
 	double shift_step = atof(argv[9]), shift_accuracy = atof(argv[10]);
@@ -95,11 +98,14 @@ int main(int argc, char** argv) {
 		else if ( flags ) { fprintf(stderr, "refine_probe: a CTF needs def_std > 0\n"); return 4; }
 		long number = 0;
 		double fom = img_refine_grid(p, pref, hi_res, 0, flags, alpha_step, accuracy, shift_step, shift_accuracy,
-			0, 0, weight, &c, def_std, kernel, number);
+			max_mag, fom_type, weight, &c, def_std, kernel, number);
 		View v = p->image->view();
 		Vector3<double> o = p->image->origin() / scale;
-		printf("%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %ld %.17g\n", v[0], v[1], v[2], v[3], o[0], o[1],
+		printf("%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %ld %.17g", v[0], v[1], v[2], v[3], o[0], o[1],
 			fom, p->image->FOM(), number, c.defocus_average());
+		// with the magnification grid: the refined sampling of the cut transform
+		if ( max_mag > 0 ) printf(" %.17g %.17g", p->image->sampling()[0], p->image->sampling()[1]);
+		printf("\n");
 		delete p;
 	}
 	return 0;

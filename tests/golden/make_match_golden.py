@@ -115,17 +115,20 @@ def _isnum(t: str) -> bool:
         return False
 
 
-# asymmetric_unit_views (views_probe): point group order, theta and phi steps
-# in degrees, flag (1 full sphere, 2 no in-plane angle)
-VIEW_CASES = [(1, 3.0, 3.0, 1), (1, 7.5, 7.5, 1), (1, 10.0, 5.0, 0), (3, 6.0, 6.0, 1), (1, 3.0, 3.0, 3)]
+# asymmetric_unit_views (views_probe): point group, theta and phi steps in
+# degrees, flag (1 full sphere, 2 no in-plane angle)
+VIEW_CASES = [("C1", 3.0, 3.0, 1), ("C1", 7.5, 7.5, 1), ("C1", 10.0, 5.0, 0), ("C3", 6.0, 6.0, 1),
+              ("C1", 3.0, 3.0, 3), ("D2", 5.0, 5.0, 1), ("D3", 4.0, 4.0, 0), ("D7", 6.0, 3.0, 1),
+              ("T", 3.0, 4.0, 0), ("T", 2.0, 2.0, 1), ("O", 4.0, 4.0, 1), ("O", 3.0, 3.0, 0),
+              ("I", 3.0, 3.0, 1), ("I", 2.0, 2.0, 0), ("I90", 3.0, 3.0, 1), ("I90", 2.5, 2.5, 0)]
 
 
 def make_views() -> str:
     out = {}
-    for order, t, p, f in VIEW_CASES:
-        r = subprocess.run([os.path.join(REF, "views_probe"), f"C{order}", repr(t), repr(p), str(f)],
+    for sym, t, p, f in VIEW_CASES:
+        r = subprocess.run([os.path.join(REF, "views_probe"), sym, repr(t), repr(p), str(f)],
                            capture_output=True, text=True, check=True)
-        out[f"C{order}_{t}_{p}_{f}"] = np.loadtxt(r.stdout.splitlines()).reshape(-1, 4)
+        out[f"{sym}_{t}_{p}_{f}"] = np.loadtxt(r.stdout.splitlines()).reshape(-1, 4)
     path = os.path.join(OUT, "views.npz")
     np.savez_compressed(path, **out)
     return path
@@ -134,6 +137,7 @@ def make_views() -> str:
 if __name__ == "__main__":
     if not os.path.exists(os.path.join(REF, "match_probe")):
         sys.exit("build the reference first: make -C oracle ref")
-    for name, case in CASES.items():
-        print(make(name, case))
+    if sys.argv[1:] != ["views"]:          # "views": only the view lists
+        for name, case in CASES.items():
+            print(make(name, case))
     print(make_views())

@@ -11,6 +11,7 @@ REFINE_CASES = ["refine64", "refine32", "refine64ctf"]
 def load(case: str):
     z = np.load(os.path.join(GOLDEN, case + ".npz"))
     d = {k: z[k] for k in z.files}
+    d["case"] = case
     d["N"] = int(d["map"].shape[0])
     d["n"] = int(d["images"].shape[1])
     for k in ("pixel", "hi_res", "alpha", "accuracy", "shift_step", "shift_accuracy", "file_avg", "file_std", "volt",

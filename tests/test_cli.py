@@ -96,11 +96,14 @@ def _write_refine_project(d, tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fomtype", ["frc", "dpr"])
 @pytest.mark.parametrize("case", ["refine64", "refine32", "refine64ctf"])
-def test_brefine_matches_reference(case, exe, tmp_path):
+def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
+    """The drop-in brefine against the reference's img_refine_grid, with the
+    FRC figure of merit (refine*.npz) and with -fomtype dpr (refine_dpr.npz)."""
     import math
     from bsoft_b200.project import read_project
-    from tests.refine_helpers import load
+    from tests.refine_helpers import GOLDEN, load
     d = load(case)
     star = _write_refine_project(d, str(tmp_path))
     out = os.path.join(str(tmp_path), "out.star")
@@ -110,9 +113,11 @@ def test_brefine_matches_reference(case, exe, tmp_path):
             "-step", f"{d['shift_step']},{d['shift_accuracy']}", "-resolution", repr(d["hi_res"]), "-output", out, star]
     if d["def_std"] > 0:
         args[1:1] = ["-defocus", repr(d["def_std"])]
+    if fomtype == "dpr":
+        args[1:1] = ["-fomtype", "dpr"]
     subprocess.run(args, capture_output=True, text=True, check=True)
     proj = read_project(out)
-    ref = d["result"]
+    ref = d["result"] if fomtype == "frc" else np.load(os.path.join(GOLDEN, "refine_dpr.npz"))[case]
     for i, mg in enumerate(proj.micrographs):
         v = mg.view[0]
         assert np.abs(v[:3] - ref[i, :3]).max() < 1e-9 and abs(v[3] - ref[i, 3]) < 1e-9, (i, v, ref[i, :4])

@@ -52,6 +52,23 @@ def test_prepared_images(matcher):
         assert rel_l2(a, b) < TOL_SPEC
 
 
+def test_figure_of_merit_dpr(matcher):
+    """The DPR figure of merit (brefine -fomtype dpr) of the fixture's
+    hypotheses against the reference's own values (tests/golden/match_dpr.npz,
+    made by make_match_dpr_golden.py): FP64 scoring to 1e-6, FP32 to 2e-5."""
+    import os
+    from tests.helpers import GOLDEN
+    m, d = matcher
+    ref = np.load(os.path.join(GOLDEN, "match_dpr.npz"))[d["name"]]
+    f64, cv64 = m.score(hypotheses(d), fp64=True, dpr=True)
+    f32, cv32 = m.score(hypotheses(d), dpr=True)
+    assert np.abs(f64 - ref[:, 0]).max() < 1e-6 and np.abs(cv64 - ref[:, 1]).max() < 1e-6
+    assert np.abs(f32 - ref[:, 0]).max() < TOL_FOM and np.abs(cv32 - ref[:, 1]).max() < TOL_FOM
+    # a different figure from the FRC of the same hypotheses
+    frc, _ = m.score(hypotheses(d), fp64=True)
+    assert np.abs(frc - f64).max() > 1e-3
+
+
 def test_figure_of_merit(matcher):
     m, d = matcher
     fom, cv = m.score(hypotheses(d))

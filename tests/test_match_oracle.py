@@ -105,16 +105,26 @@ def test_true_view_scores_best(case):
 
 
 def test_asymmetric_unit_views():
-    """The view grid restatement against asymmetric_unit_views of the reference."""
+    """The view grid restatement against asymmetric_unit_views of the
+    reference (views_probe) for cyclic, dihedral, tetrahedral, octahedral and
+    icosahedral groups: bit for bit, with the steps converted as the probe
+    converts its degrees (deg * pi / 180)."""
     import math
     import os
-    from bsoft_b200.geometry import asymmetric_unit_views_c
+    from bsoft_b200.geometry import asymmetric_unit_views, asymmetric_unit_views_c
     from tests.match_helpers import GOLDEN
     z = np.load(os.path.join(GOLDEN, "views.npz"))
+    groups = set()
     for key in z.files:
         sym, t, p, f = key.split("_")
-        v = asymmetric_unit_views_c(int(sym[1:]), math.radians(float(t)), math.radians(float(p)),
-                                    full=bool(int(f) & 1), inplane=not (int(f) & 2))
-        assert v.shape == z[key].shape
-        assert np.abs(v - z[key]).max() < 1e-12
+        groups.add(sym[0])
+        v = asymmetric_unit_views(sym, float(t) * math.pi / 180, float(p) * math.pi / 180,
+                                  full=bool(int(f) & 1), inplane=not (int(f) & 2))
+        assert v.shape == z[key].shape, key
+        assert np.array_equal(v, z[key]), (key, np.abs(v - z[key]).max())
+        if sym[0] == "C":
+            vc = asymmetric_unit_views_c(int(sym[1:]), float(t) * math.pi / 180, float(p) * math.pi / 180,
+                                         full=bool(int(f) & 1), inplane=not (int(f) & 2))
+            assert np.array_equal(vc, v)
+    assert groups == {"C", "D", "T", "O", "I"}
     assert len(z["C1_3.0_3.0_1"]) == 4586

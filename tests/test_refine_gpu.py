@@ -47,6 +47,23 @@ def test_matches_reference(setup):
     assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
 
 
+def test_dpr_matches_reference(setup):
+    """brefine -fomtype dpr: the same refinement scored with the DPR figure
+    of merit against the reference's img_refine_grid with fom_type 1
+    (tests/golden/refine_dpr.npz, make_refine_dpr_golden.py)."""
+    import os
+    from tests.refine_helpers import GOLDEN
+    m, d = setup
+    ref = np.load(os.path.join(GOLDEN, "refine_dpr.npz"))[d["case"]]
+    out = _refine(m, d, dpr=True)
+    assert np.array_equal(out[:, 8], ref[:, 8]), (out[:, 8], ref[:, 8])
+    assert np.abs(out[:, :4] - ref[:, :4]).max() < 1e-12
+    assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9
+    assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
+    assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+    assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
+
+
 def test_batch_invariant_and_repeated_images(setup):
     m, d = setup
     whole = _refine(m, d)
