@@ -74,6 +74,15 @@ class BsgError(RuntimeError):
 _lib = None
 
 
+class ShellStats(C.Structure):
+    """bsg_recon_shell_stats"""
+    _fields_ = [("friedel", C.c_double), ("coverage", C.c_long), ("coverage_pct", C.c_double),
+                ("res_snr", C.c_double), ("res_fsc", C.c_double), ("rows", C.c_int)]
+
+
+STATS_COLUMNS = 9
+
+
 def load():
     """Load libbsgpu.so (raises if it has not been built)."""
     global _lib
@@ -91,6 +100,7 @@ def load():
         "bsg_recon_accumulators": ([vp, C.c_int, vp, vp, C.c_int], C.c_int),
         "bsg_recon_add_partial": ([vp, C.c_int, vp, vp, vp, vp, C.c_int], C.c_int),
         "bsg_recon_fsc": ([vp, C.c_int, dp], C.c_int),
+        "bsg_recon_statistics": ([vp, C.c_int, C.c_double, C.POINTER(ShellStats), dp, C.c_int], C.c_int),
         "bsg_particle_spectra": ([vp, vp, vp, C.c_long, vp, C.c_int], C.c_int),
         "bsg_recon_set_timing": ([vp, C.c_int], C.c_int),
         "bsg_recon_set_tile_shape": ([vp, C.c_int], C.c_int),

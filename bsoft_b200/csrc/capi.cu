@@ -732,3 +732,198 @@ void* bsg_recon_stream(bsg_recon* h) {
 }
 
 }  // extern "C"
+
+// ---- reconstruction statistics (host, FP64 sums) -----------------------------
+namespace {
+
+// Bimage::radial(0, maxrad, 1, wrap = 1) of an N^3 real array about the
+// origin 0: value split linearly between the two shells around
+// |(x, y, z)|, sums and weights in float as the reference's Float image and
+// vector<float> hold them; maxrad is clamped to N / 2.
+std::vector<double> radial_average(const std::vector<double>& v, int N, long maxrad) {
+    const long h = N / 2;
+    if (maxrad < 1 || maxrad > h) maxrad = h;
+    std::vector<float> sum(maxrad, 0.f), num(maxrad, 0.f);
+    size_t i = 0;
+    for (int zz = 0; zz < N; ++zz) {
+        double dz = zz > h ? zz - N : zz;
+        const double z2 = dz * dz;
+        for (int yy = 0; yy < N; ++yy) {
+            double dy = yy > h ? yy - N : yy;
+            const double y2 = dy * dy;
+            for (int xx = 0; xx < N; ++xx, ++i) {
+                double dx = xx > h ? xx - N : xx;
+                const double r = sqrt(dx * dx + y2 + z2);
+                long ir = (long)r;
+                if (ir < maxrad) {
+                    const double f = r - ir, f1 = 1 - f;
+                    num[ir] = (float)((double)num[ir] + f1);
+                    sum[ir] = (float)((double)sum[ir] + f1 * v[i]);
+                    if (++ir < maxrad) {
+                        num[ir] = (float)((double)num[ir] + f);
+                        sum[ir] = (float)((double)sum[ir] + f * v[i]);
+                    }
+                }
+            }
+        }
+    }
+    std::vector<double> out(maxrad, 0.0);
+    for (long j = 0; j < maxrad; ++j) out[j] = num[j] ? (double)(float)((double)sum[j] / num[j]) : 0.0;
+    return out;
+}
+
+}  // namespace
+
+int bsg_recon_statistics(bsg_recon* h, int imap, double resolution, bsg_recon_shell_stats* out, double* table,
+                         int max_rows) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !out || imap < 0 || imap > 2 || (imap > 0 && r->nhalves < 2))
+        return fail(BSG_ERR_ARG, "bsg_recon_statistics: bad argument (map %d)", imap);
+    if (!r->g.fom) return fail(BSG_ERR_STATE, "bsg_recon_statistics: needs the power and weight^2 channels (fom = 1)");
+    CK(cudaSetDevice(r->device));
+    CK(cudaStreamSynchronize(r->stream));
+    const int N = r->g.map;
+    const size_t N3 = r->vol_elems();
+    // the map's sums: one half, or both added (imap 0 with half maps)
+    std::vector<double> v(2 * N3), w(N3), p(N3), q(N3);
+    const int h0 = (r->nhalves == 2 && imap > 0) ? imap - 1 : 0;
+    CK(cudaMemcpy(v.data(), r->d_vol[h0], sizeof(double2) * N3, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(w.data(), r->d_w[h0], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(p.data(), r->d_pow[h0], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(q.data(), r->d_w2[h0], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+    if (r->nhalves == 2 && imap == 0) {
+        std::vector<double> t(2 * N3);
+        CK(cudaMemcpy(t.data(), r->d_vol[1], sizeof(double2) * N3, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < 2 * N3; ++i) v[i] += t[i];
+        t.resize(N3);
+        CK(cudaMemcpy(t.data(), r->d_w[1], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < N3; ++i) w[i] += t[i];
+        CK(cudaMemcpy(t.data(), r->d_pow[1], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < N3; ++i) p[i] += t[i];
+        CK(cudaMemcpy(t.data(), r->d_w2[1], sizeof(double) * N3, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < N3; ++i) q[i] += t[i];
+    }
+    // fspace_reconstruction_weigh (Bimage_reconstruct.cpp:486-515); the map
+    // held as float complex as the reference holds it
+    std::vector<float> fr(N3), fi(N3);
+    long cov = 0;
+    for (size_t i = 0; i < N3; ++i) {
+        if (w[i] > 1e-30) {
+            q[i] = w[i] - q[i] / w[i];
+            fr[i] = (float)(v[2 * i] / w[i]);
+            fi[i] = (float)(v[2 * i + 1] / w[i]);
+            if (q[i] > 1) p[i] /= q[i];
+            else if (w[i] > 1) p[i] /= w[i];
+            if (p[i] < 0) p[i] = 0;
+            ++cov;
+        } else {
+            fr[i] = fi[i] = 0.f;
+            p[i] = 0;
+            w[i] = q[i] = 1e-30;
+        }
+    }
+    p[0] = 1;
+    const double real = r->g.mscale, samp = r->cfg.map_sampling;
+    // coverage against the sphere of fspace_maximum_radius(hi_res) + 1
+    auto max_radius = [&](double res) -> long { return res > 0.1 ? (long)(real / res) : (long)(N / 2.0); };
+    const double rad = (double)max_radius(resolution) + 1;
+    out->coverage = cov;
+    out->coverage_pct = cov * 100.0 / ((4.0 / 3.0) * M_PI * rad * rad * rad);
+    // Bimage::friedel_check (Bimage_fspace.cpp:2024-2066)
+    {
+        double s = 0, Rr = 0, Ri = 0;
+        for (int zz = 0; zz < N; ++zz) {
+            const int zf = zz ? N - zz : 0;
+            for (int yy = 0; yy < N; ++yy) {
+                const int yf = yy ? N - yy : 0;
+                for (int xx = 0; xx < (N + 1) / 2; ++xx) {
+                    const int xf = xx ? N - xx : 0;
+                    const size_t i = ((size_t)zz * N + yy) * N + xx, j = ((size_t)zf * N + yf) * N + xf;
+                    const double vr = fr[i], vi = fi[i], ur = fr[j], ui = fi[j];
+                    const double ww = ((vr * vr + vi * vi) + (ur * ur + ui * ui)) / 2;
+                    double d = vr - ur;
+                    Rr += d * d * ww;
+                    d = vi + ui;
+                    Ri += d * d * ww;
+                    s += ww;
+                }
+            }
+        }
+        Rr = sqrt(Rr / s);
+        Ri = sqrt(Ri / s);
+        out->friedel = sqrt(Rr * Rr + Ri * Ri);
+    }
+    // fspace_reconstruction_stats (Bimage_reconstruct.cpp:526-599)
+    const long maxrad = max_radius(resolution);
+    double res_checked = resolution;         // fspace_radial_power's check_resolution
+    if (res_checked > real) res_checked = real;
+    else res_checked = std::max(res_checked, 2.0 / sqrt(3.0 / (samp * samp)));
+    const long maxrad_p = max_radius(res_checked);
+    std::vector<double> prad(std::max(0L, maxrad_p), 0.0);
+    {
+        std::vector<float> sum(prad.size(), 0.f), num(prad.size(), 0.f);
+        const long hh = (N - 1) / 2;
+        const double fsc_ = 1.0 / real;
+        size_t i = 0;
+        for (int zz = 0; zz < N; ++zz) {
+            double rz = zz > hh ? zz - N : zz;
+            rz *= fsc_;
+            rz *= rz;
+            for (int yy = 0; yy < N; ++yy) {
+                double ry = yy > hh ? yy - N : yy;
+                ry *= fsc_;
+                ry *= ry;
+                for (int xx = 0; xx < N; ++xx, ++i) {
+                    double rx = xx > hh ? xx - N : xx;
+                    rx *= fsc_;
+                    rx *= rx;
+                    const double radius = real * sqrt(rx + ry + rz);
+                    long ir = (long)radius;
+                    if (ir < maxrad_p) {
+                        const double f = radius - ir, f1 = 1 - f;
+                        const double val = (double)fr[i] * fr[i] + (double)fi[i] * fi[i];
+                        num[ir] = (float)((double)num[ir] + f1);
+                        sum[ir] = (float)((double)sum[ir] + f1 * val);
+                        if (++ir < maxrad_p) {
+                            num[ir] = (float)((double)num[ir] + f);
+                            sum[ir] = (float)((double)sum[ir] + f * val);
+                        }
+                    }
+                }
+            }
+        }
+        for (size_t j = 0; j < prad.size(); ++j) prad[j] = num[j] ? (double)(float)((double)sum[j] / num[j]) : 0.0;
+    }
+    const std::vector<double> pfom = radial_average(p, N, maxrad), pw = radial_average(w, N, maxrad),
+                              pw2 = radial_average(q, N, maxrad);
+    auto at = [](const std::vector<double>& a, long k) { return k >= 0 && k < (long)a.size() ? a[k] : 0.0; };
+    double fscp = 1, snrp = 10, res_fsc = 0, res_snr = 0;
+    const double fsc_cut = 0.3, snr_cut = 0.5;
+    int rows = 0;
+    for (long i = 1; i < maxrad; ++i, ++rows) {
+        const double s = i / real, res = real / i;
+        double fsc = 0, snr = 0, signal = 0, noise = 0;
+        const double wi = at(pw, i);
+        if (wi > 1e-3) {
+            const double w2 = at(pw2, i);
+            noise = (at(pfom, i) - at(prad, i)) / w2;
+            signal = (wi * at(prad, i) - at(pfom, i)) / w2;
+            if (noise > 0) snr = signal / noise;
+            fsc = snr / (snr + 1);
+            if (fsc < 0) fsc = 0;
+        }
+        if (fscp >= fsc_cut && fsc < fsc_cut) res_fsc = 1 / (s - (fsc_cut - fsc) / ((fscp - fsc) * real));
+        if (snrp >= snr_cut && snr < snr_cut) res_snr = 1 / (s - (snr_cut - snr) / ((snrp - snr) * real));
+        fscp = fsc;
+        snrp = snr;
+        if (table && rows < max_rows) {
+            double* t = table + (size_t)rows * BSG_STATS_COLUMNS;
+            t[0] = (double)i; t[1] = s; t[2] = res; t[3] = wi; t[4] = at(prad, i);
+            t[5] = signal; t[6] = noise; t[7] = snr; t[8] = fsc;
+        }
+    }
+    out->rows = rows;
+    out->res_snr = res_snr;
+    out->res_fsc = res_fsc;
+    return BSG_OK;
+}

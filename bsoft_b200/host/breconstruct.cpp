@@ -43,6 +43,7 @@ struct Options {
     int interp = 0, pad = 2, ctf_action = 0, size = 0, nmaps = 0, batch = 4096, device = 0;
     double wiener = 0, resolution = 0, sampling = 0, scale = 1;
     bool bootstrap = false, plan_only = false;
+    int verbose = 0;
     std::string symmetry = "C1";
     std::string recons, fom;
     std::vector<std::string> inputs;
@@ -64,6 +65,7 @@ long part_ft_size(long xsize, double scale, int pad) {
 struct Plan {
     int n = 0, ft = 0, map = 0, nmaps = 1;
     double map_sampling = 0, hi_res = 0, wiener = 0;
+    double resolution = 0;          // the limit before check_resolution (the statistics use it)
     std::vector<double> rec;                        // BSG_PARTICLE_DOUBLES per particle
     std::vector<std::pair<int, long>> src;          // (micrograph, image index) per particle
 };
@@ -93,6 +95,7 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
     if (hr > p.map * p.map_sampling) hr = p.map * p.map_sampling;
     else hr = std::fmax(hr, 2.0 / std::sqrt(3.0 / (p.map_sampling * p.map_sampling)));
     p.hi_res = hr;
+    p.resolution = resolution;
     p.wiener = (o.ctf_action > 2 && o.wiener < 0.01) ? 0.2 : o.wiener;
     p.nmaps = o.nmaps < 1 ? 1 : (o.nmaps > 3 ? 3 : o.nmaps);
     // per-particle records (particle_reconstruct, mg_reconstruct.cpp:143-212)
@@ -133,7 +136,7 @@ void usage() {
             "Usage: breconstruct [options] input.star\n"
             "  -interpolation nearest|weighted|trilinear  -pad 2  -CTF none|flip|apply|correct|wiener\n"
             "  -wiener 0.2  -resolution 4  -size 64  -sampling 1.5  -scale 1  -fullmap  -halfmaps\n"
-            "  -bootstrap  -reconstruction out.mrc  -fom fom.mrc  -batch 4096  -device 0  -plan\n");
+            "  -bootstrap  -reconstruction out.mrc  -fom fom.mrc  -verbose 1  -batch 4096  -device 0  -plan\n");
 }
 
 int ctf_code(const std::string& v) {
@@ -174,6 +177,7 @@ Options parse(int argc, char** argv) {
         else if (a == "-batch") o.batch = atoi(val().c_str());
         else if (a == "-device") o.device = atoi(val().c_str());
         else if (a == "-plan") o.plan_only = true;
+        else if (a == "-verbose") o.verbose = atoi(val().c_str());
         else if (a == "-h" || a == "-help") { usage(); exit(0); }
         else if (a[0] == '-') throw std::runtime_error("unknown option " + a);
         else o.inputs.push_back(a);
@@ -223,7 +227,9 @@ int main(int argc, char** argv) {
         bsg_recon_config cfg = {};
         cfg.n = p.n; cfg.ft = p.ft; cfg.map = p.map; cfg.map_sampling = p.map_sampling; cfg.hi_res = p.hi_res;
         cfg.interp = o.interp; cfg.ctf_action = o.ctf_action; cfg.wiener = p.wiener; cfg.nmaps = p.nmaps;
-        cfg.fom = o.fom.empty() ? 0 : 1; cfg.batch = 0; cfg.device = o.device;
+        // the power and weight^2 channels: for the -fom map, and for the
+        // statistics -verbose prints
+        cfg.fom = (o.fom.empty() && !o.verbose) ? 0 : 1; cfg.batch = 0; cfg.device = o.device;
         bsg_recon* rec = nullptr;
         CALL(bsg_recon_create(&cfg, &rec));
         // point-group symmetry during reconstruction (mode 0)
@@ -250,11 +256,36 @@ int main(int argc, char** argv) {
         const size_t n3 = (size_t)p.map * p.map * p.map;
         std::vector<float> vol(n3), fom(cfg.fom ? n3 : 0);
         const int flags = o.interp == 2 ? BSG_SINC : 0;
+        if (o.verbose) {
+            // img_reconstruction_sum_weigh's report (mg_reconstruct.cpp:328-349):
+            // Friedel residual and coverage of every map, the shell table of
+            // the first (Bimage_reconstruct.cpp:526-599), in its format
+            for (int i = 0; i < p.nmaps; ++i) {
+                const int imap = p.nmaps == 2 ? i + 1 : (p.nmaps == 3 ? i : 0);
+                bsg_recon_shell_stats st;
+                std::vector<double> tab((size_t)(p.map + 2) * BSG_STATS_COLUMNS);
+                CALL(bsg_recon_statistics(rec, imap, p.resolution, &st, tab.data(), p.map + 2));
+                if (imap == 0) printf("Full reconstruction:\n");
+                else printf("Half reconstruction %d:\n", imap);
+                printf("Friedel symmetry residual:      %.2f\n", st.friedel);
+                printf("Coverage:                       %ld (%.2f %%)\n\n", st.coverage, st.coverage_pct);
+                if (i != 0) continue;
+                printf("Radius\ts(1/A)\tRes(A)\tWeight\tPower\tSignal\tNoise\tSNR\tFSC\n");
+                for (int k = 0; k < st.rows && k < p.map + 2; ++k) {
+                    const double* t = &tab[(size_t)k * BSG_STATS_COLUMNS];
+                    printf("%ld\t%.4f\t%.2f\t%.2f\t%.6f\t%.6f\t%.6f\t%.4f\t%.4f\n", (long)t[0], t[1], t[2], t[3],
+                           t[4], t[5], t[6], t[7], t[8]);
+                }
+                printf("\nResolution estimates:\nSNR(0.5):                       %.4f A\n"
+                       "FSC(0.3):                       %.4f A\n\n", st.res_snr, st.res_fsc);
+            }
+        }
         for (int i = 0; i < p.nmaps; ++i) {
             const int imap = p.nmaps == 2 ? i + 1 : (p.nmaps == 3 ? i : 0);
-            CALL(bsg_recon_finish(rec, imap, vol.data(), cfg.fom ? fom.data() : nullptr, flags));
+            const bool want_fom = !o.fom.empty();
+            CALL(bsg_recon_finish(rec, imap, vol.data(), want_fom ? fom.data() : nullptr, flags));
             write_mrc_volume(map_name(o.recons, imap), vol.data(), p.map, p.map_sampling, p.map / 2);
-            if (cfg.fom) write_mrc_volume(map_name(o.fom, imap), fom.data(), p.map, p.map_sampling, p.map / 2);
+            if (want_fom) write_mrc_volume(map_name(o.fom, imap), fom.data(), p.map, p.map_sampling, p.map / 2);
             printf("Writing %s\n", map_name(o.recons, imap).c_str());
         }
         bsg_recon_destroy(rec);

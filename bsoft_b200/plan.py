@@ -95,6 +95,7 @@ class ReconPlan:
     stack_index: list = field(default_factory=list)   # (stack file, image index) per particle
     nmaps: int = 1
     symmetry: str = "C1"          # point group inserted during reconstruction (mode 0)
+    resolution: float = 0.0       # breconstruct's limit before any check (the statistics' limit)
 
 
 def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
@@ -161,7 +162,7 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
     return ReconPlan(n=hdr.nx, ft=ft, map=size, map_sampling=map_sampling, hi_res=hi_res,
                      interp=opt.interp, ctf_action=opt.ctf_action, wiener=wiener,
                      params=np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES),
-                     stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1")
+                     stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1", resolution=resolution)
 
 
 def load_images(plan: ReconPlan, sel=None) -> np.ndarray:

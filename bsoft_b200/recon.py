@@ -140,6 +140,22 @@ class Reconstructor:
                    "bsg_recon_fsc")
         return out
 
+    def statistics(self, imap: int = 0, resolution: float | None = None) -> dict:
+        """Reconstruction statistics of map imap as breconstruct prints them
+        (bsg_recon_statistics): Friedel residual, coverage, the shell table
+        (columns radius, s, resolution, weight, power, signal, noise, SNR,
+        FSC) and the SNR(0.5) / FSC(0.3) resolution estimates.  resolution:
+        breconstruct's limit before checks (default: the plan's)."""
+        res = self.plan.resolution if resolution is None else resolution
+        st = _lib.ShellStats()
+        rows = max(1, int(self.plan.map * self.plan.map_sampling / res) + 1) if res > 0.1 else self.N
+        table = np.zeros((rows, _lib.STATS_COLUMNS))
+        _lib.check(_lib.load().bsg_recon_statistics(self._h, imap, float(res), C.byref(st),
+                                                    table.ctypes.data_as(C.POINTER(C.c_double)), rows),
+                   "bsg_recon_statistics")
+        return dict(friedel=st.friedel, coverage=st.coverage, coverage_pct=st.coverage_pct, res_snr=st.res_snr,
+                    res_fsc=st.res_fsc, table=table[:st.rows].copy())
+
     def spectra(self, images, params: np.ndarray) -> np.ndarray:
         params = np.ascontiguousarray(params, dtype=np.float64)
         images = np.ascontiguousarray(images, dtype=np.float32)

@@ -136,6 +136,37 @@ int  bsg_recon_add_partial(bsg_recon* r, int half, const double* vol, const doub
  * map * sampling / hi_res on are 0.  nshell doubles. */
 int  bsg_recon_fsc(bsg_recon* r, int nshell, double* fsc_out);
 
+/* Reconstruction statistics of map imap (0 full, 1/2 halves) as
+ * img_reconstruction_sum_weigh reports them (bsoft/src/mg/mg_reconstruct.cpp:
+ * 328-349) after fspace_reconstruction_weigh (bsoft/src/img/
+ * Bimage_reconstruct.cpp:486-515): the Friedel symmetry residual
+ * (Bimage::friedel_check, bsoft/src/img/Bimage_fspace.cpp:2024), the
+ * coverage (voxels with weight > 1e-30) and its percentage of the sphere of
+ * radius maxrad + 1, and the shell table of fspace_reconstruction_stats
+ * (Bimage_reconstruct.cpp:526-599): rows for radii 1 .. maxrad - 1 with
+ * maxrad = map * sampling / resolution (resolution: breconstruct's limit
+ * before any check, the sampling by default), columns BSG_STATS_COLUMNS:
+ * radius, s (1/A), resolution (A), weight, power, signal, noise, SNR, FSC;
+ * and the SNR(0.5) and FSC(0.3) resolution estimates (A, 0 when not
+ * crossed).  The radial averages follow Bimage::radial and
+ * fspace_radial_power (linear interpolation between shells); where the
+ * reference reads past the end of its arrays (radii >= map / 2 for the
+ * channel averages, radii beyond the checked resolution for the power), the
+ * values are 0, as it prints them.  Needs fom = 1 (the power and weight^2
+ * channels); computed on the host from the FP64 sums.  table: max_rows x
+ * BSG_STATS_COLUMNS doubles (rows beyond max_rows are dropped). */
+#define BSG_STATS_COLUMNS 9
+typedef struct {
+    double friedel;          /* Friedel symmetry residual                      */
+    long   coverage;         /* voxels with weight > 1e-30                     */
+    double coverage_pct;     /* coverage / (4/3 pi (maxrad + 1)^3) x 100       */
+    double res_snr;          /* SNR(0.5) resolution estimate (angstrom)        */
+    double res_fsc;          /* FSC(0.3) resolution estimate (angstrom)        */
+    int    rows;             /* shell rows (maxrad - 1)                        */
+} bsg_recon_shell_stats;
+int  bsg_recon_statistics(bsg_recon* r, int imap, double resolution, bsg_recon_shell_stats* out, double* table,
+                          int max_rows);
+
 /* The 2-D stage alone: padded FFT, origin shift and CTF of nparts images;
  * out = nparts x ft x ft complex64 (interleaved), reference pixel order. */
 int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* params,

@@ -124,3 +124,30 @@ def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
         assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 1e-9
         if d["def_std"] > 0:
             assert abs(mg.defocus[0] - ref[i, 9]) < 1e-6 * ref[i, 9]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["fom_ctf16_tri_flip", "fom_plain24_tri", "fom_ctf16_tri_flip_half"])
+def test_verbose_statistics_match_reference(case, exe, tmp_path):
+    """breconstruct -verbose 1: the Friedel residual, coverage and shell
+    table the drop-in prints against what the reference prints
+    (tests/golden/fom_stats.npz)."""
+    from tests.test_recon_gpu import close_to_printed, parse_reference_stats
+    z = np.load(os.path.join(GOLDEN, "fom_stats.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    out = os.path.join(str(tmp_path), "map.mrc")
+    r = subprocess.run([exe, "-verbose", "1", *shlex.split(str(z[case + "__options"])), "-reconstruction", out, star],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = {d["map"]: d for d in parse_reference_stats(r.stdout)}
+    want = {d["map"]: d for d in parse_reference_stats(str(z[case + "__stdout"]))}
+    assert set(got) == set(want)
+    for k, w in want.items():
+        g = got[k]
+        assert g["coverage"] == w["coverage"]
+        assert close_to_printed(float(g["friedel"]), w["friedel"], 1e-3, 1.0)
+        assert close_to_printed(float(g["coverage_pct"]), w["coverage_pct"], 1e-3, 1.0)
+        assert len(g["rows"]) == len(w["rows"])
+        for a, b in zip(g["rows"], w["rows"]):
+            for c in range(1, 9):
+                assert close_to_printed(float(a[c]), b[c], 1e-3, 1.0), (k, a, b)

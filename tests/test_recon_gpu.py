@@ -205,3 +205,83 @@ def test_gpu_fom_map_matches_reference(case, suffixes, tmp_path):
             print(case, suf, "fom rel L2", err, "same nonzero voxels", kept)
             assert err < 1e-5
             assert kept == 1.0
+
+
+def parse_reference_stats(text: str) -> list:
+    """The reconstruction reports breconstruct -verbose 1 prints
+    (img_reconstruction_sum_weigh, fspace_reconstruction_stats): one dict per
+    map with the printed strings of every number."""
+    import re
+    out = []
+    lines = text.splitlines()
+    i = 0
+    while i < len(lines):
+        m = re.match(r"(Full|Half) reconstruction\s*(\d*):", lines[i])
+        if not m:
+            i += 1
+            continue
+        d = {"map": 0 if m.group(1) == "Full" else int(m.group(2)), "rows": []}
+        d["friedel"] = lines[i + 1].split(":")[1].strip()
+        cov = lines[i + 2].split(":")[1].split()
+        d["coverage"], d["coverage_pct"] = cov[0], cov[1].strip("(")
+        i += 3
+        while i < len(lines) and not lines[i].startswith("Radius") and not re.match(r"(Full|Half) rec", lines[i]):
+            i += 1
+        if i < len(lines) and lines[i].startswith("Radius"):
+            i += 1
+            while i < len(lines) and lines[i].strip():
+                d["rows"].append(lines[i].split("\t"))
+                i += 1
+            while not lines[i].startswith("SNR(0.5)"):
+                i += 1
+            d["res_snr"] = lines[i].split(":")[1].split()[0]
+            d["res_fsc"] = lines[i + 1].split(":")[1].split()[0]
+        out.append(d)
+    # the table is printed only for the first map of a set (imap % nmaps == 0,
+    # mg_reconstruct.cpp:347); with parallel weighing it can follow another
+    # map's lines, so it belongs to the lowest map index
+    rows = [d for d in out if d["rows"]]
+    if rows and out:
+        first = min(out, key=lambda d: d["map"])
+        if rows[0] is not first:
+            for k in ("rows", "res_snr", "res_fsc"):
+                first[k] = rows[0].pop(k)
+            rows[0]["rows"] = []
+    return out
+
+
+def close_to_printed(value: float, printed: str, rel: float = 1e-4, units: float = 0.5) -> bool:
+    """|value - printed| within `units` of the printed last decimal (half a
+    unit for an unrounded value, one for a value printed the same way), plus
+    a relative slack for the FP32 (reference) against FP64 (here) sums."""
+    dec = len(printed.split(".")[1]) if "." in printed else 0
+    ref = float(printed)
+    return abs(value - ref) <= units * 10.0 ** -dec + rel * abs(ref) + 1e-12
+
+
+@pytest.mark.parametrize("case,suffixes", FOM_CASES)
+def test_gpu_reconstruction_statistics_match_reference(case, suffixes, tmp_path):
+    """Friedel residual, coverage and the shell table against what the
+    reference prints for the same reconstruction (fom_stats.npz)."""
+    from tests.helpers import options_from_args
+    z = np.load(os.path.join(GOLDEN, "fom_stats.npz"))
+    reports = parse_reference_stats(str(z[case + "__stdout"]))
+    assert len(reports) == len(suffixes)
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    plan = plan_reconstruction(read_project(star), options_from_args(str(z[case + "__options"])))
+    with Reconstructor(plan, fom=True) as rec:
+        rec.insert(load_images(plan), plan.params)
+        for rep in reports:
+            st = rec.statistics(rep["map"])
+            assert st["coverage"] == int(rep["coverage"])
+            assert close_to_printed(st["coverage_pct"], rep["coverage_pct"])
+            assert close_to_printed(st["friedel"], rep["friedel"])
+            if not rep["rows"]:
+                continue
+            assert len(st["table"]) == len(rep["rows"])
+            for got, want in zip(st["table"], rep["rows"]):
+                assert int(want[0]) == int(got[0])
+                for c in range(1, 9):
+                    assert close_to_printed(got[c], want[c]), (int(got[0]), c, got[c], want[c])
+            assert close_to_printed(st["res_snr"], rep["res_snr"], 1e-3)
+            assert close_to_printed(st["res_fsc"], rep["res_fsc"], 1e-3)
