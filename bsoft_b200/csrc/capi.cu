@@ -201,7 +201,7 @@ static void free_all(Recon* r) {
         if (r->compute_done[i]) cudaEventDestroy(r->compute_done[i]);
     }
     F(r->d_bkg); F(r->d_phase); F(r->d_rows); F(r->d_tw); F(r->d_twmap);
-    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_tile_order); F(r->d_part_sums);
+    F(r->d_work); F(r->d_map); F(r->d_fom); F(r->d_fsc); F(r->d_tile_order); F(r->d_part_sums); F(r->d_symtmp);
     if (r->h_status) cudaFreeHost(r->h_status);
     for (auto& t : r->timed) { cudaEventDestroy(t.a); cudaEventDestroy(t.b); }
     r->timed.clear();
@@ -530,9 +530,22 @@ int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int
     const bool sinc = (flags & BSG_SINC) != 0;
     const bool dev = (flags & BSG_DEVICE_PTR) != 0;
     float* dst = dev ? map_out : r->d_map;
+    const bool symz = !r->symz_orders.empty();
     CK(launch_weigh(*r, imap, r->stream));
-    CK(launch_ifft3(*r, r->d_work, dst, sinc, r->stream));
+    // with symmetrization after reconstruction (mode 1) the sinc weight
+    // follows it, as breconstruct applies filter_sinc to the written map
+    CK(launch_ifft3(*r, r->d_work, dst, sinc && !symz, r->stream));
     r->stats.launches += 4;
+    if (symz) {
+        if (!r->d_symtmp) {
+            int rc = alloc((void**)&r->d_symtmp, sizeof(float) * r->vol_elems());
+            if (rc) return rc;
+        }
+        CK(launch_symmetrize(*r, dst, r->d_symtmp, sinc, r->stream));
+        long ops = 0;
+        for (int k : r->symz_orders) ops += k > 1;
+        r->stats.launches += 2 + ops;
+    }
     const size_t N3 = r->vol_elems();
     if (!dev) CK(cudaMemcpyAsync(map_out, r->d_map, sizeof(float) * N3, cudaMemcpyDeviceToHost, r->stream));
     if (fom_out) CK(cudaMemcpyAsync(fom_out, r->d_fom, sizeof(float) * N3,
@@ -925,5 +938,17 @@ int bsg_recon_statistics(bsg_recon* h, int imap, double resolution, bsg_recon_sh
     out->rows = rows;
     out->res_snr = res_snr;
     out->res_fsc = res_fsc;
+    return BSG_OK;
+}
+
+int bsg_recon_set_symmetrize(bsg_recon* h, const double* axes, const int* orders, int nops) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || nops < 0 || nops > 8 || (nops > 0 && (!axes || !orders)))
+        return fail(BSG_ERR_ARG, "bsg_recon_set_symmetrize: bad argument (nops %d)", nops);
+    for (int i = 0; i < nops; ++i)
+        if (orders[i] < 1 || orders[i] > 9)
+            return fail(BSG_ERR_ARG, "bsg_recon_set_symmetrize: operation %d has order %d (1..9)", i, orders[i]);
+    r->symz_axes.assign(axes, axes + 3 * nops);
+    r->symz_orders.assign(orders, orders + nops);
     return BSG_OK;
 }

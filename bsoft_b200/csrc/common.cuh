@@ -75,5 +75,6 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, const DevPart
                           cudaStream_t s);
 cudaError_t launch_finish(const Context& c, int imap, float* map_out, float* fom_out, bool sinc, cudaStream_t s);
 cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream_t s);
+cudaError_t launch_symmetrize(const Context& c, float* map, float* tmp, bool sinc, cudaStream_t s);
 
 }  // namespace bsg

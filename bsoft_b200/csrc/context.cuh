@@ -25,6 +25,11 @@ struct Context {
     std::vector<double> sym;          // 9 per operator; empty = C1
     DevParticle* d_psym = nullptr;    // batch x nsym expanded records (current batch)
     std::vector<DevParticle> h_psym;
+    // point-group symmetrization after reconstruction (mode 1): generating
+    // operations (axis as given, order), applied to the finished real map
+    std::vector<double> symz_axes;    // 3 per operation
+    std::vector<int> symz_orders;
+    float* d_symtmp = nullptr;        // N^3 float work map
     double* d_bkg = nullptr;         // batch
     float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
     float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms

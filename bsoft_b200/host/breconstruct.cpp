@@ -44,6 +44,7 @@ struct Options {
     double wiener = 0, resolution = 0, sampling = 0, scale = 1;
     bool bootstrap = false, plan_only = false;
     int verbose = 0;
+    int sym_mode = 0;               // -mode: 0 during reconstruction, 1 after it
     std::string symmetry = "C1";
     std::string recons, fom;
     std::vector<std::string> inputs;
@@ -178,6 +179,12 @@ Options parse(int argc, char** argv) {
         else if (a == "-device") o.device = atoi(val().c_str());
         else if (a == "-plan") o.plan_only = true;
         else if (a == "-verbose") o.verbose = atoi(val().c_str());
+        else if (a == "-mode") {
+            o.sym_mode = atoi(val().c_str());
+            if (o.sym_mode < 0 || o.sym_mode > 1)
+                throw std::runtime_error("-mode " + std::to_string(o.sym_mode) +
+                                         ": only 0 (during) and 1 (after reconstruction) are supported");
+        }
         else if (a == "-h" || a == "-help") { usage(); exit(0); }
         else if (a[0] == '-') throw std::runtime_error("unknown option " + a);
         else o.inputs.push_back(a);
@@ -232,8 +239,20 @@ int main(int argc, char** argv) {
         cfg.fom = (o.fom.empty() && !o.verbose) ? 0 : 1; cfg.batch = 0; cfg.device = o.device;
         bsg_recon* rec = nullptr;
         CALL(bsg_recon_create(&cfg, &rec));
-        // point-group symmetry during reconstruction (mode 0)
-        CALL(bsg_recon_set_symmetry(rec, sym.data(), (int)(sym.size() / 9)));
+        if (o.sym_mode == 1) {
+            // symmetry after reconstruction (mode 1): insert once, symmetrize
+            // the finished map (Bimage::symmetrize, breconstruct.cpp:335)
+            std::vector<double> ax;
+            std::vector<int> ord;
+            for (const SymOp& g : symmetry_generators(o.symmetry)) {
+                ax.insert(ax.end(), g.a, g.a + 3);
+                ord.push_back(g.order);
+            }
+            CALL(bsg_recon_set_symmetrize(rec, ax.data(), ord.data(), (int)ord.size()));
+        } else {
+            // point-group symmetry during reconstruction (mode 0)
+            CALL(bsg_recon_set_symmetry(rec, sym.data(), (int)(sym.size() / 9)));
+        }
         // stream the particles in host batches (the library uploads and
         // overlaps them with the device work)
         const long n2 = (long)p.n * p.n;

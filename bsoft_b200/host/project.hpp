@@ -527,7 +527,10 @@ inline std::vector<Micrograph> read_project(const std::string& path) {
 // from the generating operations of Bsymmetry::Bsymmetry (:42-115) and the
 // label rules of clean_symstring (bsoft/include/symmetry.h:73-99): Cn, Dn,
 // T, O, I and their -2/-3/-4/-5 variants.  Helical and I90 are rejected.
-inline std::vector<double> symmetry_operators(const std::string& sym) {
+struct SymOp { double a[3]; int order; };
+
+// The generating operations (axis as written, order) of Bsymmetry.
+inline std::vector<SymOp> symmetry_generators(const std::string& sym) {
     std::string lbl;
     for (char ch : sym)
         if (!isspace((unsigned char)ch)) lbl += ch;
@@ -544,7 +547,7 @@ inline std::vector<double> symmetry_operators(const std::string& sym) {
     lbl[0] = (char)toupper((unsigned char)lbl[0]);
     auto has = [&](const char* t) { return lbl.find(t) != std::string::npos; };
     const double gold = 1.61803398874989484820458683436563811772;
-    struct Op { double a[3]; int order; };
+    using Op = SymOp;
     std::vector<Op> ops;
     if (lbl[0] == 'C') ops.push_back({{0, 0, 1}, lbl == "Cs" ? 1 : std::max(1, atoi(lbl.c_str() + 1))});
     else if (lbl[0] == 'D') { ops.push_back({{0, 0, 1}, atoi(lbl.c_str() + 1)}); ops.push_back({{1, 0, 0}, 2}); }
@@ -567,8 +570,13 @@ inline std::vector<double> symmetry_operators(const std::string& sym) {
     } else {
         throw std::runtime_error("unsupported symmetry " + sym);
     }
+    return ops;
+}
+
+inline std::vector<double> symmetry_operators(const std::string& sym) {
+    const std::vector<SymOp> ops = symmetry_generators(sym);
     std::vector<std::array<double, 4>> q{{1, 0, 0, 0}};
-    for (const Op& op : ops) {
+    for (const SymOp& op : ops) {
         const double n = std::sqrt(op.a[0] * op.a[0] + op.a[1] * op.a[1] + op.a[2] * op.a[2]);
         const size_t nv = q.size();
         for (int j = 1; j < op.order; ++j) {

@@ -79,6 +79,7 @@ class ReconOptions:
     fom: bool = False             # keep power / weight^2 channels
     threads: int = 2              # reference partial maps (only sets half-map parity)
     symmetry: str = ""            # point group (-symmetry; "" = C1)
+    sym_mode: int = 0             # -mode: 0 during reconstruction, 1 after it (real space)
 
 
 @dataclass
@@ -96,6 +97,7 @@ class ReconPlan:
     nmaps: int = 1
     symmetry: str = "C1"          # point group inserted during reconstruction (mode 0)
     resolution: float = 0.0       # breconstruct's limit before any check (the statistics' limit)
+    sym_mode: int = 0             # 0: symmetry inserted; 1: the finished map symmetrized
 
 
 def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
@@ -162,7 +164,8 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
     return ReconPlan(n=hdr.nx, ft=ft, map=size, map_sampling=map_sampling, hi_res=hi_res,
                      interp=opt.interp, ctf_action=opt.ctf_action, wiener=wiener,
                      params=np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES),
-                     stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1", resolution=resolution)
+                     stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1", resolution=resolution,
+                     sym_mode=opt.sym_mode)
 
 
 def load_images(plan: ReconPlan, sel=None) -> np.ndarray:

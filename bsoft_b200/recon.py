@@ -44,7 +44,10 @@ class Reconstructor:
         self._h = h
         sym = getattr(plan, "symmetry", "C1") or "C1"
         if sym != "C1":
-            self.set_symmetry(sym)
+            if getattr(plan, "sym_mode", 0) == 1:
+                self.set_symmetrize(sym)
+            else:
+                self.set_symmetry(sym)
         self.fom = fom
 
     # context management
@@ -189,6 +192,17 @@ class Reconstructor:
         ops = np.ascontiguousarray(ops, dtype=np.float64).reshape(-1, 9)
         _lib.check(_lib.load().bsg_recon_set_symmetry(self._h, ops.ctypes.data_as(C.POINTER(C.c_double)), len(ops)),
                    "bsg_recon_set_symmetry")
+
+    def set_symmetrize(self, sym):
+        """Point group applied to the finished map in real space
+        (breconstruct -symmetry with -mode 1); "C1" or None turns it off."""
+        from .symmetry import generator_axes
+        ops = [] if not sym or sym == "C1" else generator_axes(sym)
+        axes = np.ascontiguousarray([a for a, _ in ops] or [[0.0, 0.0, 1.0]], dtype=np.float64)
+        orders = np.ascontiguousarray([k for _, k in ops] or [1], dtype=np.int32)
+        _lib.check(_lib.load().bsg_recon_set_symmetrize(self._h, axes.ctypes.data_as(C.POINTER(C.c_double)),
+                                                        orders.ctypes.data_as(C.POINTER(C.c_int)), len(ops)),
+                   "bsg_recon_set_symmetrize")
 
     def set_tile_shape(self, shape: int):
         _lib.check(_lib.load().bsg_recon_set_tile_shape(self._h, shape), "bsg_recon_set_tile_shape")

@@ -52,6 +52,18 @@ def clean_label(sym: str) -> str:
 
 def generators(sym: str):
     """The (unit axis, order) operations of Bsymmetry for a point group."""
+    out = []
+    for ax, order in generator_axes(sym):
+        a = np.asarray(ax, dtype=np.float64)
+        out.append((a / np.linalg.norm(a), int(order)))
+    return out
+
+
+def generator_axes(sym: str):
+    """The (axis, order) operations of Bsymmetry for a point group, with the
+    axes as Bsymmetry::Bsymmetry writes them (bsoft/src/util/symmetry.cpp:
+    53-99), before its normalisation: the form bsg_recon_set_symmetrize
+    takes."""
     lbl = clean_label(sym)
     ops = []
     g = lbl[0]
@@ -93,11 +105,7 @@ def generators(sym: str):
             ops.append(((0, 0, 1), 2))
     else:
         raise ValueError(f"unsupported symmetry {sym!r}")
-    out = []
-    for ax, order in ops:
-        a = np.asarray(ax, dtype=np.float64)
-        out.append((a / np.linalg.norm(a), int(order)))
-    return out
+    return [(tuple(float(v) for v in ax), int(order)) for ax, order in ops]
 
 
 def _quat(axis, angle):

@@ -190,6 +190,19 @@ int  bsg_recon_set_tile_shape(bsg_recon* r, int shape);
  * each particle with matrix M(q) R for every operator, all copies from the
  * particle's one transform.  nops <= 1 restores C1. */
 int  bsg_recon_set_symmetry(bsg_recon* r, const double* ops, int nops);
+
+/* Point-group symmetry after reconstruction (breconstruct -symmetry with
+ * -mode 1): the particles are inserted once (C1), and bsg_recon_finish
+ * applies Bimage::symmetrize(sym, 1) (bsoft/src/img/Bimage_symmetry.cpp:
+ * 31-100, bsoft/src/breconstruct.cpp:335) to the real-space map before the
+ * sinc weight: for each generating operation, in order, the map becomes the
+ * sum of itself and its order - 1 rotations about the axis through the map
+ * centre (trilinear resampling as Bimage::interpolate does it, the map's
+ * background outside), then every value is divided by the group order.
+ * axes: nops axes (3 doubles each, as Bsymmetry defines them, e.g. 1,1,1
+ * for the 3-fold of T; normalised here as the reference normalises them),
+ * orders: nops orders 1..9, nops <= 8; nops = 0 turns it off. */
+int  bsg_recon_set_symmetrize(bsg_recon* r, const double* axes, const int* orders, int nops);
 int  bsg_recon_autotune(bsg_recon* r, const float* images, const double* params, long nparts,
                         int flags, double* ms_out, int* best_out);
 

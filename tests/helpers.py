@@ -71,6 +71,8 @@ def options_from_args(args: str) -> ReconOptions:
             opt.pad = int(val)
         elif "symmetry".startswith(t) and len(t) >= 3:
             opt.symmetry = val
+        elif t == "mode":
+            opt.sym_mode = int(val)
         i += 2 if val is not None else 1
     return opt
 

@@ -151,3 +151,17 @@ def test_verbose_statistics_match_reference(case, exe, tmp_path):
         for a, b in zip(g["rows"], w["rows"]):
             for c in range(1, 9):
                 assert close_to_printed(float(a[c]), b[c], 1e-3, 1.0), (k, a, b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["plain24_tri_d2_m1", "plain24_tri_i_m1"])
+def test_symmetry_mode1_matches_reference(case, exe, tmp_path):
+    """The drop-in with -symmetry X -mode 1 against the reference's map."""
+    z = np.load(os.path.join(GOLDEN, "mode1.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    out = os.path.join(str(tmp_path), "map.mrc")
+    r = subprocess.run([exe, *shlex.split(str(z[case + "__options"])), "-reconstruction", out, star],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    v, _ = mrc.read_volume(out)
+    assert rel_l2(v, z[case + "__map"]) <= 1e-5

@@ -285,3 +285,39 @@ def test_gpu_reconstruction_statistics_match_reference(case, suffixes, tmp_path)
                     assert close_to_printed(got[c], want[c]), (int(got[0]), c, got[c], want[c])
             assert close_to_printed(st["res_snr"], rep["res_snr"], 1e-3)
             assert close_to_printed(st["res_fsc"], rep["res_fsc"], 1e-3)
+
+
+MODE1_CASES = ["plain24_tri_d2_m1", "ctf16_tri_flip_c3_m1", "plain24_near_t_m1", "plain24_tri_i_m1"]
+
+
+@pytest.mark.parametrize("case", MODE1_CASES)
+def test_gpu_symmetry_after_reconstruction_matches_reference(case, tmp_path):
+    """breconstruct -symmetry X -mode 1 (tests/golden/mode1.npz): particles
+    inserted once, the finished map symmetrized in real space
+    (bsg_recon_set_symmetrize), then the sinc weight; against the reference's
+    map (rel L2 <= 1e-5, FSC >= 0.999).  The symmetrization itself equals the
+    FP64 oracle's restatement of Bimage::symmetrize applied to the GPU's own
+    unsymmetrized map, to the last bit in all but the voxels the background
+    fill reaches."""
+    from oracle.symmetrize_oracle import symmetrize
+    from tests.helpers import options_from_args
+    z = np.load(os.path.join(GOLDEN, "mode1.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    opt = options_from_args(str(z[case + "__options"]))
+    plan = plan_reconstruction(read_project(star), opt)
+    assert plan.sym_mode == 1
+    ref = z[case + "__map"]
+    with Reconstructor(plan) as rec:
+        rec.insert(load_images(plan), plan.params)
+        m = rec.finish()
+        assert rel_l2(m, ref) <= 1e-5
+        assert fsc(m, ref).min() >= 0.999
+        sym_nosinc = rec.finish(sinc=False)
+        rec.set_symmetrize(None)
+        plain = rec.finish(sinc=False)
+    N = plain.shape[0]
+    orc = symmetrize(plain, (N / 2, N / 2, N / 2), opt.symmetry)
+    same = np.mean(orc == sym_nosinc)
+    print(case, "bitwise equal voxels", same, "rel L2", rel_l2(sym_nosinc, orc))
+    assert rel_l2(sym_nosinc, orc) < 1e-7
+    assert same > 0.99
