@@ -101,6 +101,7 @@ def load():
         "bsg_recon_add_partial": ([vp, C.c_int, vp, vp, vp, vp, C.c_int], C.c_int),
         "bsg_recon_fsc": ([vp, C.c_int, dp], C.c_int),
         "bsg_recon_set_symmetrize": ([vp, dp, C.POINTER(C.c_int), C.c_int], C.c_int),
+        "bsg_recon_set_rescale": ([vp, C.c_double, C.c_double], C.c_int),
         "bsg_recon_statistics": ([vp, C.c_int, C.c_double, C.POINTER(ShellStats), dp, C.c_int], C.c_int),
         "bsg_particle_spectra": ([vp, vp, vp, C.c_long, vp, C.c_int], C.c_int),
         "bsg_recon_set_timing": ([vp, C.c_int], C.c_int),

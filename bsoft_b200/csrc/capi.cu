@@ -123,6 +123,10 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
     d.pw = (float)pw;
     d.half = (int)q[23];
     d.lat = pack_lattice(choose_lattice(d.ad, d.bd));
+    // particle_reconstruct's rescale_to_avg_std(0, 1) under -rescale
+    // (mg_reconstruct.cpp:155): v * scale + shift, scale 0 = none
+    d.na = q[24] != 0 ? q[24] : 1.0;
+    d.nb = q[24] != 0 ? q[25] : 0.0;
 }
 
 static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
@@ -530,21 +534,26 @@ int bsg_recon_finish(bsg_recon* h, int imap, float* map_out, float* fom_out, int
     const bool sinc = (flags & BSG_SINC) != 0;
     const bool dev = (flags & BSG_DEVICE_PTR) != 0;
     float* dst = dev ? map_out : r->d_map;
-    const bool symz = !r->symz_orders.empty();
+    const bool symz = !r->symz_orders.empty(), resc = r->rescale_std > 0;
     CK(launch_weigh(*r, imap, r->stream));
-    // with symmetrization after reconstruction (mode 1) the sinc weight
-    // follows it, as breconstruct applies filter_sinc to the written map
-    CK(launch_ifft3(*r, r->d_work, dst, sinc && !symz, r->stream));
+    // with symmetrization after reconstruction (mode 1) and rescaling, the
+    // sinc weight follows them, as breconstruct applies filter_sinc to the
+    // written map (breconstruct.cpp:332-346, 360)
+    CK(launch_ifft3(*r, r->d_work, dst, sinc && !symz && !resc, r->stream));
     r->stats.launches += 4;
     if (symz) {
         if (!r->d_symtmp) {
             int rc = alloc((void**)&r->d_symtmp, sizeof(float) * r->vol_elems());
             if (rc) return rc;
         }
-        CK(launch_symmetrize(*r, dst, r->d_symtmp, sinc, r->stream));
+        CK(launch_symmetrize(*r, dst, r->d_symtmp, sinc && !resc, r->stream));
         long ops = 0;
         for (int k : r->symz_orders) ops += k > 1;
         r->stats.launches += 2 + ops;
+    }
+    if (resc) {
+        CK(launch_rescale(*r, dst, r->rescale_avg, r->rescale_std, sinc, r->stream));
+        r->stats.launches += 2;
     }
     const size_t N3 = r->vol_elems();
     if (!dev) CK(cudaMemcpyAsync(map_out, r->d_map, sizeof(float) * N3, cudaMemcpyDeviceToHost, r->stream));
@@ -950,5 +959,13 @@ int bsg_recon_set_symmetrize(bsg_recon* h, const double* axes, const int* orders
             return fail(BSG_ERR_ARG, "bsg_recon_set_symmetrize: operation %d has order %d (1..9)", i, orders[i]);
     r->symz_axes.assign(axes, axes + 3 * nops);
     r->symz_orders.assign(orders, orders + nops);
+    return BSG_OK;
+}
+
+int bsg_recon_set_rescale(bsg_recon* h, double avg, double std) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r || !std::isfinite(avg) || !std::isfinite(std)) return fail(BSG_ERR_ARG, "bsg_recon_set_rescale: bad argument");
+    r->rescale_avg = avg;
+    r->rescale_std = std > 0 ? std : 0;
     return BSG_OK;
 }

@@ -33,6 +33,7 @@ struct alignas(16) DevParticle {
     double nrm[3];          // unit plane normal R[:,2]
     double inv2;            // (scale/(ft*pixel))^2: s2 per unit pixel^2
     double inv_st2;         // 1 / step^2: pixel coordinate per unit of ad.c
+    double na, nb;          // image normalisation v * na + nb (breconstruct -rescale; 1, 0 otherwise)
     float  ib[3];           // 1 / bf[i] (0 when |bf[i]| <= 1e-6)
     float  inv_step;        // 1 / step
     float  af[3], bf[3];    // float copies of ad / bd
@@ -76,5 +77,6 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, const DevPart
 cudaError_t launch_finish(const Context& c, int imap, float* map_out, float* fom_out, bool sinc, cudaStream_t s);
 cudaError_t launch_fsc(const Context& c, int nshell, double* out_dev, cudaStream_t s);
 cudaError_t launch_symmetrize(const Context& c, float* map, float* tmp, bool sinc, cudaStream_t s);
+cudaError_t launch_rescale(const Context& c, float* map, double nuavg, double nustd, bool sinc, cudaStream_t s);
 
 }  // namespace bsg

@@ -30,6 +30,7 @@ struct Context {
     std::vector<double> symz_axes;    // 3 per operation
     std::vector<int> symz_orders;
     float* d_symtmp = nullptr;        // N^3 float work map
+    double rescale_avg = 0, rescale_std = 0;   // -rescale (std > 0: on)
     double* d_bkg = nullptr;         // batch
     float2* d_phase = nullptr;       // batch x 2 x ft: exp(i h shx), exp(i k shy)
     float2* d_rows = nullptr;        // batch x n x (ft/2+1): row transforms

@@ -51,7 +51,7 @@ __global__ void background_kernel(const float* __restrict__ img, const DevPartic
         double x2, y2;
         if (pow2) { x2 = (x - P.bx) * ih; y2 = (y - P.by) * ih; }
         else { x2 = (x - P.bx) / h; y2 = (y - P.by) / h; }
-        if (x2 * x2 + y2 * y2 - 1 > 0) { sum += im[i]; ++cnt; }
+        if (x2 * x2 + y2 * y2 - 1 > 0) { sum += (float)(im[i] * P.na + P.nb); ++cnt; }
     }
     // deterministic block reduction (fixed tree)
     __shared__ double ssum[256];
@@ -85,7 +85,7 @@ constexpr int ROW_WARPS = 8;
 
 __global__ void __launch_bounds__(ROW_WARPS * 32)
 rows_kernel(const float* __restrict__ img, const double* __restrict__ bkg, const float2* __restrict__ tw,
-            int n, int ft, int logft, float2* __restrict__ rows) {
+            const DevParticle* __restrict__ part, int n, int ft, int logft, float2* __restrict__ rows) {
     extern __shared__ float2 smem[];
     float2* stw = smem;                          // ft/2 twiddles
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -100,9 +100,11 @@ rows_kernel(const float* __restrict__ img, const double* __restrict__ bkg, const
     const float fill = (float)bkg[b];
     const float* r0 = img + ((size_t)b * n + y0) * n;
     const float* r1 = r0 + n;
+    // the particle's normalisation (rescale_to_avg_std, stored as float)
+    const double na = part[b].na, nb = part[b].nb;
     for (int x = lane; x < ft; x += 32) {
-        float re = (x < n) ? r0[x] : fill;
-        float im = (y1 < n && x < n) ? r1[x] : fill;
+        float re = (x < n) ? (float)(r0[x] * na + nb) : fill;
+        float im = (y1 < n && x < n) ? (float)(r1[x] * na + nb) : fill;
         buf[swz(bitrev(x, logft))] = make_float2(re, im);
     }
     __syncwarp();
@@ -257,7 +259,7 @@ cudaError_t launch_rows(const Context& c, const float* img, int nimg, cudaStream
     const int npairs = (c.g.n + 1) / 2;
     dim3 grid((npairs + ROW_WARPS - 1) / ROW_WARPS, nimg);
     size_t smem = sizeof(float2) * ((size_t)c.g.ft / 2 + (size_t)ROW_WARPS * c.g.ft);
-    rows_kernel<<<grid, ROW_WARPS * 32, smem, s>>>(img, c.d_bkg, c.d_tw, c.g.n, c.g.ft, c.g.logft, c.d_rows);
+    rows_kernel<<<grid, ROW_WARPS * 32, smem, s>>>(img, c.d_bkg, c.d_tw, c.d_part, c.g.n, c.g.ft, c.g.logft, c.d_rows);
     return cudaGetLastError();
 }
 

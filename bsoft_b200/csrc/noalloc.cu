@@ -100,6 +100,8 @@ void to_dev_particle(const Geometry& g, const double* q, DevParticle& d) {
     d.fs = 1.0 / (g.ft * pixel);
     d.c00 = q[16]; d.c20 = q[17]; d.c22 = q[18]; d.c2m2 = q[19]; d.c40 = q[20]; d.c11 = q[21]; d.c1m1 = q[22];
     d.half = (int)q[23];
+    d.na = q[24] != 0 ? q[24] : 1.0;
+    d.nb = q[24] != 0 ? q[25] : 0.0;
 }
 
 }  // namespace

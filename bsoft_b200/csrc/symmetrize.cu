@@ -154,6 +154,51 @@ __global__ void scale_sinc_kernel(float* m, int N, double inv_order, int sinc) {
 
 constexpr int BG_BLOCKS = 148 * 4;
 
+// per-block sums of v and v^2 (Bimage::statistics of a real map)
+__global__ void moments_kernel(const float* m, long n, double* s1, double* s2) {
+    __shared__ double a[256], b[256];
+    double x = 0, y = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double v = m[i];
+        x = dadd(x, v);
+        y = dadd(y, dmul(v, v));
+    }
+    a[threadIdx.x] = x;
+    b[threadIdx.x] = y;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k; k >>= 1) {
+        if ((int)threadIdx.x < k) {
+            a[threadIdx.x] = dadd(a[threadIdx.x], a[threadIdx.x + k]);
+            b[threadIdx.x] = dadd(b[threadIdx.x], b[threadIdx.x + k]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        s1[blockIdx.x] = a[0];
+        s2[blockIdx.x] = b[0];
+    }
+}
+
+// Bimage::rescale (bsoft/src/img/Bimage_rescale.cpp:27-50): v scale + shift,
+// stored as float; then the sinc weight
+__global__ void rescale_sinc_kernel(float* m, int N, double scale, double shift, int sinc) {
+    const long NN = N, N3 = NN * NN * NN;
+    const double o = (double)(N / 2);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N3; i += (long)gridDim.x * blockDim.x) {
+        float v = (float)dadd(dmul((double)m[i], scale), shift);
+        if (sinc) {
+            const long xx = i % NN, yy = (i / NN) % NN, zz = i / (NN * NN);
+            const double dx = (xx - o) / N, dy = (yy - o) / N, dz = (zz - o) / N;
+            const double rr = 3.14159265358979323846 * sqrt(dx * dx + dy * dy + dz * dz);
+            if (rr != 0.0) {
+                const double w = rr / sin(rr);
+                v = (float)(w * w * v);
+            }
+        }
+        m[i] = v;
+    }
+}
+
 }  // namespace
 
 // Matrix3(axis, angle) of the reference: the axis normalised (as Bsymmetry
@@ -229,6 +274,35 @@ cudaError_t launch_symmetrize(const Context& c, float* map, float* tmp, bool sin
         if (e != cudaSuccess) return e;
     }
     scale_sinc_kernel<<<148 * 8, 256, 0, s>>>(map, N, order > 1 ? 1.0 / (double)order : 1.0, sinc ? 1 : 0);
+    return cudaGetLastError();
+}
+
+}  // namespace bsg
+
+namespace bsg {
+
+// Bimage::rescale_to_avg_std (bsoft/src/img/Bimage_rescale.cpp:163-182) of
+// the real map in place, from its average and standard deviation
+// (Bimage::statistics: sqrt(mean v^2 - mean^2)), then the sinc weight.
+cudaError_t launch_rescale(const Context& c, float* map, double nuavg, double nustd, bool sinc, cudaStream_t s) {
+    const int N = c.g.map;
+    const long N3 = (long)c.vol_elems();
+    double* d = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d, sizeof(double) * 2 * BG_BLOCKS, s);
+    if (e != cudaSuccess) return e;
+    moments_kernel<<<BG_BLOCKS, 256, 0, s>>>(map, N3, d, d + BG_BLOCKS);
+    std::vector<double> h(2 * BG_BLOCKS);
+    e = cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFreeAsync(d, s);
+    if (e != cudaSuccess) return e;
+    double s1 = 0, s2 = 0;
+    for (int i = 0; i < BG_BLOCKS; ++i) { s1 += h[i]; s2 += h[BG_BLOCKS + i]; }
+    const double avg = s1 / N3;
+    double sd = s2 / N3 - avg * avg;
+    sd = sd > 0 ? sqrt(sd) : 0.0;
+    const double scale = sd > 1e-30 ? nustd / sd : 1.0, shift = nuavg - avg * scale;
+    rescale_sinc_kernel<<<148 * 8, 256, 0, s>>>(map, N, scale, shift, sinc ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -45,6 +45,7 @@ struct Options {
     bool bootstrap = false, plan_only = false;
     int verbose = 0;
     int sym_mode = 0;               // -mode: 0 during reconstruction, 1 after it
+    double rescale_avg = 0, rescale_std = 0;   // -rescale avg,std (std > 0: on)
     std::string symmetry = "C1";
     std::string recons, fom;
     std::vector<std::string> inputs;
@@ -124,6 +125,23 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
             c.coefficients(r + 16);
             // round-robin partial maps; even maps form half 1 (mg_reconstruct.cpp:757-763, 283-290)
             r[23] = (double)(k % 2);
+            if (o.rescale_std > 0) {
+                // particle_reconstruct: rescale_to_avg_std(0, 1) with the
+                // statistics read_img attaches (mg_reconstruct.cpp:155)
+                double avg = h.mean(), sd = h.stddev();
+                if (sd < 1e-30) {
+                    std::vector<float> img((size_t)h.nx() * h.ny());
+                    read_stack_images(mg.particle_file, h, mg.part_id[i] - 1, 1, img.data());
+                    double s1 = 0, s2 = 0;
+                    for (float v : img) { s1 += v; s2 += (double)v * v; }
+                    avg = s1 / img.size();
+                    sd = s2 / img.size() - avg * avg;
+                    sd = sd > 0 ? std::sqrt(sd) : 0.0;
+                }
+                const double scale = sd > 1e-30 ? 1.0 / sd : 1.0;
+                r[24] = scale;
+                r[25] = 0.0 - avg * scale;
+            }
             p.rec.insert(p.rec.end(), r, r + BSG_PARTICLE_DOUBLES);
             p.src.push_back({(int)mi, mg.part_id[i] - 1});
             ++k;
@@ -179,6 +197,14 @@ Options parse(int argc, char** argv) {
         else if (a == "-device") o.device = atoi(val().c_str());
         else if (a == "-plan") o.plan_only = true;
         else if (a == "-verbose") o.verbose = atoi(val().c_str());
+        else if (a == "-rescale") {
+            const std::string v = val();
+            const size_t cpos = v.find(',');
+            if (cpos == std::string::npos) throw std::runtime_error("-rescale: both average and standard deviation must be given");
+            o.rescale_avg = atof(v.c_str());
+            o.rescale_std = atof(v.c_str() + cpos + 1);
+            if (!(o.rescale_std > 0)) throw std::runtime_error("-rescale: a positive standard deviation must be given");
+        }
         else if (a == "-mode") {
             o.sym_mode = atoi(val().c_str());
             if (o.sym_mode < 0 || o.sym_mode > 1)
@@ -239,6 +265,7 @@ int main(int argc, char** argv) {
         cfg.fom = (o.fom.empty() && !o.verbose) ? 0 : 1; cfg.batch = 0; cfg.device = o.device;
         bsg_recon* rec = nullptr;
         CALL(bsg_recon_create(&cfg, &rec));
+        if (o.rescale_std > 0) CALL(bsg_recon_set_rescale(rec, o.rescale_avg, o.rescale_std));
         if (o.sym_mode == 1) {
             // symmetry after reconstruction (mode 1): insert once, symmetrize
             // the finished map (Bimage::symmetrize, breconstruct.cpp:335)

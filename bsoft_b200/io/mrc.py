@@ -35,6 +35,8 @@ class MRCHeader:
     origin: tuple          # the header's origin field (angstrom)
     nsymbt: int
     nversion: int
+    dmean: float = 0.0     # header average and rms: the statistics read_img
+    rms: float = 0.0       # attaches to an image read from the file (rwMRC.cpp:181-184)
 
     @property
     def sampling(self):
@@ -59,6 +61,11 @@ class MRCHeader:
         """The origin of image i of the stack: the header's, for every image."""
         return self.image_origin
 
+    @property
+    def file_stats(self):
+        """(average, standard deviation) read_img attaches to an image of the file."""
+        return float(self.dmean), float(self.rms)
+
 
 def read_header(path: str) -> MRCHeader:
     with open(path, "rb") as f:
@@ -74,7 +81,9 @@ def read_header(path: str) -> MRCHeader:
     nsymbt = struct.unpack("<i", raw[92:96])[0]
     nversion = struct.unpack("<i", raw[108:112])[0]
     origin = struct.unpack("<3f", raw[196:208])
-    return MRCHeader(nx, ny, nz, mode, mx, my, mz, cell, origin, nsymbt, nversion)
+    dmean = struct.unpack("<f", raw[84:88])[0]
+    rms = struct.unpack("<f", raw[216:220])[0]
+    return MRCHeader(nx, ny, nz, mode, mx, my, mz, cell, origin, nsymbt, nversion, dmean, rms)
 
 
 def read_stack(path: str, first: int = 0, count: int | None = None) -> tuple[np.ndarray, MRCHeader]:

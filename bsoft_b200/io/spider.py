@@ -61,6 +61,11 @@ class SpiderHeader:
             return self.labbyt + i * self.image_bytes + self.labbyt
         return self.labbyt
 
+    @property
+    def file_stats(self):
+        """(average, standard deviation) read_img attaches (the global header's)."""
+        return float(self.av), float(self.sig)
+
     def image_origin_of(self, i: int):
         return tuple(float(v) for v in self.origins[min(i, len(self.origins) - 1)])
 

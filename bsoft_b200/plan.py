@@ -30,6 +30,7 @@ CTF_ACTIONS = {"none": 0, "flip": 1, "apply": 2, "correct": 3, "wiener": 4}
 # bsg_particle): 32 doubles per particle
 PARTICLE_DOUBLES = 32
 P_ORIGIN, P_BKG, P_MAT, P_PIXEL, P_SCALE, P_WEIGHT, P_CTF, P_MAP = 0, 2, 4, 13, 14, 15, 16, 23
+P_NORM = 24       # image normalisation scale, shift (breconstruct -rescale); scale 0 = none
 
 
 def find_next_power_of(n: int, base: int = 2) -> int:
@@ -80,6 +81,7 @@ class ReconOptions:
     threads: int = 2              # reference partial maps (only sets half-map parity)
     symmetry: str = ""            # point group (-symmetry; "" = C1)
     sym_mode: int = 0             # -mode: 0 during reconstruction, 1 after it (real space)
+    rescale: tuple = ()           # -rescale (average, standard deviation) of the finished map
 
 
 @dataclass
@@ -98,6 +100,7 @@ class ReconPlan:
     symmetry: str = "C1"          # point group inserted during reconstruction (mode 0)
     resolution: float = 0.0       # breconstruct's limit before any check (the statistics' limit)
     sym_mode: int = 0             # 0: symmetry inserted; 1: the finished map symmetrized
+    rescale: tuple = ()           # (average, standard deviation) of the finished map, or ()
 
 
 def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
@@ -158,6 +161,18 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
             r[P_CTF:P_CTF + 7] = c.coefficients()
             # round-robin partial maps; even maps form half 1 (mg_reconstruct.cpp:757-763, 283-290)
             r[P_MAP] = k % 2
+            if opt.rescale:
+                # particle_reconstruct: rescale_to_avg_std(0, 1) with the
+                # statistics read_img attaches (mg_reconstruct.cpp:155)
+                avg, sd = h.file_stats
+                if sd < 1e-30:
+                    img = stacks.read_stack(path, int(mg.part_id[i]) - 1, 1)[0][0].astype(np.float64)
+                    avg = img.sum() / img.size
+                    sd = (img * img).sum() / img.size - avg * avg
+                    sd = math.sqrt(sd) if sd > 0 else 0.0
+                scale = 1.0 / sd if sd > 1e-30 else 1.0
+                r[P_NORM] = scale
+                r[P_NORM + 1] = 0.0 - avg * scale
             rows.append(r)
             index.append((path, int(mg.part_id[i]) - 1))
             k += 1
@@ -165,7 +180,7 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
                      interp=opt.interp, ctf_action=opt.ctf_action, wiener=wiener,
                      params=np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES),
                      stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1", resolution=resolution,
-                     sym_mode=opt.sym_mode)
+                     sym_mode=opt.sym_mode, rescale=tuple(opt.rescale))
 
 
 def load_images(plan: ReconPlan, sel=None) -> np.ndarray:

@@ -48,6 +48,8 @@ class Reconstructor:
                 self.set_symmetrize(sym)
             else:
                 self.set_symmetry(sym)
+        if getattr(plan, "rescale", None):
+            self.set_rescale(*plan.rescale)
         self.fom = fom
 
     # context management
@@ -203,6 +205,10 @@ class Reconstructor:
         _lib.check(_lib.load().bsg_recon_set_symmetrize(self._h, axes.ctypes.data_as(C.POINTER(C.c_double)),
                                                         orders.ctypes.data_as(C.POINTER(C.c_int)), len(ops)),
                    "bsg_recon_set_symmetrize")
+
+    def set_rescale(self, avg: float = 0.0, std: float = 0.0):
+        """breconstruct -rescale avg,std of the finished map (std <= 0: off)."""
+        _lib.check(_lib.load().bsg_recon_set_rescale(self._h, float(avg), float(std)), "bsg_recon_set_rescale")
 
     def set_tile_shape(self, shape: int):
         _lib.check(_lib.load().bsg_recon_set_tile_shape(self._h, shape), "bsg_recon_set_tile_shape")

@@ -61,6 +61,10 @@ extern "C" {
  *   [15]    particle weight (1, or selection number when bootstrapping)
  *   [16..22] CTF: abw00 abw20 abw22 abw2m2 abw40 abw11 abw1m1 (ctf.h:321-351)
  *   [23]    half-map index (0 or 1)
+ *   [24..25] image normalisation: every pixel becomes v * [24] + [25]
+ *            (float) before the background and padding, as
+ *            rescale_to_avg_std(0, 1) under breconstruct -rescale
+ *            (mg_reconstruct.cpp:155); [24] = 0: none
  */
 #define BSG_PARTICLE_DOUBLES 32
 
@@ -203,6 +207,13 @@ int  bsg_recon_set_symmetry(bsg_recon* r, const double* ops, int nops);
  * for the 3-fold of T; normalised here as the reference normalises them),
  * orders: nops orders 1..9, nops <= 8; nops = 0 turns it off. */
 int  bsg_recon_set_symmetrize(bsg_recon* r, const double* axes, const int* orders, int nops);
+
+/* breconstruct -rescale avg,std: bsg_recon_finish rescales the real-space
+ * map (after the inverse transform and any symmetrization, before the sinc
+ * weight) to the given average and standard deviation from its own
+ * (Bimage::rescale_to_avg_std, bsoft/src/img/Bimage_rescale.cpp:163-182;
+ * bsoft/src/breconstruct.cpp:336).  std <= 0 turns it off. */
+int  bsg_recon_set_rescale(bsg_recon* r, double avg, double std);
 int  bsg_recon_autotune(bsg_recon* r, const float* images, const double* params, long nparts,
                         int flags, double* ms_out, int* best_out);
 

@@ -1,7 +1,8 @@
 """Golden maps of breconstruct with symmetry after reconstruction
 (-symmetry X -mode 1: particles inserted once, the finished real-space map
-symmetrized by Bimage::symmetrize, bsoft/src/breconstruct.cpp:335), from the
-reference compiled from its sources, on the golden datasets.  mode1.npz
+symmetrized by Bimage::symmetrize, bsoft/src/breconstruct.cpp:335) and with
+-rescale, from the reference compiled from its sources, on the golden
+datasets.  mode1.npz
 keeps, per case, the dataset name, the options and the map.
 
     python tests/golden/make_mode1_golden.py
@@ -29,6 +30,9 @@ CASES = [
     ("ctf16_tri_flip_c3_m1", "ctf16", "-interp trilinear -CTF flip -symmetry C3 -mode 1"),
     ("plain24_near_t_m1", "plain24", "-interp nearest -symmetry T -mode 1"),
     ("plain24_tri_i_m1", "plain24", "-interp trilinear -symmetry I -mode 1"),
+    # -rescale avg,std of the finished map (Bimage::rescale_to_avg_std, breconstruct.cpp:336)
+    ("ctf16_tri_flip_rs", "ctf16", "-interp trilinear -CTF flip -rescale 0.5,2.0"),
+    ("plain24_tri_d2_m1_rs", "plain24", "-interp trilinear -symmetry D2 -mode 1 -rescale -0.1,5.2"),
 ]
 
 if __name__ == "__main__":

@@ -58,6 +58,8 @@ def options_from_args(args: str) -> ReconOptions:
     while i < len(toks):
         t = toks[i].lstrip("-")
         val = toks[i + 1] if i + 1 < len(toks) and not toks[i + 1].startswith("-") else None
+        if t == "rescale" and i + 1 < len(toks):        # its average may be negative
+            val = toks[i + 1]
         if "interpolation".startswith(t):
             opt.interp = INTERP[{"n": "nearest", "w": "weighted", "t": "trilinear"}[val[0]]]
         elif t == "CTF":
@@ -73,6 +75,9 @@ def options_from_args(args: str) -> ReconOptions:
             opt.symmetry = val
         elif t == "mode":
             opt.sym_mode = int(val)
+        elif t == "rescale":
+            a, b = (float(x) for x in val.split(","))
+            opt.rescale = (a, b)
         i += 2 if val is not None else 1
     return opt
 

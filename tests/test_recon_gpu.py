@@ -321,3 +321,22 @@ def test_gpu_symmetry_after_reconstruction_matches_reference(case, tmp_path):
     print(case, "bitwise equal voxels", same, "rel L2", rel_l2(sym_nosinc, orc))
     assert rel_l2(sym_nosinc, orc) < 1e-7
     assert same > 0.99
+
+
+@pytest.mark.parametrize("case", ["ctf16_tri_flip_rs", "plain24_tri_d2_m1_rs"])
+def test_gpu_rescale_matches_reference(case, tmp_path):
+    """breconstruct -rescale avg,std (tests/golden/mode1.npz): every particle
+    normalised with the statistics read_img attaches before its transform,
+    and the finished real map rescaled (after any -mode 1 symmetrization,
+    before the sinc weight)."""
+    from tests.helpers import options_from_args
+    z = np.load(os.path.join(GOLDEN, "mode1.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    plan = plan_reconstruction(read_project(star), options_from_args(str(z[case + "__options"])))
+    assert plan.rescale and np.all(plan.params[:, 24] > 0)
+    ref = z[case + "__map"]
+    with Reconstructor(plan) as rec:
+        rec.insert(load_images(plan), plan.params)
+        m = rec.finish()
+    assert rel_l2(m, ref) <= 1e-5
+    assert fsc(m, ref).min() >= 0.999
