@@ -61,6 +61,7 @@ struct Recon : Context {
     std::vector<Timed> timed;
     bool broken = false;
     long seq = 0;                    // batches issued over the context's life (staging buffer = seq & 1)
+    long nexp = 0;                   // expanded gridding records of the current batch (0: none)
 };
 
 static bool is_pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
@@ -90,7 +91,8 @@ static void host_twiddles(int L, std::vector<float2>& out) {
 }
 
 // 32-double C-ABI record -> device record (see bsgpu.h for the layout)
-static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
+// ewh: the Ewald surface's +-lambda/2 for this record (0: the plane)
+static void make_dev_particle(const Recon& r, const double* q, DevParticle& d, double ewh = 0.0) {
     const Geometry& g = r.g;
     memset(&d, 0, sizeof(d));
     d.shx = q[0] / g.ft * 2.0 * M_PI;                 // Bimage_complex.cpp:510 shift = origin/size*2pi
@@ -108,6 +110,8 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
         d.af[i] = (float)d.ad[i];
         d.bf[i] = (float)d.bd[i];
     }
+    for (int i = 0; i < 3; ++i) d.cd[i] = R[3 * i + 2] * g.mscale;
+    d.inv = inv;
     double nn = sqrt(R[2] * R[2] + R[5] * R[5] + R[8] * R[8]);
     if (nn <= 0) nn = 1;
     d.nrm[0] = R[2] / nn; d.nrm[1] = R[5] / nn; d.nrm[2] = R[8] / nn;
@@ -122,7 +126,13 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d) {
     if (pad_ratio > 1) { pad_ratio *= pad_ratio * 0.6; pw /= pad_ratio; }
     d.pw = (float)pw;
     d.half = (int)q[23];
-    d.lat = pack_lattice(choose_lattice(d.ad, d.bd));
+    // the curvature bound ewh inv2 mscale |p + q| <= ewh inv2 mscale ft sqrt(2)
+    // per pixel step of a lattice vector, and the surface's largest offset
+    d.ewh = ewh;
+    const double hf = g.ft / 2.0;
+    d.ezmax = (float)(fabs(d.ewh) * 2.0 * hf * hf * d.inv2 * g.mscale * 1.0001);
+    const double curve = fabs(d.ewh) * d.inv2 * g.mscale * g.ft * 1.4142135623730951 * 1.0001;
+    d.lat = pack_lattice(choose_lattice(d.ad, d.bd, 16, curve));
     // particle_reconstruct's rescale_to_avg_std(0, 1) under -rescale
     // (mg_reconstruct.cpp:155): v * scale + shift, scale 0 = none
     d.na = q[24] != 0 ? q[24] : 1.0;
@@ -233,8 +243,7 @@ static int run_batch_kernels(Recon* r, int buf, const float* d_img, long np, boo
     if (!insert) return BSG_OK;
     for (int h = 0; h < r->nhalves; ++h) {
         if (r->timing) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
-        const long nsym = std::max(1L, (long)r->sym.size() / 9);
-        if (nsym > 1) CK(launch_insert(*r, spec_out, r->d_psym, (int)(np * nsym), r->nhalves == 2 ? h : -1, s));
+        if (r->nexp > 0) CK(launch_insert(*r, spec_out, r->d_psym, (int)r->nexp, r->nhalves == 2 ? h : -1, s));
         else CK(launch_insert(*r, spec_out, r->d_part, (int)np, r->nhalves == 2 ? h : -1, s));
         if (r->timing) { cudaEventRecord(b, s); r->timed.push_back({a, b, 0}); }
         r->stats.launches += r->replicas > 1 ? 2 : 1;     // gridding (+ replica combine)
@@ -256,12 +265,16 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
     r->d_part = r->d_partbuf[buf];
     CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->fft_stream));
-    const long nsym = (long)r->sym.size() / 9;
-    if (nsym > 1) {
+    const long nsym = std::max(1L, (long)r->sym.size() / 9);
+    bool ewald = false;
+    for (long i = 0; i < np && !ewald; ++i) ewald = params[i * BSG_PARTICLE_DOUBLES + 26] != 0;
+    r->nexp = 0;
+    r->g.ewald = ewald ? 1 : 0;
+    if (nsym > 1 || ewald) {
         // one gridding record per (particle, operator): matrix S R, the
         // particle's spectrum (fspace_pack_2D(p, View, sym, ...),
         // Bimage_reconstruct.cpp:248-266)
-        const size_t need = (size_t)np * nsym;
+        const size_t need = (size_t)np * nsym * (ewald ? 2 : 1);
         if (need > r->psymbuf_cap[buf]) {
             if (r->d_psymbuf[buf]) cudaFree(r->d_psymbuf[buf]);
             r->d_psymbuf[buf] = nullptr;
@@ -274,21 +287,31 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
         // and the device buffer is rewritten in stream order
         r->h_psym.resize(need);
         double q[BSG_PARTICLE_DOUBLES];
+        size_t k = 0;
         for (long i = 0; i < np; ++i) {
             const double* p0 = params + i * BSG_PARTICLE_DOUBLES;
+            // Ewald sphere (fspace_pack_2D with ewald_wavelength = lambda,
+            // Bimage_reconstruct.cpp:157-168): both surfaces s_z = +-(lambda/2) s^2
+            const double lam = p0[26];
+            const int nsurf = lam != 0 ? 2 : 1;
             for (long s = 0; s < nsym; ++s) {
                 memcpy(q, p0, sizeof(q));
-                const double* S = &r->sym[9 * s];
-                for (int a = 0; a < 3; ++a)
-                    for (int b = 0; b < 3; ++b)
-                        q[4 + 3 * a + b] = S[3 * a + 0] * p0[4 + 0 * 3 + b] + S[3 * a + 1] * p0[4 + 1 * 3 + b] +
-                                           S[3 * a + 2] * p0[4 + 2 * 3 + b];
-                DevParticle& d = r->h_psym[i * nsym + s];
-                make_dev_particle(*r, q, d);
-                d.spec = (int)i;
+                if (nsym > 1) {
+                    const double* S = &r->sym[9 * s];
+                    for (int a = 0; a < 3; ++a)
+                        for (int b = 0; b < 3; ++b)
+                            q[4 + 3 * a + b] = S[3 * a + 0] * p0[4 + 0 * 3 + b] + S[3 * a + 1] * p0[4 + 1 * 3 + b] +
+                                               S[3 * a + 2] * p0[4 + 2 * 3 + b];
+                }
+                for (int t = 0; t < nsurf; ++t) {
+                    DevParticle& d = r->h_psym[k++];
+                    make_dev_particle(*r, q, d, nsurf == 2 ? (t == 0 ? lam / 2 : -(lam / 2)) : 0.0);
+                    d.spec = (int)i;
+                }
             }
         }
-        CK(cudaMemcpyAsync(r->d_psym, r->h_psym.data(), sizeof(DevParticle) * need, cudaMemcpyHostToDevice,
+        r->nexp = (long)k;
+        CK(cudaMemcpyAsync(r->d_psym, r->h_psym.data(), sizeof(DevParticle) * k, cudaMemcpyHostToDevice,
                            r->fft_stream));
     }
     return BSG_OK;

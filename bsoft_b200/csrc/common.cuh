@@ -34,6 +34,12 @@ struct alignas(16) DevParticle {
     double inv2;            // (scale/(ft*pixel))^2: s2 per unit pixel^2
     double inv_st2;         // 1 / step^2: pixel coordinate per unit of ad.c
     double na, nb;          // image normalisation v * na + nb (breconstruct -rescale; 1, 0 otherwise)
+    // Ewald-sphere surface (breconstruct -ewald; Bimage_reconstruct.cpp:157-168):
+    // m += ewh s2 cd with s2 = (h^2 + k^2) inv2, one record per surface
+    double ewh;             // +-lambda/2 (0: the plane)
+    double inv;             // sqrt(inv2): s per unit pixel
+    double cd[3];           // R[:,2] * mscale
+    float  ezmax;           // max |ewh s2| mscale over the pixels (voxels)
     float  ib[3];           // 1 / bf[i] (0 when |bf[i]| <= 1e-6)
     float  inv_step;        // 1 / step
     float  af[3], bf[3];    // float copies of ad / bd
@@ -58,6 +64,7 @@ struct Geometry {
     float  rmax;            // max |m| reachable by any pixel (voxels) + 1
     int    fom;
     int    gate;           // 1: some pixel may fall outside the s^2 window or in the taper
+    int    ewald;          // 1: the batch's records include Ewald-sphere surfaces
 };
 
 __host__ __device__ inline int ilog2i(int v) { int l = 0; while ((1 << l) < v) ++l; return l; }

@@ -70,11 +70,12 @@ __device__ __forceinline__ unsigned tile_mask(const DevParticle& P, int x0, int 
     unsigned mask = 0;
     const float ex = 0.5f * (TX - 1), ey = 0.5f * (TY - 1), ez = 0.5f * (TZ - 1);
     const float hf = 0.5f * ft;
-    const float rx = hf * (fabsf(P.af[0]) + fabsf(P.bf[0])) + 1.0f;
-    const float ry = hf * (fabsf(P.af[1]) + fabsf(P.bf[1])) + 1.0f;
-    const float rz = hf * (fabsf(P.af[2]) + fabsf(P.bf[2])) + 1.0f;
+    // (an Ewald surface deviates from the plane by up to P.ezmax voxels)
+    const float rx = hf * (fabsf(P.af[0]) + fabsf(P.bf[0])) + 1.0f + P.ezmax;
+    const float ry = hf * (fabsf(P.af[1]) + fabsf(P.bf[1])) + 1.0f + P.ezmax;
+    const float rz = hf * (fabsf(P.af[2]) + fabsf(P.bf[2])) + 1.0f + P.ezmax;
     const float n0 = (float)P.nrm[0], n1 = (float)P.nrm[1], n2 = (float)P.nrm[2];
-    const float slack = P.slab + fabsf(n0) * ex + fabsf(n1) * ey + fabsf(n2) * ez + 1e-3f;
+    const float slack = P.slab + fabsf(n0) * ex + fabsf(n1) * ey + fabsf(n2) * ez + 1e-3f + P.ezmax;
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
         const float cx = x0 - ((a & 1) ? N : 0) + ex;
@@ -141,9 +142,16 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
     }
     // map frequency relative to the tile origin, in double as the reference
     // forms it
-    const double mx = h * P.ad[0] + k * P.bd[0] - ox;
-    const double my = h * P.ad[1] + k * P.bd[1] - oy;
-    const double mz = h * P.ad[2] + k * P.bd[2] - oz;
+    double mx = h * P.ad[0] + k * P.bd[0] - ox;
+    double my = h * P.ad[1] + k * P.bd[1] - oy;
+    double mz = h * P.ad[2] + k * P.bd[2] - oz;
+    if (P.ewh != 0.0) {
+        // Ewald surface: s_z = +-(lambda/2) s2 along R[:,2] (Bimage_reconstruct.cpp:157-168)
+        const double sx = h * P.inv, sy = k * P.inv, sz = P.ewh * (sx * sx + sy * sy);
+        mx += sz * P.cd[0];
+        my += sz * P.cd[1];
+        mz += sz * P.cd[2];
+    }
     const float2 f = act ? __ldg(S + (size_t)(k + hf) * a.pitch + (h + hf)) : make_float2(0.f, 0.f);
     if (a.interp != 2) {
         const double fx = floor(mx + 0.5), fy = floor(my + 0.5), fz = floor(mz + 0.5);
@@ -186,9 +194,11 @@ __device__ __forceinline__ void pixel(const InsertArgs& a, const DevParticle& P,
 template <int TX, int TY, int TZ, class Pix>
 __device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
                                           int* s_row, Pix&& pix) {
-    // open box of map frequencies whose tent touches the tile
-    const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
-    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
+    // open box of map frequencies whose tent touches the tile (an Ewald
+    // surface adds up to P.ezmax voxels to every coordinate)
+    const double e = P.ezmax;
+    const double lo[3] = {ox - 1.0 - e, oy - 1.0 - e, oz - 1.0 - e};
+    const double hi[3] = {ox + TX + e, oy + TY + e, oz + TZ + e};
     double vc = 0, hv = 0, uc = 0, hu = 0;
     for (int i = 0; i < 3; ++i) {
         const double c = 0.5 * (lo[i] + hi[i]), e = 0.5 * (hi[i] - lo[i]);
@@ -295,8 +305,9 @@ __device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double o
 template <int TX, int TY, int TZ, class Pix>
 __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
                                             int* s_row, Pix&& pix) {
-    const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
-    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
+    const double e = P.ezmax;
+    const double lo[3] = {ox - 1.0 - e, oy - 1.0 - e, oz - 1.0 - e};
+    const double hi[3] = {ox + TX + e, oy + TY + e, oz + TZ + e};
     double vc = 0, hv = 0, uc = 0, hu = 0;
     for (int i = 0; i < 3; ++i) {
         const double c = 0.5 * (lo[i] + hi[i]), e = 0.5 * (hi[i] - lo[i]);
@@ -514,7 +525,7 @@ __device__ __forceinline__ void cell_add(unsigned addr, float2 f, float w) {
     asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" :: "r"(addr), "f"(x), "f"(y), "f"(z), "f"(u) : "memory");
 }
 
-template <bool GATE, int TX, int TY, int TZ, int PX, int PP>
+template <bool GATE, bool EW, int TX, int TY, int TZ, int PX, int PP>
 __device__ __forceinline__ void pixel4(const InsertArgs& a, const DevParticle& P, const float2* S, float4* cell,
                                        unsigned cell0,
                                        float bx, float by, float bz, int hc, int kc, int h, int k, bool act) {
@@ -527,9 +538,18 @@ __device__ __forceinline__ void pixel4(const InsertArgs& a, const DevParticle& P
         wt *= tw;
     }
     const float dh = (float)(h - hc), dk = (float)(k - kc);
-    const float mx = fmaf(dh, P.af[0], fmaf(dk, P.bf[0], bx));
-    const float my = fmaf(dh, P.af[1], fmaf(dk, P.bf[1], by));
-    const float mz = fmaf(dh, P.af[2], fmaf(dk, P.bf[2], bz));
+    float mx = fmaf(dh, P.af[0], fmaf(dk, P.bf[0], bx));
+    float my = fmaf(dh, P.af[1], fmaf(dk, P.bf[1], by));
+    float mz = fmaf(dh, P.af[2], fmaf(dk, P.bf[2], bz));
+    if (EW && P.ewh != 0.0) {
+        // Ewald surface: s_z = +-(lambda/2) s2 along R[:,2] (Bimage_reconstruct.cpp:
+        // 157-168), at most P.ezmax voxels, added in FP32 to the tile-relative
+        // coordinate (the lattice keeps a margin for its variation)
+        const double sx = h * P.inv, sy = k * P.inv, sz = P.ewh * (sx * sx + sy * sy);
+        mx += (float)(sz * P.cd[0]);
+        my += (float)(sz * P.cd[1]);
+        mz += (float)(sz * P.cd[2]);
+    }
     const float2 f = act ? __ldg(S + (size_t)(k + hf) * a.pitch + (h + hf)) : make_float2(0.f, 0.f);
     if (a.interp != 2) {
         const float fx = floorf(mx + 0.5f), fy = floorf(my + 0.5f), fz = floorf(mz + 0.5f);
@@ -569,7 +589,7 @@ __device__ __forceinline__ void pixel4(const InsertArgs& a, const DevParticle& P
     }
 }
 
-template <bool GATE, int TX, int TY, int TZ, int PX, int PP, int NW>
+template <bool GATE, bool EW, int TX, int TY, int TZ, int PX, int PP, int NW>
 __global__ void __launch_bounds__(NW * 32) grid4_kernel(InsertArgs a) {
     constexpr int SLOTS = PP * TZ;
     constexpr int TV = TX * TY * TZ;
@@ -617,7 +637,7 @@ __global__ void __launch_bounds__(NW * 32) grid4_kernel(InsertArgs a) {
                 const float by = (float)(hc * P.ad[1] + kc * P.bd[1] - oy);
                 const float bz = (float)(hc * P.ad[2] + kc * P.bd[2] - oz);
                 walk_groups<TX, TY, TZ>(P, hf, ox, oy, oz, lane, s_rows[warp], [&](int h, int k, bool act) {
-                    pixel4<GATE, TX, TY, TZ, PX, PP>(a, P, S, cell, cell0, bx, by, bz, hc, kc, h, k, act);
+                    pixel4<GATE, EW, TX, TY, TZ, PX, PP>(a, P, S, cell, cell0, bx, by, bz, hc, kc, h, k, act);
                 });
             }
         }
@@ -691,8 +711,10 @@ template <int TX, int TY, int TZ, int PX, int PP, int NW>
 static cudaError_t set_smem_shape4() {
     const int smem = (int)(NW * PP * TZ * sizeof(float4));
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(grid4_kernel<true, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
-    return cudaFuncSetAttribute(grid4_kernel<false, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if ((e = cudaFuncSetAttribute(grid4_kernel<true, false, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(grid4_kernel<false, false, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(grid4_kernel<true, true, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(grid4_kernel<false, true, TX, TY, TZ, PX, PP, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
 cudaError_t prepare_insert_attributes() {
@@ -745,8 +767,13 @@ static cudaError_t launch_shape4(const InsertArgs& a0, const Context& c, cudaStr
     const int ntiles = a.ntx * a.nty * a.ntz;
     const unsigned blocks = (unsigned)(((long)ntiles * a.R + NW - 1) / NW);
     const size_t smem = (size_t)NW * PP * TZ * sizeof(float4);
-    if (c.g.gate) grid4_kernel<true, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
-    else grid4_kernel<false, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+    if (c.g.ewald) {
+        if (c.g.gate) grid4_kernel<true, true, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+        else grid4_kernel<false, true, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+    } else {
+        if (c.g.gate) grid4_kernel<true, false, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+        else grid4_kernel<false, false, TX, TY, TZ, PX, PP, NW><<<blocks, NW * 32, smem, s>>>(a);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || a.R == 1) return e;
     combine_kernel<false><<<148 * 8, 256, 0, s>>>(a);

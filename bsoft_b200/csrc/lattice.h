@@ -33,7 +33,7 @@ struct PhaseLattice {
 // Length (in pixel steps) beyond which a pixel-step vector cannot fail:
 // sqrt(3) / (smallest singular value of [ad bd]), since max_c |d_c| >=
 // |d| / sqrt(3).  Infinite when ad, bd are degenerate.
-inline double lattice_reach(const double ad[3], const double bd[3]) {
+inline double lattice_reach(const double ad[3], const double bd[3], double curve = 0.0) {
     double aa = 0, ab = 0, bb = 0;
     for (int c = 0; c < 3; ++c) {
         aa += ad[c] * ad[c];
@@ -44,13 +44,18 @@ inline double lattice_reach(const double ad[3], const double bd[3]) {
     const double disc = std::sqrt(std::max(0.0, tr * tr - 4.0 * det));
     const double smin2 = 0.5 * (tr - disc);
     if (!(smin2 > 0)) return HUGE_VAL;
-    return std::sqrt(3.0 / smin2) * (1.0 + 1e-9) + 1e-9;
+    // a curved surface (Ewald sphere) moves two points |v| pixel steps apart
+    // by at most curve |v| voxels more: |d| >= |v| (sigma_min - curve)
+    const double smin = std::sqrt(smin2) - curve;
+    if (!(smin > 0)) return HUGE_VAL;
+    return std::sqrt(3.0) / smin * (1.0 + 1e-9) + 1e-9;
 }
 
 // True when no nonzero vector of the lattice {(lh i + sh j, lk j)} maps to a
 // displacement with all three |d_c| < 1 + margin.  Only vectors shorter than
 // `reach` pixel steps need checking, and of each pair +-v only one.
-inline bool lattice_ok(const double ad[3], const double bd[3], int lh, int lk, int sh, double reach) {
+inline bool lattice_ok(const double ad[3], const double bd[3], int lh, int lk, int sh, double reach,
+                       double curve = 0.0) {
     const double margin = 2e-5;
     const int jmax = (int)std::floor(reach / lk);
     for (int j = 0; j <= jmax; ++j) {
@@ -62,7 +67,7 @@ inline bool lattice_ok(const double ad[3], const double bd[3], int lh, int lk, i
             if (dh * dh + dk * dk > reach * reach) continue;
             double m = 0;
             for (int c = 0; c < 3; ++c) m = std::max(m, std::fabs(dh * ad[c] + dk * bd[c]));
-            if (m < 1.0 + margin) return false;
+            if (m < 1.0 + margin + curve * std::sqrt(dh * dh + dk * dk)) return false;
         }
     }
     return true;
@@ -72,15 +77,17 @@ inline bool lattice_ok(const double ad[3], const double bd[3], int lh, int lk, i
 // rows lk first, then the smallest shift), else the square lattice of side
 // ceil(reach), which no vector shorter than `reach` belongs to; {0, 0, 0}
 // when that side would not fit the 12-bit fields of pack_lattice.
-inline PhaseLattice choose_lattice(const double ad[3], const double bd[3], int max_phases = 16) {
-    const double reach = lattice_reach(ad, bd);
+// curve: bound on the extra displacement (voxels per pixel step of the
+// lattice vector) of a curved insertion surface; 0 for the plane.
+inline PhaseLattice choose_lattice(const double ad[3], const double bd[3], int max_phases = 16, double curve = 0.0) {
+    const double reach = lattice_reach(ad, bd, curve);
     if (reach < 64.0) {
         for (int d = 1; d <= max_phases; ++d)
             for (int lk = 1; lk <= d; ++lk) {
                 if (d % lk) continue;
                 const int lh = d / lk;
                 for (int sh = 0; sh < lh; ++sh)
-                    if (lattice_ok(ad, bd, lh, lk, sh, reach)) return {lh, lk, sh};
+                    if (lattice_ok(ad, bd, lh, lk, sh, reach, curve)) return {lh, lk, sh};
             }
     }
     if (!(reach < 4095.0)) return {0, 0, 0};

@@ -46,6 +46,7 @@ struct Options {
     int verbose = 0;
     int sym_mode = 0;               // -mode: 0 during reconstruction, 1 after it
     double rescale_avg = 0, rescale_std = 0;   // -rescale avg,std (std > 0: on)
+    bool ewald = false;             // -ewald: Ewald-sphere insertion
     std::string symmetry = "C1";
     std::string recons, fom;
     std::vector<std::string> inputs;
@@ -125,6 +126,8 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
             c.coefficients(r + 16);
             // round-robin partial maps; even maps form half 1 (mg_reconstruct.cpp:757-763, 283-290)
             r[23] = (double)(k % 2);
+            // particle_reconstruct: ew_wl = em_ctf.lambda() (mg_reconstruct.cpp:209-210)
+            if (o.ewald) r[26] = c.lambda();
             if (o.rescale_std > 0) {
                 // particle_reconstruct: rescale_to_avg_std(0, 1) with the
                 // statistics read_img attaches (mg_reconstruct.cpp:155)
@@ -155,7 +158,8 @@ void usage() {
             "Usage: breconstruct [options] input.star\n"
             "  -interpolation nearest|weighted|trilinear  -pad 2  -CTF none|flip|apply|correct|wiener\n"
             "  -wiener 0.2  -resolution 4  -size 64  -sampling 1.5  -scale 1  -fullmap  -halfmaps\n"
-            "  -bootstrap  -reconstruction out.mrc  -fom fom.mrc  -verbose 1  -batch 4096  -device 0  -plan\n");
+            "  -bootstrap  -ewald  -rescale avg,std  -mode 0|1  -reconstruction out.mrc  -fom fom.mrc  -verbose 1\n"
+            "  -batch 4096  -device 0  -plan\n");
 }
 
 int ctf_code(const std::string& v) {
@@ -197,6 +201,7 @@ Options parse(int argc, char** argv) {
         else if (a == "-device") o.device = atoi(val().c_str());
         else if (a == "-plan") o.plan_only = true;
         else if (a == "-verbose") o.verbose = atoi(val().c_str());
+        else if (a == "-ewald") o.ewald = true;
         else if (a == "-rescale") {
             const std::string v = val();
             const size_t cpos = v.find(',');

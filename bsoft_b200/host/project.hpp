@@ -384,10 +384,13 @@ inline void view_matrix(double x, double y, double z, double a, double* m) {
 struct Ctf {
     double volt = 300000, cs = 2.7e7, amp_shift = 0, defocus = 20000, def_dev = 0, ast_angle = 0;
     double btx = 0, bty = 0;
-    void coefficients(double* c) const {
-        // relativistic electron wavelength in angstrom (ctf.h:309-317)
+    // relativistic electron wavelength in angstrom (ctf.h:309-317)
+    double lambda() const {
         const double h = 6.626070e-34, me = 9.109384e-31, e = 1.602177e-19, cl = 299792458.0;
-        const double wl = volt > 0 ? h * 1e10 / std::sqrt(2.0 * me * e * volt * (1.0 + e * volt / (2.0 * me * cl * cl))) : 0;
+        return volt > 0 ? h * 1e10 / std::sqrt(2.0 * me * e * volt * (1.0 + e * volt / (2.0 * me * cl * cl))) : 0;
+    }
+    void coefficients(double* c) const {
+        const double wl = lambda();
         const double t1 = M_PI / 2 * wl * wl * wl, t2 = -M_PI * wl, dev = std::fabs(def_dev);
         c[0] = -amp_shift;
         c[1] = t2 * defocus;

@@ -17,7 +17,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .ctf import CTFParams
+from .ctf import CTFParams, electron_wavelength
 from .geometry import view_to_matrix
 from .io import mrc, stacks  # noqa: F401
 from .project import Project
@@ -31,6 +31,7 @@ CTF_ACTIONS = {"none": 0, "flip": 1, "apply": 2, "correct": 3, "wiener": 4}
 PARTICLE_DOUBLES = 32
 P_ORIGIN, P_BKG, P_MAT, P_PIXEL, P_SCALE, P_WEIGHT, P_CTF, P_MAP = 0, 2, 4, 13, 14, 15, 16, 23
 P_NORM = 24       # image normalisation scale, shift (breconstruct -rescale); scale 0 = none
+P_EWALD = 26      # electron wavelength (angstrom) for Ewald-sphere insertion (-ewald); 0 = plane
 
 
 def find_next_power_of(n: int, base: int = 2) -> int:
@@ -82,6 +83,7 @@ class ReconOptions:
     symmetry: str = ""            # point group (-symmetry; "" = C1)
     sym_mode: int = 0             # -mode: 0 during reconstruction, 1 after it (real space)
     rescale: tuple = ()           # -rescale (average, standard deviation) of the finished map
+    ewald: bool = False           # -ewald: insert on the Ewald sphere (both surfaces)
 
 
 @dataclass
@@ -161,6 +163,9 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
             r[P_CTF:P_CTF + 7] = c.coefficients()
             # round-robin partial maps; even maps form half 1 (mg_reconstruct.cpp:757-763, 283-290)
             r[P_MAP] = k % 2
+            if opt.ewald:
+                # particle_reconstruct: ew_wl = em_ctf.lambda() (mg_reconstruct.cpp:209-210)
+                r[P_EWALD] = electron_wavelength(c.volt)
             if opt.rescale:
                 # particle_reconstruct: rescale_to_avg_std(0, 1) with the
                 # statistics read_img attaches (mg_reconstruct.cpp:155)

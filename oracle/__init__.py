@@ -26,7 +26,7 @@ class ReconCfg(C.Structure):
 class Particle(C.Structure):
     _fields_ = [("origin", C.c_double * 2), ("bkg_center", C.c_double * 2), ("mat", C.c_double * 9),
                 ("pixel", C.c_double), ("scale", C.c_double), ("weight", C.c_double),
-                ("ctf", C.c_double * 7)]
+                ("ctf", C.c_double * 7), ("ewald", C.c_double)]
 
 
 _lib = None
@@ -82,7 +82,7 @@ def cfg_from_plan(plan) -> ReconCfg:
 
 
 def particles_from_params(params: np.ndarray):
-    from bsoft_b200.plan import P_ORIGIN, P_BKG, P_MAT, P_PIXEL, P_SCALE, P_WEIGHT, P_CTF
+    from bsoft_b200.plan import P_ORIGIN, P_BKG, P_MAT, P_PIXEL, P_SCALE, P_WEIGHT, P_CTF, P_EWALD
     arr = (Particle * len(params))()
     for i, r in enumerate(params):
         p = arr[i]
@@ -91,6 +91,7 @@ def particles_from_params(params: np.ndarray):
         p.mat[:] = list(r[P_MAT:P_MAT + 9])
         p.pixel, p.scale, p.weight = r[P_PIXEL], r[P_SCALE], r[P_WEIGHT]
         p.ctf[:] = list(r[P_CTF:P_CTF + 7])
+        p.ewald = r[P_EWALD]
     return arr
 
 

@@ -37,6 +37,8 @@ typedef struct {
     double scale;         /* 1/magnification (1 if none)                     */
     double weight;        /* particle weight (1, or selection for bootstrap) */
     double ctf[7];        /* abw00 abw20 abw22 abw2m2 abw40 abw11 abw1m1     */
+    double ewald;         /* electron wavelength (angstrom) for Ewald-sphere
+                             insertion (breconstruct -ewald), 0 = plane      */
 } orc_particle;
 
 /* Accumulate particles into FP64 volumes: vol (2*N^3, complex), weight

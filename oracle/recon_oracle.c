@@ -181,6 +181,16 @@ int orc_insert(const orc_recon_cfg* cfg, const float* images, const orc_particle
                 double d = (maxs2 - s2) * mscale;
                 if (d < 1) w *= sqrt(d);
                 double m[3];
+                if (p->ewald) {
+                    /* Ewald sphere (Bimage_reconstruct.cpp:157-168): s_z =
+                     * +-(lambda/2) s2, m = (R s) mscale, inserted twice */
+                    const double sz = p->ewald / 2 * s2;
+                    for (int i = 0; i < 3; ++i) m[i] = (R[3*i]*sx + R[3*i+1]*sy + R[3*i+2]*sz) * mscale;
+                    interpolate(N, F + 2*(yy*ft + xx), m, w, cfg->interp, vol, weight, power, weight2);
+                    for (int i = 0; i < 3; ++i) m[i] = (R[3*i]*sx + R[3*i+1]*sy + R[3*i+2]*(-sz)) * mscale;
+                    interpolate(N, F + 2*(yy*ft + xx), m, w, cfg->interp, vol, weight, power, weight2);
+                    continue;
+                }
                 for (int i = 0; i < 3; ++i) m[i] = (R[3*i]*sx + R[3*i+1]*sy) * mscale;
                 interpolate(N, F + 2*(yy*ft + xx), m, w, cfg->interp, vol, weight, power, weight2);
             }

@@ -1,7 +1,7 @@
 """Golden maps of breconstruct with symmetry after reconstruction
 (-symmetry X -mode 1: particles inserted once, the finished real-space map
-symmetrized by Bimage::symmetrize, bsoft/src/breconstruct.cpp:335) and with
--rescale, from the reference compiled from its sources, on the golden
+symmetrized by Bimage::symmetrize, bsoft/src/breconstruct.cpp:335), with
+-rescale and with -ewald, from the reference compiled from its sources, on the golden
 datasets.  mode1.npz
 keeps, per case, the dataset name, the options and the map.
 
@@ -33,6 +33,11 @@ CASES = [
     # -rescale avg,std of the finished map (Bimage::rescale_to_avg_std, breconstruct.cpp:336)
     ("ctf16_tri_flip_rs", "ctf16", "-interp trilinear -CTF flip -rescale 0.5,2.0"),
     ("plain24_tri_d2_m1_rs", "plain24", "-interp trilinear -symmetry D2 -mode 1 -rescale -0.1,5.2"),
+    # Ewald-sphere insertion (-ewald: both surfaces s_z = +-(lambda/2) s^2,
+    # Bimage_reconstruct.cpp:157-168, mg_reconstruct.cpp:209-210)
+    ("ctf16_tri_flip_ew", "ctf16", "-interp trilinear -CTF flip -ewald"),
+    ("ctf16_near_apply_ew", "ctf16", "-interp nearest -CTF apply -ewald"),
+    ("ctf16_tri_flip_d3_ew", "ctf16", "-interp trilinear -CTF flip -symmetry D3 -ewald"),
 ]
 
 if __name__ == "__main__":

@@ -75,6 +75,8 @@ def options_from_args(args: str) -> ReconOptions:
             opt.symmetry = val
         elif t == "mode":
             opt.sym_mode = int(val)
+        elif t == "ewald":
+            opt.ewald = True
         elif t == "rescale":
             a, b = (float(x) for x in val.split(","))
             opt.rescale = (a, b)

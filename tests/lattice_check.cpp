@@ -68,6 +68,44 @@ int main(int argc, char** argv) {
             }
         }
     }
+    // Ewald sphere: points on the curved surface m = h ad + k bd + kappa
+    // (h^2 + k^2) n (kappa = lambda/2 inv^2 mscale, up to ~2 voxels of offset
+    // at the corner of a 512^2 transform), with the lattice chosen for the
+    // curvature bound kappa ft sqrt(2); windows all over the pixel square
+    long curved = 0, curved_checked = 0;
+    for (int v = 0; v < nviews; ++v) {
+        double w = nd(rng), x = nd(rng), y = nd(rng), z = nd(rng);
+        const double qn = std::sqrt(w * w + x * x + y * y + z * z);
+        double R[9];
+        quat_matrix(w / qn, x / qn, y / qn, z / qn, R);
+        const double step = 0.5, ft = 512;
+        const double kappa = (v % 3 + 1) * 1.0e-5;
+        double ad[3], bd[3], nv[3];
+        for (int i = 0; i < 3; ++i) { ad[i] = R[3 * i] * step; bd[i] = R[3 * i + 1] * step; nv[i] = R[3 * i + 2]; }
+        const bsg::PhaseLattice L = bsg::choose_lattice(ad, bd, 16, kappa * ft * 1.4142135623730951 * 1.0001);
+        if (L.lh <= 0) { printf("no curved lattice\n"); return 1; }
+        const int W = 10;
+        for (int win = 0; win < 4; ++win) {
+            const int hc = (int)((ud(rng) * 2 - 1) * (ft / 2 - 2 * W)), kc = (int)((ud(rng) * 2 - 1) * (ft / 2 - 2 * W));
+            const double o[3] = {ud(rng) * 7, ud(rng) * 7, ud(rng) * 7};
+            for (int pk = 0; pk < L.lk; ++pk)
+                for (int ph = 0; ph < L.lh; ++ph) {
+                    std::unordered_set<int64_t> cells;
+                    for (int j = -W; j <= W; ++j)
+                        for (int i = -W; i <= W; ++i) {
+                            const int h = hc + ph + L.lh * i + L.sh * j, k = kc + pk + L.lk * j;
+                            const double ez = kappa * ((double)h * h + (double)k * k);
+                            int64_t key = 0;
+                            for (int c = 0; c < 3; ++c) {
+                                const double m = h * ad[c] + k * bd[c] + ez * nv[c] - o[c];
+                                key = key * 4096 + (int64_t)std::floor(m) + 2048;
+                            }
+                            if (!cells.insert(key).second) ++curved;
+                            ++curved_checked;
+                        }
+                }
+        }
+    }
     // very fine steps: the square lattice of side ceil(reach) (packable), and
     // beyond the 12-bit fields no lattice at all (the kernel's own rule)
     {
@@ -86,6 +124,6 @@ int main(int argc, char** argv) {
     printf("points %ld collisions %ld more_phases_than_before %ld phases_at_step_0.5:", checked, collisions, worse);
     for (int d = 1; d <= 16; ++d)
         if (hist[d]) printf(" %d:%ld", d, hist[d]);
-    printf("\n");
-    return (collisions || worse) ? 1 : 0;
+    printf(" curved_points %ld curved_collisions %ld \n", curved_checked, curved);
+    return (collisions || worse || curved) ? 1 : 0;
 }

@@ -179,3 +179,17 @@ def test_rescale_matches_reference(case, exe, tmp_path):
     assert r.returncode == 0, r.stderr
     v, _ = mrc.read_volume(out)
     assert rel_l2(v, z[case + "__map"]) <= 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ctf16_tri_flip_ew", "ctf16_tri_flip_d3_ew"])
+def test_ewald_matches_reference(case, exe, tmp_path):
+    """The drop-in with -ewald against the reference's map."""
+    z = np.load(os.path.join(GOLDEN, "mode1.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    out = os.path.join(str(tmp_path), "map.mrc")
+    r = subprocess.run([exe, *shlex.split(str(z[case + "__options"])), "-reconstruction", out, star],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    v, _ = mrc.read_volume(out)
+    assert rel_l2(v, z[case + "__map"]) <= 1e-5

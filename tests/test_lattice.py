@@ -20,3 +20,5 @@ def test_phase_lattice_is_conflict_free(tmp_path):
     r = subprocess.run([exe, "120"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert " collisions 0 " in r.stdout and " more_phases_than_before 0 " in r.stdout, r.stdout
+    # the Ewald sphere's curved surfaces, with the lattice's curvature margin
+    assert " curved_collisions 0 " in r.stdout, r.stdout

@@ -340,3 +340,47 @@ def test_gpu_rescale_matches_reference(case, tmp_path):
         m = rec.finish()
     assert rel_l2(m, ref) <= 1e-5
     assert fsc(m, ref).min() >= 0.999
+
+
+EWALD_CASES = ["ctf16_tri_flip_ew", "ctf16_near_apply_ew", "ctf16_tri_flip_d3_ew"]
+
+
+@pytest.mark.parametrize("case", EWALD_CASES)
+def test_gpu_ewald_matches_reference(case, tmp_path):
+    """breconstruct -ewald (tests/golden/mode1.npz): every pixel inserted on
+    both Ewald-sphere surfaces s_z = +-(lambda/2) s^2; against the
+    reference's map and the FP64 oracle.  The maps differ from the plane
+    insertion's by ~20%, so the test tells the two apart."""
+    from tests.helpers import options_from_args
+    z = np.load(os.path.join(GOLDEN, "mode1.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    plan = plan_reconstruction(read_project(star), options_from_args(str(z[case + "__options"])))
+    assert np.all(plan.params[:, 26] > 0.02)
+    images = load_images(plan)
+    ref = z[case + "__map"]
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        m = rec.finish()
+    assert rel_l2(m, ref) <= 1e-5
+    assert fsc(m, ref).min() >= 0.999
+    assert rel_l2(m, oracle.reconstruct(plan, images)) <= 1e-5
+
+
+def test_gpu_ewald_full_size_against_fp64_oracle():
+    """Ewald insertion at the batched-insertion size (256^2, ft 512, 256^3,
+    lambda of 200 kV: up to ~1 voxel of curvature at the transform's corners)
+    against the FP64 oracle's accumulators on a few particles."""
+    from bsoft_b200.plan import ReconPlan
+    from bsoft_b200.synth import batched_insertion_workload
+    w = batched_insertion_workload(n_particles=8, box=256, pool=8, seed=5)
+    P = w["params"].copy()
+    P[:, 26] = 0.025079336205768955
+    plan = ReconPlan(n=256, ft=512, map=256, map_sampling=w["pixel"], hi_res=w["hi_res"], interp=2,
+                     ctf_action=1, wiener=0.0, params=P, nmaps=1)
+    images = np.ascontiguousarray(w["pool"])
+    with Reconstructor(plan) as rec:
+        rec.insert(images, P)
+        v, wt = rec.accumulators(0)
+    ov, ow, _, _ = oracle.insert(plan, images, P)
+    assert rel_l2(v.reshape(-1), ov.view(np.complex128)) < 1e-6
+    assert rel_l2(wt.reshape(-1), ow) < 1e-6
