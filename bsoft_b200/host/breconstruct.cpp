@@ -23,6 +23,7 @@
 #include "bsgpu.h"
 #include "project.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -34,6 +35,8 @@
 #include <string>
 #include <vector>
 
+#include <unistd.h>
+
 namespace {
 
 using namespace bsh;
@@ -44,7 +47,9 @@ struct Options {
     double wiener = 0, resolution = 0, sampling = 0, scale = 1;
     bool bootstrap = false, plan_only = false;
     int verbose = 0;
-    int sym_mode = 0;               // -mode: 0 during reconstruction, 1 after it
+    int sym_mode = 0;               // -mode: 0 during reconstruction, 1 after it, 2 random view
+    int threads = 2;                // -threads: the reference's partial maps (-mode 2's draw order)
+    long seed = -1;                 // -seed: random() seed of -mode 2 (default: the process id)
     double rescale_avg = 0, rescale_std = 0;   // -rescale avg,std (std > 0: on)
     bool ewald = false;             // -ewald: Ewald-sphere insertion
     std::string symmetry = "C1";
@@ -72,6 +77,41 @@ struct Plan {
     std::vector<double> rec;                        // BSG_PARTICLE_DOUBLES per particle
     std::vector<std::pair<int, long>> src;          // (micrograph, image index) per particle
 };
+
+// breconstruct -mode 2: every particle inserted once, with a random one of its
+// symmetry-related views (random_symmetric_view, bsoft/src/util/
+// symmetry.cpp:816-832, called per particle by particle_reconstruct,
+// mg_reconstruct.cpp:175).  random() is seeded once (srandom(getpid()),
+// random_numbers.cpp:41-48; -seed replaces the process id); per particle the
+// index is floor(order random() 0.99999 / get_rand_max()) in long double, and
+// get_rand_max() draws 100 numbers of its own after the index's draw
+// (random_numbers.cpp:22-30).  Particles draw partial map by partial map (k
+// mod T, T = the reference's thread_limit, breconstruct.cpp:204-205), the
+// order of its OpenMP loop on one thread.
+void random_symmetric_views(Plan& p, const Options& o) {
+    const std::vector<double> S = symmetry_operators(o.symmetry);
+    const long order = (long)(S.size() / 9), np = (long)p.src.size();
+    if (order < 2 || np < 1) return;
+    long t = std::max(2, o.threads);
+    t = std::max(1L, std::min(t, np / 2));
+    if ((p.nmaps & 2) && (t % 2)) ++t;
+    srandom((unsigned)(o.seed >= 0 ? o.seed : (long)getpid()));
+    for (long m = 0; m < t; ++m)
+        for (long k = m; k < np; k += t) {
+            const long r = random();
+            long rand_max = 32767;
+            for (int j = 0; j < 100; ++j)
+                if (random() > rand_max) rand_max = 2147483647;
+            const long i = (long)((long double)(order * r) * 0.99999L / (long double)rand_max);
+            double* R = &p.rec[k * BSG_PARTICLE_DOUBLES + 4];
+            const double* G = &S[9 * i];
+            double out[9];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    out[3 * a + b] = G[3 * a] * R[b] + G[3 * a + 1] * R[3 + b] + G[3 * a + 2] * R[6 + b];
+            std::copy(out, out + 9, R);
+        }
+}
 
 Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
     int first = -1;
@@ -150,6 +190,7 @@ Plan plan_reconstruction(const std::vector<Micrograph>& mgs, const Options& o) {
             ++k;
         }
     }
+    if (o.sym_mode == 2) random_symmetric_views(p, o);
     return p;
 }
 
@@ -158,7 +199,8 @@ void usage() {
             "Usage: breconstruct [options] input.star\n"
             "  -interpolation nearest|weighted|trilinear  -pad 2  -CTF none|flip|apply|correct|wiener\n"
             "  -wiener 0.2  -resolution 4  -size 64  -sampling 1.5  -scale 1  -fullmap  -halfmaps\n"
-            "  -bootstrap  -ewald  -rescale avg,std  -mode 0|1  -reconstruction out.mrc  -fom fom.mrc  -verbose 1\n"
+            "  -bootstrap  -ewald  -rescale avg,std  -mode 0|1|2  -seed 1  -threads 2  -reconstruction out.mrc\n"
+            "  -fom fom.mrc  -verbose 1\n"
             "  -batch 4096  -device 0  -plan\n");
 }
 
@@ -212,10 +254,12 @@ Options parse(int argc, char** argv) {
         }
         else if (a == "-mode") {
             o.sym_mode = atoi(val().c_str());
-            if (o.sym_mode < 0 || o.sym_mode > 1)
+            if (o.sym_mode < 0 || o.sym_mode > 2)
                 throw std::runtime_error("-mode " + std::to_string(o.sym_mode) +
-                                         ": only 0 (during) and 1 (after reconstruction) are supported");
+                                         ": 0 (during), 1 (after reconstruction) or 2 (random view)");
         }
+        else if (a == "-threads") o.threads = atoi(val().c_str());
+        else if (a == "-seed") o.seed = atol(val().c_str());
         else if (a == "-h" || a == "-help") { usage(); exit(0); }
         else if (a[0] == '-') throw std::runtime_error("unknown option " + a);
         else o.inputs.push_back(a);
@@ -281,10 +325,10 @@ int main(int argc, char** argv) {
                 ord.push_back(g.order);
             }
             CALL(bsg_recon_set_symmetrize(rec, ax.data(), ord.data(), (int)ord.size()));
-        } else {
+        } else if (o.sym_mode == 0) {
             // point-group symmetry during reconstruction (mode 0)
             CALL(bsg_recon_set_symmetry(rec, sym.data(), (int)(sym.size() / 9)));
-        }
+        }   // mode 2: the records already carry each particle's random view
         // stream the particles in host batches (the library uploads and
         // overlaps them with the device work)
         const long n2 = (long)p.n * p.n;

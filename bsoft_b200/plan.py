@@ -13,6 +13,7 @@ Sources (all under bsoft/src):
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -84,6 +85,7 @@ class ReconOptions:
     sym_mode: int = 0             # -mode: 0 during reconstruction, 1 after it (real space)
     rescale: tuple = ()           # -rescale (average, standard deviation) of the finished map
     ewald: bool = False           # -ewald: insert on the Ewald sphere (both surfaces)
+    seed: int = -1                # -mode 2's random() seed (< 0: the process id, as the reference)
 
 
 @dataclass
@@ -103,6 +105,28 @@ class ReconPlan:
     resolution: float = 0.0       # breconstruct's limit before any check (the statistics' limit)
     sym_mode: int = 0             # 0: symmetry inserted; 1: the finished map symmetrized
     rescale: tuple = ()           # (average, standard deviation) of the finished map, or ()
+
+
+def partial_maps(npart: int, opt: ReconOptions) -> int:
+    """Number of partial maps breconstruct splits the selection into
+    (thread_limit: at least 2, at most npart/2, even with half maps;
+    breconstruct.cpp:204-205, mg_reconstruct.cpp:676)."""
+    t = max(2, opt.threads)
+    t = max(1, min(t, npart // 2))
+    if opt.nmaps & 2 and t % 2:
+        t += 1
+    return t
+
+
+def mode2_draw_order(npart: int, opt: ReconOptions) -> list:
+    """Selected-particle indices in the order breconstruct -mode 2 draws their
+    random views: particle k belongs to partial map k mod T (the round-robin of
+    project_configure_for_reconstruction, mg_reconstruct.cpp:757-763), and the
+    partial maps run one after another when its OpenMP loop has one thread
+    (breconstruct.cpp:281-289).  With more threads the reference's draws
+    interleave unpredictably; this order is the reproducible one."""
+    t = partial_maps(npart, opt)
+    return [k for m in range(t) for k in range(m, npart, t)]
 
 
 def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
@@ -181,9 +205,18 @@ def plan_reconstruction(project: Project, opt: ReconOptions) -> ReconPlan:
             rows.append(r)
             index.append((path, int(mg.part_id[i]) - 1))
             k += 1
+    params = np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES)
+    if opt.sym_mode == 2 and (opt.symmetry or "C1") != "C1":
+        # particle_reconstruct with sym_mode 2: each particle inserted once,
+        # with a random one of its symmetry-related views
+        # (random_symmetric_view, mg_reconstruct.cpp:175)
+        from .symmetry import operators, random_view_indices
+        S = operators(opt.symmetry)
+        for j, i in zip(mode2_draw_order(len(params), opt), random_view_indices(len(params), len(S), opt.seed if opt.seed >= 0 else os.getpid())):
+            params[j, P_MAT:P_MAT + 9] = (S[i] @ params[j, P_MAT:P_MAT + 9].reshape(3, 3)).reshape(-1)
     return ReconPlan(n=hdr.nx, ft=ft, map=size, map_sampling=map_sampling, hi_res=hi_res,
                      interp=opt.interp, ctf_action=opt.ctf_action, wiener=wiener,
-                     params=np.array(rows, dtype=np.float64).reshape(-1, PARTICLE_DOUBLES),
+                     params=params,
                      stack_index=index, nmaps=opt.nmaps, symmetry=opt.symmetry or "C1", resolution=resolution,
                      sym_mode=opt.sym_mode, rescale=tuple(opt.rescale))
 

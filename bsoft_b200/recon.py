@@ -44,10 +44,13 @@ class Reconstructor:
         self._h = h
         sym = getattr(plan, "symmetry", "C1") or "C1"
         if sym != "C1":
-            if getattr(plan, "sym_mode", 0) == 1:
+            mode = getattr(plan, "sym_mode", 0)
+            if mode == 1:
                 self.set_symmetrize(sym)
-            else:
+            elif mode == 0:
                 self.set_symmetry(sym)
+            # mode 2: the plan's records already carry each particle's random
+            # symmetry-related view
         if getattr(plan, "rescale", None):
             self.set_rescale(*plan.rescale)
         self.fom = fom

@@ -138,3 +138,28 @@ def operators(sym: str) -> np.ndarray:
             for k in range(n):
                 quats.append(_qmul(q, quats[k]))
     return np.stack([_qmat(q) for q in quats])
+
+
+def random_view_indices(n: int, order: int, seed: int) -> list:
+    """The group element breconstruct -mode 2 picks for each of n particles,
+    in particle order (random_symmetric_view, bsoft/src/util/symmetry.cpp:
+    816-832): the C library's random() after srandom(seed) (the reference
+    seeds it with its process id), index floor(order random() 0.99999 /
+    get_rand_max()) in long double, where get_rand_max() itself draws 100
+    further numbers (bsoft/src/util/random_numbers.cpp:22-30) after the
+    index's draw.  Index into symmetry_get_all_views' order (operators())."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    libc.random.restype = ctypes.c_long
+    libc.srandom.argtypes = [ctypes.c_uint]
+    libc.srandom(int(seed) & 0xFFFFFFFF)
+    out = []
+    for _ in range(n):
+        r = libc.random()
+        rand_max = 32767
+        for _ in range(100):
+            if libc.random() > rand_max:
+                rand_max = 2147483647
+        i = int(np.longdouble(order * r) * np.longdouble("0.99999") / np.longdouble(rand_max))
+        out.append(i)
+    return out

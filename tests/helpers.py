@@ -75,6 +75,10 @@ def options_from_args(args: str) -> ReconOptions:
             opt.symmetry = val
         elif t == "mode":
             opt.sym_mode = int(val)
+        elif t == "threads":
+            opt.threads = int(val)
+        elif t == "seed":
+            opt.seed = int(val)
         elif t == "ewald":
             opt.ewald = True
         elif t == "rescale":

@@ -128,3 +128,23 @@ def test_asymmetric_unit_views():
             assert np.array_equal(vc, v)
     assert groups == {"C", "D", "T", "O", "I"}
     assert len(z["C1_3.0_3.0_1"]) == 4586
+
+
+@pytest.mark.parametrize("sym", ["D3", "C5", "T", "O", "I"])
+def test_random_symmetric_views_match_reference(sym):
+    """breconstruct -mode 2's view per particle (random_symmetric_view after
+    srandom(seed)): the group element random_view_indices picks, applied to
+    the particle's matrix, equals the matrix of the view the reference
+    returned (oracle/_ref/symview_probe, tests/golden/mode2.npz)."""
+    import os
+    from bsoft_b200.geometry import view_to_matrix
+    from tests.match_helpers import GOLDEN
+    from bsoft_b200.symmetry import operators, random_view_indices
+    z = np.load(os.path.join(GOLDEN, "mode2.npz"))
+    views, out = z[f"views_{sym}__in"], z[f"views_{sym}__out"]
+    S = operators(sym)
+    idx = random_view_indices(len(views), len(S), int(z[f"views_{sym}__seed"]))
+    assert len(set(idx)) > 1
+    for v, i, o in zip(views, idx, out):
+        got = S[i] @ view_to_matrix(v)
+        assert np.abs(got - view_to_matrix(o)).max() < 1e-12, (sym, i)

@@ -384,3 +384,35 @@ def test_gpu_ewald_full_size_against_fp64_oracle():
     ov, ow, _, _ = oracle.insert(plan, images, P)
     assert rel_l2(v.reshape(-1), ov.view(np.complex128)) < 1e-6
     assert rel_l2(wt.reshape(-1), ow) < 1e-6
+
+
+MODE2_CASES = ["ctf16_tri_flip_d3_m2", "plain24_tri_i_m2", "plain24_near_t_m2_half"]
+
+
+@pytest.mark.parametrize("case", MODE2_CASES)
+def test_gpu_symmetry_mode2_matches_reference(case, tmp_path):
+    """breconstruct -symmetry X -mode 2 (tests/golden/mode2.npz): each
+    particle inserted once with a random symmetry-related view, drawn with
+    the seed the reference's random() had; against the reference's maps
+    (half maps too) and the FP64 oracle."""
+    from tests.helpers import options_from_args
+    z = np.load(os.path.join(GOLDEN, "mode2.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    opt = options_from_args(str(z[case + "__options"]))
+    opt.seed = int(z[case + "__seed"])
+    plan = plan_reconstruction(read_project(star), opt)
+    assert plan.sym_mode == 2
+    images = load_images(plan)
+    with Reconstructor(plan) as rec:
+        rec.insert(images, plan.params)
+        if plan.nmaps == 2:
+            for h in (1, 2):
+                m = rec.finish(h)
+                assert rel_l2(m, z[f"{case}__map_0{h}"]) <= 1e-5
+        else:
+            m = rec.finish()
+            ref = z[case + "__map"]
+            assert rel_l2(m, ref) <= 1e-5
+            assert fsc(m, ref).min() >= 0.999
+            plan.symmetry = "C1"
+            assert rel_l2(m, oracle.reconstruct(plan, images)) <= 1e-5
