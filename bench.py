@@ -857,7 +857,7 @@ def main():
         # spread over the launch) and writes 767.2 MB (the two replicas'
         # partial sums, fixed per launch); scaled to the launch's batch
         traffic = (3.754e6 * B + 0.767e9) if (int(shape) == 0 and BOX == 256) else None
-        roof = {"kernel": "insert_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+        roof = {"kernel": "grid4_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                 "traffic_unit": ("bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
                                  "256-particle launch, reads scaled per particle)"),
