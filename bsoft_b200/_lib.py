@@ -49,6 +49,14 @@ class MatchStats(C.Structure):
                 ("refine_ms", C.c_double), ("refine_launches", C.c_long)]
 
 
+class BackprojConfig(C.Structure):
+    _fields_ = [("n", C.c_int), ("map", C.c_int), ("pixel", C.c_double), ("resolution", C.c_double),
+                ("nmaps", C.c_int), ("batch", C.c_int), ("device", C.c_int)]
+
+
+BACKPROJ_DOUBLES = 16
+
+
 class CnnConfig(C.Structure):
     _fields_ = [("box", C.c_int), ("channels", C.c_int * 6), ("hidden", C.c_int), ("batch", C.c_int),
                 ("shift_weight", C.c_float), ("device", C.c_int), ("seed", C.c_ulonglong)]
@@ -131,6 +139,13 @@ def load():
         "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
                               C.c_int],
                              C.c_int),
+        "bsg_backproj_create": ([C.POINTER(BackprojConfig), C.POINTER(vp)], C.c_int),
+        "bsg_backproj_destroy": ([vp], None),
+        "bsg_backproj_add": ([vp, vp, dp, C.c_long, C.c_int], C.c_int),
+        "bsg_backproj_finish": ([vp, C.c_int, vp, C.c_int], C.c_int),
+        "bsg_backproj_set_symmetrize": ([vp, dp, C.POINTER(C.c_int), C.c_int], C.c_int),
+        "bsg_backproj_set_rescale": ([vp, C.c_double, C.c_double], C.c_int),
+        "bsg_backproj_reset": ([vp], C.c_int),
         "bsg_cnn_create": ([C.POINTER(CnnConfig), C.POINTER(vp)], C.c_int),
         "bsg_cnn_destroy": ([vp], None),
         "bsg_cnn_num_params": ([vp], C.c_long),

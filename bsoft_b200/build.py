@@ -35,7 +35,7 @@ def up_to_date() -> bool:
 
 
 HOSTDIR = os.path.join(HERE, "host")
-HOST_PROGRAMS = ("breconstruct", "brefine")
+HOST_PROGRAMS = ("breconstruct", "brefine", "bbackproj")
 
 
 def build_host(force: bool = False) -> list:

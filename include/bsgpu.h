@@ -471,6 +471,67 @@ int  bsg_cnn_train(bsg_cnn* c, const float* images, const float* targets, long n
  * inscribed circle; counter-based, reproducible for a seed. */
 int  bsg_add_noise(float* d_images, long n, int box, double snr, unsigned long long seed, void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Real-space weighted back-projection (bbackproj).
+ *
+ *   bsg_backproj_create  <- the map set-up of project_back_projection
+ *                           (bsoft/src/mg/mg_reconstruct.cpp:1524-1560) and the
+ *                           plans of bbackproj (bsoft/src/bbackproj.cpp:170-171)
+ *   bsg_backproj_add     <- its per-particle loop (mg_reconstruct.cpp:1570-1614)
+ *                           over Bimage::back_project (bsoft/src/img/
+ *                           Bimage_project.cpp:466-509): ramp filter
+ *                           (fspace_weigh_ramp), rescale to average 0 and
+ *                           standard deviation 1, background fill, every voxel
+ *                           adds the image sampled along its projection
+ *   bsg_backproj_finish  <- img_backprojection_accumulate (mg_reconstruct.cpp:
+ *                           1640-1684) and bbackproj's -symmetry / -rescale
+ *                           (bbackproj.cpp:199-207)
+ *
+ * Record per image: BSG_BACKPROJ_DOUBLES doubles
+ *   [0..1]  image origin x, y (pixels)      Bparticle::ori as project_back_
+ *                                           projection resolves it
+ *   [2..10] rotation matrix, row-major      View::matrix (View.h:153-156)
+ *   [11]    magnification (part->mag / scale; > 0)
+ *   [12]    map index: 0, or 1 for the second half map
+ *   [13]    image pixel size (angstrom; 0: the config's), which sets the
+ *           ramp's frequencies and resolution check (Bparticle::pixel_size)
+ *   [14..15] reserved (0)
+ * The map is N^3 float32, z slowest, origin at its integer half size.
+ */
+#define BSG_BACKPROJ_DOUBLES 16
+
+typedef struct {
+    int    n;             /* image edge (square images), 2..1024 with no    */
+                          /* prime factor above 7                           */
+    int    map;           /* map edge N, 2..1024                            */
+    double pixel;         /* image pixel size (angstrom) of records with 0  */
+    double resolution;    /* ramp limit (angstrom), checked per image as    */
+                          /* Bimage::check_resolution does                  */
+    int    nmaps;         /* 1 full map; 2 (or 3) two half maps as well     */
+    int    batch;         /* images per device batch (0: 256)               */
+    int    device;
+} bsg_backproj_config;
+
+typedef struct bsg_backproj bsg_backproj;
+
+int  bsg_backproj_create(const bsg_backproj_config* cfg, bsg_backproj** out);
+void bsg_backproj_destroy(bsg_backproj* b);
+/* count images (n^2 float32 each, host, or device with BSG_DEVICE_PTR) and
+ * their records; the map(s) grow in image order.  Returns when the inputs
+ * may be reused. */
+int  bsg_backproj_add(bsg_backproj* b, const float* images, const double* records, long count, int flags);
+/* Map imap (0: the full map, the float sum of the halves when there are
+ * two; 1, 2: a half map), after the optional symmetrization and rescaling,
+ * into map_out (N^3 float32; a device pointer with BSG_DEVICE_PTR). */
+int  bsg_backproj_finish(bsg_backproj* b, int imap, float* map_out, int flags);
+/* bbackproj -symmetry: Bimage::symmetrize(sym, 1) of the finished map
+ * (generating operations as bsg_recon_set_symmetrize takes them); nops 0
+ * turns it off. */
+int  bsg_backproj_set_symmetrize(bsg_backproj* b, const double* axes, const int* orders, int nops);
+/* bbackproj -rescale avg,std (std <= 0: off) */
+int  bsg_backproj_set_rescale(bsg_backproj* b, double avg, double std);
+int  bsg_backproj_reset(bsg_backproj* b);
+
 const char* bsg_last_error(void);
 const char* bsg_version(void);
 

@@ -96,3 +96,37 @@ def load_case(name: str, directory: str):
     images = load_images(plan)
     refs = {k: z[k] for k in z.files if k.startswith("map")}
     return plan, images, refs
+
+
+def backproj_options_from_args(args: str):
+    """bbackproj's command-line options (the subset the golden cases use) as
+    BackprojOptions: -resolution, -fullmap / -halfmaps, -threads, -symmetry,
+    -rescale, -size, -scale."""
+    from bsoft_b200.backproj import BackprojOptions
+    opt = BackprojOptions()
+    toks = shlex.split(args)
+    full = half = False
+    i = 0
+    while i < len(toks):
+        t = toks[i].lstrip("-")
+        val = toks[i + 1] if i + 1 < len(toks) else None
+        if "resolution".startswith(t):
+            opt.resolution = float(val); i += 2
+        elif t == "fullmap":
+            full = True; i += 1
+        elif t == "halfmaps":
+            half = True; i += 1
+        elif t == "threads":
+            opt.threads = int(val); i += 2
+        elif "symmetry".startswith(t) and len(t) >= 3:
+            opt.symmetry = val; i += 2
+        elif t == "rescale":
+            opt.rescale = tuple(float(x) for x in val.split(",")); i += 2
+        elif t == "size":
+            opt.size = int(val.split(",")[0]); i += 2
+        elif t == "scale":
+            opt.scale = float(val); i += 2
+        else:
+            raise ValueError(f"option {toks[i]}")
+    opt.nmaps = (1 if full or not half else 0) + (2 if half else 0)
+    return opt

@@ -230,3 +230,46 @@ def test_symmetry_mode2_matches_reference(case, exe, tmp_path):
         tag = k[len(case) + 5:]
         v, _ = mrc.read_volume(out.replace(".mrc", tag + ".mrc"))
         assert rel_l2(v, z[k]) <= 1e-5, (k, rel_l2(v, z[k]))
+
+
+# ---- bbackproj: the reference's back-projection maps through the drop-in
+BP_EXE = os.path.join(ROOT, "bsoft_b200", "_build", "bbackproj")
+BP_CASES = ["ctf16_bp", "plain24_bp", "plain24_bp_half", "plain24_bp_full_half", "plain24_bp_d2", "ctf16_bp_rs"]
+
+
+@pytest.mark.parametrize("case", BP_CASES)
+def test_bbackproj_plan_matches_host_mirror(case, exe, tmp_path):
+    """The drop-in's records (origins, matrices, magnification, half maps,
+    pixel sizes) equal the Python planner's."""
+    from bsoft_b200.backproj import plan_backprojection
+    from bsoft_b200.project import read_project
+    from tests.helpers import backproj_options_from_args
+    z = np.load(os.path.join(GOLDEN, "bbackproj.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    args = shlex.split(str(z[case + "__options"]))
+    plan = plan_backprojection(read_project(star), backproj_options_from_args(str(z[case + "__options"])))
+    r = subprocess.run([BP_EXE, *args, "-plan", star], capture_output=True, text=True, check=True)
+    lines = r.stdout.strip().splitlines()
+    head = lines[0].split()
+    kv = {head[i]: head[i + 1] for i in range(0, len(head), 2)}
+    assert int(kv["n"]) == plan.n and int(kv["map"]) == plan.map and int(kv["nmaps"]) == plan.nmaps
+    rec = np.array([[float(t) for t in ln.split()] for ln in lines[1:]])
+    assert rec.shape == plan.records.shape
+    assert np.abs(rec - plan.records).max() <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", BP_CASES)
+def test_bbackproj_matches_reference(case, exe, tmp_path):
+    """The drop-in bbackproj against the reference's maps (every map it
+    writes: full, half maps)."""
+    z = np.load(os.path.join(GOLDEN, "bbackproj.npz"))
+    star = materialize_dataset(str(z[case + "__dataset"]), str(tmp_path))
+    out = os.path.join(str(tmp_path), "map.mrc")
+    r = subprocess.run([BP_EXE, *shlex.split(str(z[case + "__options"])), "-reconstruction", out, star],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for k in [k for k in z.files if k.startswith(case + "__map")]:
+        tag = k[len(case) + 5:]
+        v, _ = mrc.read_volume(out.replace(".mrc", tag + ".mrc"))
+        assert rel_l2(v, z[k]) <= 1e-5, (k, rel_l2(v, z[k]))
