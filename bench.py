@@ -409,6 +409,44 @@ def train_proposer(sw, local, torch, n_train: int, epochs: float):
                  "loss_first": round(float(losses[:100].mean()), 4), "loss_last": round(float(losses[-100:].mean()), 4)}
 
 
+def learned_controls(m, net, mats, pviews, origins, radius, torch, n=256):
+    """The learned pipeline on the same particles at SNR 0.1, SNR 1 and
+    without noise: the proposal, the local search and grid refinement
+    (brefine -defocus) from the local search's best pose.  Every set is
+    generated from the search map's phantom with the same views, shifts and
+    CTFs (the noise is drawn last), so the rows differ only by the noise;
+    the medians show what the noise, not the pipeline, limits."""
+    from bsoft_b200.synth import DatasetSpec, generate
+    from bsoft_b200.match import ctf_record
+    from bsoft_b200.geometry import angular_distance_deg, views_to_matrices
+    out = {}
+    for label, snr in (("snr_0.1", 0.1), ("snr_1", 1.0), ("noise_free", None)):
+        spec = DatasetSpec(box=SEARCH_BOX, n_particles=n, n_blobs=100, pixel=SEARCH_PIXEL, snr=snr, seed=21,
+                           defocus_range=(1.0e4, 3.0e4), shift_range=2.0)
+        _, imgs, meta = generate(spec)
+        ctf = np.stack([ctf_record(spec.volt, c) for c in meta["coefs"]])
+        dev = torch.from_numpy(np.ascontiguousarray(imgs)).cuda()
+        pred = torch.empty((n, 11), dtype=torch.float32, device="cuda")
+        net.predict(dev, out=pred)
+        m.set_images(dev, ctf)
+        res = m.search_local(pred, origins, radius, 1.5, 8)
+        best = res[:, 0, 0].astype(int)
+        start = np.column_stack([np.arange(n), pviews[best], origins[res[:, 0, 1].astype(int)]])
+        rout = m.refine(start, REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP,
+                        REFINE_SACC, REFINE_DEF)
+        pr = pred.cpu().numpy()[:, :9].reshape(-1, 3, 3).astype(np.float64)
+        e_p = angular_distance_deg(pr, meta["mats"])
+        e_l = angular_distance_deg(mats[best], meta["mats"])
+        e_r = angular_distance_deg(views_to_matrices(rout[:, :4]), meta["mats"])
+        out[label] = {"proposal": round(float(np.median(e_p)), 3), "local_search": round(float(np.median(e_l)), 3),
+                      "refined": round(float(np.median(e_r)), 3),
+                      "refined_frac_within_1_deg": round(float(np.mean(e_r <= 1.0)), 4)}
+    out["particles"] = n
+    out["what"] = ("median angular error (degrees) against the true poses: the proposal, the local search from it "
+                   "(3-degree panel), and grid refinement from the local search (2 -> 0.5 degrees, defocus search)")
+    return out
+
+
 def fsc_of_poses(sw, sel, mats_by_method, origins_by_method, local):
     """Reconstructions (trilinear, CTF flip, pad 2) of the images `sel` with
     each method's poses, and their Fourier shell correlation with the map
@@ -549,6 +587,8 @@ def search_leg(args, local, dist, world, rank, torch):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             lms = float(t.item())
         learned = {"ms": lms, "stats": lst, "results": lres, "train": train_info}
+        if rank == 0 and "refine" in args.legs:
+            learned["controls"] = learned_controls(m, net, mats, pviews, origins, args.local_radius, torch)
         net.close()
     # ---- grid refinement of the last step's best poses (brefine -defocus)
     refine = None
@@ -678,6 +718,7 @@ def search_leg(args, local, dist, world, rank, torch):
                          "proposal_frac_within_radius": round(float(np.mean(perr < args.local_radius)), 4)},
             "fsc_vs_true_pose_map": fsc, "training": learned["train"],
             "gpu_launches": int(lst["launches"]),
+            "controls": learned.get("controls"),
         }
     return {
         "metric": "particles/s (exhaustive orientation search)", "value": round(value, 1), "unit": "particles/s",

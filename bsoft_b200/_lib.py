@@ -72,7 +72,7 @@ MATCH_HYP_DOUBLES = 12
 MATCH_REFINE_START_DOUBLES = 7
 MATCH_SCORE_FP64 = 4
 MATCH_SCORE_DPR = 8
-MATCH_REFINE_RESULT_DOUBLES = 10
+MATCH_REFINE_RESULT_DOUBLES = 12
 
 
 class BsgError(RuntimeError):
@@ -136,7 +136,8 @@ def load():
         "bsg_match_get_stats": ([vp, C.POINTER(MatchStats)], C.c_int),
         "bsg_match_reset_stats": ([vp], C.c_int),
         "bsg_match_stream": ([vp], vp),
-        "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, dp,
+        "bsg_match_refine": ([vp, dp, C.c_long, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                              C.c_double, dp,
                               C.c_int],
                              C.c_int),
         "bsg_backproj_create": ([C.POINTER(BackprojConfig), C.POINTER(vp)], C.c_int),

@@ -157,6 +157,8 @@ struct ImgCtf {
     double c[5];     // abw00 abw20 abw22 abw2m2 abw40
     int apply;       // multiply the reference by the CTF
     int invert;      // negate the CTF (contrast inversion)
+    double fsx, fsy; // frequency per index on x and y (1 / real size of the image
+                     // with its per-axis sampling); 0: the context's isotropic step
 };
 
 // sin(chi) of one figure-of-merit pixel (img_recip_space_fom's CTF factor,
@@ -164,8 +166,8 @@ struct ImgCtf {
 // ctf.h:321-334); 1 when the record does not apply
 __device__ __forceinline__ float ctf_factor(const ImgCtf& C, const MPix& q, double fs) {
     if (!C.apply) return 1.f;
-    double sx2 = fs * q.h; sx2 *= sx2;
-    double sy2 = fs * q.k; sy2 *= sy2;
+    double sx2 = (C.fsx > 0 ? C.fsx : fs) * q.h; sx2 *= sx2;
+    double sy2 = (C.fsy > 0 ? C.fsy : fs) * q.k; sy2 *= sy2;
     const double s2 = sx2 + sy2;
     const double a = atan2((double)q.k, (double)q.h);
     const double chi = C.c[0] + s2 * (C.c[3] * sin(2 * a) + C.c[1] + C.c[2] * cos(2 * a)) + s2 * s2 * C.c[4];

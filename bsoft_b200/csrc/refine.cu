@@ -34,6 +34,7 @@ constexpr double TRIGPREC = 1e-30;   // TRIGPRECISION / SMALLFLOAT (bsoft/includ
 constexpr int NVIEW = 27;            // views_for_refinement: 3 x 3 x 3
 constexpr int MAX_LEVELS = 32;       // shift grid levels (shift_step / shift_accuracy <= 2^31)
 constexpr long MAX_ROUNDS = 100000;  // angular rounds per particle (the reference has no bound)
+constexpr int MAX_MAG_STEPS = 64;    // magnification factors per axis (the reference's grid has 21)
 
 // angle_set_negPI_to_PI (bsoft/src/util/utilities.cpp:606-615)
 double angle_neg_pi_to_pi(double a) {
@@ -266,6 +267,7 @@ struct Particle {
     long row0 = 0;                 // first row of this particle in the call's CTF table
     int vk[NVIEW];                 // this round: chosen trial per view
     double vfom[NVIEW], vcv[NVIEW];
+    double bmx = 1, bmy = 1;       // magnification stage: the winning per-axis sampling factors
 };
 
 }  // namespace
@@ -274,7 +276,8 @@ struct Particle {
 using namespace bsg;
 
 extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, double alpha_step, double accuracy,
-                                double shift_step, double shift_accuracy, double def_std, double* out, int flags) {
+                                double shift_step, double shift_accuracy, double def_std, double max_mag, double* out,
+                                int flags) {
     const bool dpr = (flags & BSG_MATCH_SCORE_DPR) != 0;
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !start || !out || nstart < 1) return match_fail(BSG_ERR_ARG, "bsg_match_refine: bad argument");
@@ -292,6 +295,22 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         return match_fail(BSG_ERR_ARG, "bsg_match_refine: shift accuracy must be positive (got %g)", shift_accuracy);
     if (!(def_std >= 0) || !isfinite(def_std))
         return match_fail(BSG_ERR_ARG, "bsg_match_refine: bad defocus step %g", def_std);
+    // img_refine_grid's magnification grid (mg_refine.cpp:1151-1154): factors
+    // 1 - max_mag .. 1 + max_mag in floating steps of max_mag / 10, y outer
+    std::vector<std::pair<double, double>> mags;
+    if (!(max_mag >= 0) || !(max_mag < 1))
+        return match_fail(BSG_ERR_ARG, "bsg_match_refine: magnification range %g outside [0, 1)", max_mag);
+    if (max_mag > 0) {
+        const double mmin = 1.0 - max_mag, mmax = 1.0 + max_mag, mstep = max_mag / 10;
+        std::vector<double> axis;
+        for (double m = mmin; m <= mmax; m += mstep) {
+            if ((int)axis.size() >= MAX_MAG_STEPS || m + mstep == m)
+                return match_fail(BSG_ERR_ARG, "bsg_match_refine: magnification step %g too small", mstep);
+            axis.push_back(m);
+        }
+        for (double my : axis)
+            for (double mx : axis) mags.push_back({mx, my});
+    }
     std::vector<double> steps;
     for (double st = shift_step; st >= shift_accuracy; st /= 2) {
         if ((int)steps.size() >= MAX_LEVELS)
@@ -393,8 +412,9 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         }
     }
 
-    // score `groups` (FP64) with the given CTF table; results in go
-    auto score = [&](const float* table) -> int {
+    // score `groups` (FP64) with the given CTF table and gathered sections;
+    // results in go
+    auto score_with = [&](const float* table, const double2* sec) -> int {
         const long ng = (long)groups.size();
         int r = ensure_groups(*M, ng);
         if (r != BSG_OK) return r;
@@ -402,7 +422,7 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         cudaError_t e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaEventRecord(e0, s);
         if (e == cudaSuccess)
-            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table, d_sec, dpr);
+            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, table, sec, dpr);
         if (e == cudaSuccess) e = cudaEventRecord(e1, s);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
@@ -414,6 +434,7 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         ++launches;
         return BSG_OK;
     };
+    auto score = [&](const float* table) -> int { return score_with(table, d_sec); };
     // group of the t-th active particle's view v (its gathered section t * 27 + v)
     auto view_group = [&](const Particle& P, long t, int v) {
         MHypG g;
@@ -426,6 +447,246 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
     };
     // phase_shift_to_origin's slopes, as bsg_match_score forms them
     auto slope = [&](double o) { return o / M->D * 2 * M_PI; };
+
+    // img_refine_grid's magnification stage (mg_refine.cpp:1145-1187), after
+    // the angular rounds: for every factor pair (mx, my), in grid order, the
+    // particle's sampling becomes (s mx, s my); the best view's section is
+    // gathered with rows 0 and 1 scaled by (pref sampling / that sampling) per
+    // axis (img_fit_in_recip_space_grid :873-882), the CTF uses the per-axis
+    // frequency steps 1 / (D s mx), 1 / (D s my) (img_recip_space_fom :694),
+    // and the fit runs its defocus trials (with -defocus, around the
+    // particle's defocus) and shift levels 0.4, 0.2, 0.1 around the best
+    // origin of the angular stage.  A fit replaces the best one only when it
+    // scores strictly higher; the best fom restarts at -1.
+    const double mag_samp = M->cfg.pixel / M->cut_scale;    // Bimage::change_transform_size's sampling
+    const double ref_samp = M->cfg.map_sampling / (double)((long double)M->D / M->N);
+    std::vector<double> mag_steps;
+    for (double st = 0.4; st >= 0.1; st /= 2) mag_steps.push_back(st);
+    auto mag_stage = [&](long c0, long c1) -> int {
+        const long nmag = (long)mags.size();
+        long maxd = 1;
+        for (long i = c0; i < c1; ++i) maxd = std::max(maxd, (long)parts[i].dvals.size());
+        const long per_sec = nmag * (long)npix * (long)sizeof(double2);
+        const long per_ctf = nmag * maxd * (long)npix * (long)sizeof(float);
+        long sub = std::max(1L, (1L << 30) / std::max(per_sec, 1L));
+        sub = std::min(sub, std::max(1L, (1L << 30) / std::max(per_ctf, 1L)));
+        sub = std::min(sub, std::max(1L, 65536L / (nmag * std::max(maxd, 3L))));
+        sub = std::min(sub, c1 - c0);
+        double* d_mm = nullptr;
+        double2* d_msec = nullptr;
+        float* d_mctf = nullptr;
+        ImgCtf* d_mrec = nullptr;
+        cudaError_t e = cudaMalloc(&d_mm, sizeof(double) * 9 * sub * nmag);
+        if (e == cudaSuccess) e = cudaMalloc(&d_msec, sizeof(double2) * (size_t)npix * sub * nmag);
+        if (e == cudaSuccess) e = cudaMalloc(&d_mctf, sizeof(float) * (size_t)npix * sub * nmag * maxd);
+        if (e == cudaSuccess) e = cudaMalloc(&d_mrec, sizeof(ImgCtf) * sub * nmag * maxd);
+        int r = BSG_OK;
+        if (e != cudaSuccess) r = match_fail(BSG_ERR_NOMEM, "bsg_match_refine: magnification stage: %s", cudaGetErrorString(e));
+        std::vector<double> mm;
+        std::vector<ImgCtf> recs;
+        for (long p0 = c0; p0 < c1 && r == BSG_OK; p0 += sub) {
+            const long p1 = std::min(c1, p0 + sub), np_ = p1 - p0;
+            std::vector<std::vector<Level>> lev(np_);
+            for (long t = 0; t < np_; ++t) {
+                const Particle& P = parts[p0 + t];
+                for (double st : mag_steps) {
+                    lev[t].push_back(origin_level(P.box, P.boy, st));
+                    if (lev[t].back().n > MAXORG) {
+                        r = match_fail(BSG_ERR_ARG, "bsg_match_refine: origin grid of %d points", lev[t].back().n);
+                        break;
+                    }
+                }
+            }
+            if (r != BSG_OK) break;
+            // sections of the best views, one per factor pair
+            mm.assign(9 * np_ * nmag, 0.0);
+            for (long t = 0; t < np_; ++t) {
+                double mat[9];
+                view_matrix(renormalised(parts[p0 + t].bestview, 3), mat);
+                for (long m = 0; m < nmag; ++m) {
+                    const double kx = ref_samp / (mag_samp * mags[m].first);
+                    const double ky = ref_samp / (mag_samp * mags[m].second);
+                    double* o = &mm[9 * (t * nmag + m)];
+                    for (int a = 0; a < 3; ++a)
+                        for (int c = 0; c < 3; ++c) {
+                            double v = mat[3 * a + c];
+                            if (a < 2) v *= (c == 0 ? kx : (c == 1 ? ky : 1.0));
+                            o[3 * a + c] = v;
+                        }
+                }
+            }
+            e = cudaMemcpyAsync(d_mm, mm.data(), sizeof(double) * mm.size(), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            if (e == cudaSuccess) e = launch_secgather(*M, d_mm, np_ * nmag, d_msec, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) { r = match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(e)); break; }
+            {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tsum += ms;
+                ++launches;
+            }
+            // CTF rows at the factor pairs' frequency steps: every defocus
+            // trial with -defocus, else the image's own record
+            bool need_rows = dsearch;
+            for (long t = 0; t < np_; ++t) need_rows = need_rows || M->h_ictf[parts[p0 + t].img].apply;
+            std::vector<long> rowbase(np_, 0), nd(np_, 1);
+            recs.clear();
+            if (need_rows) {
+                for (long t = 0; t < np_; ++t) {
+                    const Particle& P = parts[p0 + t];
+                    rowbase[t] = (long)recs.size();
+                    nd[t] = dsearch ? (long)P.dvals.size() : 1;
+                    const DefocusTerm dz(dsearch ? M->h_volt[P.img] : 0.0);
+                    for (long m = 0; m < nmag; ++m) {
+                        const double fsx = 1.0 / ((mag_samp * mags[m].first) * M->D);
+                        const double fsy = 1.0 / ((mag_samp * mags[m].second) * M->D);
+                        for (long k = 0; k < nd[t]; ++k) {
+                            ImgCtf C = M->h_ictf[P.img];
+                            if (dsearch) {
+                                C.c[1] = dz.abw20(P.dvals[k]);
+                                C.apply = dz.defocus(C.c[1]) >= 1 ? 1 : 0;
+                            }
+                            C.fsx = fsx;
+                            C.fsy = fsy;
+                            recs.push_back(C);
+                        }
+                    }
+                }
+                e = cudaMemcpyAsync(d_mrec, recs.data(), sizeof(ImgCtf) * recs.size(), cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = launch_ctf_rows(*M, d_mrec, (long)recs.size(), d_mctf, s);
+                if (e != cudaSuccess) { r = match_fail(BSG_ERR_CUDA, "bsg_match_refine: %s", cudaGetErrorString(e)); break; }
+            }
+            const float* table = need_rows ? d_mctf : nullptr;
+            auto mgroup = [&](long t, long m) {
+                const Particle& P = parts[p0 + t];
+                MHypG g;
+                memset(&g, 0, sizeof(g));
+                memcpy(g.m, &mm[9 * (t * nmag + m)], sizeof(g.m));
+                g.img = (int)P.img;
+                g.ctf = need_rows ? (int)(rowbase[t] + m * nd[t] + nd[t] - 1) : (int)P.img;
+                g.sec = (int)(t * nmag + m);
+                return g;
+            };
+            // pass A: the fits' defocus trials at the best origin
+            std::vector<int> vk(np_ * nmag);
+            std::vector<double> vfom(np_ * nmag, -1.0), vcv(np_ * nmag, 0.0);
+            for (long t = 0; t < np_; ++t)
+                for (long m = 0; m < nmag; ++m) vk[t * nmag + m] = (int)nd[t] - 1;
+            if (dsearch) {
+                groups.clear();
+                gfirst.clear();
+                for (long t = 0; t < np_; ++t) {
+                    const Particle& P = parts[p0 + t];
+                    gfirst.push_back((long)groups.size());
+                    for (long m = 0; m < nmag; ++m) {
+                        MHypG g = mgroup(t, m);
+                        g.norg = 1;
+                        g.sx[0] = slope(P.box);
+                        g.sy[0] = slope(P.boy);
+                        for (long k = 0; k + 1 < nd[t]; ++k) {
+                            g.ctf = (int)(rowbase[t] + m * nd[t] + k);
+                            groups.push_back(g);
+                        }
+                    }
+                }
+                r = score_with(table, d_msec);
+                if (r != BSG_OK) break;
+                for (long t = 0; t < np_; ++t) {
+                    Particle& P = parts[p0 + t];
+                    const long ntr = nd[t] - 1;
+                    for (long m = 0; m < nmag; ++m)
+                        for (long k = 0; k < ntr; ++k) {
+                            const long g = gfirst[t] + m * ntr + k;
+                            const double f = go[g * MAXORG];
+                            P.number++;
+                            if (vfom[t * nmag + m] < f) {
+                                vfom[t * nmag + m] = f;
+                                vk[t * nmag + m] = (int)k;
+                                vcv[t * nmag + m] = go[(long)groups.size() * MAXORG + g * MAXORG];
+                            }
+                        }
+                }
+            }
+            // pass B: the shift levels with each fit's chosen defocus
+            groups.clear();
+            const int nml = (int)mag_steps.size();
+            for (long t = 0; t < np_; ++t)
+                for (long m = 0; m < nmag; ++m) {
+                    MHypG g = mgroup(t, m);
+                    if (need_rows) g.ctf = (int)(rowbase[t] + m * nd[t] + vk[t * nmag + m]);
+                    for (int k = 0; k < nml; ++k) {
+                        const Level& L = lev[t][k];
+                        g.norg = L.n;
+                        for (int o = 0; o < L.n; ++o) {
+                            g.sx[o] = slope(L.x[o]);
+                            g.sy[o] = slope(L.y[o]);
+                        }
+                        groups.push_back(g);
+                    }
+                }
+            r = score_with(table, d_msec);
+            if (r != BSG_OK) break;
+            const long ng = (long)groups.size();
+            const double* gfom = go.data();
+            const double* gcv = go.data() + ng * MAXORG;
+            for (long t = 0; t < np_; ++t) {
+                Particle& P = parts[p0 + t];
+                const DefocusTerm dz(dsearch ? M->h_volt[P.img] : 0.0);
+                double best = -1, bcv = P.bestcv, bx = P.box, by = P.boy, bdef = P.bestdef, bmx = 1, bmy = 1;
+                bool won = false;
+                for (long m = 0; m < nmag; ++m) {
+                    const long q = t * nmag + m;
+                    double fbest = vfom[q], prevfom, fcv = vcv[q], fx = P.box, fy = P.boy;
+                    int k = 0;
+                    while (k < nml) {
+                        const Level& L = lev[t][k];
+                        const long g = q * nml + k;
+                        prevfom = fbest;
+                        fbest = -1;
+                        int ib = 0;
+                        for (int o = 0; o < L.n; ++o) {
+                            const double f = gfom[g * MAXORG + o];
+                            P.number++;
+                            if (fbest < f) {
+                                fbest = f;
+                                ib = o;
+                                fx = L.x[o];
+                                fy = L.y[o];
+                                fcv = gcv[g * MAXORG + o];
+                            }
+                        }
+                        if (ib == L.n / 2 || fabs(prevfom - fbest) < 1e-6) ++k;
+                    }
+                    if (best < fbest) {
+                        best = fbest;
+                        won = true;
+                        bmx = mags[m].first;
+                        bmy = mags[m].second;
+                        bx = fx;
+                        by = fy;
+                        bcv = fcv;
+                        if (dsearch) bdef = dz.defocus(dz.abw20(P.dvals[vk[q]]));
+                    }
+                }
+                P.bestfom = best;
+                if (won) {
+                    P.bmx = bmx;
+                    P.bmy = bmy;
+                    P.box = bx;
+                    P.boy = by;
+                    P.bestcv = bcv;
+                    P.bestdef = bdef;
+                }
+            }
+        }
+        cudaFree(d_mm);
+        cudaFree(d_msec);
+        cudaFree(d_mctf);
+        cudaFree(d_mrec);
+        return r;
+    };
 
     for (long c0 = 0; c0 < nstart && rc == BSG_OK; c0 += chunk) {
         const long c1 = std::min(nstart, c0 + chunk);
@@ -614,6 +875,7 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
                 if (!(P.alpha >= accuracy) || ++P.rounds >= MAX_ROUNDS) P.done = true;
             }
         }
+        if (rc == BSG_OK && !mags.empty()) rc = mag_stage(c0, c1);
     }
     cudaFree(d_rctf);
     cudaFree(d_rrec);
@@ -637,6 +899,10 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
         o[7] = P.bestcv;
         o[8] = (double)P.number;
         o[9] = 0;
+        // part->pixel_size = refined sampling x the cut scale (part_refine_orientation,
+        // mg_refine.cpp:633): the particle's pixel size after the magnification stage
+        o[10] = (mag_samp * P.bmx) * M->cut_scale;
+        o[11] = (mag_samp * P.bmy) * M->cut_scale;
         if (dsearch) {
             // the final defocus check (:1186-1191), read back through the CTF
             const DefocusTerm dz(M->h_volt[P.img]);

@@ -17,8 +17,10 @@
 //   -output out.star          output project
 //   -batch 4096  -device 0
 //   -fomtype frc|dpr          figure of merit (brefine.cpp:124-127: the first letter decides)
-// Not supported (rejected): -monte, -symmetry, -magnification, -mask, -FSC,
-// -edge.
+//   -magnification 0.01       magnification search: per-axis pixel-size factors 1 +- m
+//                             (img_refine_grid's second stage); the refined pixel
+//                             sizes x, y are written with the particle
+// Not supported (rejected): -monte, -symmetry, -mask, -FSC, -edge.
 //
 // Flow as project_refine_orientations / part_refine_orientation
 // (bsoft/src/mg/mg_refine.cpp:249-457, 491-648): one reference preparation,
@@ -43,7 +45,7 @@ struct Options {
     std::string reference, output;
     double alpha = 0, accuracy = 0.5 * M_PI / 180.0;   // radians (brefine.cpp:80)
     double shift_step = 0.4, shift_accuracy = 0.1;
-    double def_std = 0, hi_res = 0, lo_res = 0;
+    double def_std = 0, hi_res = 0, lo_res = 0, max_mag = 0;
     int kernel_w = 8, kernel_p = 2, select = -1, batch = 4096, device = 0, fom_type = 0;
     bool contrast = false, all = false;
     std::vector<std::string> inputs;
@@ -89,6 +91,9 @@ Options parse(int argc, char** argv) {
             const std::string v = val();
             if (!v.empty() && v[0] == 'f') o.fom_type = 0;
             if (!v.empty() && v[0] == 'd') o.fom_type = 1;
+        } else if (a == "-magnification") {
+            o.max_mag = atof(val().c_str());
+            if (o.max_mag < 0) throw std::runtime_error("-magnification: a maximum magnification adjustment must be specified");
         } else if (a == "-contrast") o.contrast = true;
         else if (a == "-select") o.select = atoi(val().c_str());
         else if (a == "-all") o.all = true;
@@ -183,7 +188,7 @@ int main(int argc, char** argv) {
                 CALL(bsg_match_set_images(m, imgs.data(), (long)cnt, ctf.data(), h.mean(), h.stddev(), 0));
                 std::vector<double> out(cnt * BSG_MATCH_REFINE_RESULT_DOUBLES);
                 CALL(bsg_match_refine(m, start.data(), (long)cnt, o.alpha, o.accuracy, o.shift_step, o.shift_accuracy,
-                                      o.def_std, out.data(), o.fom_type == 1 ? BSG_MATCH_SCORE_DPR : 0));
+                                      o.def_std, o.max_mag, out.data(), o.fom_type == 1 ? BSG_MATCH_SCORE_DPR : 0));
                 for (size_t j = 0; j < cnt; ++j) {
                     const long i = sel[b0 + j];
                     const double* r = &out[j * BSG_MATCH_REFINE_RESULT_DOUBLES];
@@ -192,6 +197,10 @@ int main(int argc, char** argv) {
                     fom[mi][i] = r[6];
                     fcv[mi][i] = r[7];
                     if (o.def_std > 0 && r[9] > 1) mg.defocus[i] = r[9];
+                    if (o.max_mag > 0) {
+                        mg.pixel[i] = r[10];
+                        mg.pixel_y[i] = r[11];
+                    }
                 }
                 done += (long)cnt;
             }

@@ -411,6 +411,7 @@ struct Micrograph {
     Ctf ctf;
     std::vector<long> part_id;
     std::vector<double> ox, oy, vx, vy, vz, va, defocus, mag, pixel;
+    std::vector<double> pixel_y;     // particle pixel size along y (the x one where the file has none)
     std::vector<long> select;
 };
 
@@ -501,6 +502,9 @@ inline std::vector<Micrograph> read_project(const std::string& path) {
                                                                      : col("particle.pixel_size", 0);
         for (auto& p : mg.pixel)
             if (!(p > 0)) p = mg.pixel_size;
+        mg.pixel_y = (lp && lp->index("particle.pixel_size_y") >= 0) ? col("particle.pixel_size_y", 0) : mg.pixel;
+        for (size_t r = 0; r < mg.pixel_y.size(); ++r)
+            if (!(mg.pixel_y[r] > 0)) mg.pixel_y[r] = mg.pixel[r];
         // read_project post-processing (rwmg.cpp:650-659): an origin further
         // than box_x/4 from the box centre (integer halves, z included) is
         // reset to the centre; then origin z = 0
@@ -629,12 +633,14 @@ inline void write_project(const std::string& path, const std::vector<Micrograph>
         }
         const bool has_fom = m < fom.size() && !fom[m].empty();
         fprintf(f, "\nloop_\n_particle.id\n_particle.defocus\n_particle.magnification\n_particle.pixel_size_x\n"
+                   "_particle.pixel_size_y\n"
                    "_particle.origin_x\n_particle.origin_y\n_particle.origin_z\n_particle.view_x\n_particle.view_y\n"
                    "_particle.view_z\n_particle.view_angle\n_particle.select\n");
         if (has_fom) fprintf(f, "_particle.fom\n_particle.fom_crossvalidation\n");
         for (size_t i = 0; i < mg.part_id.size(); ++i) {
-            fprintf(f, "%ld %.17g %.17g %.17g %.17g %.17g 0 %.17g %.17g %.17g %.17g %ld", mg.part_id[i], mg.defocus[i],
-                    mg.mag[i], mg.pixel[i], mg.ox[i], mg.oy[i], mg.vx[i], mg.vy[i], mg.vz[i],
+            const double py = i < mg.pixel_y.size() ? mg.pixel_y[i] : mg.pixel[i];
+            fprintf(f, "%ld %.17g %.17g %.17g %.17g %.17g %.17g 0 %.17g %.17g %.17g %.17g %ld", mg.part_id[i],
+                    mg.defocus[i], mg.mag[i], mg.pixel[i], py, mg.ox[i], mg.oy[i], mg.vx[i], mg.vy[i], mg.vz[i],
                     mg.va[i] * 180.0 / M_PI, mg.select[i]);
             if (has_fom) fprintf(f, " %.17g %.17g", fom[m][i], fom_cv[m][i]);
             fprintf(f, "\n");

@@ -146,19 +146,23 @@ class Matcher:
         return fom, cv
 
     def refine(self, start, alpha_step: float, accuracy: float, shift_step: float = 0.4,
-               shift_accuracy: float = 0.1, def_std: float = 0.0, dpr: bool = False) -> np.ndarray:
+               shift_accuracy: float = 0.1, def_std: float = 0.0, dpr: bool = False,
+               max_mag: float = 0.0) -> np.ndarray:
         """img_refine_grid for every start record (n, 7): image index, view
         x, y, z, angle (radians), origin x, y (particle pixels).  Angular
         step and accuracy in radians, shift step and accuracy in pixels of
         the cut transform (the reference's arguments); def_std > 0 adds
-        brefine's defocus search (angstrom).  Returns (n, 10): view x, y, z,
+        brefine's defocus search (angstrom); max_mag > 0 its magnification
+        search (brefine -magnification).  Returns (n, 12): view x, y, z,
         angle, origin x, y, figure of merit, cross-validation figure,
-        hypotheses scored, defocus (0 without the search).  dpr scores with
-        the DPR figure of merit (brefine -fomtype dpr)."""
+        hypotheses scored, defocus (0 without the search), pixel size x, y
+        after refinement.  dpr scores with the DPR figure of merit (brefine
+        -fomtype dpr)."""
         s = np.ascontiguousarray(start, dtype=np.float64).reshape(-1, _lib.MATCH_REFINE_START_DOUBLES)
         out = np.empty((len(s), _lib.MATCH_REFINE_RESULT_DOUBLES))
         _lib.check(_lib.load().bsg_match_refine(self._h, _dp(s), len(s), float(alpha_step), float(accuracy),
-                                                float(shift_step), float(shift_accuracy), float(def_std), _dp(out),
+                                                float(shift_step), float(shift_accuracy), float(def_std),
+                                                float(max_mag), _dp(out),
                                                 _lib.MATCH_SCORE_DPR if dpr else 0), "bsg_match_refine")
         return out
 

@@ -43,6 +43,7 @@ class Micrograph:
     magnification: np.ndarray      # (n,)
     select: np.ndarray             # (n,) int
     pixel: np.ndarray              # (n,) particle pixel size (angstrom)
+    pixel_y: np.ndarray | None = None   # (n,) along y, where it differs from x (brefine -magnification)
 
     @property
     def n(self) -> int:
@@ -139,6 +140,10 @@ def read_project(path: str) -> Project:
         if lp is not None and lp.index("particle.pixel_size_x") < 0:
             pix = col("particle.pixel_size", 0.0)
         pix = np.where(pix > 0, pix, mg_pixel)
+        pix_y = None
+        if lp is not None and lp.index("particle.pixel_size_y") >= 0:
+            pix_y = col("particle.pixel_size_y", 0.0)
+            pix_y = np.where(pix_y > 0, pix_y, pix)
         # read_project post-processing (rwmg.cpp:650-659): an origin further
         # than box_x/4 (integer division) from box/2 (integer halves, z
         # included) is reset to box/2; then origin z = 0.
@@ -150,7 +155,7 @@ def read_project(path: str) -> Project:
         mg = Micrograph(id=str(mgid), particle_file=pfile, box_size=box, pixel_size=mg_pixel,
                         ctf=_ctf_from_block(b), part_id=ids, origin=origin, view=view,
                         defocus=col("particle.defocus"), magnification=col("particle.magnification"),
-                        select=col("particle.select", 1, int).astype(np.int64), pixel=pix)
+                        select=col("particle.select", 1, int).astype(np.int64), pixel=pix, pixel_y=pix_y)
         proj.micrographs.append(mg)
     if not proj.micrographs:
         raise ValueError(f"{path}: no micrograph blocks found")
@@ -184,7 +189,8 @@ def write_project(path: str, proj: Project) -> None:
                             "particle.view_angle", "particle.select"])
         for i in range(mg.n):
             lp.rows.append([int(mg.part_id[i]), float(mg.defocus[i]), float(mg.magnification[i]),
-                            float(mg.pixel[i]), float(mg.pixel[i]), float(mg.pixel[i]),
+                            float(mg.pixel[i]), float(mg.pixel[i] if mg.pixel_y is None else mg.pixel_y[i]),
+                            float(mg.pixel[i]),
                             float(mg.origin[i, 0]), float(mg.origin[i, 1]), float(mg.origin[i, 2]),
                             float(mg.view[i, 0]), float(mg.view[i, 1]), float(mg.view[i, 2]),
                             float(mg.view[i, 3] * 180.0 / math.pi), int(mg.select[i])])

@@ -417,14 +417,22 @@ void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
  * out: nstart records of BSG_MATCH_REFINE_RESULT_DOUBLES doubles: view x,
  * y, z, angle, origin x, y (pixels of the particle image), figure of merit,
  * cross-validation figure, hypotheses scored (the reference's `number`),
- * defocus after refinement (angstrom; 0 without the defocus search).
+ * defocus after refinement (angstrom; 0 without the defocus search),
+ * particle pixel size x, y after refinement (angstrom: the refined sampling
+ * of the cut transform times the cut scale, part_refine_orientation,
+ * mg_refine.cpp:633).
+ * max_mag in (0, 1): brefine -magnification: after the angular rounds,
+ * img_refine_grid's magnification stage (mg_refine.cpp:1145-1187) fits the
+ * best view at every pair of per-axis sampling factors 1 - max_mag ..
+ * 1 + max_mag (steps max_mag / 10, y outer; 441 pairs) with shift steps
+ * 0.4 -> 0.1 around the best origin, and keeps the best fit; 0: none.
  * flags: BSG_MATCH_SCORE_DPR scores with the DPR figure of merit (brefine
- * -fomtype dpr).  The magnification search (max_mag > 0) is not part of
- * this call. */
+ * -fomtype dpr). */
 #define BSG_MATCH_REFINE_START_DOUBLES 7
-#define BSG_MATCH_REFINE_RESULT_DOUBLES 10
+#define BSG_MATCH_REFINE_RESULT_DOUBLES 12
 int  bsg_match_refine(bsg_match* m, const double* start, long nstart, double alpha_step, double accuracy,
-                      double shift_step, double shift_accuracy, double def_std, double* out, int flags);
+                      double shift_step, double shift_accuracy, double def_std, double max_mag, double* out,
+                      int flags);
 
 /* ---- learned orientation proposer ------------------------------------------
  * No counterpart in the reference.  A convolutional network maps a particle

@@ -96,11 +96,13 @@ def _write_refine_project(d, tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("fomtype", ["frc", "dpr"])
+@pytest.mark.parametrize("fomtype", ["frc", "dpr", "mag"])
 @pytest.mark.parametrize("case", ["refine64", "refine32", "refine64ctf"])
 def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
     """The drop-in brefine against the reference's img_refine_grid, with the
-    FRC figure of merit (refine*.npz) and with -fomtype dpr (refine_dpr.npz)."""
+    FRC figure of merit (refine*.npz), with -fomtype dpr (refine_dpr.npz)
+    and with -magnification (refine_mag.npz: the refined pixel sizes x, y
+    are written with the particles)."""
     import math
     from bsoft_b200.project import read_project
     from tests.refine_helpers import GOLDEN, load
@@ -115,15 +117,25 @@ def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
         args[1:1] = ["-defocus", repr(d["def_std"])]
     if fomtype == "dpr":
         args[1:1] = ["-fomtype", "dpr"]
+    zmag = np.load(os.path.join(GOLDEN, "refine_mag.npz"))
+    if fomtype == "mag":
+        args[1:1] = ["-magnification", repr(float(zmag[case + "_max_mag"]))]
     subprocess.run(args, capture_output=True, text=True, check=True)
     proj = read_project(out)
-    ref = d["result"] if fomtype == "frc" else np.load(os.path.join(GOLDEN, "refine_dpr.npz"))[case]
+    ref = {"frc": d["result"], "dpr": np.load(os.path.join(GOLDEN, "refine_dpr.npz"))[case], "mag": zmag[case]}[fomtype]
     for i, mg in enumerate(proj.micrographs):
         v = mg.view[0]
         assert np.abs(v[:3] - ref[i, :3]).max() < 1e-9 and abs(v[3] - ref[i, 3]) < 1e-9, (i, v, ref[i, :4])
         assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 1e-9
         if d["def_std"] > 0:
             assert abs(mg.defocus[0] - ref[i, 9]) < 1e-6 * ref[i, 9]
+        if fomtype == "mag":
+            # the probe prints the cut transform's sampling; the project holds
+            # it times the cut scale
+            # it times the cut scale D / n (D: the cut transform's edge)
+            cut_x, cut_y = mg.pixel[0] / ref[i, 10], mg.pixel_y[0] / ref[i, 11]
+            assert abs(cut_x - cut_y) < 1e-12 and 0 < cut_x <= 1
+            assert abs(cut_x * d["n"] - round(cut_x * d["n"])) < 1e-9
 
 
 @pytest.mark.gpu

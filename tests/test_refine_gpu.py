@@ -64,6 +64,32 @@ def test_dpr_matches_reference(setup):
     assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
 
 
+def test_magnification_matches_reference(setup):
+    """brefine -magnification: the angular rounds, then img_refine_grid's
+    magnification stage over 21 x 21 per-axis sampling factors, against the
+    reference's img_refine_grid with max_mag > 0 (tests/golden/
+    refine_mag.npz, make_refine_mag_golden.py): same hypotheses, views,
+    origins, defocus and refined sampling.  The probe prints the sampling of
+    the cut transform; the result holds it times the cut scale."""
+    import os
+    from tests.refine_helpers import GOLDEN
+    m, d = setup
+    z = np.load(os.path.join(GOLDEN, "refine_mag.npz"))
+    ref, max_mag = z[d["case"]], float(z[d["case"] + "_max_mag"])
+    out = _refine(m, d, max_mag=max_mag)
+    assert np.array_equal(out[:, 8], ref[:, 8]), (out[:, 8], ref[:, 8])
+    assert np.abs(out[:, :4] - ref[:, :4]).max() < 1e-12
+    assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9
+    assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
+    assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+    assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
+    cut = float(np.float64(np.longdouble(m.diam) / np.longdouble(d["n"])))
+    assert np.abs(out[:, 10:12] - ref[:, 10:12] * cut).max() < 1e-12 * d["pixel"]
+    # without the search the pixel size is the particle's own
+    plain = _refine(m, d)
+    assert np.abs(plain[:, 10:12] - d["pixel"]).max() < 1e-12 * d["pixel"]
+
+
 def test_batch_invariant_and_repeated_images(setup):
     m, d = setup
     whole = _refine(m, d)
