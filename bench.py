@@ -510,7 +510,9 @@ def search_leg(args, local, dist, world, rank, torch):
                 device=local)
     m.set_reference(sw["volume"], (SEARCH_BOX // 2,) * 3)
     m.set_panel(mats)
-    panel_ms = m.stats()["panel_ms"]
+    pst = m.stats()
+    panel_ms = pst["panel_ms"]
+    panel_exact = {"ms": round(pst["panel_exact_ms"], 1), "gb": round(pst["panel_exact_bytes"] / 1e9, 2)}
     host = [torch.from_numpy(np.ascontiguousarray(imgs[i * B:(i + 1) * B])).pin_memory() for i in range(2)]
     dev = [h.cuda() for h in host]
     s = torch.cuda.ExternalStream(m.stream)
@@ -736,6 +738,8 @@ def search_leg(args, local, dist, world, rank, torch):
                      "flops_per_hypothesis": 2 * st["coarse_k"], "gemm_ms": round(st["gemm_ms"], 2)},
         "stages_ms": {k: round(st[k], 2) for k in ("agen_ms", "gemm_ms", "merge_ms", "rescore_ms")},
         "panel_ms": round(panel_ms, 1),
+        "panel_exact_sections": {**panel_exact, "what": "the panel's FP32 sections at the figure-of-merit pixels, "
+                                 "built once with the panel; the exact rescoring reads them"},
         "accuracy": {"median_angular_error_deg": round(float(np.median(errs)), 3),
                      "frac_within_5_deg": round(float(np.mean(errs < 5)), 4)},
         "cpu_baseline": cpu, "gpu_launches": int(st["launches"]), "clocks": clk.summary(),

@@ -46,7 +46,8 @@ class MatchStats(C.Structure):
                 ("gemm_flops", C.c_double),
                 ("hypotheses", C.c_double), ("launches", C.c_long), ("gemm_launches", C.c_long),
                 ("images", C.c_long), ("rescored", C.c_long), ("coarse_k", C.c_int), ("kpad", C.c_int),
-                ("refine_ms", C.c_double), ("refine_launches", C.c_long)]
+                ("refine_ms", C.c_double), ("refine_launches", C.c_long),
+                ("panel_exact_ms", C.c_double), ("panel_exact_bytes", C.c_double)]
 
 
 class BackprojConfig(C.Structure):
@@ -73,6 +74,7 @@ MATCH_REFINE_START_DOUBLES = 7
 MATCH_SCORE_FP64 = 4
 MATCH_SCORE_DPR = 8
 MATCH_REFINE_RESULT_DOUBLES = 12
+MATCH_PANEL_GATHER = 1
 
 
 class BsgError(RuntimeError):

@@ -357,6 +357,7 @@ struct FomArgs {
     double* fom;             // per group x MAXORG
     double* cv;
     const double2* sec;      // gathered sections (npix per view, FP64), or null: gather here
+    const float2* psec;      // FP32 panel sections (npix per panel view, row H.sec; T = float), or null
     int dpr;                 // 1: the DPR form (fom_type 1) instead of the FRC
 };
 
@@ -385,7 +386,13 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
     for (int base = warp * 32; base < a.npix; base += FOM_WARPS * 32) {
         T Rx = 0, Ry = 0;
         const int cnt = min(32, a.npix - base);
-        if (a.sec) {                                      // section gathered once per view
+        if (a.psec) {                                     // the panel's FP32 section, gathered once
+            if (lane < cnt) {
+                const float2 r = a.psec[(long)H.sec * a.npix + base + lane];
+                Rx = (T)r.x;
+                Ry = (T)r.y;
+            }
+        } else if (a.sec) {                               // section gathered once per view
             if (lane < cnt) {
                 const double2 r = a.sec[(long)H.sec * a.npix + base + lane];
                 Rx = (T)r.x;
@@ -750,7 +757,7 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
                     M->d_hyp, M->d_out, M->d_full, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
                     M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_rots, M->d_gA, M->d_slopes,
                     M->d_lprop, M->d_lorg, M->d_nlorg, M->d_lcand, M->d_lcount,
-                    M->d_status};
+                    M->d_status, M->d_pexact};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);
     if (M->ref_tex) cudaDestroyTextureObject(M->ref_tex);
@@ -777,6 +784,12 @@ extern "C" int bsg_match_set_reference(bsg_match* h, const float* map, const dou
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !map || !origin) return mfail(BSG_ERR_ARG, "bsg_match_set_reference: null argument");
     MCK(cudaSetDevice(M->device));
+    // the panel's exact sections belong to the previous map
+    if (M->d_pexact) {
+        cudaStreamSynchronize(M->stream);
+        cudaFree(M->d_pexact);
+        M->d_pexact = nullptr;
+    }
     const int N = M->N, D = M->D;
     const size_t n3 = (size_t)N * N * N;
     int rc = ensure_work(*M, n3);
@@ -924,6 +937,56 @@ cudaError_t launch_secgather(const Match& M, const double* d_mats, long nv, doub
     return cudaGetLastError();
 }
 
+// The panel's FP32 sections at the figure-of-merit pixels: one CTA per view,
+// the pixels in the warp-strided blocks of 32 that fom_kernel<float> walks,
+// each gathered by the whole warp with the same coordinates and the same
+// FP32 FSI gather, so the stored values are the ones fom_kernel<float> would
+// compute for that view.
+__global__ void __launch_bounds__(FOM_WARPS * 32) panel_exact_kernel(cudaTextureObject_t tex, int D,
+                                                                   const float* __restrict__ lut_g, int wd,
+                                                                   const MPix* __restrict__ pix, int npix,
+                                                                   const MHyp* __restrict__ secs, double inv,
+                                                                   double real, float2* __restrict__ out) {
+    __shared__ float lut[(NDIV + 1) * MAXW];
+    for (int i = threadIdx.x; i < (NDIV + 1) * wd; i += blockDim.x) lut[i] = lut_g[i];
+    __syncthreads();
+    const MHyp& H = secs[blockIdx.x];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2* o = out + (size_t)blockIdx.x * npix;
+    for (int base = warp * 32; base < npix; base += FOM_WARPS * 32) {
+        float Rx = 0, Ry = 0;
+        const int cnt = min(32, npix - base);
+        for (int q = 0; q < cnt; ++q) {
+            const MPix pq = pix[base + q];
+            if (!pq.insec) continue;                      // warp-uniform
+            const double ix = pq.h * inv, iy = pq.k * inv;
+            const double mx = (H.m[0] * ix + H.m[1] * iy) * real;
+            const double myy = (H.m[3] * ix + H.m[4] * iy) * real;
+            const double mz = (H.m[6] * ix + H.m[7] * iy) * real;
+            float vr, vi;
+            fsi_gather<float>(TexSrc{tex}, D, mx, myy, mz, lut, wd, lane, vr, vi);
+            if (lane == q) {
+                Rx = vr;
+                Ry = vi;
+            }
+        }
+        if (lane < cnt) o[base + lane] = make_float2(Rx, Ry);
+    }
+}
+
+cudaError_t launch_panel_exact(const Match& M, const MHyp* d_secs, long nsec, float2* d_out, cudaStream_t s) {
+    const long npix = (long)M.h_pix.size();
+    for (long v0 = 0; v0 < nsec; v0 += 1L << 20) {
+        const long cnt = std::min(nsec - v0, 1L << 20);
+        panel_exact_kernel<<<(unsigned)cnt, FOM_WARPS * 32, 0, s>>>(M.ref_tex, M.D, M.d_lutf, M.wd, M.d_pix, (int)npix,
+                                                                   d_secs + v0, 1.0 / M.real_map, M.real_map,
+                                                                   d_out + (size_t)v0 * npix);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, float* d_out, cudaStream_t s) {
     if (nrec > 0)
         ctf_rows_kernel<<<(unsigned)nrec, 256, 0, s>>>(d_rec, M.d_pix, (int)M.h_pix.size(), 1.0 / M.real_img, d_out);
@@ -931,9 +994,10 @@ cudaError_t launch_ctf_rows(const Match& M, const ImgCtf* d_rec, long nrec, floa
 }
 
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
-                       bool fp64, const float* ctf_table, const double2* sec, bool dpr) {
+                       bool fp64, const float* ctf_table, const double2* sec, bool dpr, const float2* psec) {
     FomArgs a{};
     a.dpr = dpr ? 1 : 0;
+    a.psec = fp64 ? nullptr : psec;
     a.tex = M.ref_tex; a.D = M.D; a.wd = M.wd; a.lut = M.d_lutf; a.lutd = M.d_lut;
     a.pix = M.d_pix; a.npix = (int)M.h_pix.size(); a.hyps = d_groups;
     a.spec = M.d_spec; a.ctf = ctf_table ? ctf_table : M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;

@@ -234,6 +234,8 @@ struct Match {
     std::vector<MHyp> h_secs;          // host copy
     float* d_rots = nullptr;           // panel rotations (unscaled, float) for local selection
     __nv_bfloat16* d_panel = nullptr;  // nsec x kpad
+    float2* d_pexact = nullptr;        // nsec x npix: the panel's FP32 sections at the figure-of-merit
+                                       // pixels, as fom_kernel<float> gathers them (rescoring reads them)
     __nv_bfloat16* d_A = nullptr;      // rows x kpad
     size_t a_elems = 0;
     float* d_pscore = nullptr;         // partial top-8 per (range, row)
@@ -265,7 +267,11 @@ struct Match {
 // the DPR figure of merit instead of the FRC
 cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d_fom, double* d_cv, cudaStream_t s,
                        bool fp64 = false, const float* ctf_table = nullptr, const double2* sec = nullptr,
-                       bool dpr = false);
+                       bool dpr = false, const float2* psec = nullptr);
+// FP32 sections of nsec panel views at the figure-of-merit pixels, gathered
+// as fom_kernel<float> gathers them: nsec x npix float2 (0 where a pixel is
+// outside the section)
+cudaError_t launch_panel_exact(const Match& M, const MHyp* d_secs, long nsec, float2* d_out, cudaStream_t s);
 // FP64 section values of nv views (9 doubles each, MHyp's scaled rows) at
 // the figure-of-merit pixels: nv x npix double2
 cudaError_t launch_secgather(const Match& M, const double* d_mats, long nv, double2* d_out, cudaStream_t s);

@@ -721,6 +721,7 @@ static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<dou
                 memcpy(ng.m, M->h_secs[csec[c]].m, sizeof(ng.m));
                 ng.img = (int)i;
                 ng.ctf = (int)i;
+                ng.sec = csec[c];          // row of the panel's exact sections
                 groups.push_back(ng);
                 gsec.push_back(csec[c]);
             }
@@ -743,7 +744,9 @@ static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<dou
         cudaEventCreate(&e1);
         e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
         cudaEventRecord(e0, s);
-        if (e == cudaSuccess) e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s);
+        if (e == cudaSuccess)
+            e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, false, nullptr, nullptr, false,
+                           M->d_pexact);
         cudaEventRecord(e1, s);
         if (e == cudaSuccess) e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -784,7 +787,6 @@ static cudaError_t rescore_candidates(Match& Mr, int topk, const std::vector<dou
 using namespace bsg;
 
 extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, int flags) {
-    (void)flags;
     Match* M = reinterpret_cast<Match*>(h);
     if (!M || !mats || nsec < 1) return match_fail(BSG_ERR_ARG, "bsg_match_set_panel: bad argument");
     if (!M->have_ref) return match_fail(BSG_ERR_STATE, "bsg_match_set_panel: set the reference first");
@@ -807,6 +809,7 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     cudaFree(M->d_cpix); M->d_cpix = nullptr;
     cudaFree(M->d_cstart); M->d_cstart = nullptr;
     cudaFree(M->d_rots); M->d_rots = nullptr;
+    cudaFree(M->d_pexact); M->d_pexact = nullptr;
     M->nsec = 0;
     std::vector<MHyp> sv(nsec);
     for (long v = 0; v < nsec; ++v) {
@@ -850,6 +853,37 @@ extern "C" int bsg_match_set_panel(bsg_match* h, const double* mats, long nsec, 
     M->h_secs.swap(sv);
     M->sstats.panel_ms += ms;
     M->sstats.launches += (nsec + (1L << 20) - 1) >> 20;
+    // the panel's FP32 sections at the figure-of-merit pixels, kept for the
+    // exact rescoring when they fit with 8 GB to spare (else the rescoring
+    // gathers them per candidate)
+    if (!(flags & BSG_MATCH_PANEL_GATHER)) {
+        const size_t bytes = sizeof(float2) * (size_t)nsec * M->h_pix.size();
+        size_t freeb = 0, total = 0;
+        if (cudaMemGetInfo(&freeb, &total) == cudaSuccess && bytes + (8ull << 30) < freeb &&
+            cudaMalloc(&M->d_pexact, bytes) == cudaSuccess) {
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, s);
+            e = launch_panel_exact(*M, M->d_secs, nsec, M->d_pexact, s);
+            cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            float xms = 0;
+            cudaEventElapsedTime(&xms, e0, e1);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (e != cudaSuccess) {
+                cudaFree(M->d_pexact);
+                M->d_pexact = nullptr;
+                return match_fail(BSG_ERR_CUDA, "bsg_match_set_panel: exact sections: %s", cudaGetErrorString(e));
+            }
+            M->sstats.panel_exact_ms += xms;
+            M->sstats.panel_exact_bytes = (double)bytes;
+            M->sstats.launches += (nsec + (1L << 20) - 1) >> 20;
+        } else {
+            cudaGetLastError();     // a failed allocation leaves no sticky error; clear the last one
+            M->sstats.panel_exact_bytes = 0;
+        }
+    }
     return BSG_OK;
 }
 

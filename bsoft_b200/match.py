@@ -168,10 +168,13 @@ class Matcher:
 
 
     # ---- exhaustive search ----
-    def set_panel(self, mats) -> None:
-        """Search panel of central sections for row-major view matrices (nsec, 3, 3)."""
+    def set_panel(self, mats, exact_sections: bool = True) -> None:
+        """Search panel of central sections for row-major view matrices (nsec,
+        3, 3).  exact_sections keeps the panel's FP32 sections for the exact
+        rescoring (when they fit); False makes the rescoring gather them."""
         m = np.ascontiguousarray(mats, dtype=np.float64).reshape(-1, 9)
-        _lib.check(_lib.load().bsg_match_set_panel(self._h, _dp(m), len(m), 0), "bsg_match_set_panel")
+        flags = 0 if exact_sections else _lib.MATCH_PANEL_GATHER
+        _lib.check(_lib.load().bsg_match_set_panel(self._h, _dp(m), len(m), flags), "bsg_match_set_panel")
         self.nsec = len(m)
 
     def search(self, origins, topk: int = 8) -> np.ndarray:

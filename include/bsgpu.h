@@ -346,7 +346,11 @@ int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, d
  * bsg_match_set_panel: the search panel for nsec views (row-major matrices):
  * the central section of each at the coarse pixels (Hermitian half plane,
  * shells 1 .. ceil(max_rad) - 1), every shell normalised to unit power,
- * stored as BF16 (nsec x ~2 npix/2 x 2 bytes on the device).
+ * stored as BF16 (nsec x ~2 npix/2 x 2 bytes on the device).  Unless flags
+ * has BSG_MATCH_PANEL_GATHER, the panel's FP32 sections at the
+ * figure-of-merit pixels are kept too (nsec x npix x 8 bytes, when they fit
+ * with 8 GB to spare): the exact rescoring then reads them instead of
+ * gathering every candidate's section, with the same values.
  *
  * bsg_match_search: every held image at each of norigin trial origins
  * (origins: norigin x 2 doubles, pixels of the particle image) against every
@@ -360,6 +364,7 @@ int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, d
  * cross-validation figure (section -1 if fewer candidates exist). */
 #define BSG_MATCH_RESULT_DOUBLES 5
 #define BSG_MATCH_TOPK_MAX 8
+#define BSG_MATCH_PANEL_GATHER 1
 int  bsg_match_set_panel(bsg_match* m, const double* mats, long nsec, int flags);
 int  bsg_match_search(bsg_match* m, const double* origins, int norigin, int topk, double* out, int flags);
 /* The same scoring restricted to the neighbourhood of a proposal per held
@@ -390,6 +395,8 @@ typedef struct {
     int    kpad;           /* K padded to the 64-element stage width        */
     double refine_ms;      /* grid refinement: figure-of-merit launches     */
     long   refine_launches;
+    double panel_exact_ms; /* the panel's FP32 sections for the rescoring  */
+    double panel_exact_bytes;  /* their device bytes (0: not kept)          */
 } bsg_match_stats;
 int  bsg_match_get_stats(bsg_match* m, bsg_match_stats* st);
 int  bsg_match_reset_stats(bsg_match* m);

@@ -134,6 +134,26 @@ def test_rescored_figure_of_merit(setup):
     assert np.all(np.diff(res[:, :, 3], axis=1) <= 0)     # best first
 
 
+def test_rescoring_reads_the_panels_exact_sections(setup):
+    """The panel keeps its FP32 sections at the figure-of-merit pixels and
+    the rescoring reads them: the search gives the same records, to the
+    bit, as with the sections gathered per candidate, and the local search
+    too."""
+    m, d, mats, origins, ctf, res, ref = setup
+    assert m.stats()["panel_exact_bytes"] > 0
+    m.set_panel(mats, exact_sections=False)
+    try:
+        gathered = m.search(origins, topk=8)
+        props = np.zeros((len(d["images"]), 11), np.float32)
+        props[:, :9] = mats[:len(d["images"])].reshape(-1, 9)
+        props[:, 9:] = 0
+        local_g = m.search_local(props, origins, 10.0, 1.5, 8)
+    finally:
+        m.set_panel(mats)
+    assert np.array_equal(gathered, res)
+    assert np.array_equal(m.search_local(props, origins, 10.0, 1.5, 8), local_g)
+
+
 def test_generating_views_found(setup):
     """Images whose CTF is applied recover their own view and a trial
     origin within 1.5 pixels of the true one (the grid step is 1 pixel and
