@@ -18,9 +18,10 @@
 // K = 9 x input channels, N = output channels): forward C = X_col W^T,
 // weight gradient W' = dY^T X_col (split over M, partial sums reduced in a
 // fixed order), input gradient dX_col = dY W gathered back by col2im.  One
-// tiled FP32 GEMM kernel (128 x 64 tiles, 8 x 4 outputs per thread) serves
-// all of them.  Every reduction has a fixed order, so training is
-// bitwise reproducible for a given seed.
+// tensor-core GEMM kernel (BF16 mma.sync with the operands split into two
+// BF16 terms, FP32 accumulation, 128 x 64 tiles) serves all of them.  Every
+// reduction has a fixed order, so training is bitwise reproducible for a
+// given seed.
 #include "common.cuh"
 
 #include <cuda_bf16.h>
@@ -47,75 +48,117 @@ constexpr int NRES = 11;    // R (9, row-major) and shift (2)
 // B(n, k) = BT ? B[k * ldb + n] : B[n * ldb + k]
 // blockIdx.z splits k into `splits` ranges; with splits > 1 each range
 // writes its own partial product C + z * M * N (reduced afterwards).
-constexpr int GBM = 128, GBN = 64, GBK = 8;
+// On the tensor cores:
+// mma.sync m16n8k16, BF16 operands, FP32 accumulation.  Every FP32 operand
+// value v is split into hi = bf16(v) and lo = bf16(v - hi) while its tile is
+// staged in shared memory, and each 16-deep step adds Ahi Bhi + Ahi Blo +
+// Alo Bhi (the lo x lo term is below 2^-16 of the product), so a product
+// keeps ~17 significant bits and the weights, which are BF16 values already,
+// enter exactly (their lo parts are zero).  Block tile 128 x 64, eight warps
+// of 32 x 32 (2 x 4 mma tiles); shared rows of 24 BF16 (12 words) so the
+// fragment loads of the 8 row groups x 4 lanes fall on distinct banks.  The
+// mma accumulation order is fixed, so results are bitwise reproducible.
+constexpr int TBM = 128, TBN = 64, TBK = 16, TROW = 24;
+
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
 
 template <bool AT, bool BT>
-__global__ void __launch_bounds__(256) sgemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
+__global__ void __launch_bounds__(256) tgemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
                                                     const float* __restrict__ B, int ldb, float* __restrict__ C,
                                                     int splits, int accumulate) {
-    __shared__ float As[GBK][GBM + 4];
-    __shared__ float Bs[GBK][GBN + 4];
-    const int tid = threadIdx.x;
-    const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
+    __shared__ __align__(16) __nv_bfloat16 Ah[TBM * TROW], Al[TBM * TROW], Bh[TBN * TROW], Bl[TBN * TROW];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * TBN;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
     const int kper = (K + splits - 1) / splits;
     const int kb = blockIdx.z * kper, ke = min(K, kb + kper);
-    const int ty = tid / 16, tx = tid % 16;          // 16 x 16 threads: 8 rows x 4 cols each
-    float acc[8][4];
+    float acc[2][4][4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-    for (int k0 = kb; k0 < ke; k0 += GBK) {
-        // A tile: GBM x GBK = 1024 values, 4 per thread
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+    for (int k0 = kb; k0 < ke; k0 += TBK) {
+        // A tile: TBM x TBK = 2048 values, 8 per thread
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
             const int idx = tid + r * 256;
             int mm, kk;
-            if (AT) { kk = idx / GBM; mm = idx % GBM; } else { mm = idx / GBK; kk = idx % GBK; }
+            if (AT) { kk = idx / TBM; mm = idx % TBM; } else { mm = idx / TBK; kk = idx % TBK; }
             const int gm = m0 + mm, gk = k0 + kk;
             float v = 0.f;
             if (gm < M && gk < ke) v = AT ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
-            As[kk][mm] = v;
+            split_bf16(v, Ah[mm * TROW + kk], Al[mm * TROW + kk]);
         }
-        // B tile: GBN x GBK = 512 values, 2 per thread
+        // B tile: TBN x TBK = 1024 values, 4 per thread
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
+        for (int r = 0; r < 4; ++r) {
             const int idx = tid + r * 256;
             int nn, kk;
-            if (BT) { kk = idx / GBN; nn = idx % GBN; } else { nn = idx / GBK; kk = idx % GBK; }
+            if (BT) { kk = idx / TBN; nn = idx % TBN; } else { nn = idx / TBK; kk = idx % TBK; }
             const int gn = n0 + nn, gk = k0 + kk;
             float v = 0.f;
             if (gn < N && gk < ke) v = BT ? B[(size_t)gk * ldb + gn] : B[(size_t)gn * ldb + gk];
-            Bs[kk][nn] = v;
+            split_bf16(v, Bh[nn * TROW + kk], Bl[nn * TROW + kk]);
         }
         __syncthreads();
+        uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
 #pragma unroll
-        for (int kk = 0; kk < GBK; ++kk) {
-            float a[8], b[4];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = As[kk][ty * 8 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int mt = 0; mt < 2; ++mt) {
+            const int r0 = (wm + mt * 16 + g) * TROW, r8 = r0 + 8 * TROW;
+            ah[mt][0] = *reinterpret_cast<const uint32_t*>(&Ah[r0 + 2 * t]);
+            ah[mt][1] = *reinterpret_cast<const uint32_t*>(&Ah[r8 + 2 * t]);
+            ah[mt][2] = *reinterpret_cast<const uint32_t*>(&Ah[r0 + 2 * t + 8]);
+            ah[mt][3] = *reinterpret_cast<const uint32_t*>(&Ah[r8 + 2 * t + 8]);
+            al[mt][0] = *reinterpret_cast<const uint32_t*>(&Al[r0 + 2 * t]);
+            al[mt][1] = *reinterpret_cast<const uint32_t*>(&Al[r8 + 2 * t]);
+            al[mt][2] = *reinterpret_cast<const uint32_t*>(&Al[r0 + 2 * t + 8]);
+            al[mt][3] = *reinterpret_cast<const uint32_t*>(&Al[r8 + 2 * t + 8]);
         }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const int c0 = (wn + nt * 8 + g) * TROW;
+            bh[nt][0] = *reinterpret_cast<const uint32_t*>(&Bh[c0 + 2 * t]);
+            bh[nt][1] = *reinterpret_cast<const uint32_t*>(&Bh[c0 + 2 * t + 8]);
+            bl[nt][0] = *reinterpret_cast<const uint32_t*>(&Bl[c0 + 2 * t]);
+            bl[nt][1] = *reinterpret_cast<const uint32_t*>(&Bl[c0 + 2 * t + 8]);
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                mma_bf16(acc[mt][nt], ah[mt], bh[nt]);
+                mma_bf16(acc[mt][nt], ah[mt], bl[nt]);
+                mma_bf16(acc[mt][nt], al[mt], bh[nt]);
+            }
         __syncthreads();
     }
     float* Cz = C + (splits > 1 ? (size_t)blockIdx.z * M * N : 0);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int gm = m0 + ty * 8 + i;
-        if (gm >= M) continue;
+    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int gn = n0 + tx * 4 + j;
-            if (gn >= N) continue;
-            float* c = Cz + (size_t)gm * N + gn;
-            *c = (accumulate && splits == 1) ? *c + acc[i][j] : acc[i][j];
-        }
-    }
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int gm = m0 + wm + mt * 16 + g + (q >= 2 ? 8 : 0);
+                const int gn = n0 + wn + nt * 8 + 2 * t + (q & 1);
+                if (gm >= M || gn >= N) continue;
+                float* c = Cz + (size_t)gm * N + gn;
+                *c = (accumulate && splits == 1) ? *c + acc[mt][nt][q] : acc[mt][nt][q];
+            }
 }
 
 // sum of `splits` partial products into C (fixed order)
@@ -399,7 +442,7 @@ cudaError_t colsum(Cnn& c, const float* g, long M, int N, float* out, cudaStream
 
 cudaError_t gemm(Cnn& c, bool at, bool bt, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
                  float* C, int accumulate, cudaStream_t s) {
-    dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM, 1);
+    dim3 grid((N + TBN - 1) / TBN, (M + TBM - 1) / TBM, 1);
     int splits = 1;
     const long tiles = (long)grid.x * grid.y;
     if (tiles < 148 && K > 4096) {
@@ -409,10 +452,10 @@ cudaError_t gemm(Cnn& c, bool at, bool bt, int M, int N, int K, const float* A, 
     }
     grid.z = splits;
     float* out = splits > 1 ? c.d_part : C;
-    if (!at && !bt) sgemm_kernel<false, false><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
-    else if (!at && bt) sgemm_kernel<false, true><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
-    else if (at && !bt) sgemm_kernel<true, false><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
-    else sgemm_kernel<true, true><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
+    if (!at && !bt) tgemm_kernel<false, false><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
+    else if (!at && bt) tgemm_kernel<false, true><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
+    else if (at && !bt) tgemm_kernel<true, false><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
+    else tgemm_kernel<true, true><<<grid, 256, 0, s>>>(M, N, K, A, lda, B, ldb, out, splits, accumulate);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && splits > 1) {
         const long cnt = (long)M * N;
