@@ -565,6 +565,15 @@ def search_leg(args, local, dist, world, rank, torch):
     if "learned" in args.legs:
         net, train_info = train_proposer(sw, local, torch, args.train_images, args.train_epochs)
         pred = torch.empty((B, 11), dtype=torch.float32, device="cuda")
+        # the network's inference alone, one batch, after two warm-up passes
+        # (bsg_cnn_predict returns when its stream is done: wall time)
+        for _ in range(2):
+            net.predict(dev[0], out=pred)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        net.predict(dev[0], out=pred)
+        train_info["predict_ms_per_batch"] = round((time.perf_counter() - t0) * 1e3, 3)
+        train_info["predict_batch"] = B
         for i in range(nwarm):
             j = i % 2
             net.predict(dev[j], out=pred)
@@ -747,6 +756,79 @@ def search_leg(args, local, dist, world, rank, torch):
     }
 
 
+def iteration384_leg(args, local, torch):
+    """The reconstruction half of configs[4]: 384^2 particles (SNR 0.05,
+    defocus U[0.5, 4] um) inserted into two 384^3 half maps (ft 1024,
+    trilinear, CTF flip), then both halves weighed, inverse-transformed with
+    the sinc weight and their FSC computed.  Insertion is timed like the
+    main leg (device-resident images, CUDA events); the finishing (weigh,
+    3-D inverse FFT of both halves, FSC) separately.  The learned proposal
+    and local search of configs[4] are the search leg's, at 128^2."""
+    from bsoft_b200.plan import ReconPlan
+    from bsoft_b200.recon import Reconstructor
+    from bsoft_b200.synth import batched_insertion_workload
+    box, B, warm, steps = 384, args.iter_batch, 2, args.iter_steps
+    w = batched_insertion_workload(n_particles=B * (warm + steps), box=box, pool=256, snr=0.05,
+                                   defocus_range=(5000.0, 40000.0), seed=4)
+    plan = ReconPlan(n=box, ft=2 * 512, map=box, map_sampling=w["pixel"], hi_res=w["hi_res"], interp=2,
+                     ctf_action=1, wiener=0.0, params=w["params"], nmaps=3)
+    P = w["params"]
+    pool = w["pool"]
+    dev = [torch.from_numpy(np.ascontiguousarray(pool[(np.arange(B) + i * B) % pool.shape[0]])).cuda()
+           for i in range(2)]
+    rec = Reconstructor(plan, batch=B, device=local)
+    shape, shape_ms = rec.autotune(dev[0][: min(B, 256)], P[: min(B, 256)])
+    rec.set_tile_shape(shape)
+    s = torch.cuda.ExternalStream(rec.stream)
+    for i in range(warm):
+        rec.insert(dev[i % 2], P[i * B:(i + 1) * B])
+    rec.synchronize()
+    rec.reset()
+    rec.set_timing(True)
+    st0 = rec.stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0.record(s)
+        for i in range(steps):
+            j = warm + i
+            rec.insert(dev[j % 2], P[j * B:(j + 1) * B])
+        ev1.record(s)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    st1 = rec.stats()
+    out = torch.empty((box, box, box), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for h in (1, 2):
+        rec.finish(h, out=out)
+    fsc = rec.fsc()
+    torch.cuda.synchronize()
+    finish_ms = (time.perf_counter() - t0) * 1e3
+    ins_launch = st1["insert_launches"] - st0["insert_launches"]
+    ins_ms = st1["insert_ms"] - st0["insert_ms"]
+    rec.close()
+    peak, peak_kind = peaks()
+    per_particle = 22.0 * box * box
+    avg = ins_ms / max(1, ins_launch)
+    achieved = per_particle * B / (avg / 1e3) / 1e9
+    below = np.nonzero(fsc[1:] < 0.5)[0]
+    return {
+        "metric": "particles/s (insertion into two 384^3 half maps)", "value": round(B * steps / (ms / 1e3), 1),
+        "unit": "particles/s", "steps": steps, "warmup": warm, "ms_per_step": round(ms / steps, 2),
+        "config": {"workload": "iteration-384", "box": box, "ft": 1024, "map": box, "batch_per_step": B,
+                   "interp": "trilinear", "ctf": "flip", "nmaps": "two halves (+ full)", "snr": 0.05,
+                   "defocus_um": [0.5, 4.0], "l2": f"inputs larger than L2 ({B * box * box * 4 / 1e6:.0f} MB per step)"},
+        "finish_ms": {"weigh_ifft_both_halves_and_fsc": round(finish_ms, 1)},
+        "fsc_first_shell_below_0.5": int(below[0] + 1) if below.size else None,
+        "roofline": {"kernel": "grid4_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "avg_launch_ms": round(avg, 3), "algorithmic_bytes_per_particle": per_particle,
+                     "tile_shape": int(shape), "autotune_ms_per_shape": [round(float(x), 2) for x in shape_ms]},
+        "gpu_launches": int(st1["launches"] - st0["launches"]), "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -759,7 +841,9 @@ def main():
     ap.add_argument("--search-steps", type=int, default=3)
     ap.add_argument("--search-warmup", type=int, default=3)
     ap.add_argument("--search-psi", type=int, default=SEARCH_PSI)
-    ap.add_argument("--legs", default="insert,search,refine,learned")
+    ap.add_argument("--legs", default="insert,search,refine,learned,iter384")
+    ap.add_argument("--iter-batch", type=int, default=1000)
+    ap.add_argument("--iter-steps", type=int, default=5)
     ap.add_argument("--refine-images", type=int, default=512)
     ap.add_argument("--tile-shape", type=int, default=-1, help="gridding tile shape (default: autotuned)")
     ap.add_argument("--train-images", type=int, default=200000)
@@ -880,6 +964,7 @@ def main():
 
     ins = insertion_leg() if "insert" in args.legs else None
     search = search_leg(args, local, dist, world, rank, torch) if "search" in args.legs else None
+    iter384 = iteration384_leg(args, local, torch) if ("iter384" in args.legs and rank == 0) else None
 
     if rank != 0:
         if dist is not None:
@@ -937,6 +1022,9 @@ def main():
             line["gpu_launches"] = int(launches) + search["gpu_launches"] + (
                 search["learned"]["gpu_launches"] if search.get("learned") else 0) + (
                 search["refine"]["gpu_launches"] if search.get("refine") else 0)
+        if iter384 is not None:
+            line["iteration_384"] = iter384
+            line["gpu_launches"] += iter384["gpu_launches"]
     else:
         line = {"metric": search["metric"], "value": search["value"], "unit": "particles/s", "n_gpus": world,
                 "steps": search["steps"], "warmup": search["warmup"], "ms_per_step": search["ms_per_step"],
