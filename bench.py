@@ -315,7 +315,8 @@ REFINE_ALPHA, REFINE_ACC, REFINE_STEP, REFINE_SACC, REFINE_DEF = 2.0, 0.5, 0.4, 
 def refine_reference_sample(sw, start_row, ctf_row, alpha=REFINE_ALPHA, accuracy=REFINE_ACC):
     """The reference's img_refine_grid (refine_probe, one thread) on one
     particle of the search workload with the bench's shift and defocus
-    steps and the given angular steps (degrees)."""
+    steps, the given angular steps (degrees) and brefine's C_curve shell
+    weights."""
     import oracle
     from bsoft_b200.io import mrc
     exe = oracle.ref_binary("refine_probe")
@@ -331,7 +332,7 @@ def refine_reference_sample(sw, start_row, ctf_row, alpha=REFINE_ALPHA, accuracy
     r = subprocess.run([exe, os.path.join(d, "ref.mrc"), os.path.join(d, "p.mrcs"), repr(SEARCH_PIXEL),
                         repr(SEARCH_RES), os.path.join(d, "start.txt"), os.path.join(d, "ctf.txt"),
                         repr(alpha), repr(accuracy), repr(REFINE_STEP), repr(REFINE_SACC), "0",
-                        repr(REFINE_DEF)], capture_output=True, text=True)
+                        repr(REFINE_DEF), "0", "0", "1"], capture_output=True, text=True)
     dt = time.perf_counter() - t0
     if r.returncode != 0:
         return None, None, f"refine_probe failed: {r.stderr[-200:]}"
@@ -396,17 +397,27 @@ def train_proposer(sw, local, torch, n_train: int, epochs: float):
     torch.cuda.synchronize()
     data_s = time.perf_counter() - t0
     tg = torch.from_numpy(pose_targets(mats, shifts)).cuda()
-    net = Proposer(box=SEARCH_BOX, batch=256, seed=1, device=local)
     steps = int(epochs * n_train / 256)
-    t0 = time.perf_counter()
-    losses = net.train(imgs, tg, steps=steps, lr=1e-3)
-    torch.cuda.synchronize()
-    train_s = time.perf_counter() - t0
+    # two restarts (seeds 1, 2); the one with the lower training loss over its
+    # last 100 steps is kept (the training data only; some seeds settle in a
+    # worse minimum)
+    runs = []
+    for seed in (1, 2):
+        net = Proposer(box=SEARCH_BOX, batch=256, seed=seed, device=local)
+        t0 = time.perf_counter()
+        losses = net.train(imgs, tg, steps=steps, lr=1e-3)
+        torch.cuda.synchronize()
+        runs.append((float(losses[-100:].mean()), seed, net, time.perf_counter() - t0, losses))
+    runs.sort(key=lambda r: r[0])
+    for r in runs[1:]:
+        r[2].close()
+    loss_last, seed, net, train_s, losses = runs[0]
     del imgs, tg
     torch.cuda.empty_cache()
     return net, {"train_images": n_train, "epochs": epochs, "steps": steps, "params": net.nparams,
-                 "data_s": round(data_s, 2), "train_s": round(train_s, 2),
-                 "loss_first": round(float(losses[:100].mean()), 4), "loss_last": round(float(losses[-100:].mean()), 4)}
+                 "data_s": round(data_s, 2), "train_s": round(train_s, 2), "restarts": len(runs), "seed": seed,
+                 "loss_last_per_seed": {str(r[1]): round(r[0], 4) for r in runs},
+                 "loss_first": round(float(losses[:100].mean()), 4), "loss_last": round(loss_last, 4)}
 
 
 def learned_controls(m, net, mats, pviews, origins, radius, torch, n=256):
@@ -432,8 +443,10 @@ def learned_controls(m, net, mats, pviews, origins, radius, torch, n=256):
         res = m.search_local(pred, origins, radius, 1.5, 8)
         best = res[:, 0, 0].astype(int)
         start = np.column_stack([np.arange(n), pviews[best], origins[res[:, 0, 1].astype(int)]])
+        m.set_c_curve_weights()             # brefine's shell weights for the refinement
         rout = m.refine(start, REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP,
                         REFINE_SACC, REFINE_DEF)
+        m.set_shell_weights(None)
         pr = pred.cpu().numpy()[:, :9].reshape(-1, 3, 3).astype(np.float64)
         e_p = angular_distance_deg(pr, meta["mats"])
         e_l = angular_distance_deg(mats[best], meta["mats"])
@@ -609,6 +622,7 @@ def search_leg(args, local, dist, world, rank, torch):
         best = res[:R, 0, 0].astype(int)
         start = np.column_stack([np.arange(R), pviews[best], origins[res[:R, 0, 1].astype(int)]])
         m.set_images(dev[j], ctf[j * B:(j + 1) * B])
+        m.set_c_curve_weights()             # brefine's shell weights
         # radians as the reference's CLI converts degrees (atof(x) * M_PI / 180.0)
         rargs = (REFINE_ALPHA * math.pi / 180.0, REFINE_ACC * math.pi / 180.0, REFINE_STEP, REFINE_SACC, REFINE_DEF)
         m.refine(start[:16], *rargs)                                # warm-up
@@ -671,6 +685,7 @@ def search_leg(args, local, dist, world, rank, torch):
                              hi_res=SEARCH_RES, device=local)
                 m2.set_reference(sw["volume"], (SEARCH_BOX // 2,) * 3)
                 m2.set_images(sw["images"][j * B:j * B + 1], ctf[j * B:j * B + 1])
+                m2.set_c_curve_weights()
                 a1 = REFINE_ALPHA * math.pi / 180.0
                 g1 = m2.refine(start[:1], a1, a1, REFINE_STEP, REFINE_SACC, REFINE_DEF)[0]
                 m2.close()
@@ -686,7 +701,8 @@ def search_leg(args, local, dist, world, rank, torch):
         refine_obj = {
             "metric": "particles/s (grid refinement, img_refine_grid with defocus search)",
             "value": round(rvalue, 1), "unit": "particles/s", "particles": R,
-            "config": {"start": "best pose of the exhaustive search", "alpha_deg": REFINE_ALPHA,
+            "config": {"start": "best pose of the exhaustive search", "shell_weights": "C_curve (brefine)",
+                       "alpha_deg": REFINE_ALPHA,
                        "accuracy_deg": REFINE_ACC, "shift_step_px": REFINE_STEP, "shift_accuracy_px": REFINE_SACC,
                        "defocus_step_A": REFINE_DEF, "scoring": "FP64 figure of merit"},
             "hypotheses_per_particle": round(float(rout[:, 8].mean()), 1),

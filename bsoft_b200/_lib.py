@@ -131,6 +131,7 @@ def load():
         "bsg_match_set_images": ([vp, vp, C.c_long, dp, C.c_double, C.c_double, C.c_int], C.c_int),
         "bsg_match_prepared": ([vp, C.c_long, C.c_long, vp, C.c_int], C.c_int),
         "bsg_match_score": ([vp, dp, C.c_long, dp, dp, C.c_int], C.c_int),
+        "bsg_match_set_shell_weights": ([vp, dp, C.c_int], C.c_int),
         "bsg_match_project": ([vp, dp, C.c_long, C.c_double, dp, dp, vp, C.c_int], C.c_int),
         "bsg_match_set_panel": ([vp, dp, C.c_long, C.c_int], C.c_int),
         "bsg_match_search": ([vp, dp, C.c_int, C.c_int, dp, C.c_int], C.c_int),
@@ -149,6 +150,8 @@ def load():
         "bsg_backproj_set_symmetrize": ([vp, dp, C.POINTER(C.c_int), C.c_int], C.c_int),
         "bsg_backproj_set_rescale": ([vp, C.c_double, C.c_double], C.c_int),
         "bsg_backproj_reset": ([vp], C.c_int),
+        "bsg_match_refine_monte": ([vp, dp, C.c_long, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.c_ulonglong, dp, C.c_int], C.c_int),
         "bsg_cnn_create": ([C.POINTER(CnnConfig), C.POINTER(vp)], C.c_int),
         "bsg_cnn_destroy": ([vp], None),
         "bsg_cnn_num_params": ([vp], C.c_long),

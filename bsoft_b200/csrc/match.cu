@@ -354,6 +354,8 @@ struct FomArgs {
     double inv, real;        // section frequency step and real size
     int nf;                  // shells j < max_rad
     int cv0, cv1;            // cross-validation shells [cv0, cv1)
+    const double* wshell;    // per-shell weights
+    double wf, wc;           // their sums over [0, nf) and [cv0, cv1)
     double* fom;             // per group x MAXORG
     double* cv;
     const double2* sec;      // gathered sections (npix per view, FP64), or null: gather here
@@ -486,11 +488,12 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
                 fj += wsum[(w * a.nshell + j) * NV + 1 + o];
             }
             double t;
+            const double wj = a.wshell[j];
             if (a.dpr) {
-                t = mj != 0.0 ? cos(sqrt(fj / mj)) : 0.0;
+                t = mj != 0.0 ? wj * cos(sqrt(fj / mj)) : 0.0;
             } else {
                 const double den = ds[j] * mj;
-                t = den > 0 ? fj / sqrt(den) : 0.0;
+                t = den > 0 ? wj * fj / sqrt(den) : 0.0;
             }
             if (j < a.nf) tf += t;
             if (j >= a.cv0 && j < a.cv1) tc += t;
@@ -501,8 +504,8 @@ __global__ void __launch_bounds__(FOM_WARPS * 32) fom_kernel(FomArgs a) {
             tc += __shfl_xor_sync(0xffffffffu, tc, k);
         }
         if (lane == 0) {
-            a.fom[(long)blockIdx.x * MAXORG + o] = a.nf > 0 ? tf / a.nf : 0.0;
-            a.cv[(long)blockIdx.x * MAXORG + o] = (a.cv1 > a.cv0) ? tc / (a.cv1 - a.cv0) : 0.0;
+            a.fom[(long)blockIdx.x * MAXORG + o] = a.nf > 0 ? tf / a.wf : 0.0;
+            a.cv[(long)blockIdx.x * MAXORG + o] = (a.cv1 > a.cv0) ? tc / a.wc : 0.0;
         }
     }
 }
@@ -696,6 +699,10 @@ extern "C" int bsg_match_create(const bsg_match_config* cfg, bsg_match** out) {
     M->cv1 = M->cv0;
     for (long j = (long)M->max_rad; j < M->max_rad_cv; ++j) M->cv1 = (int)j + 1;
     if (M->nf > M->nshell || M->cv1 > M->nshell) M->nshell = std::max(M->nf, M->cv1);
+    // unit shell weights until the caller sets a curve
+    M->h_wshell.assign(M->nshell, 1.0);
+    M->wf = (double)M->nf;
+    M->wc = (double)(M->cv1 - M->cv0);
     M->h_shell_start.resize(M->nshell + 1, M->h_shell_start.back());
 
     // FSI kernel table (FSI_Kernel.h:28-68): row r = fraction r/512, tap j
@@ -725,7 +732,10 @@ extern "C" int bsg_match_create(const bsg_match_config* cfg, bsg_match** out) {
     ALLOC(M->d_tw_map, sizeof(double2) * twm.size());
     ALLOC(M->d_tw_img, sizeof(double2) * twi.size());
     ALLOC(M->d_ref, sizeof(float2) * (size_t)D * D * D);
+    ALLOC(M->d_wshell, sizeof(double) * std::max<size_t>(1, M->h_wshell.size()));
 #undef ALLOC
+    if (e == cudaSuccess)
+        e = cudaMemcpy(M->d_wshell, M->h_wshell.data(), sizeof(double) * M->h_wshell.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(M->d_pix, M->h_pix.data(), sizeof(MPix) * M->h_pix.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(M->d_shell_start, M->h_shell_start.data(), sizeof(int) * M->h_shell_start.size(),
@@ -757,7 +767,7 @@ extern "C" void bsg_match_destroy(bsg_match* h) {
                     M->d_hyp, M->d_out, M->d_full, M->d_grp, M->d_gout, M->d_cpix, M->d_cstart, M->d_secs, M->d_panel, M->d_A, M->d_pscore,
                     M->d_pidx, M->d_csec, M->d_corg, M->d_cscore, M->d_rots, M->d_gA, M->d_slopes,
                     M->d_lprop, M->d_lorg, M->d_nlorg, M->d_lcand, M->d_lcount,
-                    M->d_status, M->d_pexact};
+                    M->d_status, M->d_pexact, M->d_wshell};
     for (void* p : ptrs) if (p) cudaFree(p);
     if (M->h_pin) cudaFreeHost(M->h_pin);
     if (M->ref_tex) cudaDestroyTextureObject(M->ref_tex);
@@ -1003,6 +1013,7 @@ cudaError_t launch_fom(const Match& M, const MHypG* d_groups, long ng, double* d
     a.spec = M.d_spec; a.ctf = ctf_table ? ctf_table : M.d_ctf; a.dsum = M.d_dsum; a.nshell = M.nshell;
     a.inv = 1.0 / M.real_map; a.real = M.real_map;
     a.nf = M.nf; a.cv0 = M.cv0; a.cv1 = M.cv1;
+    a.wshell = M.d_wshell; a.wf = M.wf; a.wc = M.wc;
     a.fom = d_fom; a.cv = d_cv; a.sec = sec;
     const size_t words = (NDIV + 1) * MAXW + FOM_WARPS * M.nshell * (1 + MAXORG);
     if (fp64 && sizeof(double) * words > 220 * 1024) return cudaErrorInvalidValue;
@@ -1331,5 +1342,30 @@ extern "C" int bsg_match_project(bsg_match* h, const double* mats, long nviews, 
     }
     cudaFree(d_px); cudaFree(d_v); cudaFree(d_c); cudaFree(d_o);
     if (e != cudaSuccess) return mfail(BSG_ERR_CUDA, "bsg_match_project: %s", cudaGetErrorString(e));
+    return BSG_OK;
+}
+
+// img_recip_space_fom's shell weights (mg_refine.cpp:702-704): w[j] = 1,
+// replaced by the caller's weight[j] where that is non-zero, for shells j
+// < n; their sums over the FRC and cross-validation shells are formed in
+// shell order as the reference's loops form them (:757-767).
+extern "C" int bsg_match_set_shell_weights(bsg_match* h, const double* w, int n) {
+    Match* M = reinterpret_cast<Match*>(h);
+    if (!M || n < 0 || (n > 0 && !w)) return match_fail(BSG_ERR_ARG, "bsg_match_set_shell_weights: bad argument");
+    std::vector<double> ws(M->nshell, 1.0);
+    for (int j = 0; j < n && j < M->nshell; ++j) {
+        if (!std::isfinite(w[j])) return match_fail(BSG_ERR_ARG, "bsg_match_set_shell_weights: weight %d not finite", j);
+        if (w[j] != 0.0) ws[j] = w[j];
+    }
+    double wf = 0, wc = 0;
+    for (int j = 0; j < M->nf; ++j) wf += ws[j];
+    for (int j = M->cv0; j < M->cv1; ++j) wc += ws[j];
+    cudaError_t e = cudaSetDevice(M->device);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(M->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(M->d_wshell, ws.data(), sizeof(double) * ws.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_set_shell_weights: %s", cudaGetErrorString(e));
+    M->h_wshell.swap(ws);
+    M->wf = wf;
+    M->wc = wc;
     return BSG_OK;
 }

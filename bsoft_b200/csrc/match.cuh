@@ -6,6 +6,8 @@
 
 #include <cuda_bf16.h>
 
+#include <stdlib.h>
+
 #include <vector>
 
 namespace bsg {
@@ -186,6 +188,17 @@ struct Match {
     double scx = 1, scy = 1;           // pref sampling / particle sampling
     double cut_scale = 1;              // diam / n (long double in the reference)
     int nshell = 0, nf = 0, cv0 = 0, cv1 = 0;
+    // per-shell weights of the figure of merit (img_recip_space_fom's w[j]:
+    // 1, or the caller's curve where it is non-zero) and their sums over the
+    // FRC shells [0, nf) and the cross-validation shells [cv0, cv1)
+    // brefine -monte's random() stream (glibc random_r on a private TYPE_3
+    // state), kept between calls so that batches continue one sequence
+    random_data rng_data;
+    char rng_state[128];
+    bool rng_init = false;
+    std::vector<double> h_wshell;
+    double* d_wshell = nullptr;
+    double wf = 0, wc = 0;
     std::vector<MPix> h_pix;           // figure-of-merit pixels, shell-sorted
     std::vector<int> h_shell_start;
     std::vector<MPix> h_secpix;        // section pixels

@@ -22,6 +22,7 @@
 #include "match.cuh"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -909,6 +910,391 @@ extern "C" int bsg_match_refine(bsg_match* h, const double* start, long nstart, 
             const double d = (P.bestdef > P.def0 - 5 * def_std && P.bestdef < P.def0 + 5 * def_std) ? P.bestdef : P.def0;
             o[9] = dz.defocus(dz.abw20(d));
         }
+    }
+    M->sstats.refine_ms += tsum;
+    M->sstats.refine_launches += launches;
+    M->sstats.launches += launches;
+    return BSG_OK;
+}
+
+// ---- brefine -monte: img_refine_monte (mg_refine.cpp:979-1050) with its
+// origin/defocus chain img_fit_in_recip_space_monte (:783-860).
+//
+// The reference draws every random number from the C library's random()
+// (seeded once, mg_refine.cpp:276), particle after particle.  Which numbers
+// are drawn, and where, never depends on a score, so the host draws each
+// start record's whole sequence first, in record order, with glibc's
+// generator (random_r on a private TYPE_3 state seeded like srandom): per
+// record get_rand_max's 100 draws, then per outer iteration the view step
+// (vector3_random_gaussian, random_numbers.cpp:502-510, and the in-plane
+// angle), the magnification pair, the fit's own get_rand_max, its defocus
+// and origin steps (random_gaussian :123-137, vector3_xy_random_gaussian
+// :522-531) and acceptance draws, and the outer acceptance draw.  The
+// chains then run in lockstep over all records: one section gather per
+// outer iteration, one CTF-row pass and one FP64 figure-of-merit launch per
+// inner iteration, and the host applies the reference's acceptance rule
+// fom / prefom > u in its order.
+namespace bsg {
+namespace {
+
+constexpr double TWO_PI_REF = 6.28318530717958647692528676655900576;   // TWOPI (utilities.h)
+
+// the context's random() stream: seed != 0 starts it as srandom(seed)
+// does (glibc treats srandom(0) as srandom(1)); 0 continues it
+void monte_seed(Match& M, unsigned long long seed) {
+    if (seed != 0 || !M.rng_init) {
+        memset(&M.rng_data, 0, sizeof(M.rng_data));
+        memset(M.rng_state, 0, sizeof(M.rng_state));
+        initstate_r(seed != 0 ? (unsigned)seed : 1u, M.rng_state, sizeof(M.rng_state), &M.rng_data);
+        M.rng_init = true;
+    }
+}
+
+long monte_next(Match& M) {
+    int32_t r = 0;
+    random_r(&M.rng_data, &r);
+    return (long)r;
+}
+
+struct MonteOuter {
+    double r[3] = {0, 0, 0};   // view vector step
+    double a = 0;              // in-plane angle step
+    double mx = 1, my = 1;     // sampling factors
+    double u = 0;              // acceptance draw (random() * irm)
+};
+
+struct MonteInner {
+    double g = 0;              // defocus step (angstrom)
+    double dx = 0, dy = 0;     // origin step (pixels of the cut transform)
+    double u = 0;              // acceptance draw
+};
+
+struct MonteRec {
+    long img = 0;
+    bool fit_ctf = false;          // the fit draws defocus steps (flags & APPLY_CTF)
+    bool dsearch = false;          // def_std > 0 with a defocus: the defocus chain
+    double ox = 0, oy = 0;         // original origin (cut pixels)
+    double def0 = 0;               // the particle's defocus
+    std::vector<MonteOuter> outer;
+    std::vector<MonteInner> inner; // max_iter x max_iter
+    // outer chain
+    View4 view, preview, bestview;
+    double prefom = -1, bestfom = -1, bestcv = 0, bx = 0, by = 0, bestdef = 0, bmx = 1, bmy = 1;
+    double mx = 1, my = 1;
+    long number = 0;
+    // inner chain of the current outer iteration
+    double x = 0, y = 0, px = 0, py = 0, fbx = 0, fby = 0;
+    double fprefom = -1, fbestfom = -1, fbestcv = 0;
+    double abw = 0, pabw = 0, fbestabw = 0;   // CTF abw[2,0] of the current / accepted / best defocus
+};
+
+}  // namespace
+}  // namespace bsg
+
+extern "C" int bsg_match_refine_monte(bsg_match* h, const double* start, long nstart, int max_iter, double def_std,
+                                      double shift_std, double view_std, double max_angle, double max_mag,
+                                      unsigned long long seed, double* out, int flags) {
+    using namespace bsg;
+    const bool dpr = (flags & BSG_MATCH_SCORE_DPR) != 0;
+    Match* M = reinterpret_cast<Match*>(h);
+    if (!M || !start || !out || nstart < 1) return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: bad argument");
+    if (!M->have_ref || M->nimg < 1)
+        return match_fail(BSG_ERR_STATE, "bsg_match_refine_monte: set the reference and images first");
+    if (max_iter < 1 || max_iter > 10000)
+        return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: %d iterations outside 1..10000", max_iter);
+    if (!(def_std >= 0) || !(shift_std >= 0) || !(view_std >= 0) || !(max_angle >= 0) || !(max_mag >= 0) ||
+        !(max_mag < 1) || !isfinite(def_std + shift_std + view_std + max_angle))
+        return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: bad step sizes");
+    cudaError_t ce = cudaSetDevice(M->device);
+    if (ce != cudaSuccess) return match_fail(BSG_ERR_CUDA, "bsg_match_refine_monte: %s", cudaGetErrorString(ce));
+
+    // ---- the random draws, record after record (the reference's order)
+    monte_seed(*M, seed);
+    auto rnd = [&]() { return monte_next(*M); };
+    auto get_rand_max = [&]() {          // random_numbers.cpp:22-30
+        long rm = 32767;
+        for (int i = 0; i < 100; ++i)
+            if (rnd() > rm) rm = 2147483647;
+        return rm;
+    };
+    // random_numbers.cpp's file-scope irm = 1.0L / get_rand_max(), formed
+    // before main from the unseeded generator: 2^31 - 1 for 31-bit random()
+    const double girm = (double)(1.0L / 2147483647.0L);
+    auto gauss = [&](double avg, double sd) {
+        double r = -2 * log(rnd() * girm);
+        if (r > 0) r = avg + sd * sqrt(r) * cos(TWO_PI_REF * (rnd() * girm));
+        else r = avg;
+        return r;
+    };
+    const long ni = (long)max_iter;
+    std::vector<MonteRec> recs(nstart);
+    for (long i = 0; i < nstart; ++i) {
+        const double* r = start + BSG_MATCH_REFINE_START_DOUBLES * i;
+        const long img = (long)r[0];
+        if (!(r[0] >= 0) || img >= M->nimg)
+            return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: start record %ld names image %g", i, r[0]);
+        MonteRec& R = recs[i];
+        R.img = img;
+        R.ox = M->cut_scale * r[5];
+        R.oy = M->cut_scale * r[6];
+        R.view = R.preview = R.bestview = renormalised(make_view(r[1], r[2], r[3], r[4]), 3);
+        R.bx = R.ox;
+        R.by = R.oy;
+        R.dsearch = def_std > 0;
+        R.fit_ctf = R.dsearch || M->h_ictf[img].apply;
+        if (R.fit_ctf && !(M->h_volt[img] > 0))
+            return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: image %ld has a CTF but no voltage", img);
+        if (R.dsearch) {
+            const DefocusTerm dz(M->h_volt[img]);
+            R.def0 = dz.defocus(M->h_ictf[img].c[1]);
+            if (R.def0 == 0)
+                return match_fail(BSG_ERR_ARG, "bsg_match_refine_monte: image %ld has no defocus to vary", img);
+        }
+        R.bestdef = R.def0;
+        R.outer.resize(ni);
+        R.inner.resize(ni * ni);
+        const double irm = 1.0 / get_rand_max();              // img_refine_monte's irm
+        for (long o = 0; o < ni; ++o) {
+            MonteOuter& od = R.outer[o];
+            if (o > 0) {
+                // vector3_random_gaussian: a unit vector (3 gaussians), then the length
+                Vec3 u{{gauss(0, 1), gauss(0, 1), gauss(0, 1)}};
+                u.normalize();
+                const double amp = gauss(0, view_std);
+                for (int k = 0; k < 3; ++k) od.r[k] = u.d[k] * amp;
+                od.a = max_angle * (rnd() * irm * 2 - 1);
+                if (max_mag > 0) {
+                    od.mx = 1 + max_mag * (rnd() * irm * 2 - 1);
+                    od.my = 1 + max_mag * (rnd() * irm * 2 - 1);
+                }
+            }
+            const double firm = 1.0 / get_rand_max();         // the fit's irm
+            for (long it = 0; it < ni; ++it) {
+                MonteInner& id = R.inner[o * ni + it];
+                if (it > 0) {
+                    if (R.fit_ctf) id.g = gauss(0, def_std);
+                    // vector3_xy_random_gaussian: the length first, then x and y
+                    const double amp = gauss(0, shift_std);
+                    Vec3 v{{gauss(0, 1), gauss(0, 1), 0}};
+                    v.normalize();
+                    id.dx = v.d[0] * amp;
+                    id.dy = v.d[1] * amp;
+                }
+                id.u = rnd() * firm;
+            }
+            od.u = rnd() * irm;
+        }
+    }
+
+    // ---- the chains, all records in lockstep
+    const int npix = (int)M->h_pix.size();
+    const double mag_samp = M->cfg.pixel / M->cut_scale;
+    const double ref_samp = M->cfg.map_sampling / (double)((long double)M->D / M->N);
+    const long cap = std::max(1L, std::min(nstart, (long)((1L << 30) / ((long)sizeof(double2) * std::max(npix, 1)))));
+    cudaStream_t s = M->stream;
+    double* d_mats = nullptr;
+    double2* d_sec = nullptr;
+    float* d_ctfrows = nullptr;
+    ImgCtf* d_crec = nullptr;
+    ce = cudaMalloc(&d_mats, sizeof(double) * 9 * cap);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_sec, sizeof(double2) * (size_t)npix * cap);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_ctfrows, sizeof(float) * (size_t)npix * cap);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_crec, sizeof(ImgCtf) * cap);
+    int rc = BSG_OK;
+    if (ce != cudaSuccess) rc = match_fail(BSG_ERR_NOMEM, "bsg_match_refine_monte: %s", cudaGetErrorString(ce));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float tsum = 0;
+    long launches = 0;
+    auto slope = [&](double o) { return o / M->D * 2 * M_PI; };
+    std::vector<double> mats;
+    std::vector<MHypG> groups;
+    std::vector<ImgCtf> crec;
+    std::vector<double> go;
+    for (long c0 = 0; c0 < nstart && rc == BSG_OK; c0 += cap) {
+        const long c1 = std::min(nstart, c0 + cap), nc = c1 - c0;
+        for (long o = 0; o < ni && rc == BSG_OK; ++o) {
+            // the outer step: view, sampling; p->view(view) stores a copy the fit reads back
+            mats.assign(9 * nc, 0.0);
+            for (long t = 0; t < nc; ++t) {
+                MonteRec& R = recs[c0 + t];
+                const MonteOuter& od = R.outer[o];
+                if (o > 0) {
+                    R.view.v[0] += od.r[0];
+                    R.view.v[1] += od.r[1];
+                    R.view.v[2] += od.r[2];
+                    R.view.a += od.a;
+                    R.view.normalize();
+                    R.mx = od.mx;
+                    R.my = od.my;
+                }
+                double mat[9];
+                view_matrix(renormalised(R.view, 3), mat);
+                const double kx = ref_samp / (mag_samp * R.mx), ky = ref_samp / (mag_samp * R.my);
+                double* mo = &mats[9 * t];
+                for (int a = 0; a < 3; ++a)
+                    for (int c = 0; c < 3; ++c) {
+                        double v = mat[3 * a + c];
+                        if (a < 2) v *= (c == 0 ? kx : (c == 1 ? ky : 1.0));
+                        mo[3 * a + c] = v;
+                    }
+                // the fit starts from the original origin and defocus
+                R.x = R.px = R.fbx = R.ox;
+                R.y = R.py = R.fby = R.oy;
+                R.fprefom = -1;
+                R.fbestfom = -1;
+                R.fbestcv = 0;
+                if (R.dsearch) {
+                    const DefocusTerm dz(M->h_volt[R.img]);
+                    R.abw = R.pabw = R.fbestabw = dz.abw20(R.def0);
+                } else {
+                    R.abw = R.pabw = R.fbestabw = M->h_ictf[R.img].c[1];
+                }
+            }
+            cudaError_t e = cudaMemcpyAsync(d_mats, mats.data(), sizeof(double) * mats.size(), cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            if (e == cudaSuccess) e = launch_secgather(*M, d_mats, nc, d_sec, s);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) { rc = match_fail(BSG_ERR_CUDA, "bsg_match_refine_monte: %s", cudaGetErrorString(e)); break; }
+            {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tsum += ms;
+                ++launches;
+            }
+            for (long it = 0; it < ni; ++it) {
+                groups.assign(nc, MHypG{});
+                crec.resize(nc);
+                for (long t = 0; t < nc; ++t) {
+                    MonteRec& R = recs[c0 + t];
+                    const MonteInner& id = R.inner[o * ni + it];
+                    if (it > 0) {
+                        if (R.fit_ctf) {
+                            // em_ctf->defocus_average(em_ctf->defocus_average() + g)
+                            const DefocusTerm dz(M->h_volt[R.img]);
+                            R.abw = dz.abw20(dz.defocus(R.abw) + id.g);
+                        }
+                        R.x += id.dx;
+                        R.y += id.dy;
+                    }
+                    MHypG& g = groups[t];
+                    memset(&g, 0, sizeof(g));
+                    memcpy(g.m, &mats[9 * t], sizeof(g.m));
+                    g.img = (int)R.img;
+                    g.ctf = (int)t;
+                    g.sec = (int)t;
+                    g.norg = 1;
+                    g.sx[0] = slope(R.x);
+                    g.sy[0] = slope(R.y);
+                    ImgCtf C = M->h_ictf[R.img];
+                    if (R.fit_ctf) {
+                        C.c[1] = R.abw;
+                        if (R.dsearch) {
+                            const DefocusTerm dz(M->h_volt[R.img]);
+                            C.apply = dz.defocus(C.c[1]) >= 1 ? 1 : 0;
+                        }
+                    }
+                    C.fsx = 1.0 / ((mag_samp * R.mx) * M->D);
+                    C.fsy = 1.0 / ((mag_samp * R.my) * M->D);
+                    crec[t] = C;
+                }
+                const long ng = nc;
+                int r2 = ensure_groups(*M, ng);
+                if (r2 != BSG_OK) { rc = r2; break; }
+                go.resize(2 * ng * MAXORG);
+                e = cudaMemcpyAsync(M->d_grp, groups.data(), sizeof(MHypG) * ng, cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(d_crec, crec.data(), sizeof(ImgCtf) * nc, cudaMemcpyHostToDevice, s);
+                if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+                if (e == cudaSuccess) e = launch_ctf_rows(*M, d_crec, nc, d_ctfrows, s);
+                if (e == cudaSuccess)
+                    e = launch_fom(*M, M->d_grp, ng, M->d_gout, M->d_gout + ng * MAXORG, s, true, d_ctfrows, d_sec, dpr);
+                if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(go.data(), M->d_gout, sizeof(double) * go.size(), cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) { rc = match_fail(BSG_ERR_CUDA, "bsg_match_refine_monte: %s", cudaGetErrorString(e)); break; }
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tsum += ms;
+                launches += 2;
+                // img_fit_in_recip_space_monte's bookkeeping (:827-850)
+                for (long t = 0; t < nc; ++t) {
+                    MonteRec& R = recs[c0 + t];
+                    const MonteInner& id = R.inner[o * ni + it];
+                    double fom = go[t * MAXORG];
+                    const double cv = go[ng * MAXORG + t * MAXORG];
+                    R.number++;
+                    if (R.fbestfom < fom) {
+                        R.fbestfom = fom;
+                        R.fbestabw = R.abw;
+                        R.fbx = R.x;
+                        R.fby = R.y;
+                        R.fbestcv = cv;
+                    }
+                    if (fom / R.fprefom > id.u) {
+                        R.pabw = R.abw;
+                        R.px = R.x;
+                        R.py = R.y;
+                        R.fprefom = fom;
+                    } else {
+                        R.abw = R.pabw;
+                        R.x = R.px;
+                        R.y = R.py;
+                    }
+                }
+            }
+            if (rc != BSG_OK) break;
+            // img_refine_monte's bookkeeping (:1025-1046)
+            for (long t = 0; t < nc; ++t) {
+                MonteRec& R = recs[c0 + t];
+                const double fom = R.fbestfom;
+                if (R.bestfom < fom) {
+                    R.bestfom = fom;
+                    R.bestview = R.view;
+                    R.bmx = R.mx;
+                    R.bmy = R.my;
+                    R.bx = R.fbx;
+                    R.by = R.fby;
+                    if (R.dsearch) {
+                        const DefocusTerm dz(M->h_volt[R.img]);
+                        R.bestdef = dz.defocus(R.fbestabw);
+                    }
+                    R.bestcv = R.fbestcv;
+                }
+                if (fom / R.prefom > R.outer[o].u) {
+                    R.preview = R.view;
+                    R.prefom = fom;
+                } else {
+                    R.view = R.preview;
+                }
+            }
+        }
+    }
+    cudaFree(d_mats);
+    cudaFree(d_sec);
+    cudaFree(d_ctfrows);
+    cudaFree(d_crec);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != BSG_OK) return rc;
+    for (long i = 0; i < nstart; ++i) {
+        const MonteRec& R = recs[i];
+        const View4 w = renormalised(R.bestview, 3);
+        double* o = out + BSG_MATCH_REFINE_RESULT_DOUBLES * i;
+        o[0] = w.v[0];
+        o[1] = w.v[1];
+        o[2] = w.v[2];
+        o[3] = w.a;
+        o[4] = R.bx / M->cut_scale;
+        o[5] = R.by / M->cut_scale;
+        o[6] = R.bestfom;
+        o[7] = R.bestcv;
+        o[8] = (double)R.number;
+        o[9] = R.dsearch ? R.bestdef : 0.0;
+        o[10] = (mag_samp * R.bmx) * M->cut_scale;
+        o[11] = (mag_samp * R.bmy) * M->cut_scale;
     }
     M->sstats.refine_ms += tsum;
     M->sstats.refine_launches += launches;

@@ -609,6 +609,100 @@ inline std::vector<double> symmetry_operators(const std::string& sym) {
     return m;
 }
 
+// The reference's View (x, y, z, angle) with its normalisation (View.h:30-35,
+// 110-116: unit vector, components below 1e-30 zeroed, angle wrapped to
+// [-pi, pi] and zeroed below 1e-30)
+struct RefView {
+    double v[3] = {0, 0, 1}, a = 0;
+    void normalize() {
+        const double size = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        if (size < TRIG) { v[0] = v[1] = 0; v[2] = 1; }
+        else { v[0] /= size; v[1] /= size; v[2] /= size; }
+        for (double& c : v)
+            if (std::fabs(c) < TRIG) c = 0;
+        a = angle_neg_pi_to_pi(a);
+        if (std::fabs(a) < TRIG) a = 0;
+    }
+};
+
+// symmetry_get_all_views (bsoft/src/util/symmetry.cpp:277-319): the view
+// (copied by value, assigned, normalised), then for each generating
+// operation and j = 1 .. order - 1, for each view so far, the quaternion of
+// the rotation by j 2 pi / order about the operation's axis times the view's
+// quaternion (View::quaternion, which normalises the stored view first),
+// turned back into a View (View(Quaternion&), View.h:60-72).  Quaternion
+// copies zero components below 1e-30 (Quaternion.h:28-32, 52-54).
+inline std::vector<RefView> symmetry_views(const std::string& sym, double x, double y, double z, double a) {
+    auto qcheck = [](double* q) {
+        for (int i = 0; i < 4; ++i)
+            if (std::fabs(q[i]) < TRIG) q[i] = 0;
+    };
+    auto view_quat = [&](RefView& w, double* q) {
+        w.normalize();
+        const double ang = (double)((long double)w.a / 2.0L);
+        const double ca = std::cos(ang), sa = std::sin(ang);
+        const double z1 = w.v[2] + 1;
+        q[0] = ca; q[1] = 0; q[2] = 0; q[3] = sa;
+        if (w.v[2] < 1.0L - TRIG) {
+            if (w.v[2] <= TRIG - 1.0L) {
+                q[0] = 0; q[1] = sa; q[2] = ca; q[3] = 0;
+            } else {
+                const double f1 = std::sqrt(z1 / 2.0), f2 = std::sqrt(1.0 / (2 * z1));
+                q[0] = f1 * ca;
+                q[1] = f2 * (w.v[0] * sa - w.v[1] * ca);
+                q[2] = f2 * (w.v[0] * ca + w.v[1] * sa);
+                q[3] = f1 * sa;
+            }
+        }
+        qcheck(q);                                   // returned by value
+    };
+    RefView first;
+    first.v[0] = x; first.v[1] = y; first.v[2] = z; first.a = a;
+    first.normalize();                               // the by-value parameter
+    first.normalize();                               // vn->normalize()
+    std::vector<RefView> views{first};
+    for (const SymOp& g : symmetry_generators(sym)) {
+        // Bsymmetry stores the axis normalised; from_axis_angle normalises it again
+        double ax[3] = {g.a[0], g.a[1], g.a[2]};
+        for (int pass = 0; pass < 2; ++pass) {
+            const double len = std::sqrt(ax[0] * ax[0] + ax[1] * ax[1] + ax[2] * ax[2]);
+            if (len < TRIG) { ax[0] = ax[1] = 0; ax[2] = 1; }
+            else { const double d = 1.0 / len; ax[0] *= d; ax[1] *= d; ax[2] *= d; }
+        }
+        const size_t nv = views.size();
+        for (int j = 1; j < g.order; ++j) {
+            const double angle = (double)((long double)(j * 6.28318530717958647692528676655900576) / g.order);
+            const double h = (double)((long double)angle / 2.0L);
+            double q[4] = {std::cos(h), ax[0] * std::sin(h), ax[1] * std::sin(h), ax[2] * std::sin(h)};
+            qcheck(q);
+            for (size_t k = 0; k < nv; ++k) {
+                double p[4];
+                view_quat(views[k], p);
+                double r[4];
+                r[0] = q[0] * p[0] - (q[1] * p[1] + q[2] * p[2] + q[3] * p[3]);
+                r[1] = q[0] * p[1] + q[1] * p[0] + q[2] * p[3] - q[3] * p[2];
+                r[2] = q[0] * p[2] + q[2] * p[0] + q[3] * p[1] - q[1] * p[3];
+                r[3] = q[0] * p[3] + q[3] * p[0] + q[1] * p[2] - q[2] * p[1];
+                qcheck(r);                           // the product returned by value
+                // View(Quaternion&)
+                double ang = std::atan2(r[3], r[0]);
+                const double ca = std::cos(ang), sa = std::sin(ang);
+                const double q2 = r[0] * r[0] + r[3] * r[3];
+                const double f2 = 2 * std::sqrt(q2);
+                if (q2 < TRIG) ang = std::atan2(r[1], r[2]);
+                RefView w;
+                w.v[0] = f2 * (r[2] * ca + r[1] * sa);
+                w.v[1] = f2 * (r[2] * sa - r[1] * ca);
+                w.v[2] = 2 * q2 - 1;
+                w.a = 2 * ang;
+                w.normalize();
+                views.push_back(w);
+            }
+        }
+    }
+    return views;
+}
+
 // STAR project with the particle parameters the readers above take, plus
 // the figures of merit (mg_tags.h:227-228); one block per micrograph
 inline void write_project(const std::string& path, const std::vector<Micrograph>& mgs,

@@ -168,6 +168,31 @@ class Matcher:
 
 
     # ---- exhaustive search ----
+    def refine_monte(self, start, max_iter: int, def_std: float = 0.0, shift_std: float = 0.0,
+                     view_std: float = 0.0, max_angle: float = 0.0, max_mag: float = 0.0, seed: int = 1,
+                     dpr: bool = False) -> np.ndarray:
+        """img_refine_monte for every start record (brefine -monte); max_angle
+        in radians, shift_std in pixels of the cut transform; random() seeded
+        with `seed`.  Returns (n, 12) as refine()."""
+        s = np.ascontiguousarray(start, dtype=np.float64).reshape(-1, _lib.MATCH_REFINE_START_DOUBLES)
+        out = np.empty((len(s), _lib.MATCH_REFINE_RESULT_DOUBLES))
+        _lib.check(_lib.load().bsg_match_refine_monte(self._h, _dp(s), len(s), int(max_iter), float(def_std),
+                                                      float(shift_std), float(view_std), float(max_angle),
+                                                      float(max_mag), int(seed), _dp(out),
+                                                      _lib.MATCH_SCORE_DPR if dpr else 0), "bsg_match_refine_monte")
+        return out
+
+    def set_shell_weights(self, w=None) -> None:
+        """Per-shell weights of the figure of merit (None: unit weights)."""
+        a = np.ascontiguousarray([] if w is None else w, dtype=np.float64)
+        _lib.check(_lib.load().bsg_match_set_shell_weights(self._h, _dp(a) if a.size else None, int(a.size)),
+                   "bsg_match_set_shell_weights")
+
+    def set_c_curve_weights(self) -> None:
+        """brefine's default weighting: C_curve(diam, 1 / real size of the cut
+        map) (mg_refine.cpp:366-367, ctf.cpp:795-810)."""
+        self.set_shell_weights(c_curve(self.diam, 1.0 / (self.diam * self.info.map_sampling_cut)))
+
     def set_panel(self, mats, exact_sections: bool = True) -> None:
         """Search panel of central sections for row-major view matrices (nsec,
         3, 3).  exact_sections keeps the panel's FP32 sections for the exact
@@ -222,3 +247,11 @@ def ctf_record(volt: float, coefs, apply: bool = True, invert: bool = False) -> 
 def hypothesis(img: int, mat, origin) -> np.ndarray:
     m = np.asarray(mat, dtype=np.float64).reshape(9)
     return np.array([img, *m, origin[0], origin[1]], dtype=np.float64)
+
+
+def c_curve(n: int, freq_step: float) -> np.ndarray:
+    """The reference's C_curve (bsoft/src/util/ctf.cpp:795-810): a sum of five
+    Gaussians in s^2 at s = i * freq_step."""
+    s2 = (np.arange(n) * freq_step) ** 2
+    return (0.893 * np.exp(-0.2465 * s2) + 0.2563 * np.exp(-1.7100 * s2) + 0.7570 * np.exp(-6.4094 * s2)
+            + 1.0487 * np.exp(-18.6113 * s2) + 0.3575 * np.exp(-50.2523 * s2))

@@ -339,6 +339,16 @@ int  bsg_match_prepared(bsg_match* m, long first, long count, float* out, int fl
 #define BSG_MATCH_SCORE_DPR  8
 int  bsg_match_score(bsg_match* m, const double* hyps, long nhyp, double* fom, double* cv, int flags);
 
+/* Shell weights of the figure of merit (img_recip_space_fom's weight curve,
+ * bsoft/src/mg/mg_refine.cpp:702-704): w[j] for shells j < n replaces the
+ * unit weight where it is non-zero.  brefine always passes one:
+ * project_refine_orientations uses C_curve(diam, 1 / (diam x cut sampling))
+ * unless a curve is given (mg_refine.cpp:366-367, bsoft/src/util/
+ * ctf.cpp:795-810).  n = 0 restores unit weights.  Applies to every later
+ * scoring call (bsg_match_score, bsg_match_refine, the searches' exact
+ * rescoring). */
+int  bsg_match_set_shell_weights(bsg_match* m, const double* w, int n);
+
 /* Exhaustive search (no counterpart in the reference, which refines locally
  * with img_refine_grid and scores with img_recip_space_fom; this is the
  * global search that scoring generalises to).
@@ -440,6 +450,24 @@ void* bsg_match_stream(bsg_match* m);        /* the context's cudaStream_t */
 int  bsg_match_refine(bsg_match* m, const double* start, long nstart, double alpha_step, double accuracy,
                       double shift_step, double shift_accuracy, double def_std, double max_mag, double* out,
                       int flags);
+
+/* brefine -monte: Monte Carlo refinement, img_refine_monte (bsoft/src/mg/
+ * mg_refine.cpp:979-1050) with img_fit_in_recip_space_monte (:783-860), for
+ * every start record (layout as bsg_match_refine's).  max_iter outer
+ * iterations perturb the view (vector3_random_gaussian of view_std, an
+ * in-plane step of up to max_angle radians, per-axis sampling factors 1 +-
+ * max_mag), each fitted by max_iter inner iterations that perturb the
+ * origin (shift_std, pixels of the cut transform) and, with def_std > 0
+ * (angstrom), the defocus; steps are accepted when fom / previous fom
+ * exceeds a uniform draw.  The random numbers are the C library's random()
+ * after srandom(seed) (the reference seeds with its process id), drawn
+ * record after record in the reference's order, so a seed reproduces the
+ * reference's run; seed 0 continues the context's stream from the previous
+ * call (a run split into batches draws one sequence).  out: as
+ * bsg_match_refine's (hypotheses = max_iter^2). */
+int  bsg_match_refine_monte(bsg_match* m, const double* start, long nstart, int max_iter, double def_std,
+                            double shift_std, double view_std, double max_angle, double max_mag,
+                            unsigned long long seed, double* out, int flags);
 
 /* ---- learned orientation proposer ------------------------------------------
  * No counterpart in the reference.  A convolutional network maps a particle

@@ -99,17 +99,18 @@ def _write_refine_project(d, tmp_path):
 @pytest.mark.parametrize("fomtype", ["frc", "dpr", "mag"])
 @pytest.mark.parametrize("case", ["refine64", "refine32", "refine64ctf"])
 def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
-    """The drop-in brefine against the reference's img_refine_grid, with the
-    FRC figure of merit (refine*.npz), with -fomtype dpr (refine_dpr.npz)
-    and with -magnification (refine_mag.npz: the refined pixel sizes x, y
-    are written with the particles)."""
+    """The drop-in brefine against the compiled reference brefine program on
+    the same STAR project (tests/golden/refine_ccurve.npz and
+    refine_mag.npz, ``<case>_brefine*``): the FRC and DPR figures of merit
+    with brefine's C_curve shell weights, and -magnification (the refined
+    pixel sizes x, y written with the particles).  The program writes six
+    decimals."""
     import math
     from bsoft_b200.project import read_project
     from tests.refine_helpers import GOLDEN, load
     d = load(case)
     star = _write_refine_project(d, str(tmp_path))
     out = os.path.join(str(tmp_path), "out.star")
-    deg = lambda x: repr(x * 180.0 / math.pi)
     args = [os.path.join(ROOT, "bsoft_b200", "_build", "brefine"), "-reference", os.path.join(str(tmp_path), "ref.mrc"),
             "-grid", f"{round(d['alpha'] * 180 / math.pi, 6)},{round(d['accuracy'] * 180 / math.pi, 6)}",
             "-step", f"{d['shift_step']},{d['shift_accuracy']}", "-resolution", repr(d["hi_res"]), "-output", out, star]
@@ -122,20 +123,31 @@ def test_brefine_matches_reference(case, fomtype, exe, tmp_path):
         args[1:1] = ["-magnification", repr(float(zmag[case + "_max_mag"]))]
     subprocess.run(args, capture_output=True, text=True, check=True)
     proj = read_project(out)
-    ref = {"frc": d["result"], "dpr": np.load(os.path.join(GOLDEN, "refine_dpr.npz"))[case], "mag": zmag[case]}[fomtype]
+    if fomtype == "mag":
+        ref = zmag[case + "_brefine"]
+    else:
+        ref = np.load(os.path.join(GOLDEN, "refine_ccurve.npz"))[f"{case}_brefine_{fomtype}"]
+    fom = _star_column(out, "particle.fom")
     for i, mg in enumerate(proj.micrographs):
         v = mg.view[0]
-        assert np.abs(v[:3] - ref[i, :3]).max() < 1e-9 and abs(v[3] - ref[i, 3]) < 1e-9, (i, v, ref[i, :4])
-        assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 1e-9
+        assert np.abs(v - ref[i, :4]).max() < 2e-6, (i, v, ref[i, :4])
+        assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 2e-6
+        assert abs(fom[i] - ref[i, 7]) < 2e-6
         if d["def_std"] > 0:
-            assert abs(mg.defocus[0] - ref[i, 9]) < 1e-6 * ref[i, 9]
+            assert abs(mg.defocus[0] - ref[i, 6]) < 2e-6 * ref[i, 6]
         if fomtype == "mag":
-            # the probe prints the cut transform's sampling; the project holds
-            # it times the cut scale
-            # it times the cut scale D / n (D: the cut transform's edge)
-            cut_x, cut_y = mg.pixel[0] / ref[i, 10], mg.pixel_y[0] / ref[i, 11]
-            assert abs(cut_x - cut_y) < 1e-12 and 0 < cut_x <= 1
-            assert abs(cut_x * d["n"] - round(cut_x * d["n"])) < 1e-9
+            assert abs(mg.pixel[0] - ref[i, 9]) < 2e-6 and abs(mg.pixel_y[0] - ref[i, 10]) < 2e-6
+
+
+def _star_column(path, tag):
+    """Values of a STAR loop column over all blocks, in order."""
+    from bsoft_b200.io.star import read_star
+    vals = []
+    for b in read_star(path):
+        for lp in b.loops:
+            if lp.index(tag) >= 0:
+                vals.extend(float(v) for v in lp.column(tag))
+    return np.array(vals)
 
 
 @pytest.mark.gpu
@@ -285,3 +297,70 @@ def test_bbackproj_matches_reference(case, exe, tmp_path):
         tag = k[len(case) + 5:]
         v, _ = mrc.read_volume(out.replace(".mrc", tag + ".mrc"))
         assert rel_l2(v, z[k]) <= 1e-5, (k, rel_l2(v, z[k]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["refine64", "refine32", "refine64ctf"])
+def test_brefine_monte_matches_reference(case, exe, tmp_path):
+    """The drop-in brefine -monte -seed S against the compiled brefine with
+    its process id pinned to S (tests/golden/refine_monte.npz,
+    ``<case>_brefine``): one random() stream over the run, the particles
+    drawing one after another."""
+    from bsoft_b200.project import read_project
+    from tests.refine_helpers import GOLDEN, load
+    d = load(case)
+    z = np.load(os.path.join(GOLDEN, "refine_monte.npz"))
+    it, sh, vw, ang, mag, seed = z[case + "_params"]
+    ref = z[case + "_brefine"]
+    star = _write_refine_project(d, str(tmp_path))
+    out = os.path.join(str(tmp_path), "out.star")
+    args = [os.path.join(ROOT, "bsoft_b200", "_build", "brefine"), "-reference", os.path.join(str(tmp_path), "ref.mrc"),
+            "-monte", str(int(it)), "-shift", repr(float(sh)), "-view", repr(float(vw)), "-angle", repr(float(ang)),
+            "-seed", str(int(seed)), "-resolution", repr(d["hi_res"]), "-output", out, star]
+    if mag > 0:
+        args[1:1] = ["-magnification", repr(float(mag))]
+    if d["def_std"] > 0:
+        args[1:1] = ["-defocus", repr(d["def_std"])]
+    r = subprocess.run(args, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    proj = read_project(out)
+    fom = _star_column(out, "particle.fom")
+    for i, mg in enumerate(proj.micrographs):
+        assert np.abs(mg.view[0] - ref[i, :4]).max() < 2e-6, (i, mg.view[0], ref[i, :4])
+        assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 2e-6
+        assert abs(fom[i] - ref[i, 7]) < 2e-6
+        if d["def_std"] > 0:
+            assert abs(mg.defocus[0] - ref[i, 6]) < 2e-6 * ref[i, 6]
+        if mag > 0:
+            assert abs(mg.pixel[0] - ref[i, 9]) < 2e-6 and abs(mg.pixel_y[0] - ref[i, 10]) < 2e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case,sym", [("refine32", "D2"), ("refine64", "C3")])
+def test_brefine_symmetry_matches_reference(case, sym, exe, tmp_path):
+    """The drop-in brefine -symmetry X against the compiled brefine
+    (tests/golden/refine_sym.npz): every particle refined from each view of
+    symmetry_get_all_views, the best kept and its view number written as
+    the selection."""
+    import math
+    from bsoft_b200.project import read_project
+    from tests.refine_helpers import GOLDEN, load
+    d = load(case)
+    ref = np.load(os.path.join(GOLDEN, "refine_sym.npz"))[f"{case}_{sym}"]
+    star = _write_refine_project(d, str(tmp_path))
+    out = os.path.join(str(tmp_path), "out.star")
+    args = [os.path.join(ROOT, "bsoft_b200", "_build", "brefine"), "-reference", os.path.join(str(tmp_path), "ref.mrc"),
+            "-grid", f"{round(d['alpha'] * 180 / math.pi, 6)},{round(d['accuracy'] * 180 / math.pi, 6)}",
+            "-step", f"{d['shift_step']},{d['shift_accuracy']}", "-resolution", repr(d["hi_res"]),
+            "-symmetry", sym, "-output", out, star]
+    r = subprocess.run(args, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    proj = read_project(out)
+    fom = _star_column(out, "particle.fom")
+    sel = _star_column(out, "particle.select")
+    for i, mg in enumerate(proj.micrographs):
+        assert np.abs(mg.view[0] - ref[i, :4]).max() < 2e-6, (i, mg.view[0], ref[i, :4])
+        assert np.abs(mg.origin[0, :2] - ref[i, 4:6]).max() < 2e-6
+        assert abs(fom[i] - ref[i, 6]) < 2e-6
+        assert sel[i] == ref[i, 7]
+

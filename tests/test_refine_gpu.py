@@ -64,6 +64,63 @@ def test_dpr_matches_reference(setup):
     assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
 
 
+@pytest.mark.parametrize("fom", ["frc", "dpr"])
+def test_c_curve_weights_match_reference(setup, fom):
+    """brefine weighs the figure of merit's shells with C_curve
+    (project_refine_orientations, mg_refine.cpp:366-367): with those weights
+    the refinement makes the reference's decisions (tests/golden/
+    refine_ccurve.npz, the probe with the same curve), which differ from
+    the unit-weight ones by up to a degree."""
+    import os
+    from tests.refine_helpers import GOLDEN
+    m, d = setup
+    ref = np.load(os.path.join(GOLDEN, "refine_ccurve.npz"))[f"{d['case']}_{fom}"]
+    m.set_c_curve_weights()
+    try:
+        out = _refine(m, d, dpr=fom == "dpr")
+    finally:
+        m.set_shell_weights(None)
+    assert np.array_equal(out[:, 8], ref[:, 8]), (out[:, 8], ref[:, 8])
+    assert np.abs(out[:, :4] - ref[:, :4]).max() < 1e-12
+    assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9
+    assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
+    assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+    assert np.array_equal(out[:, 9], ref[:, 9]) or np.abs(out[:, 9] - ref[:, 9]).max() < 1e-9 * np.abs(ref[:, 9]).max()
+    # unit weights again: the unit-weight fixture's results
+    again = _refine(m, d)
+    assert np.array_equal(again[:, 8], d["result"][:, 8])
+
+
+def test_monte_carlo_matches_reference(setup):
+    """brefine -monte: img_refine_monte with brefine's shell weights and the
+    reference's random() stream for a seed (tests/golden/refine_monte.npz,
+    the probe seeded the same way): the same hypotheses, views, origins,
+    defoci and sampling (with the magnification steps)."""
+    import math
+    import os
+    from tests.refine_helpers import GOLDEN
+    m, d = setup
+    z = np.load(os.path.join(GOLDEN, "refine_monte.npz"))
+    ref = z[d["case"]]
+    it, sh, vw, ang, mag, seed = z[d["case"] + "_params"]
+    m.set_c_curve_weights()
+    try:
+        out = m.refine_monte(d["start_rec"], int(it), def_std=d["def_std"], shift_std=sh, view_std=vw,
+                             max_angle=ang * math.pi / 180.0, max_mag=mag, seed=int(seed))
+    finally:
+        m.set_shell_weights(None)
+    assert np.array_equal(out[:, 8], ref[:, 8])
+    assert np.abs(out[:, :4] - ref[:, :4]).max() < 1e-9, np.abs(out[:, :4] - ref[:, :4]).max()
+    assert np.abs(out[:, 4:6] - ref[:, 4:6]).max() < 1e-9
+    assert np.abs(out[:, 6] - ref[:, 6]).max() < TOL_FOM
+    assert np.abs(out[:, 7] - ref[:, 7]).max() < TOL_FOM
+    if d["def_std"] > 0:
+        assert np.abs(out[:, 9] - ref[:, 9]).max() < 1e-6 * np.abs(ref[:, 9]).max()
+    if mag > 0:
+        cut = float(np.float64(np.longdouble(m.diam) / np.longdouble(d["n"])))
+        assert np.abs(out[:, 10:12] - ref[:, 10:12] * cut).max() < 1e-12 * d["pixel"]
+
+
 def test_magnification_matches_reference(setup):
     """brefine -magnification: the angular rounds, then img_refine_grid's
     magnification stage over 21 x 21 per-axis sampling factors, against the
