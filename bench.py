@@ -975,8 +975,16 @@ def main():
             e2e_s = float(t.item())
         e2e = particles / e2e_s
         rec.close()
+        # the host-to-device copy rate of one step's pinned images alone (the
+        # e2e leg moves them every step): a plain copy, CUDA events
+        ev0.record()
+        dev[0].copy_(host[0], non_blocking=True)
+        ev1.record()
+        torch.cuda.synchronize()
+        h2d_gbs = host[0].numel() * 4 / (ev0.elapsed_time(ev1) / 1e3) / 1e9
         return dict(value=value, ms=ms, e2e=e2e, launches=launches, ins_launch=ins_launch, ins_ms=ins_ms,
-                    fft_ms=fft_ms, shape=shape, shape_ms=shape_ms, clk=clk, w=w, B=B, particles=particles)
+                    fft_ms=fft_ms, shape=shape, shape_ms=shape_ms, clk=clk, w=w, B=B, particles=particles,
+                    h2d_gbs=h2d_gbs)
 
     ins = insertion_leg() if "insert" in args.legs else None
     search = search_leg(args, local, dist, world, rank, torch) if "search" in args.legs else None
@@ -1029,7 +1037,9 @@ def main():
                        "batch_per_step": B, "box": BOX, "map": BOX, "ft": 2 * BOX, "interp": "trilinear",
                        "ctf": "flip", "l2": "inputs larger than L2 (524 MB per step)", "parallelism": f"dp{world}"},
             "e2e": {"value": round(e2e, 1), "unit": "particles/s", "h2d_bytes_per_step": B * BOX * BOX * 4,
-                    "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps},
+                    "d2h_bytes_per_step": BOX ** 3 * 4 // args.steps,
+                    "h2d_copy_gbs": round(ins["h2d_gbs"], 1),
+                    "copy_bound_particles_per_s": round(ins["h2d_gbs"] * 1e9 / (BOX * BOX * 4), 1)},
             "roofline": roof, "cpu_baseline": cpu, "parity": parity, "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
