@@ -116,6 +116,7 @@ def load():
         "bsg_particle_spectra": ([vp, vp, vp, C.c_long, vp, C.c_int], C.c_int),
         "bsg_recon_set_timing": ([vp, C.c_int], C.c_int),
         "bsg_recon_set_tile_shape": ([vp, C.c_int], C.c_int),
+        "bsg_recon_set_half_space": ([vp, C.c_int, C.POINTER(C.c_int)], C.c_int),
         "bsg_recon_set_symmetry": ([vp, dp, C.c_int], C.c_int),
         "bsg_recon_autotune": ([vp, vp, vp, C.c_long, C.c_int, dp, C.POINTER(C.c_int)], C.c_int),
         "bsg_recon_get_stats": ([vp, C.POINTER(ReconStats)], C.c_int),

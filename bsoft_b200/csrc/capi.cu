@@ -32,6 +32,8 @@ cudaError_t launch_ifft3(const Context& c, float2* vol, float* real_out, bool si
 int insert_num_shapes();
 void insert_shape(int i, int* tx, int* ty, int* tz);
 cudaError_t prepare_insert_attributes();
+cudaError_t launch_map_sums(double2* dv, double* dw, const double2* vol, const double* w, const double2* e,
+                            const double* ew, int N, int zsplit, cudaStream_t s);
 
 struct Timed {
     cudaEvent_t a, b;
@@ -150,13 +152,27 @@ static bool needs_gate(const Recon& r, const DevParticle* parts, long np) {
     return false;
 }
 
+// Half-space gridding (insert.cu, walk_edges) applies to trilinear
+// insertion of planes without the FOM channels; the split is the first
+// multiple of 8 above N/2, a tile boundary for every shape.  0: full map.
+static int half_space_split(const Recon& r) {
+    if (!r.half_space || r.ewald_seen || r.g.interp != 2 || r.g.fom) return 0;
+    const int N = r.g.map, z = (N / 2 / 8 + 1) * 8;
+    return z < N ? z : 0;
+}
+
 // Tile visiting order for the current shape: nearest to the Fourier origin
-// (counting wrap-around) first, since every particle's plane passes there.
+// (counting wrap-around) first, since every particle's plane passes there;
+// with half-space gridding the tiles above the split, which grid only the
+// unpaired pixels, come last.
 static int set_shape(Recon* r, int shape) {
     if (shape < 0 || shape >= insert_num_shapes()) return fail(BSG_ERR_ARG, "tile shape %d out of range", shape);
+    // in-flight gridding reads the tile order and the replica buffers
+    CK(cudaStreamSynchronize(r->stream));
     int tx, ty, tz;
     insert_shape(shape, &tx, &ty, &tz);
     const int N = r->g.map;
+    const int zs = r->zsplit;
     const int nx = (N + tx - 1) / tx, ny = (N + ty - 1) / ty, nz = (N + tz - 1) / tz;
     std::vector<std::pair<double, int>> d((size_t)nx * ny * nz);
     for (int z = 0; z < nz; ++z)
@@ -165,7 +181,8 @@ static int set_shape(Recon* r, int shape) {
                 auto dist = [N](double c) { return std::min(fabs(c), fabs(c - N)); };
                 const double cx = dist((x + 0.5) * tx), cy = dist((y + 0.5) * ty), cz = dist((z + 0.5) * tz);
                 const int i = (z * ny + y) * nx + x;
-                d[i] = {cx * cx + cy * cy + cz * cz, i};
+                const double last = (zs > 0 && z * tz >= zs) ? 4.0 * N * N : 0.0;
+                d[i] = {last + cx * cx + cy * cy + cz * cz, i};
             }
     std::stable_sort(d.begin(), d.end());
     std::vector<int> order(d.size());
@@ -188,6 +205,57 @@ static int set_shape(Recon* r, int shape) {
     return BSG_OK;
 }
 
+// Switch half-space gridding on or off.  Off: the accumulators become the
+// full map's sums (read_sums, in place).  On: only while they are empty (a
+// full map's sums cannot be split into paired and unpaired parts).
+static int set_half_space(Recon* r, bool on) {
+    const int old = r->zsplit;
+    const bool was = r->half_space;
+    r->half_space = on;
+    const int z = half_space_split(*r);
+    if (z == old) return BSG_OK;
+    const int N = r->g.map;
+    if (z > 0 && r->dirty) {
+        r->half_space = was;
+        return fail(BSG_ERR_STATE, "half-space gridding can be switched on only with empty accumulators "
+                                   "(before inserting, or after bsg_recon_reset)");
+    }
+    CK(cudaStreamSynchronize(r->stream));
+    auto free_e = [r]() {
+        for (int i = 0; i < 2; ++i) {
+            if (r->d_evol[i]) cudaFree(r->d_evol[i]);
+            if (r->d_ew[i]) cudaFree(r->d_ew[i]);
+            r->d_evol[i] = nullptr;
+            r->d_ew[i] = nullptr;
+        }
+    };
+    if (old > 0) {
+        for (int i = 0; i < r->nhalves; ++i)
+            CK(launch_map_sums(r->d_vol[i], r->d_w[i], r->d_vol[i], r->d_w[i], r->d_evol[i], r->d_ew[i], N, old,
+                               r->stream));
+        CK(cudaStreamSynchronize(r->stream));
+        free_e();
+    }
+    r->zsplit = 0;
+    if (z > 0) {
+        const size_t n = (size_t)z * N * N;
+        for (int i = 0; i < r->nhalves; ++i) {
+            if (cudaMalloc((void**)&r->d_evol[i], sizeof(double2) * n) != cudaSuccess ||
+                cudaMalloc((void**)&r->d_ew[i], sizeof(double) * n) != cudaSuccess) {
+                // not enough memory for the unpaired sums: the full map
+                cudaGetLastError();
+                free_e();
+                r->half_space = false;
+                return set_shape(r, r->shape);
+            }
+            CK(cudaMemsetAsync(r->d_evol[i], 0, sizeof(double2) * n, r->stream));
+            CK(cudaMemsetAsync(r->d_ew[i], 0, sizeof(double) * n, r->stream));
+        }
+        r->zsplit = z;
+    }
+    return set_shape(r, r->shape);
+}
+
 // Failures the kernels report through the mapped status word (bounded waits).
 static int check_status(Recon* r) {
     if (r->h_status && *(volatile int*)r->h_status) {
@@ -207,6 +275,7 @@ static void free_all(Recon* r) {
     auto F = [](void* p) { if (p) cudaFree(p); };
     for (int i = 0; i < 2; ++i) {
         F(r->d_imgbuf[i]); F(r->d_vol[i]); F(r->d_w[i]); F(r->d_pow[i]); F(r->d_w2[i]);
+        F(r->d_evol[i]); F(r->d_ew[i]);
         F(r->d_half_weighed[i]);
         F(r->d_partbuf[i]); F(r->d_psymbuf[i]); F(r->d_specbuf[i]);
         if (r->h_partbuf[i]) cudaFreeHost(r->h_partbuf[i]);
@@ -263,6 +332,19 @@ static int upload_params(Recon* r, int buf, const double* params, long np) {
         hp[i].spec = (int)i;
     }
     r->g.gate = needs_gate(*r, hp, np) ? 1 : 0;
+    // half-space gridding: the unpaired pixels (row or column -ft/2) lie at
+    // least ft/2 pixel steps from the origin, and no pixel lies beyond the
+    // transform's corner, ft/2 sqrt(2) steps
+    {
+        double smin = 1e300, smax = 0;
+        for (long i = 0; i < np; ++i) {
+            smin = std::min(smin, (double)hp[i].step);
+            smax = std::max(smax, (double)hp[i].step);
+        }
+        const double hf = r->g.ft / 2.0;
+        r->edge_rmin = np ? hf * smin * (1.0 - 1e-6) - 1e-3 : 0.0;
+        r->edge_rmax = hf * smax * 1.4142136 * (1.0 + 1e-6) + 2.0;
+    }
     r->d_part = r->d_partbuf[buf];
     CK(cudaMemcpyAsync(r->d_part, hp, sizeof(DevParticle) * np, cudaMemcpyHostToDevice, r->fft_stream));
     const long nsym = std::max(1L, (long)r->sym.size() / 9);
@@ -328,6 +410,13 @@ static int process(Recon* r, const float* images, const double* params, long npa
         const int buf = (int)(r->seq++ & 1);
         int rc = upload_params(r, buf, params + off * BSG_PARTICLE_DOUBLES, np);
         if (rc) return rc;
+        if (!spectra_out && r->g.ewald && !r->ewald_seen) {
+            // an Ewald surface is not Hermitian: the full map from here on
+            r->ewald_seen = true;
+            rc = set_half_space(r, r->half_space);
+            if (rc) return rc;
+        }
+        if (!spectra_out) r->dirty = true;
         const float* d_img;
         if (dev) {
             d_img = images + off * img_elems;
@@ -484,7 +573,9 @@ int bsg_recon_create(const bsg_recon_config* cfg, bsg_recon** out) {
         cudaEventRecord(r->compute_done[i], r->stream);
     }
     {
-        const int rc2 = set_shape(r, 0);
+        r->shape = 0;
+        r->zsplit = 0;
+        const int rc2 = half_space_split(*r) > 0 ? set_half_space(r, true) : set_shape(r, 0);
         if (rc2) { free_all(r); delete r; return rc2; }
     }
     *out = reinterpret_cast<bsg_recon*>(r);
@@ -510,11 +601,17 @@ int bsg_recon_reset(bsg_recon* h) {
     for (int i = 0; i < r->nhalves; ++i) {
         CK(cudaMemsetAsync(r->d_vol[i], 0, sizeof(double2) * N3, r->stream));
         CK(cudaMemsetAsync(r->d_w[i], 0, sizeof(double) * N3, r->stream));
+        if (r->zsplit > 0) {
+            const size_t n = (size_t)r->zsplit * r->g.map * r->g.map;
+            CK(cudaMemsetAsync(r->d_evol[i], 0, sizeof(double2) * n, r->stream));
+            CK(cudaMemsetAsync(r->d_ew[i], 0, sizeof(double) * n, r->stream));
+        }
         if (r->g.fom) {
             CK(cudaMemsetAsync(r->d_pow[i], 0, sizeof(double) * N3, r->stream));
             CK(cudaMemsetAsync(r->d_w2[i], 0, sizeof(double) * N3, r->stream));
         }
     }
+    r->dirty = false;
     return BSG_OK;
 }
 
@@ -591,10 +688,51 @@ int bsg_recon_accumulators(bsg_recon* h, int half, double* vol_out, double* weig
     if (!r || half < 0 || half >= r->nhalves) return fail(BSG_ERR_ARG, "bsg_recon_accumulators: bad half %d", half);
     CK(cudaSetDevice(r->device));
     const size_t N3 = r->vol_elems();
-    const cudaMemcpyKind k = (flags & BSG_DEVICE_PTR) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const bool dev = (flags & BSG_DEVICE_PTR) != 0;
+    const cudaMemcpyKind k = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const int zs = r->zsplit, N = r->g.map;
+    if (zs > 0 && (!vol_out || !weight_out)) {
+        // the map's sums above the split need both channels' mirrors
+        if (dev) return fail(BSG_ERR_ARG, "bsg_recon_accumulators: give both outputs with BSG_DEVICE_PTR");
+        std::vector<double> tv(vol_out ? 0 : 2 * N3), tw(weight_out ? 0 : N3);
+        return bsg_recon_accumulators(h, half, vol_out ? vol_out : tv.data(), weight_out ? weight_out : tw.data(),
+                                      flags);
+    }
+    if (zs > 0 && dev) {
+        // half-space form -> the map's sums, on the device
+        CK(launch_map_sums(reinterpret_cast<double2*>(vol_out), weight_out, r->d_vol[half], r->d_w[half],
+                           r->d_evol[half], r->d_ew[half], N, zs, r->stream));
+        CK(cudaStreamSynchronize(r->stream));
+        return BSG_OK;
+    }
     if (vol_out) CK(cudaMemcpyAsync(vol_out, r->d_vol[half], sizeof(double2) * N3, k, r->stream));
     if (weight_out) CK(cudaMemcpyAsync(weight_out, r->d_w[half], sizeof(double) * N3, k, r->stream));
+    std::vector<double> ev, ew;
+    if (zs > 0) {
+        const size_t n = (size_t)zs * N * N;
+        ev.resize(2 * n);
+        ew.resize(n);
+        CK(cudaMemcpyAsync(ev.data(), r->d_evol[half], sizeof(double2) * n, cudaMemcpyDeviceToHost, r->stream));
+        CK(cudaMemcpyAsync(ew.data(), r->d_ew[half], sizeof(double) * n, cudaMemcpyDeviceToHost, r->stream));
+    }
     CK(cudaStreamSynchronize(r->stream));
+    if (zs > 0) {
+        // half-space form -> the map's sums (as launch_map_sums, on the
+        // host): above the split from the paired sums below it, then the rest
+        const size_t n = N, n2 = n * n;
+        for (size_t i = (size_t)zs * n2; i < N3; ++i) {
+            const size_t x = i % n, y = (i / n) % n, z = i / n2;
+            const size_t m = (((n - z) % n) * n + (n - y) % n) * n + (n - x) % n;
+            vol_out[2 * i] += vol_out[2 * m];
+            vol_out[2 * i + 1] -= vol_out[2 * m + 1];
+            weight_out[i] = weight_out[i] + weight_out[m];
+        }
+        for (size_t i = 0; i < (size_t)zs * n2; ++i) {
+            vol_out[2 * i] += ev[2 * i];
+            vol_out[2 * i + 1] += ev[2 * i + 1];
+            weight_out[i] += ew[i];
+        }
+    }
     return BSG_OK;
 }
 
@@ -615,6 +753,11 @@ int bsg_recon_add_partial(bsg_recon* h, int half, const double* vol, const doubl
         return fail(BSG_ERR_ARG, "bsg_recon_add_partial: give power and weight2 together");
     if (power && !r->g.fom) return fail(BSG_ERR_STATE, "bsg_recon_add_partial: power sums need fom = 1");
     CK(cudaSetDevice(r->device));
+    if (r->zsplit > 0) {
+        // the incoming sums are a full map's: this context's become one too
+        int rc = set_half_space(r, false);
+        if (rc) return rc;
+    }
     const size_t N3 = r->vol_elems();
     const bool dev = flags & BSG_DEVICE_PTR;
     double* stage = nullptr;
@@ -690,6 +833,16 @@ int bsg_recon_set_tile_shape(bsg_recon* h, int shape) {
     if (!r) return fail(BSG_ERR_ARG, "bsg_recon_set_tile_shape: null context");
     CK(cudaSetDevice(r->device));
     return set_shape(r, shape);
+}
+
+int bsg_recon_set_half_space(bsg_recon* h, int enable, int* zsplit_out) {
+    Recon* r = reinterpret_cast<Recon*>(h);
+    if (!r) return fail(BSG_ERR_ARG, "bsg_recon_set_half_space: null context");
+    CK(cudaSetDevice(r->device));
+    const int rc = set_half_space(r, enable != 0);
+    if (rc) return rc;
+    if (zsplit_out) *zsplit_out = r->zsplit;
+    return BSG_OK;
 }
 
 int bsg_recon_autotune(bsg_recon* h, const float* images, const double* params, long nparts, int flags,

@@ -61,7 +61,6 @@ struct Geometry {
     double maxs2, mins2;    // insertion s^2 window
     double ctf_shi2;        // CTF s^2 upper limit (mg_ctf.cpp:50-60)
     double mscale;          // map real size N * sampling
-    float  rmax;            // max |m| reachable by any pixel (voxels) + 1
     int    fom;
     int    gate;           // 1: some pixel may fall outside the s^2 window or in the taper
     int    ewald;          // 1: the batch's records include Ewald-sphere surfaces

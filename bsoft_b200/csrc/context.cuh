@@ -56,6 +56,17 @@ struct Context {
     int shape = 0;                   // gridding tile shape (insert.cu kShapes)
     int* d_tile_order = nullptr;     // tile visiting order for `shape`
     int replicas = 1;                // warps per tile, each on a slice of the particles
+    // half-space gridding (insert.cu, walk_edges): > 0 when the accumulators
+    // below zsplit hold the paired pixels' sums (their unpaired pixels' sums
+    // in d_evol / d_ew) and those at or above it the unpaired pixels' sums,
+    // the rest being the conjugate of the mirrored voxels; 0: full map
+    int zsplit = 0;
+    bool half_space = true;          // allowed (bsg_recon_set_half_space)
+    bool ewald_seen = false;         // an Ewald batch was gridded: full map for good
+    bool dirty = false;              // something was inserted since the last reset
+    double2* d_evol[2] = {nullptr, nullptr};   // half-space: unpaired pixels' sums below zsplit (zsplit N^2)
+    double* d_ew[2] = {nullptr, nullptr};
+    double edge_rmin = 0, edge_rmax = 0;       // current batch: unpaired pixels' least |m|, any pixel's largest
     double* d_part_sums = nullptr;   // replica partial sums (replicas > 1)
     int* d_status = nullptr;         // device view of h_status (mapped)
     int* h_status = nullptr;         // kernel-reported failures (bounded waits)

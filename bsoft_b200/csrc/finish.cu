@@ -26,18 +26,53 @@ struct WeighArgs {
     float2* out;      // weighed, centre-shifted complex volume
     float* fom;       // optional SNR map
     int N;
+    int zsplit;       // > 0: half-space accumulators (insert.cu walk_edges)
+    const double2* e0; const double* ew0;   // their unpaired pixels' sums below zsplit
+    const double2* e1; const double* ew1;
 };
+
+// Index of the voxel at minus the frequency of voxel (x, y, z) (wrap-around).
+__device__ __forceinline__ size_t mirror_index(size_t x, size_t y, size_t z, size_t N) {
+    return ((((N - z) % N) * N + (N - y) % N) * N + (N - x) % N);
+}
+
+// The map's sums at voxel i.  Half-space accumulators (zsplit > 0) hold
+// the paired pixels' sums P below zsplit, with the unpaired pixels' sums U
+// there in (e, ew), and U alone at and above zsplit: the map is P(v) + U(v)
+// below the split and conj(P(-v)) + U(v) above it.
+__device__ __forceinline__ void read_sums(const double2* vol, const double* w, const double2* e, const double* ew,
+                                          size_t i, size_t N, int zsplit, double2& v, double& wt) {
+    v = vol[i];
+    wt = w[i];
+    if (zsplit <= 0) return;
+    const size_t z = i / (N * N);
+    if (z >= (size_t)zsplit) {
+        const size_t m = mirror_index(i % N, (i / N) % N, z, N);
+        const double2 u = vol[m];
+        v.x += u.x;
+        v.y -= u.y;
+        wt += w[m];
+    } else {
+        const double2 u = e[i];
+        v.x += u.x;
+        v.y += u.y;
+        wt += ew[i];
+    }
+}
 
 __global__ void weigh_kernel(WeighArgs a) {
     const size_t N = a.N, N3 = N * N * N;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3; i += (size_t)gridDim.x * blockDim.x) {
-        double2 v = a.v0[i];
-        double w = a.w0[i];
+        double2 v;
+        double w;
+        read_sums(a.v0, a.w0, a.e0, a.ew0, i, N, a.zsplit, v, w);
         double p = a.p0 ? a.p0[i] : 0.0, q = a.q0 ? a.q0[i] : 0.0;
         if (a.v1) {
-            const double2 v1 = a.v1[i];
+            double2 v1;
+            double w1;
+            read_sums(a.v1, a.w1, a.e1, a.ew1, i, N, a.zsplit, v1, w1);
             v.x += v1.x; v.y += v1.y;
-            w += a.w1[i];
+            w += w1;
             if (a.p1) { p += a.p1[i]; q += a.q1[i]; }
         }
         float2 F = make_float2(0.f, 0.f);
@@ -177,6 +212,9 @@ cudaError_t launch_weigh(const Context& c, int imap, cudaStream_t s) {
     a.out = c.d_work;
     a.fom = c.g.fom ? c.d_fom : nullptr;
     a.N = N;
+    a.zsplit = c.zsplit;
+    a.e0 = c.d_evol[h0]; a.ew0 = c.d_ew[h0];
+    if (both) { a.e1 = c.d_evol[1]; a.ew1 = c.d_ew[1]; }
     weigh_kernel<<<148 * 8, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -230,7 +268,49 @@ cudaError_t launch_weigh_into(const Context& c, int imap, float2* out, cudaStrea
     const int h0 = imap - 1;
     a.v0 = c.d_vol[h0]; a.w0 = c.d_w[h0]; a.p0 = nullptr; a.q0 = nullptr;
     a.out = out; a.fom = nullptr; a.N = c.g.map;
+    a.zsplit = c.zsplit;
+    a.e0 = c.d_evol[h0]; a.ew0 = c.d_ew[h0];
     weigh_kernel<<<148 * 8, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Half-space accumulators -> the map's sums (read_sums), into (dv, dw); in
+// place (dv == vol) too: the voxels at and above zsplit are written first,
+// from the paired sums below it, then (e, ew) is added below it.
+__global__ void map_sums_upper_kernel(double2* dv, double* dw, const double2* vol, const double* w, int N,
+                                      int zsplit) {
+    const size_t n = N, n2 = n * n, first = (size_t)zsplit * n2, N3 = n2 * n;
+    for (size_t i = first + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N3;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t m = mirror_index(i % n, (i / n) % n, i / n2, n);
+        const double2 u = vol[m];
+        double2 v = vol[i];
+        v.x += u.x;
+        v.y -= u.y;
+        dv[i] = v;
+        dw[i] = w[i] + w[m];
+    }
+}
+
+__global__ void map_sums_lower_kernel(double2* dv, double* dw, const double2* vol, const double* w,
+                                      const double2* e, const double* ew, size_t count) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        double2 v = vol[i];
+        const double2 u = e[i];
+        v.x += u.x;
+        v.y += u.y;
+        dv[i] = v;
+        dw[i] = w[i] + ew[i];
+    }
+}
+
+cudaError_t launch_map_sums(double2* dv, double* dw, const double2* vol, const double* w, const double2* e,
+                            const double* ew, int N, int zsplit, cudaStream_t s) {
+    if (zsplit <= 0) return cudaSuccess;
+    map_sums_upper_kernel<<<148 * 8, 256, 0, s>>>(dv, dw, vol, w, N, zsplit);
+    cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return err;
+    map_sums_lower_kernel<<<148 * 8, 256, 0, s>>>(dv, dw, vol, w, e, ew, (size_t)zsplit * N * N);
     return cudaGetLastError();
 }
 

@@ -55,6 +55,11 @@ struct InsertArgs {
     const int* order;          // tile visiting order (heaviest first)
     int R;                     // replicas per tile (each takes a slice of the particles)
     double* psum;              // R > 1: replica partial sums, R x channels x N^3
+    int zsplit;                // > 0: half-space gridding (walk_edges)
+    double2* evol;             // half-space: unpaired pixels' sums below zsplit (zsplit x N^2)
+    double* ew;
+    double edge_rmin;          // unpaired pixels lie at least this far from the origin (voxels)
+    double edge_rmax;          // and no pixel farther than this
     int interp;
     double maxs2, mins2, mscale;
     double2* vol;
@@ -302,9 +307,11 @@ __device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double o
 // phase still holds, and pix() ends each step with __syncwarp.  The row
 // search is done once per group instead of once per point, and neighbouring
 // lanes read neighbouring pixels of the spectrum.
+// excl = 1 leaves out the row k = -hf and the column h = -hf (half-space
+// gridding grids them separately, walk_edges).
 template <int TX, int TY, int TZ, class Pix>
 __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
-                                            int* s_row, Pix&& pix) {
+                                            int* s_row, int excl, Pix&& pix) {
     const double e = P.ezmax;
     const double lo[3] = {ox - 1.0 - e, oy - 1.0 - e, oz - 1.0 - e};
     const double hi[3] = {ox + TX + e, oy + TY + e, oz + TZ + e};
@@ -315,8 +322,8 @@ __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double
         uc += P.ad[i] * c; hu += fabs(P.ad[i]) * e;
     }
     vc *= P.inv_st2; hv *= P.inv_st2; uc *= P.inv_st2; hu *= P.inv_st2;
-    const int k_lo = max((int)ceil(vc - hv), -hf), k_hi = min((int)floor(vc + hv), hf - 1);
-    const int h_lo = max((int)ceil(uc - hu), -hf), h_hi = min((int)floor(uc + hu), hf - 1);
+    const int k_lo = max((int)ceil(vc - hv), -hf + excl), k_hi = min((int)floor(vc + hv), hf - 1);
+    const int h_lo = max((int)ceil(uc - hu), -hf + excl), h_hi = min((int)floor(uc + hu), hf - 1);
     if (k_lo > k_hi || h_lo > h_hi) return;
     int Lh, Lk, sh;
     if (P.lat) {
@@ -398,6 +405,80 @@ __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double
             __syncwarp();
         }
     }
+}
+
+// Half-space gridding.  A real image's transform is Hermitian, F(-q) =
+// conj(F(q)), and a pixel q and its mate -q land at mirrored map positions
+// m and -m (m is linear in q) with mirrored trilinear corners of equal
+// weights.  So the sums P of the pixels that have their mate in the stored
+// transform (q in [-ft/2, ft/2 - 1]^2) satisfy P(-v) = conj(P(v)),
+// P_w(-v) = P_w(v); the others - the row k = -ft/2 and the column
+// h = -ft/2 - make sums U of their own.  With zsplit > N/2 (so every voxel
+// or its mirror lies below it), the tiles below zsplit grid P (walk_groups
+// without the unpaired pixels) into the map accumulators and U into evol /
+// ew; the tiles at or above zsplit grid only U, into the map accumulators.
+// Reading the map gives P(v) + U(v) below the split and conj(P(-v)) + U(v)
+// above it: sums of the same contributions as the full map's, none of them
+// subtracted, so a voxel that nothing reaches reads exactly zero.
+// walk_edges visits the unpaired pixels whose tents reach the tile, one
+// line at a time, points L pixels apart (L step >= sqrt(3) voxels) so that
+// the lanes of a call touch distinct cells; pix(h, k, act) as walk_groups.
+template <int TX, int TY, int TZ, class Pix>
+__device__ __forceinline__ void walk_edges(const DevParticle& P, int hf, double ox, double oy, double oz, int lane,
+                                           Pix&& pix) {
+    const double lo[3] = {ox - 1.0, oy - 1.0, oz - 1.0};
+    const double hi[3] = {ox + TX, oy + TY, oz + TZ};
+    const int L = max(1, (int)ceilf(1.7320508f * 1.0001f * P.inv_step));
+    for (int line = 0; line < 2; ++line) {
+        // 0: (t, -hf), t in [-hf, hf - 1];  1: (-hf, t), t in [-hf + 1, hf - 1]
+        const bool along_h = line == 0;
+        double tl = line == 0 ? -hf : -hf + 1;
+        double th = hf - 1;
+        bool live = true;
+        for (int i = 0; i < 3; ++i) {
+            const double dir = along_h ? P.ad[i] : P.bd[i];
+            const double base = -hf * (along_h ? P.bd[i] : P.ad[i]);
+            if (fabs(dir) > 1e-12) {
+                double p0 = (lo[i] - base) / dir, p1 = (hi[i] - base) / dir;
+                if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
+                tl = fmax(tl, p0);
+                th = fmin(th, p1);
+            } else if (!(base >= lo[i] && base <= hi[i])) {
+                live = false;
+            }
+        }
+        if (!live) continue;
+        const int t0 = (int)ceil(tl), t1 = (int)floor(th);
+        for (int ph = 0; ph < L; ++ph) {
+            const int first = t0 + ph;
+            if (first > t1) break;
+            const int cnt = (t1 - first) / L + 1;
+            for (int j0 = 0; j0 < cnt; j0 += 32) {
+                const int j = j0 + lane;
+                const int t = first + L * j;
+                pix(along_h ? t : -hf, along_h ? -hf : t, j < cnt);
+            }
+        }
+    }
+}
+
+// Can an unpaired pixel (at least rmin voxels from the origin, and no pixel
+// beyond rmax) reach the tile, under some wrap-around alias?
+template <int TX, int TY, int TZ>
+__device__ __forceinline__ bool tile_reaches_edges(int x0, int y0, int z0, int N, double rmin, double rmax) {
+    const int o[3] = {x0, y0, z0}, T[3] = {TX, TY, TZ};
+    for (int a = 0; a < 8; ++a) {
+        double nr = 0, fr = 0;
+        for (int i = 0; i < 3; ++i) {
+            const double lo = o[i] - (((a >> i) & 1) ? N : 0) - 1.0, hi = lo + T[i] + 1.0;
+            const double n = (lo <= 0 && hi >= 0) ? 0.0 : fmin(fabs(lo), fabs(hi));
+            const double f = fmax(fabs(lo), fabs(hi));
+            nr += n * n;
+            fr += f * f;
+        }
+        if (nr <= rmax * rmax && fr >= rmin * rmin) return true;
+    }
+    return false;
 }
 
 template <bool FOM, bool GATE, int TX, int TY, int TZ>
@@ -590,7 +671,7 @@ __device__ __forceinline__ void pixel4(const InsertArgs& a, const DevParticle& P
 }
 
 template <bool GATE, bool EW, int TX, int TY, int TZ, int PX, int PP, int NW>
-__global__ void __launch_bounds__(NW * 32) grid4_kernel(InsertArgs a) {
+__global__ void __launch_bounds__(NW * 32, 5) grid4_kernel(InsertArgs a) {
     constexpr int SLOTS = PP * TZ;
     constexpr int TV = TX * TY * TZ;
     extern __shared__ float4 s_cells[];                 // NW x SLOTS
@@ -607,63 +688,91 @@ __global__ void __launch_bounds__(NW * 32) grid4_kernel(InsertArgs a) {
     const int hf = a.ft / 2;
     const size_t spec_stride = (size_t)(2 * hf + 1) * a.pitch;
     const unsigned cell0 = (unsigned)__cvta_generic_to_shared(cell);
+    // half-space gridding (walk_edges): tiles at or above zsplit grid only
+    // the unpaired pixels; those below it grid the others, and then (one
+    // replica, all particles) the unpaired ones into evol / ew
+    const bool hs = a.zsplit > 0;
+    const bool upper = hs && z0 >= a.zsplit;
+    const bool edges = hs && tile_reaches_edges<TX, TY, TZ>(x0, y0, z0, N, a.edge_rmin, a.edge_rmax);
     for (int i = lane; i < SLOTS; i += 32) cell[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncwarp();
 
-    for (int base = p_lo; base < p_hi; base += 32) {
-        const int p = base + lane;
-        unsigned mask = 0;
-        if (p < p_hi) {
-            const DevParticle& P = a.part[p];
-            if (P.half == a.half || a.half < 0) mask = tile_mask<TX, TY, TZ>(P, x0, y0, z0, N, a.ft);
-        }
-        unsigned todo = __ballot_sync(0xffffffffu, mask != 0);
-        while (todo) {
-            const int src = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const unsigned am = __shfl_sync(0xffffffffu, mask, src);
-            const DevParticle& P = a.part[base + src];
-            const float2* S = a.spec + (size_t)P.spec * spec_stride;
-            for (int al = 0; al < 8; ++al) {
-                if (!((am >> al) & 1u)) continue;
-                const double ox = (double)(x0 - ((al & 1) ? N : 0));
-                const double oy = (double)(y0 - ((al & 2) ? N : 0));
-                const double oz = (double)(z0 - ((al & 4) ? N : 0));
-                // anchor pixel: the tile centre's projection on the plane
-                const double cx = ox + 0.5 * (TX - 1), cy = oy + 0.5 * (TY - 1), cz = oz + 0.5 * (TZ - 1);
-                const int hc = (int)rint((P.ad[0] * cx + P.ad[1] * cy + P.ad[2] * cz) * P.inv_st2);
-                const int kc = (int)rint((P.bd[0] * cx + P.bd[1] * cy + P.bd[2] * cz) * P.inv_st2);
-                const float bx = (float)(hc * P.ad[0] + kc * P.bd[0] - ox);
-                const float by = (float)(hc * P.ad[1] + kc * P.bd[1] - oy);
-                const float bz = (float)(hc * P.ad[2] + kc * P.bd[2] - oz);
-                walk_groups<TX, TY, TZ>(P, hf, ox, oy, oz, lane, s_rows[warp], [&](int h, int k, bool act) {
-                    pixel4<GATE, EW, TX, TY, TZ, PX, PP>(a, P, S, cell, cell0, bx, by, bz, hc, kc, h, k, act);
-                });
+    // pass 0: the tile's sums (all pixels; with half-space gridding the
+    // paired ones, or above the split the unpaired ones); pass 1: the
+    // unpaired pixels of a tile below the split
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1 && !(hs && !upper && edges && rep == 0)) break;
+        const bool edge_walk = pass == 1 || upper;
+        const int b_lo = pass ? 0 : p_lo, b_hi = pass ? a.np : p_hi;
+        // (a tile that no unpaired pixel reaches skips the edge walks)
+        const int b_end = (edge_walk && !edges) ? b_lo : b_hi;
+        for (int base = b_lo; base < b_end; base += 32) {
+            const int p = base + lane;
+            unsigned mask = 0;
+            if (p < b_hi) {
+                const DevParticle& P = a.part[p];
+                if (P.half == a.half || a.half < 0) mask = tile_mask<TX, TY, TZ>(P, x0, y0, z0, N, a.ft);
+            }
+            unsigned todo = __ballot_sync(0xffffffffu, mask != 0);
+            while (todo) {
+                const int src = __ffs(todo) - 1;
+                todo &= todo - 1;
+                const unsigned am = __shfl_sync(0xffffffffu, mask, src);
+                const DevParticle& P = a.part[base + src];
+                const float2* S = a.spec + (size_t)P.spec * spec_stride;
+                for (int al = 0; al < 8; ++al) {
+                    if (!((am >> al) & 1u)) continue;
+                    const double ox = (double)(x0 - ((al & 1) ? N : 0));
+                    const double oy = (double)(y0 - ((al & 2) ? N : 0));
+                    const double oz = (double)(z0 - ((al & 4) ? N : 0));
+                    // anchor pixel: the tile centre's projection on the plane
+                    const double cx = ox + 0.5 * (TX - 1), cy = oy + 0.5 * (TY - 1), cz = oz + 0.5 * (TZ - 1);
+                    const int hc = (int)rint((P.ad[0] * cx + P.ad[1] * cy + P.ad[2] * cz) * P.inv_st2);
+                    const int kc = (int)rint((P.bd[0] * cx + P.bd[1] * cy + P.bd[2] * cz) * P.inv_st2);
+                    const float bx = (float)(hc * P.ad[0] + kc * P.bd[0] - ox);
+                    const float by = (float)(hc * P.ad[1] + kc * P.bd[1] - oy);
+                    const float bz = (float)(hc * P.ad[2] + kc * P.bd[2] - oz);
+                    auto pix = [&](int h, int k, bool act) {
+                        pixel4<GATE, EW, TX, TY, TZ, PX, PP>(a, P, S, cell, cell0, bx, by, bz, hc, kc, h, k, act);
+                    };
+                    if (edge_walk) walk_edges<TX, TY, TZ>(P, hf, ox, oy, oz, lane, pix);
+                    else walk_groups<TX, TY, TZ>(P, hf, ox, oy, oz, lane, s_rows[warp], hs ? 1 : 0, pix);
+                }
             }
         }
-    }
-    // tile sums -> HBM (one replica: add to the map; else this replica's
-    // partial sums, combined later in replica order)
-    const size_t N3 = (size_t)N * N * N;
-    for (int i = lane; i < TV; i += 32) {
-        const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        const float4 c = cell[lx + PX * ly + PP * lz];
-        if (x < N && y < N && z < N) {
-            const size_t idx = ((size_t)z * N + y) * N + x;
-            if (a.R > 1) {
-                double* pb = a.psum + (size_t)rep * 3 * N3 + idx;
-                pb[0] = c.x;
-                pb[N3] = c.y;
-                pb[2 * N3] = c.z;
-            } else {
-                double2 o = a.vol[idx];
-                o.x += c.x;
-                o.y += c.y;
-                a.vol[idx] = o;
-                a.w[idx] += c.z;
+        // tile sums -> HBM: pass 0 adds to the map (one replica) or stores
+        // this replica's partial sums (combined later in replica order);
+        // pass 1 adds to evol / ew.  The cells are cleared for the next pass.
+        const size_t N3 = (size_t)N * N * N;
+        for (int i = lane; i < TV; i += 32) {
+            const int lx = i % TX, ly = (i / TX) % TY, lz = i / (TX * TY);
+            const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+            const int ci = lx + PX * ly + PP * lz;
+            const float4 c = cell[ci];
+            if (x < N && y < N && z < N) {
+                const size_t idx = ((size_t)z * N + y) * N + x;
+                if (pass == 1) {
+                    double2 o = a.evol[idx];
+                    o.x += c.x;
+                    o.y += c.y;
+                    a.evol[idx] = o;
+                    a.ew[idx] += c.z;
+                } else if (a.R > 1) {
+                    double* pb = a.psum + (size_t)rep * 3 * N3 + idx;
+                    pb[0] = c.x;
+                    pb[N3] = c.y;
+                    pb[2 * N3] = c.z;
+                } else {
+                    double2 o = a.vol[idx];
+                    o.x += c.x;
+                    o.y += c.y;
+                    a.vol[idx] = o;
+                    a.w[idx] += c.z;
+                }
             }
+            cell[ci] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        __syncwarp();
     }
 }
 
@@ -802,6 +911,11 @@ cudaError_t launch_insert(const Context& c, const float2* spectra, const DevPart
     a.order = c.d_tile_order;
     a.R = c.replicas;
     a.psum = c.d_part_sums;
+    a.zsplit = c.g.fom ? 0 : c.zsplit;
+    a.evol = c.d_evol[h];
+    a.ew = c.d_ew[h];
+    a.edge_rmin = c.edge_rmin;
+    a.edge_rmax = c.edge_rmax;
     if (!c.g.fom) {
         switch (c.shape) {
             case 0: return launch_shape4<8, 8, 8, 8, 68, 4>(a, c, s);

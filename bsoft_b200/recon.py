@@ -216,6 +216,15 @@ class Reconstructor:
     def set_tile_shape(self, shape: int):
         _lib.check(_lib.load().bsg_recon_set_tile_shape(self._h, shape), "bsg_recon_set_tile_shape")
 
+    def set_half_space(self, on: bool = True) -> int:
+        """Half-space gridding (on by default for trilinear insertion without
+        the FOM channels): about half the gridding work, the full map's sums
+        when read.  Switching on needs empty accumulators.  Returns the split
+        zsplit (0: the full map)."""
+        z = C.c_int(0)
+        _lib.check(_lib.load().bsg_recon_set_half_space(self._h, int(on), C.byref(z)), "bsg_recon_set_half_space")
+        return z.value
+
     def reset(self):
         _lib.check(_lib.load().bsg_recon_reset(self._h), "bsg_recon_reset")
 

@@ -117,9 +117,11 @@ int  bsg_recon_insert(bsg_recon* r, const float* images, const double* params,
  * N^3 float32 signal-to-noise map (fspace_reconstruction_snr). */
 int  bsg_recon_finish(bsg_recon* r, int imap, float* map_out, float* fom_out, int flags);
 
-/* Raw accumulators of half h (0/1; 0 when nmaps == 1): complex volume
+/* Accumulated sums of half h (0/1; 0 when nmaps == 1): complex volume
  * (2*N^3 doubles) and weights (N^3 doubles), reference index order (the
- * accumulators are kept in FP64 on the device). */
+ * accumulators are kept in FP64 on the device; with half-space gridding,
+ * see bsg_recon_set_half_space, the map's sums are formed on the way out).
+ * With BSG_DEVICE_PTR and half-space gridding, give both outputs. */
 int  bsg_recon_accumulators(bsg_recon* r, int half, double* vol_out, double* weight_out, int flags);
 
 /* Add another reconstruction's partial sums into half h of this context:
@@ -130,7 +132,9 @@ int  bsg_recon_accumulators(bsg_recon* r, int half, double* vol_out, double* wei
  * into one context, which then finishes the map; the sum is FP64, so the
  * result depends only on that order.  vol: 2*N^3 doubles, weight: N^3;
  * power and weight2 (N^3 each, both or neither) need fom = 1.  Host or
- * device (BSG_DEVICE_PTR) pointers; returns when the sums have been added. */
+ * device (BSG_DEVICE_PTR) pointers; returns when the sums have been added.
+ * A context in half-space form (bsg_recon_set_half_space) first turns its
+ * sums into the full map's. */
 int  bsg_recon_add_partial(bsg_recon* r, int half, const double* vol, const double* weight,
                            const double* power, const double* weight2, int flags);
 
@@ -183,6 +187,24 @@ int  bsg_particle_spectra(bsg_recon* r, const float* images, const double* param
  * (-1 where the shape does not apply); best_out the chosen shape.  The
  * reference has no counterpart (it has no tunable tiling). */
 int  bsg_recon_set_tile_shape(bsg_recon* r, int shape);
+
+/* Half-space gridding (on by default; applies to trilinear insertion
+ * without the FOM channels).  A real particle image has a Hermitian
+ * transform, so the sums P of the pixels whose Friedel mate is in the
+ * stored transform satisfy P(-v) = conj(P(v)), P_w(-v) = P_w(v); the
+ * unpaired pixels (row and column -ft/2) make sums U of their own.  The
+ * tiles below zsplit (the first multiple of 8 above N/2) grid P and,
+ * apart, U; the tiles at or above it grid only U; every read of the sums
+ * (finish, FSC, bsg_recon_accumulators) gives P(v) + U(v) below the split
+ * and conj(P(-v)) + U(v) above it: the full map's contributions, none
+ * subtracted, for about half the gridding work.  The reference grids the
+ * full map (fspace_pack_2D, bsoft/src/img/Bimage_reconstruct.cpp:112-174).
+ * enable 0 turns the accumulators into the full map's sums and grids the
+ * full map from then on; switching on needs empty accumulators (before
+ * inserting or after bsg_recon_reset).  bsg_recon_add_partial and a batch
+ * with Ewald surfaces (not Hermitian) switch it off the same way.
+ * zsplit_out (optional): the split in use, 0 for the full map. */
+int  bsg_recon_set_half_space(bsg_recon* r, int enable, int* zsplit_out);
 
 /* Point-group symmetry during reconstruction (breconstruct -symmetry, mode
  * 0): Bimage::fspace_pack_2D(p, View, sym, ...) (bsoft/src/img/
