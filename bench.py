@@ -1005,12 +1005,13 @@ def main():
         avg_launch_ms = ins_ms / max(1, ins_launch)
         achieved = per_particle * B / (avg_launch_ms / 1e3) / 1e9
         # DRAM bytes of one gridding launch, from one ncu capture of this
-        # kernel (8^3 tiles, two replicas, 256^3 map) on a 256-particle batch
-        # of this workload: reads 961.1 MB (the spectra, 3.754 MB per
-        # particle, read ~1.8 times as the tiles a particle reaches are
-        # spread over the launch) and writes 767.2 MB (the two replicas'
-        # partial sums, fixed per launch); scaled to the launch's batch
-        traffic = (3.754e6 * B + 0.767e9) if (int(shape) == 0 and BOX == 256) else None
+        # kernel (8^3 tiles, two replicas, half-space gridding, 256^3 map) on
+        # a 256-particle batch of this workload: reads 574.2 MB (mostly the
+        # spectra, 2.243 MB per particle: the tiles below the split read each
+        # particle's spectrum about once) and writes 922.7 MB (the two
+        # replicas' partial sums and the unpaired pixels' sums, fixed per
+        # launch); scaled to the launch's batch
+        traffic = (2.243e6 * B + 0.923e9) if (int(shape) == 0 and BOX == 256) else None
         roof = {"kernel": "grid4_kernel", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                 "traffic_unit": ("bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum of a "
