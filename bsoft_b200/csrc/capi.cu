@@ -113,6 +113,10 @@ static void make_dev_particle(const Recon& r, const double* q, DevParticle& d, d
         d.bf[i] = (float)d.bd[i];
     }
     for (int i = 0; i < 3; ++i) d.cd[i] = R[3 * i + 2] * g.mscale;
+    for (int i = 0; i < 3; ++i) {
+        d.iad[i] = fabs(d.ad[i]) > 1e-12 ? 1.0 / d.ad[i] : 0.0;
+        d.ibd[i] = fabs(d.bd[i]) > 1e-12 ? 1.0 / d.bd[i] : 0.0;
+    }
     d.inv = inv;
     double nn = sqrt(R[2] * R[2] + R[5] * R[5] + R[8] * R[8]);
     if (nn <= 0) nn = 1;

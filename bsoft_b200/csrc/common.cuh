@@ -30,6 +30,7 @@ struct alignas(16) DevParticle {
     double c00, c20, c22, c2m2, c40, c11, c1m1;   // aberration weights (ctf.h:321-348)
     // insertion (fspace_pack_2D, Bimage_reconstruct.cpp:131-160)
     double ad[3], bd[3];    // map frequency per unit pixel step: R[:,0]*inv*mscale, R[:,1]*inv*mscale
+    double iad[3], ibd[3];  // 1 / ad, 1 / bd (0 where |.| <= 1e-12): the gridding walks' row and line bounds
     double nrm[3];          // unit plane normal R[:,2]
     double inv2;            // (scale/(ft*pixel))^2: s2 per unit pixel^2
     double inv_st2;         // 1 / step^2: pixel coordinate per unit of ad.c

@@ -139,6 +139,20 @@ struct ColArgs {
     double shi2;
 };
 
+// The particle's CTF terms, held in registers for the epilogue: read through
+// the record in global memory they would be loaded again after every store
+// of the spectrum (the compiler cannot tell that the stores leave them alone).
+struct CtfTerms {
+    double fs, c00, c20, c22, c2m2, c40, c11, c1m1;
+};
+
+__device__ __forceinline__ CtfTerms ctf_terms(const DevParticle& P) {
+    CtfTerms t;
+    t.fs = P.fs; t.c00 = P.c00; t.c20 = P.c20; t.c22 = P.c22; t.c2m2 = P.c2m2; t.c40 = P.c40;
+    t.c11 = P.c11; t.c1m1 = P.c1m1;
+    return t;
+}
+
 // CTF weight of one pixel from its reduced even aberration r in (-pi, pi].
 __device__ __forceinline__ float ctf_weight(const ColArgs& a, double r) {
     if (a.ctf_action == 1) return (r < 0.0) ? -1.f : 1.f;
@@ -155,7 +169,7 @@ __device__ __forceinline__ float ctf_weight(const ColArgs& a, double r) {
 // in double.  Mirroring h changes only the sign of the 2 sx sy term (and of
 // sx in the odd, beam-tilt aberration psi = c1m1 sy + c11 sx).
 template <bool MIRROR>
-__device__ __forceinline__ void pixel_factors(const ColArgs& a, const DevParticle& P, float2 exh, float2 eyk,
+__device__ __forceinline__ void pixel_factors(const ColArgs& a, const CtfTerms& P, float2 exh, float2 eyk,
                                               int h, int k, float2& f, float2& fm) {
     const float sc = 1.0f / (float)a.ft;
     const float2 ph = cmul(exh, eyk);
@@ -193,7 +207,7 @@ __device__ __forceinline__ void pixel_factors(const ColArgs& a, const DevParticl
     }
 }
 
-__global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
+__global__ void __launch_bounds__(COL_W * 32, 2) cols_kernel(ColArgs a) {
     extern __shared__ float2 smem[];
     const int ft = a.ft, n = a.n, logft = a.logft;
     float2* stw = smem;
@@ -220,7 +234,7 @@ __global__ void __launch_bounds__(COL_W * 32) cols_kernel(ColArgs a) {
     const int warp = threadIdx.x >> 5;
     if (h0 + warp < hw) warp_fft<false, true>(cols + warp * cs, ft, logft, stw);
     __syncthreads();
-    const DevParticle& P = a.part[b];
+    const CtfTerms P = ctf_terms(a.part[b]);
     const float2* ex = a.phase + (size_t)b * 2 * ft;
     const float2* ey = ex + ft;
     // centred, padded layout: [k + ft/2][h + ft/2], row pitch ft + 2

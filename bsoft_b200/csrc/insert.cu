@@ -232,8 +232,7 @@ __device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double o
         else { Lh = L; Lk = L; sh = 0; }
     }
     // per-axis 1 / ad (0 when the axis does not vary along h)
-    double ia[3];
-    for (int i = 0; i < 3; ++i) ia[i] = fabs(P.ad[i]) > 1e-12 ? 1.0 / P.ad[i] : 0.0;
+    const double* ia = P.iad;
     for (int pk = 0; pk < Lk; ++pk) {
         const int k0 = k_lo + pk;
         if (k0 > k_hi) break;
@@ -333,8 +332,7 @@ __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double
         if (L * L > 12 && 3.6055513f * P.step >= 1.7320508f * 1.0001f) { Lh = 4; Lk = 3; sh = 2; }
         else { Lh = L; Lk = L; sh = 0; }
     }
-    double ia[3];
-    for (int i = 0; i < 3; ++i) ia[i] = fabs(P.ad[i]) > 1e-12 ? 1.0 / P.ad[i] : 0.0;
+    const double* ia = P.iad;
     for (int pk = 0; pk < Lk; ++pk) {
         const int k0 = k_lo + pk;
         if (k0 > k_hi) break;
@@ -436,10 +434,10 @@ __device__ __forceinline__ void walk_edges(const DevParticle& P, int hf, double 
         double th = hf - 1;
         bool live = true;
         for (int i = 0; i < 3; ++i) {
-            const double dir = along_h ? P.ad[i] : P.bd[i];
+            const double idir = along_h ? P.iad[i] : P.ibd[i];
             const double base = -hf * (along_h ? P.bd[i] : P.ad[i]);
-            if (fabs(dir) > 1e-12) {
-                double p0 = (lo[i] - base) / dir, p1 = (hi[i] - base) / dir;
+            if (idir != 0.0) {
+                double p0 = (lo[i] - base) * idir, p1 = (hi[i] - base) * idir;
                 if (p0 > p1) { const double t = p0; p0 = p1; p1 = t; }
                 tl = fmax(tl, p0);
                 th = fmin(th, p1);
