@@ -46,12 +46,17 @@ __global__ void background_kernel(const float* __restrict__ img, const DevPartic
     const double ih = 1.0 / h;
     double sum = 0.0;
     int cnt = 0;
+    // pixel i = y n + x, stepped by blockDim.x without a division per pixel
+    int y = threadIdx.x / n, x = threadIdx.x - y * n;
+    const int dy = blockDim.x / n, dx = blockDim.x - dy * n;
     for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
-        int y = i / n, x = i - y * n;
         double x2, y2;
         if (pow2) { x2 = (x - P.bx) * ih; y2 = (y - P.by) * ih; }
         else { x2 = (x - P.bx) / h; y2 = (y - P.by) / h; }
         if (x2 * x2 + y2 * y2 - 1 > 0) { sum += (float)(im[i] * P.na + P.nb); ++cnt; }
+        x += dx;
+        y += dy;
+        if (x >= n) { x -= n; ++y; }
     }
     // deterministic block reduction (fixed tree)
     __shared__ double ssum[256];
