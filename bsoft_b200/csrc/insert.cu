@@ -298,6 +298,17 @@ __device__ __forceinline__ void walk_pair(const DevParticle& P, int hf, double o
     }
 }
 
+// floor(x / d) for 0 < d and |x| < 2^20, from an approximate reciprocal of
+// d: the float quotient is within one of the answer, and the remainder
+// corrects it (the integers a division would give, without one per row).
+__device__ __forceinline__ int floor_div(int x, int d, float inv_d) {
+    int q = __float2int_rd((float)x * inv_d);
+    int r = x - q * d;
+    if (r < 0) { --q; r += d; }
+    if (r >= d) ++q;
+    return q;
+}
+
 // The same walk with the lattice phases of one row block interleaved: lane t
 // takes a group of Lh consecutive pixels of one lattice row (h = g, g + 1,
 // ..., g + Lh - 1 with g = h_lo + sh j + Lh i), one pixel of each column
@@ -333,15 +344,15 @@ __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double
         else { Lh = L; Lk = L; sh = 0; }
     }
     const double* ia = P.iad;
+    const float iLh = __fdividef(1.0f, (float)Lh);
     for (int pk = 0; pk < Lk; ++pk) {
         const int k0 = k_lo + pk;
         if (k0 > k_hi) break;
-        const int nrows = (k_hi - k0) / Lk + 1;
-        for (int jb = 0; jb < nrows; jb += 32) {
+        for (int jb = 0; k0 + Lk * jb <= k_hi; jb += 32) {
             const int j = jb + lane;
             const int k = k0 + Lk * j;
             double hl = h_lo, hh = h_hi;
-            bool live = j < nrows;
+            bool live = k <= k_hi;
             if (live) {
                 for (int i = 0; i < 3; ++i) {
                     const double base = k * P.bd[i];
@@ -364,8 +375,8 @@ __device__ __forceinline__ void walk_groups(const DevParticle& P, int hf, double
                 hmax = (int)floor(hh);
                 if (hmax >= hmin) {
                     const int g0 = h_lo + sh * j;
-                    const int i0 = (int)floorf(__fdiv_rn((float)(hmin - g0), (float)Lh));
-                    const int i1 = (int)floorf(__fdiv_rn((float)(hmax - g0), (float)Lh));
+                    const int i0 = floor_div(hmin - g0, Lh, iLh);
+                    const int i1 = floor_div(hmax - g0, Lh, iLh);
                     gfirst = g0 + Lh * i0;
                     cnt = i1 - i0 + 1;
                 }
@@ -450,11 +461,9 @@ __device__ __forceinline__ void walk_edges(const DevParticle& P, int hf, double 
         for (int ph = 0; ph < L; ++ph) {
             const int first = t0 + ph;
             if (first > t1) break;
-            const int cnt = (t1 - first) / L + 1;
-            for (int j0 = 0; j0 < cnt; j0 += 32) {
-                const int j = j0 + lane;
-                const int t = first + L * j;
-                pix(along_h ? t : -hf, along_h ? -hf : t, j < cnt);
+            for (int tb = first; tb <= t1; tb += 32 * L) {
+                const int t = tb + L * lane;
+                pix(along_h ? t : -hf, along_h ? -hf : t, t <= t1);
             }
         }
     }
