@@ -786,6 +786,7 @@ int bsg_recon_add_partial(bsg_recon* h, int half, const double* vol, const doubl
         }
         return BSG_OK;
     };
+    r->dirty = true;            // the accumulators hold sums (a full map's)
     int rc = add(reinterpret_cast<double*>(r->d_vol[half]), vol, 2 * N3);
     if (!rc) rc = add(r->d_w[half], weight, N3);
     if (!rc && power) rc = add(r->d_pow[half], power, N3);

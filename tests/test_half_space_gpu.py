@@ -147,6 +147,21 @@ def test_half_space_partial_maps(work):
         assert a.set_half_space(True) == 40
 
 
+def test_half_space_not_switched_on_over_added_sums(work):
+    """A fresh context given another's sums by add_partial holds a full map:
+    half-space gridding stays off until reset, as after inserting."""
+    w, images = work
+    plan = _plan(w)
+    with Reconstructor(plan) as a, Reconstructor(plan) as b:
+        b.insert(images, w["params"])
+        vb, wb = b.accumulators(0)
+        a.add_partial(vb, wb, 0)
+        with pytest.raises(_lib.BsgError):
+            a.set_half_space(True)
+        va, wa = a.accumulators(0)
+        assert np.array_equal(va, vb) and np.array_equal(wa, wb)
+
+
 def test_ewald_batch_switches_to_full_map(work):
     """A plane batch gridded in half-space form, then an Ewald batch: the
     context switches to the full map and holds both batches' sums."""
